@@ -1,0 +1,212 @@
+/* mb3d_cu: the distance-estimated ray march ("Calculate 3D") and the Monte
+ * Carlo path tracer of Mandelbulb3D on one NVIDIA B200 (sm_100a).
+ *
+ * This is the C ABI a host renderer calls in place of its graphics-card
+ * backend.  Every entry point replaces one function of mb3d-rs's card
+ * backend `src/gpu.rs`; the comment above each names it.  The host keeps its
+ * scene model and its CPU renderer; this library has no CPU fallback inside:
+ * it returns a negative status and the caller decides.
+ *
+ * Conventions (those of mb3d-rs's C API, capi/include/mb3d.h:12-15):
+ *  - 0 is success, a negative errno-style status is a failure, and
+ *    mb3d_cu_last_error() tells why, on the same thread;
+ *  - a context is used by one thread at a time; contexts on different
+ *    threads may run concurrently (each has its own CUDA stream);
+ *  - buffers may be host or device memory (the library finds out which);
+ *    host buffers are copied in and out inside the call.
+ *
+ * Precision modes: MB3D_CU_FP64 is the plain double precision march, the
+ * drop-in for the reference's FP64 CPU march.  MB3D_CU_FP32_FP64 marches in
+ * single precision with the camera origin and the ray parameter in double
+ * precision and finishes every surface (hit re-check, binary search, depth)
+ * in double precision; deep zooms where single precision cannot resolve the
+ * DE offset switch to double precision per pixel.
+ */
+#ifndef MB3D_CU_H
+#define MB3D_CU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (negative errno values) ---- */
+#define MB3D_CU_OK 0
+#define MB3D_CU_EINVAL (-22)     /* bad scene, size or pointer */
+#define MB3D_CU_ENOMEM (-12)     /* device memory exhausted */
+#define MB3D_CU_ENODEV (-19)     /* no CUDA device / not an sm_100 device */
+#define MB3D_CU_EIO (-5)         /* a CUDA call failed (text in last_error) */
+#define MB3D_CU_ECANCELED (-125) /* *cancel became non-zero */
+#define MB3D_CU_ETIMEDOUT (-110) /* the device time budget ran out (resumable) */
+#define MB3D_CU_EOVERFLOW (-75)  /* more than 1/500 of the pixels had a NaN DE */
+#define MB3D_CU_ENOTSUP (-95)    /* a scene feature this backend does not do */
+
+/* ---- formula numbers: MB3D's internal formula numbers as a .m3p slot
+ * stores them (src/m3p.rs:797-823), plus the Menger IFS, which mb3d-rs runs
+ * as a custom .m3f formula and this library has built in. ---- */
+#define MB3D_CU_F_INTPOW 0        /* Integer Power: options power(2..8), z_mul */
+#define MB3D_CU_F_REALPOWER 1     /* Real Power: power, z_mul */
+#define MB3D_CU_F_TRICORN 3       /* Tricorn: z_mul, cz_mul */
+#define MB3D_CU_F_AMAZINGBOX 4    /* Amazing Box: scale, min_r, fold */
+#define MB3D_CU_F_BULBOX 5        /* Bulbox: scale, min_r, fold, bulb_scale, r_thr, r_thr2 */
+#define MB3D_CU_F_FOLDINGINTPOW 6 /* Folding Int Pow: power, z_mul, fold */
+#define MB3D_CU_F_MENGERIFS 100   /* Menger IFS: scale, cscale_x, cscale_y, cscale_z */
+
+#define MB3D_CU_SLOTS 6
+
+/* One hybrid slot (a .m3p THeaderCustomAddon slot, src/m3p.rs:771-777). */
+typedef struct mb3d_cu_slot {
+    int32_t iterations; /* consecutive iterations; negative: not counted; 0: empty */
+    int32_t formula;    /* MB3D_CU_F_* */
+    double options[16]; /* the formula's option values in .m3p order */
+} mb3d_cu_slot;
+
+/* One global light (TLight8, src/lighting.rs:95-122): its angles. */
+typedef struct mb3d_cu_light {
+    int32_t on;
+    int32_t pad;
+    double x_angle; /* radians (LXpos) */
+    double y_angle; /* radians (LYpos) */
+} mb3d_cu_light;
+
+/* The scene fields the march, the post passes and the Monte Carlo tracer
+ * read (Scene, src/scene.rs:398-530; defaults src/scene.rs:628-697). */
+typedef struct mb3d_cu_scene {
+    int32_t width, height;
+    int32_t iterations;     /* maximum iterations */
+    int32_t min_iterations; /* MB3D's minimum iterations (default 1) */
+    double rstop;           /* bailout radius; <= 0: the formulas' default */
+    double zoom;
+    double mid[3];
+    double z_start, z_end;
+    double vgrads[3][3];    /* camera rows: screen x, screen y, view axis */
+    double fov_y;           /* degrees */
+    double de_stop;         /* in pixels */
+    double z_step_div;      /* raystep */
+    double raystep_limiter;
+    int32_t smooth_normals; /* 0..8 */
+    int32_t bin_search_steps;
+    int32_t first_step_random;
+    int32_t step_sub_de_stop;
+    int32_t vary_de_stop_on_fov;
+    int32_t normals_on_de;
+    int32_t disable_analytic_de;
+    int32_t julia;
+    double julia_c[4];
+    int32_t color_option;
+    int32_t color_on_it;
+    double color_mul;
+    int32_t dfog_on_it;
+    int32_t repeat_from;
+    int32_t n_slots;        /* 1..6 */
+    int32_t pad0;
+    mb3d_cu_slot slots[MB3D_CU_SLOTS];
+    /* lighting (for the shadow pass and the Monte Carlo tracer) */
+    mb3d_cu_light lights[6];
+    /* the hard shadow pass: bit i = light i casts shadows (0 = no pass) */
+    int32_t shadow_lights;
+    int32_t shadow_soft;    /* 1: one soft shadow (the last selected light) */
+    float soft_radius;
+    float hs_max_len_mul;   /* default 1 */
+    /* the DE ambient occlusion pass: quality 0..3 = 3/7/17/33 rays, -1 off */
+    int32_t deao_quality;
+    int32_t deao_dither;    /* 0 (only 0 on the card path) */
+    float deao_max_len;     /* default 1 */
+    int32_t deao_first_step_random;
+} mb3d_cu_scene;
+
+/* The G-buffer record SiLight (src/gbuffer.rs:5-20), 20 bytes; mb3d-rs's
+ * card backend packs the same fields into 5 u32 (src/gpu_march.wgsl:4765). */
+typedef struct mb3d_cu_silight {
+    int16_t normal[3];  /* view space, +-32767 */
+    uint16_t pad;
+    uint32_t zpos_fine; /* bits 8..31 depth, 0..7 roughness; zpos >= 32768: background */
+    uint16_t shadow;    /* bits 0..9 step count, 10..15 shadow bits */
+    uint16_t amb_shadow;
+    uint16_t si_gradient;
+    uint16_t otrap;
+} mb3d_cu_silight;
+
+/* Monte Carlo options (the fixed-spp subset of src/mc.rs). */
+typedef struct mb3d_cu_mc_opts {
+    int32_t spp;          /* rays per pixel */
+    int32_t depth;        /* diffuse bounces (mc_depth) */
+    uint64_t seed;        /* frame seed */
+    float soft_shadow_radius;
+    float pad;
+} mb3d_cu_mc_opts;
+
+/* Per-render counters the last call measured on the device. */
+typedef struct mb3d_cu_stats {
+    float ms_march;       /* primary march (+ finish) kernels, CUDA events */
+    float ms_finish;      /* the FP64 finish kernel alone */
+    float ms_shadow;
+    float ms_deao;
+    float ms_total;       /* first launch to last, device time */
+    uint32_t launches;    /* this library's kernel launches in the call */
+    uint32_t fp64_pixels; /* pixels the mixed mode marched in double precision */
+    uint64_t de_evals;    /* DE evaluations (counting builds only, else 0) */
+} mb3d_cu_stats;
+
+typedef struct mb3d_cu_ctx mb3d_cu_ctx;
+
+#define MB3D_CU_FP64 0
+#define MB3D_CU_FP32_FP64 1
+
+#define MB3D_CU_POST_SHADOW 1
+#define MB3D_CU_POST_DEAO 2
+
+/* Library version text; not to be freed. */
+const char *mb3d_cu_version(void);
+
+/* Why the last failed call on this thread failed (capi/src/lib.rs:18-40). */
+const char *mb3d_cu_last_error(void);
+
+/* A context on CUDA device `device`, with its own stream.  Replaces the
+ * card set-up of gpu.rs (device open, src/gpu.rs:1840-1900). */
+int mb3d_cu_init(int device, mb3d_cu_ctx **out);
+void mb3d_cu_free(mb3d_cu_ctx *ctx);
+
+/* Launch the context's work on this CUDA stream (a cudaStream_t) instead
+ * of its own; NULL goes back to its own. */
+int mb3d_cu_set_stream(mb3d_cu_ctx *ctx, void *stream);
+
+/* Replaces gpu::unsupported (src/gpu.rs:445): 0 when this backend can
+ * render the scene, 1 when it cannot (the reason, user-visible, in
+ * `reason`), negative on a bad scene. */
+int mb3d_cu_unsupported(const mb3d_cu_scene *scene, char *reason, size_t cap);
+
+/* Replaces gpu::march (src/gpu.rs:2296) and gpu::march_bands
+ * (src/gpu.rs:1586): the rows row0 .. row0+rows of the picture marched into
+ * `gbuf` (rows * width records, row-major).  `cancel` (may be NULL) is
+ * polled between launches. */
+int mb3d_cu_march(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, uint32_t row0, uint32_t rows,
+                  mb3d_cu_silight *gbuf, const volatile int *cancel);
+
+/* Replaces gpu::post_on_card (src/gpu.rs:1649) / post_bands (:1715): the
+ * hard (or soft) shadows and/or the DE ambient occlusion computed in place
+ * on the marched G-buffer rows.  `passes` is MB3D_CU_POST_* bits. */
+int mb3d_cu_post(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, int passes, uint32_t row0,
+                 uint32_t rows, mb3d_cu_silight *gbuf, const volatile int *cancel);
+
+/* The march and the post passes of the whole picture in one call (what
+ * render::calculate_with does on the card, src/render.rs:328-746). */
+int mb3d_cu_render(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, mb3d_cu_silight *gbuf,
+                   const volatile int *cancel);
+
+/* Replaces gpu::de_probe (src/gpu.rs:3193) and calc::de_at
+ * (src/calc.rs:2695): the distance estimate (world units) and iteration
+ * count at n world positions (xyz triples). */
+int mb3d_cu_de_probe(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, const double *pos, uint32_t n,
+                     double *de, int32_t *its);
+
+/* The counters of the last call on this context. */
+int mb3d_cu_stats_get(const mb3d_cu_ctx *ctx, mb3d_cu_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

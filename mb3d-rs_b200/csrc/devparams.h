@@ -1,0 +1,51 @@
+// The flat per-render parameter block the kernels read: the fields of
+// mb3d-rs's CalcParams (src/calc.rs:21-134) that the march, the post passes
+// and the Monte Carlo tracer use, plus single precision copies for the
+// mixed-precision march.  Passed to every kernel by value (kernel
+// parameters live in the constant bank, uniform across the grid), so
+// concurrent contexts with different scenes never share state.
+#pragma once
+#include <stdint.h>
+
+#define MB3D_MAX_SLOTS 6
+#define MB3D_MAX_LIGHTS 6
+#define MB3D_MAX_AO_RAYS 40
+
+struct DevSlot {
+    int32_t formula;    // MB3D_CU_F_*
+    int32_t iterations; // >= 0
+    int32_t uncounted;
+    int32_t ade;
+    int32_t julia_add;
+    int32_t ipow;       // the integer power (IntPow, FoldingIntPow)
+    double o[6];        // options
+    float of[6];        // options, single precision
+};
+
+struct DevParams {
+    DevSlot slots[MB3D_MAX_SLOTS];
+    int32_t n_slots, end_to, repeat_from, is_custom_de;
+    int32_t de_option, max_it, min_it, de_add_steps;
+    int32_t sm_normals, color_option, color_on_it, dfog_on_it;
+    int32_t normals_on_de, first_step_random, do_julia, width;
+    int32_t height, all_fp64, n_lights, shadow_soft;
+    float d_de_scale, de_stop, z_step_div, mh04zsd;
+    float de_stop_factor, ln_rstop, de_offset, de_offset006;
+    float mcts_m, ms_de_sub, d_col_plus, col_var;
+    float fovx_off, fovx_mul, pl_optic_z, mct_color_mul;
+    float fhln[6];
+    float d_rstop_f, rstop3d_f, soft_radius, hs_max_len_mul;
+    double d_rstop, rstop3d, zcorr, zc_mul;
+    double zend, step_width, fov_y, coord_eps;
+    double ju[4];
+    float ju_f[4];
+    double vgrads[3][3];
+    double ystart[3];
+    // the shadow pass: light index and HSvecs (world, -step width long)
+    int32_t light_idx[MB3D_MAX_LIGHTS];
+    double light_vec[MB3D_MAX_LIGHTS][3];
+    // the DE AO pass (src/deao.rs:75-104): ray directions of the quality
+    int32_t ao_quality, ao_rays, ao_first_step_random, pad1;
+    float ao_d_step_mul, ao_d_min_a_dif, ao_corr_weight, ao_max_len;
+    float ao_dirs[MB3D_MAX_AO_RAYS][3];
+};

@@ -1,0 +1,250 @@
+// The built-in formulas as inlined device functions, one template for the
+// double precision march and the single precision bulk march.  Each is one
+// iteration on v (x, y, z, w) with the constant j added, as in mb3d-rs's
+// Formula::iterate (src/formulas.rs:576-857); the Menger IFS is the
+// published KIFS Menger step (the reference runs it as .m3f machine code).
+// The formula of a slot is chosen by its number (`DevSlot::formula`), the
+// same for every lane of a warp at a given iteration, so the switch does not
+// diverge.
+#pragma once
+#include "devparams.h"
+#include "../../include/mb3d_cu.h"
+
+namespace mb3dcu {
+
+template <typename R> struct Num;
+template <> struct Num<double> {
+    static __device__ __forceinline__ double sqrt_(double x) { return sqrt(x); }
+    static __device__ __forceinline__ double div_(double a, double b) { return a / b; }
+    static __device__ __forceinline__ double eps() { return 1e-40; }
+    static __device__ __forceinline__ double opt(const DevSlot &s, int k) { return s.o[k]; }
+    static __device__ __forceinline__ double atan2_(double y, double x) { return atan2(y, x); }
+    static __device__ __forceinline__ void sincos_(double a, double *s, double *c) { sincos(a, s, c); }
+    static __device__ __forceinline__ double pow_(double a, double b) { return pow(a, b); }
+};
+// single precision: 1e-40 is a denormal, flushed to zero in the bulk march;
+// the smallest normal single keeps the division defined on the z axis
+template <> struct Num<float> {
+    static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
+    static __device__ __forceinline__ float eps() { return 1.2e-38f; }
+    static __device__ __forceinline__ float opt(const DevSlot &s, int k) { return s.of[k]; }
+    static __device__ __forceinline__ float atan2_(float y, float x) { return atan2f(y, x); }
+    static __device__ __forceinline__ void sincos_(float a, float *s, float *c) { __sincosf(a, s, c); }
+    static __device__ __forceinline__ float pow_(float a, float b) { return __powf(a, b); }
+};
+
+template <typename R>
+__device__ __forceinline__ R box_fold(R x, R fold) {
+    return fabs(x + fold) - (fabs(x - fold) + x);
+}
+
+// Amazing Box (HybridCube / HybridCubeDE)
+template <typename R>
+__device__ __forceinline__ void f_amazing_box(R scale, R min_r, R fold, R v[4], const R j[3], bool ade) {
+    R x = box_fold(v[0], fold);
+    R y = box_fold(v[1], fold);
+    R z = box_fold(v[2], fold);
+    R r = z * z + y * y + x * x;
+    R m = fmax(min_r, Num<R>::eps());
+    R sqr_min_r = m * m;
+    R mul;
+    if (r < sqr_min_r) mul = Num<R>::div_(scale, sqr_min_r);
+    else if (R(1) < r) mul = scale;
+    else mul = Num<R>::div_(scale, r);
+    if (ade) v[3] *= mul;
+    v[2] = z * mul + j[2];
+    v[1] = y * mul + j[1];
+    v[0] = x * mul + j[0];
+}
+
+// sine bulb power 2 with scaling (HybridItIntPow2scale, for the Bulbox)
+template <typename R>
+__device__ __forceinline__ void f_int_pow2_scale(R scaling, R v[4], const R j[3]) {
+    R s = Num<R>::div_(R(1), scaling);
+    R x = v[0] * s, y = v[1] * s, z = v[2] * s;
+    R xx = x * x, yy = y * y;
+    R r = xx + yy;
+    v[2] = -((Num<R>::sqrt_(r) * z) * R(2)) * scaling + j[2];
+    R a = Num<R>::div_(r - z * z, r);
+    v[0] = (xx - yy) * a * scaling + j[0];
+    v[1] = (x * y * a) * R(2) * scaling + j[1];
+}
+
+// the integer power triplex formulas (fHIntFunctions)
+template <typename R>
+__device__ __forceinline__ void f_int_pow(int power, R zmul, R v[4], const R j[3]) {
+    const R x = v[0], y = v[1], z = v[2];
+    const R EPS = Num<R>::eps();
+    if (power == 8) {
+        // White's / Nylander's power 8 without trigonometry (HybridIntP8)
+        R xx = x * x, yy = y * y, zz = z * z;
+        R r = xx + yy;
+        R rr = r * r;
+        R zzzz = zz * zz;
+        R t = (zzzz - R(6) * r * zz + rr) * (zz - r) * Num<R>::sqrt_(r);
+        v[2] = -(t * z * R(8) * zmul) + j[2];
+        R num = (rr * R(70) + zzzz) * zzzz - R(28) * zz * r * (zzzz + rr);
+        R a = Num<R>::div_(num, rr * rr + EPS) + R(1);
+        R xxxx = xx * xx, yyyy = yy * yy;
+        v[1] = (yyyy * (R(7) * xx - yy) + xxxx * (xx - R(7) * yy)) * R(8) * x * y * a + j[1];
+        v[0] = a * (xxxx * xxxx + yyyy * (R(70) * xxxx + yyyy) - R(28) * (xx * yy * (yyyy + xxxx))) + j[0];
+        return;
+    }
+    switch (power) {
+        case 2: {
+            R yy = y * y, xx = x * x;
+            R r = xx + yy;
+            v[2] = (Num<R>::sqrt_(r) * zmul * z) * R(2) + j[2];
+            R a = Num<R>::div_(r - z * z, r);
+            v[0] = (xx - yy) * a + j[0];
+            v[1] = (x * y * a) * R(2) + j[1];
+            break;
+        }
+        case 3: {
+            R sy = y * y, sx = x * x;
+            R r = sx + sy;
+            R sz = z * z;
+            R a = R(1) - Num<R>::div_(R(3) * sz, r + EPS);
+            v[0] = (sx - R(3) * sy) * a * x + j[0];
+            v[2] = j[2] - (sz - R(3) * r) * z * zmul;
+            v[1] = a * (R(3) * sx - sy) * y + j[1];
+            break;
+        }
+        case 4: {
+            R sy = y * y, sx = x * x;
+            R r = sx + sy;
+            R sz = z * z;
+            R a = R(1) + Num<R>::div_(sz * (sz - R(6) * r), r * r + EPS);
+            v[0] = (sx * (sx - R(6) * sy) + sy * sy) * a + j[0];
+            v[2] = Num<R>::sqrt_(r) * (r - sz) * z * R(4) * zmul + j[2];
+            v[1] = a * x * (sx - sy) * R(4) * y + j[1];
+            break;
+        }
+        case 5: {
+            R sy = y * y, sx = x * x;
+            R r = sx + sy;
+            R sz = z * z;
+            R a = R(1) + Num<R>::div_((sz * sz - sz * r * R(2)) * R(5), r * r + EPS);
+            v[1] = (R(5) * sx * sx - sy * (R(10) * sx - sy)) * a * y + j[1];
+            v[2] = (sz * (sz - R(10) * r) + R(5) * r * r) * z * zmul + j[2];
+            v[0] = a * x * (sx * (sx - R(10) * sy) + R(5) * sy * sy) + j[0];
+            break;
+        }
+        case 6: {
+            R sy = y * y, sx = x * x;
+            R r = sx + sy;
+            R sz = z * z;
+            R rr = r * r;
+            R a = R(1) - Num<R>::div_(sz * (R(15) * rr + sz * (sz - r * R(15))), rr * r + EPS);
+            v[1] = (R(3) * sy * sy + sx * (R(3) * sx - R(10) * sy)) * a * y * x * R(2) + j[1];
+            v[2] = (sz * (R(3) * sz - R(10) * r) + R(3) * rr) * Num<R>::sqrt_(r) * z * zmul * R(2) + j[2];
+            v[0] = (sy * sy * (R(15) * sx - sy) + sx * sx * (sx - R(15) * sy)) * a + j[0];
+            break;
+        }
+        default: {  // 7
+            R sy = y * y, sx = x * x;
+            R r = sx + sy;
+            R sz = z * z;
+            R rr = r * r;
+            R a = R(1) - Num<R>::div_(R(7) * (sz * (R(3) * rr + sz * (sz - R(5) * r))), rr * r + EPS);
+            v[1] = (sx * (R(21) * sy * sy + sx * (R(7) * sx - R(35) * sy)) - sy * sy * sy) * a * y + j[1];
+            v[2] = j[2] - (sz * sz * sz - R(7) * r * (rr + sz * (R(3) * sz - R(5) * r))) * z * zmul;
+            v[0] = a * x * (sx * (R(35) * sy * sy + sx * (sx - R(21) * sy)) - R(7) * sy * sy * sy) + j[0];
+            break;
+        }
+    }
+}
+
+// Real Power (HybridFloatPow), uses the squared radius of the last iteration
+template <typename R>
+__device__ __forceinline__ void f_real_power(R pw, R z_mul, R v[4], const R j[3], R rout) {
+    R x = v[0], y = v[1], z = v[2];
+    R st, ct, sp, cp;
+    Num<R>::sincos_(Num<R>::atan2_(y, x) * pw, &st, &ct);
+    Num<R>::sincos_(Num<R>::atan2_(z, Num<R>::sqrt_(x * x + y * y)) * pw, &sp, &cp);
+    R r = Num<R>::pow_(rout, pw * R(0.5));
+    v[0] = ct * cp * r + j[0];
+    v[1] = st * cp * r + j[1];
+    v[2] = sp * r * z_mul + j[2];
+}
+
+// the KIFS Menger sponge step
+template <typename R>
+__device__ __forceinline__ void f_menger(R s, R cx, R cy, R cz, R v[4], bool ade) {
+    R x = fabs(v[0]), y = fabs(v[1]), z = fabs(v[2]);
+    R t;
+    if (x < y) { t = x; x = y; y = t; }
+    if (x < z) { t = x; x = z; z = t; }
+    if (y < z) { t = y; y = z; z = t; }
+    R s1 = s - R(1);
+    x = s * x - cx * s1;
+    y = s * y - cy * s1;
+    z = s * z;
+    if (z > R(0.5) * cz * s1) z -= cz * s1;
+    if (ade) v[3] *= fabs(s);
+    v[0] = x;
+    v[1] = y;
+    v[2] = z;
+}
+
+template <typename R>
+__device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], const R j[3], R rout) {
+    const bool ade = s.ade != 0;
+    switch (s.formula) {
+        case MB3D_CU_F_INTPOW: f_int_pow<R>(s.ipow, Num<R>::opt(s, 1), v, j); break;
+        case MB3D_CU_F_AMAZINGBOX:
+            f_amazing_box<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), Num<R>::opt(s, 2), v, j, ade);
+            break;
+        case MB3D_CU_F_MENGERIFS:
+            f_menger<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), Num<R>::opt(s, 2), Num<R>::opt(s, 3), v, ade);
+            break;
+        case MB3D_CU_F_REALPOWER: f_real_power<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), v, j, rout); break;
+        case MB3D_CU_F_TRICORN: {
+            R x = v[0], y = v[1], z = v[2];
+            v[2] = z * x * Num<R>::opt(s, 0) + j[2] * Num<R>::opt(s, 1);
+            v[0] = x * x - (y * y + z * z) + j[0];
+            v[1] = R(2) * (y * x) + j[1];
+            break;
+        }
+        case MB3D_CU_F_FOLDINGINTPOW: {
+            R fold = Num<R>::opt(s, 2);
+            v[0] = box_fold(v[0], fold);
+            v[1] = box_fold(v[1], fold);
+            v[2] = box_fold(v[2], fold);
+            f_int_pow<R>(s.ipow, Num<R>::opt(s, 1), v, j);
+            break;
+        }
+        case MB3D_CU_F_BULBOX: {
+            R scale = Num<R>::opt(s, 0), min_r = Num<R>::opt(s, 1), fold = Num<R>::opt(s, 2);
+            R bulb = Num<R>::opt(s, 3), t1 = Num<R>::opt(s, 4), t2 = Num<R>::opt(s, 5);
+            R rt1 = t1 * t1, rt2 = t2 * t2;
+            if (rout < rt1) {
+                if (rout < rt2) {
+                    f_int_pow2_scale<R>(bulb, v, j);
+                } else {
+                    R m = Num<R>::div_(rout - rt2, rt1 - rt2);
+                    R in0 = v[0], in1 = v[1], in2 = v[2];
+                    f_int_pow2_scale<R>(bulb, v, j);
+                    R o0 = v[0], o1 = v[1], o2 = v[2];
+                    v[0] = in0; v[1] = in1; v[2] = in2;
+                    f_amazing_box<R>(scale, min_r, fold, v, j, false);
+                    R r1 = Num<R>::sqrt_(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                    R m2 = R(1) - m;
+                    R r2 = r1 * m + m2 * Num<R>::sqrt_(o0 * o0 + o1 * o1 + o2 * o2);
+                    v[0] = v[0] * m + m2 * o0;
+                    v[1] = v[1] * m + m2 * o1;
+                    v[2] = v[2] * m + m2 * o2;
+                    R rb = Num<R>::div_(r2, Num<R>::sqrt_(v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + Num<R>::eps()));
+                    v[0] *= rb; v[1] *= rb; v[2] *= rb;
+                }
+            } else {
+                f_amazing_box<R>(scale, min_r, fold, v, j, false);
+            }
+            break;
+        }
+        default: break;
+    }
+}
+
+}  // namespace mb3dcu

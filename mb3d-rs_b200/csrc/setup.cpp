@@ -1,0 +1,378 @@
+// Host set-up of the per-render parameters: the scene (mb3d_cu_scene) turned
+// into the flat DevParams block, as mb3d-rs's CalcParams::new does it
+// (`GetMCTparasFromHeader`, src/calc.rs:375-891), for the alternating 3D
+// hybrid with the built-in formulas; plus the shadow light vectors
+// (render::shadow_job, src/render.rs:2383-2415) and the DE AO ray table
+// (deao::build_rays, src/deao.rs:75-104).
+#include "setup.h"
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+#include <string>
+
+namespace mb3dcu {
+
+static const double kPi = 3.14159265358979323846;
+static inline double deg2rad(double d) { return d * (kPi / 180.0); }
+
+// Formula meta data (src/formulas.rs:492-569); the Menger IFS has its .m3f
+// header's values (.DEoption 2, .DEscale 0.2, .RStop 1024).
+static int f_de_option(int f) { return f == MB3D_CU_F_AMAZINGBOX ? 11 : f == MB3D_CU_F_MENGERIFS ? 2 : 0; }
+static double f_de_scale(int f) {
+    if (f == MB3D_CU_F_AMAZINGBOX || f == MB3D_CU_F_BULBOX || f == MB3D_CU_F_MENGERIFS) return 0.2;
+    if (f == MB3D_CU_F_FOLDINGINTPOW) return 0.5;
+    return 1.0;
+}
+static double f_rstop(int f) {
+    return (f == MB3D_CU_F_AMAZINGBOX || f == MB3D_CU_F_BULBOX || f == MB3D_CU_F_FOLDINGINTPOW || f == MB3D_CU_F_MENGERIFS)
+               ? 1024.0
+               : 16.0;
+}
+static int f_ipow(const mb3d_cu_slot &s) {
+    double r = std::round(s.options[0]);
+    int p = std::isnan(r) ? 0 : (r > 1e9 ? 1000000000 : (r < -1e9 ? -1000000000 : (int)r));
+    return std::min(8, std::max(2, p));
+}
+static double f_si_pow(const mb3d_cu_slot &s) {
+    switch (s.formula) {
+        case MB3D_CU_F_INTPOW: return (double)f_ipow(s);
+        case MB3D_CU_F_REALPOWER: return s.options[0] == 0.0 ? 1e-40 : s.options[0];
+        case MB3D_CU_F_MENGERIFS: return 0.0;
+        default: return 2.0;
+    }
+}
+static bool f_first_is_zmul(int f) { return f == MB3D_CU_F_INTPOW || f == MB3D_CU_F_FOLDINGINTPOW; }
+static double f_first_option(const mb3d_cu_slot &s) { return f_first_is_zmul(s.formula) ? s.options[1] : s.options[0]; }
+static bool f_known(int f) {
+    return f == MB3D_CU_F_INTPOW || f == MB3D_CU_F_REALPOWER || f == MB3D_CU_F_TRICORN || f == MB3D_CU_F_AMAZINGBOX ||
+           f == MB3D_CU_F_BULBOX || f == MB3D_CU_F_FOLDINGINTPOW || f == MB3D_CU_F_MENGERIFS;
+}
+
+// CheckFormulaOptions (src/calc.rs:315-372)
+static int de_option_of(const int *des, const int *its, int n) {
+    int opt = -1;
+    for (int x = 0; x < n; x++) {
+        if (its[x] == 0) continue;
+        int de = des[x];
+        if (de < 0 || de == opt) continue;
+        if (opt == -1 || opt == 21 || opt == 22) opt = de;
+        else if (opt == 2) opt = (de == 2 || de == 5 || de == 6 || de == 11) ? 2 : 0;
+        else if (opt == 4) opt = (de == 5 || de == 6) ? 4 : 0;
+        else if (opt == 5) opt = de == 4 ? 4 : (de == 2 || de == 11) ? 2 : (de != 6 ? 0 : 5);
+        else if (opt == 6) opt = (de == 2 || de == 4 || de == 5 || de == 11) ? de : 0;
+        else if (opt == 11) opt = (de == 2 || de == 5) ? 2 : (de != 6 ? 0 : 11);
+    }
+    return opt;
+}
+
+int unsupported_reason(const mb3d_cu_scene &sc, std::string &why) {
+    if (sc.width <= 0 || sc.height <= 0 || sc.width > 65536 || sc.height > 65536) {
+        why = "the picture size must be 1..65536 pixels each way";
+        return MB3D_CU_EINVAL;
+    }
+    if (sc.n_slots < 1 || sc.n_slots > MB3D_CU_SLOTS) {
+        why = "n_slots must be 1..6";
+        return MB3D_CU_EINVAL;
+    }
+    if (!(sc.zoom > 0.0) || !(sc.fov_y > 0.0) || sc.iterations < 1) {
+        why = "zoom and fov must be positive and iterations at least 1";
+        return MB3D_CU_EINVAL;
+    }
+    bool any = false;
+    for (int i = 0; i < sc.n_slots; i++) {
+        if (sc.slots[i].iterations == 0) continue;
+        any = true;
+        if (!f_known(sc.slots[i].formula)) {
+            why = "formula #" + std::to_string(sc.slots[i].formula) + " is not built into this backend";
+            return 1;
+        }
+    }
+    if (!any) {
+        why = "no formula with iterations > 0";
+        return MB3D_CU_EINVAL;
+    }
+    if (sc.deao_quality >= 0 && sc.deao_dither != 0) {
+        why = "DE ambient occlusion with dithering is not on the card";
+        return 1;
+    }
+    return 0;
+}
+
+int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
+    int u = unsupported_reason(sc, err);
+    if (u < 0) return u;
+    if (u > 0) return MB3D_CU_ENOTSUP;
+    std::memset(&p, 0, sizeof(p));
+    int n = sc.n_slots;
+    int its[6] = {0}, des[6] = {0}, fs[6] = {0};
+    bool unc[6] = {false};
+    for (int i = 0; i < n; i++) {
+        its[i] = std::abs(sc.slots[i].iterations);
+        unc[i] = sc.slots[i].iterations < 0;
+        fs[i] = sc.slots[i].iterations != 0 ? sc.slots[i].formula : MB3D_CU_F_INTPOW;
+        des[i] = f_de_option(fs[i]);
+    }
+    // CheckHybridOptions: the last slot with iterations ends the hybrid
+    int last = n - 1;
+    while (last > 0 && its[last] == 0) last--;
+    int nsl = last + 1;
+    int end_to = last;
+    int rep = std::min(std::max(sc.repeat_from, 0), end_to);
+    while (rep > 0 && its[rep] <= 0) rep--;
+    int de_option = de_option_of(des, its, nsl);
+    if (sc.disable_analytic_de) {
+        if (de_option == 2 || de_option == 11) de_option = 0;
+        else if (de_option == 5 || de_option == 6) de_option = 4;
+    }
+    if (de_option < 0) {
+        err = "formula option is not valid";
+        return MB3D_CU_EINVAL;
+    }
+    if (de_option >= 4 && de_option <= 6) {
+        err = "4D hybrids are not built into this backend";
+        return MB3D_CU_ENOTSUP;
+    }
+    bool custom = de_option == 2 || de_option == 5 || de_option == 6 || de_option == 11 || de_option == 20;
+    for (int i = 0; i < nsl; i++) unc[i] = unc[i] || des[i] < 0 || des[i] > 20;
+
+    // DE scale, colour helpers and the smooth iteration logs
+    float fhln[6];
+    for (int k = 0; k < 6; k++) fhln[k] = (float)(1.0 / std::log(2.0));
+    double cnt_n = 0, sum_x = 0, sum_y = 0, cnt_i = 0;
+    for (int x = 0; x < nsl; x++) {
+        if (its[x] == 0) continue;
+        const mb3d_cu_slot &s = sc.slots[x];
+        if (!unc[x]) {
+            double sip = f_si_pow(s);
+            double z1 = sip > 1.0 ? sip : f_first_option(s);
+            fhln[x] = (float)(1.0 / std::log(std::fmax(2.0, std::fabs(z1))));
+        }
+        double w = (double)its[x];
+        int j = des[x];
+        if (custom && !unc[x] && (j == 5 || j == 11)) {
+            cnt_n += w;
+            cnt_i += w;
+            double x2 = f_first_option(s);
+            if (x2 == 0.0) x2 = 1e-40;
+            sum_x += x2 < 0.0 ? 0.65 * w : (x2 * 1.2 + 1.0) / x2 * w;
+            sum_y += std::fabs(x2) * w;
+        } else if (j >= 0) {
+            cnt_n += w;
+            sum_x += (custom ? 1.0 : f_de_scale(fs[x])) * w;
+        }
+    }
+    double dde = 1.0;
+    float col_plus = 0.f;
+    if (cnt_n > 0.0 && de_option != 20) dde = sum_x / cnt_n;
+    if (cnt_n > 0.0 && cnt_i > 0.0) col_plus = (float)(std::pow(std::fabs(sum_y / cnt_i), 0.25) * 40.0 - 49.0);
+    // mctColVarDEstopMul (src/calc.rs:591-652), one hybrid part
+    float col_var = 0.6f;
+    {
+        double a = 0, b = 0;
+        int ia = 0, itmp = 0;
+        for (int x = 0; x < nsl; x++) {
+            if (!(its[x] > 0 && !unc[x])) {
+                if (its[x] > 0) (x > end_to ? ia : itmp)++;
+                continue;
+            }
+            double w = (double)its[x];
+            int de = des[x];
+            if (de == 0 || de == 4) {
+                a += w * 0.6;
+                b += w;
+            } else if (((de >= 1 && de <= 3) || (de >= 5 && de <= 40)) && !f_first_is_zmul(fs[x])) {
+                double v = f_first_option(sc.slots[x]);
+                if (v > 1.0) {
+                    if (v < 1.2) v = 1.1 + (v - 1.0) * (v - 1.0) * 2.5;
+                    a += w * 0.5 / (std::log(v) + 0.03);
+                    b += w;
+                } else if (v < -1.0) {
+                    if (v > -1.2) v = -1.1 - (v + 1.0) * (v + 1.0) * 2.5;
+                    a += w * 0.5 / (std::log(-v) + 0.03);
+                    b += w;
+                }
+            }
+        }
+        if ((b >= 0.0 && b > 1e-3) || (ia > itmp && std::fabs(b) < 1e-3 && b > 1e-3)) col_var = (float)(a / b);
+        else col_var = 0.6f;
+    }
+    double rstop = sc.rstop;
+    if (!(rstop > 0.0)) {
+        rstop = 0.0;
+        for (int i = 0; i < n; i++)
+            if (sc.slots[i].iterations > 0) rstop = std::fmax(rstop, f_rstop(sc.slots[i].formula));
+        rstop = std::fmax(rstop, 1.0001);
+    }
+    const double W = sc.width, H = sc.height;
+    double sw = 2.1345 / (sc.zoom * W);
+    double fov = deg2rad(sc.fov_y);
+    float zsd0 = (float)std::fmax(sc.z_step_div, 0.0001);
+    float de_stop = (float)std::fmax(sc.de_stop, 0.001);
+    double half = fov * 0.5;
+    if (half < 0.01) half = 0.01;
+    if (half > 1.5) half = 1.5;
+    p.pl_optic_z = (float)(std::cos(half) * half / std::sin(half));
+    p.fovx_off = 0.5f * (float)sc.width;
+    p.fovx_mul = (float)(fov / H);
+    // CalcPPZvals
+    p.zcorr = std::sin(std::fmax(deg2rad(sc.fov_y), 1.0) / H);
+    p.zc_mul = 32767.0 * 256.0 / (std::sqrt((sc.z_end - sc.z_start) * p.zcorr / sw + 1.0) - 0.999999999);
+    p.zend = std::fmax(1e-10, (sc.z_end - sc.z_start) / sw);
+    p.mh04zsd = (float)((double)std::max(sc.width, sc.height) * 0.5 * std::sqrt((double)zsd0 + 0.001) *
+                        std::fmax(0.01, sc.raystep_limiter));
+    // GetDEstopFactor
+    if (sc.vary_de_stop_on_fov) {
+        double ze = std::fmax(1e-16, (sc.z_end - sc.z_start) / sw);
+        double a = 0.01 * H / (std::sin(0.01) * std::fmax(1.0 / 65535.0, deg2rad(sc.fov_y)));
+        double b = sw * (a + ze) / a;
+        p.de_stop_factor = (float)((b - sw) / (sw * std::fmax(1e-6, ze)));
+    }
+    // the camera's start plane: its corner and the per-pixel/per-step rows
+    double z1 = (sc.z_start - sc.mid[2]) / sw;
+    for (int i = 0; i < 3; i++) {
+        const double *r = sc.vgrads[i];
+        double d = sw / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        for (int k = 0; k < 3; k++) p.vgrads[i][k] = r[k] * d;
+    }
+    for (int k = 0; k < 3; k++)
+        p.ystart[k] = sc.mid[k] + z1 * p.vgrads[2][k] - (H * 0.5) * p.vgrads[1][k] - (W * 0.5) * p.vgrads[0][k];
+    float de_off = std::fmin(de_stop * 0.1f, 0.004f);
+    p.d_de_scale = custom ? (float)((double)(float)dde / sw) : (float)dde * de_off;
+    p.de_offset006 = de_off * 0.06f;
+    p.de_offset = (float)((double)de_off * sw);
+    p.z_step_div = zsd0;
+    p.ms_de_sub = 0.f;
+    if (sc.step_sub_de_stop) {
+        float s = zsd0 * zsd0 + (1.2f * zsd0) * (1.0f - zsd0);
+        p.z_step_div = s;
+        p.ms_de_sub = std::fmin(std::sqrt(s), 0.9f);
+    }
+    p.ln_rstop = (float)std::log(std::log(rstop));
+    p.d_rstop = (double)(float)(rstop * rstop);
+    p.rstop3d = (double)(float)((p.d_rstop * p.d_rstop) * 64.0);
+    p.d_rstop_f = (float)p.d_rstop;
+    p.rstop3d_f = (float)p.rstop3d;
+    p.mcts_m = 32767.0f / (float)std::max(sc.iterations + 1, 1);
+    p.d_col_plus = col_plus + (float)sc.iterations * 0.1f;
+    p.col_var = col_var;
+    p.mct_color_mul = (float)(sc.color_mul * 512.0);
+    p.de_stop = de_stop;
+    p.step_width = sw;
+    p.fov_y = fov;
+    p.n_slots = nsl;
+    p.end_to = end_to;
+    p.repeat_from = rep;
+    p.is_custom_de = custom;
+    p.de_option = de_option;
+    p.max_it = sc.iterations;
+    p.min_it = std::min(sc.min_iterations, sc.iterations);
+    p.de_add_steps = sc.bin_search_steps;
+    p.sm_normals = std::min(8, std::max(0, sc.smooth_normals));
+    p.color_option = std::min(sc.color_option, 5);
+    p.color_on_it = sc.color_on_it;
+    p.dfog_on_it = sc.dfog_on_it;
+    p.normals_on_de = (sc.normals_on_de || custom) ? 1 : 0;
+    p.first_step_random = sc.first_step_random ? 1 : 0;
+    p.do_julia = sc.julia ? 1 : 0;
+    p.width = sc.width;
+    p.height = sc.height;
+    for (int k = 0; k < 6; k++) p.fhln[k] = fhln[k];
+    for (int k = 0; k < 4; k++) {
+        p.ju[k] = sc.julia_c[k];
+        p.ju_f[k] = (float)sc.julia_c[k];
+    }
+    for (int i = 0; i < nsl; i++) {
+        DevSlot &d = p.slots[i];
+        d.formula = fs[i];
+        d.iterations = its[i];
+        d.uncounted = unc[i];
+        d.ade = custom;
+        d.julia_add = sc.julia && fs[i] == MB3D_CU_F_MENGERIFS;
+        d.ipow = f_ipow(sc.slots[i]);
+        for (int k = 0; k < 6; k++) {
+            d.o[k] = sc.slots[i].options[k];
+            d.of[k] = (float)sc.slots[i].options[k];
+        }
+    }
+    // single precision coordinates are good enough when the numerical DE
+    // offset spans >= 3 single steps at the size of the coordinates, or a
+    // pixel step >= 64 of them with an analytic DE (gpu::precision,
+    // gpu::step_precision, src/gpu.rs:1019-1040)
+    double coord = std::fmax(std::fabs(p.ystart[0]), std::fmax(std::fabs(p.ystart[1]), std::fabs(p.ystart[2]))) +
+                   sw * (W + H) + 2.0;
+    double eps32 = 1.1920928955078125e-07;
+    double prec = custom ? sw / (coord * eps32) : (double)p.de_offset / (coord * eps32);
+    p.all_fp64 = custom ? (prec < 64.0) : (prec < 3.0);
+    p.coord_eps = coord * eps32;
+
+    // shadow lights (render::shadow_job): HSvecs = RotateVectorReverse(-sw * LN, M)
+    p.n_lights = 0;
+    double m[3][3];
+    for (int i = 0; i < 3; i++) {
+        const double *r = p.vgrads[i];
+        double d = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        for (int k = 0; k < 3; k++) m[i][k] = r[k] * d;
+    }
+    for (int idx = 0; idx < 6; idx++) {
+        const mb3d_cu_light &li = sc.lights[idx];
+        if (!li.on || !((sc.shadow_lights >> idx) & 1)) continue;
+        double a = -li.x_angle, b = li.y_angle;
+        double v[3] = {-std::sin(a), std::sin(b), std::cos(b) * std::cos(a)};
+        double nv = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        double ln[3] = {(double)(float)(-v[0] / nv), (double)(float)(-v[1] / nv), (double)(float)(-v[2] / nv)};
+        double l = std::sqrt(ln[0] * ln[0] + ln[1] * ln[1] + ln[2] * ln[2]);
+        if (l > 0.0)
+            for (int k = 0; k < 3; k++) ln[k] = ln[k] * (1.0 / l);
+        double w[3] = {-ln[0] * sw, -ln[1] * sw, -ln[2] * sw};
+        int q = p.n_lights++;
+        p.light_idx[q] = idx;
+        for (int k = 0; k < 3; k++) p.light_vec[q][k] = w[0] * m[0][k] + w[1] * m[1][k] + w[2] * m[2][k];
+    }
+    if (sc.shadow_soft && p.n_lights > 1) {
+        p.light_idx[0] = p.light_idx[p.n_lights - 1];
+        for (int k = 0; k < 3; k++) p.light_vec[0][k] = p.light_vec[p.n_lights - 1][k];
+        p.n_lights = 1;
+    }
+    p.shadow_soft = sc.shadow_soft ? 1 : 0;
+    p.soft_radius = sc.soft_radius;
+    p.hs_max_len_mul = sc.hs_max_len_mul;
+
+    // DE AO rays (deao::build_rays)
+    p.ao_quality = sc.deao_quality;
+    p.ao_max_len = sc.deao_max_len;
+    p.ao_first_step_random = sc.deao_first_step_random;
+    if (sc.deao_quality >= 0) {
+        int q = std::min(sc.deao_quality, 3);
+        int nr = 0;
+        auto put = [&](double ya, double za) {
+            double sy = std::sin(ya), cy = std::cos(ya), sz = std::sin(za), cz = std::cos(za);
+            p.ao_dirs[nr][0] = (float)(sy * cz);
+            p.ao_dirs[nr][1] = (float)(-sy * sz);
+            p.ao_dirs[nr][2] = (float)(-cy);
+            nr++;
+        };
+        const double tau = 2.0 * kPi;
+        if (q == 0) {
+            double abr = deg2rad(60.0);
+            for (int x = 0; x < 3; x++) put(0.5 * abr, (double)x * tau / 3.0);
+            p.ao_d_step_mul = 1.8f;
+            p.ao_d_min_a_dif = -1.0f;
+            p.ao_corr_weight = 0.3f;
+        } else {
+            put(0.0, 0.0);
+            double abr = (kPi / 2.0) / ((double)q + 0.9);
+            for (int y = 1; y <= q; y++) {
+                double t = (double)y * abr;
+                int cnt = (int)std::nearbyint(std::sin(t) * tau / abr);
+                for (int x = 0; x < cnt && nr < MB3D_MAX_AO_RAYS; x++) put(t, (double)x * tau / (double)cnt);
+            }
+            p.ao_d_step_mul = (float)(1.0 + std::sin(abr));
+            p.ao_d_min_a_dif = (float)std::cos(abr * 1.2);
+            p.ao_corr_weight = q == 1 ? 0.2f : 0.1666f;
+        }
+        p.ao_rays = nr;
+    }
+    return 0;
+}
+
+}  // namespace mb3dcu

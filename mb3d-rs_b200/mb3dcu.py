@@ -1,0 +1,211 @@
+"""Python host binding of libmb3dcu.so (include/mb3d_cu.h) through ctypes.
+
+The class `Card` mirrors the functions of mb3d-rs's card backend that the
+library replaces (src/gpu.rs): `unsupported` (gpu::unsupported, :445),
+`march` (gpu::march / march_bands, :2296 / :1586), `post_on_card`
+(:1649), `de_probe` (:3193), plus `render` (the march and its post passes,
+render::calculate_with, src/render.rs:328).  Errors raise `CardError` with
+the library's status and text, the way the reference returns
+`Err(String)`; there is no CPU fallback here.
+
+Buffers are numpy arrays (host: copied inside the call) or torch CUDA
+tensors (device: used in place), viewed as `SILIGHT` records.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmb3dcu.so")
+
+OK, EINVAL, ENOMEM, ENODEV, EIO, ECANCELED, ETIMEDOUT, EOVERFLOW, ENOTSUP = 0, -22, -12, -19, -5, -125, -110, -75, -95
+
+F_INTPOW, F_REALPOWER, F_TRICORN, F_AMAZINGBOX, F_BULBOX, F_FOLDINGINTPOW, F_MENGERIFS = 0, 1, 3, 4, 5, 6, 100
+FP64, FP32_FP64 = 0, 1
+POST_SHADOW, POST_DEAO = 1, 2
+
+
+class Slot(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("formula", ctypes.c_int32), ("options", ctypes.c_double * 16)]
+
+
+class Light(ctypes.Structure):
+    _fields_ = [("on", ctypes.c_int32), ("pad", ctypes.c_int32), ("x_angle", ctypes.c_double),
+                ("y_angle", ctypes.c_double)]
+
+
+class Scene(ctypes.Structure):
+    _fields_ = [
+        ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+        ("iterations", ctypes.c_int32), ("min_iterations", ctypes.c_int32),
+        ("rstop", ctypes.c_double), ("zoom", ctypes.c_double),
+        ("mid", ctypes.c_double * 3),
+        ("z_start", ctypes.c_double), ("z_end", ctypes.c_double),
+        ("vgrads", (ctypes.c_double * 3) * 3),
+        ("fov_y", ctypes.c_double), ("de_stop", ctypes.c_double), ("z_step_div", ctypes.c_double),
+        ("raystep_limiter", ctypes.c_double),
+        ("smooth_normals", ctypes.c_int32), ("bin_search_steps", ctypes.c_int32),
+        ("first_step_random", ctypes.c_int32), ("step_sub_de_stop", ctypes.c_int32),
+        ("vary_de_stop_on_fov", ctypes.c_int32), ("normals_on_de", ctypes.c_int32),
+        ("disable_analytic_de", ctypes.c_int32), ("julia", ctypes.c_int32),
+        ("julia_c", ctypes.c_double * 4),
+        ("color_option", ctypes.c_int32), ("color_on_it", ctypes.c_int32),
+        ("color_mul", ctypes.c_double),
+        ("dfog_on_it", ctypes.c_int32), ("repeat_from", ctypes.c_int32),
+        ("n_slots", ctypes.c_int32), ("pad0", ctypes.c_int32),
+        ("slots", Slot * 6),
+        ("lights", Light * 6),
+        ("shadow_lights", ctypes.c_int32), ("shadow_soft", ctypes.c_int32),
+        ("soft_radius", ctypes.c_float), ("hs_max_len_mul", ctypes.c_float),
+        ("deao_quality", ctypes.c_int32), ("deao_dither", ctypes.c_int32),
+        ("deao_max_len", ctypes.c_float), ("deao_first_step_random", ctypes.c_int32),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("ms_march", ctypes.c_float), ("ms_finish", ctypes.c_float), ("ms_shadow", ctypes.c_float),
+                ("ms_deao", ctypes.c_float), ("ms_total", ctypes.c_float), ("launches", ctypes.c_uint32),
+                ("fp64_pixels", ctypes.c_uint32), ("de_evals", ctypes.c_uint64)]
+
+
+# the G-buffer record (mb3d_cu_silight, 20 bytes)
+SILIGHT = np.dtype([("normal", "<i2", (3,)), ("pad", "<u2"), ("zpos_fine", "<u4"), ("shadow", "<u2"),
+                    ("amb_shadow", "<u2"), ("si_gradient", "<u2"), ("otrap", "<u2")])
+assert SILIGHT.itemsize == 20
+
+
+class CardError(RuntimeError):
+    def __init__(self, status, text):
+        super().__init__(f"{text} (status {status})")
+        self.status = status
+        self.text = text
+
+
+_lib = None
+
+
+def lib():
+    """The loaded library; fails loudly when it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C mb3d-rs_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, sp = ctypes.c_void_p, ctypes.POINTER(Scene)
+        L.mb3d_cu_version.restype = ctypes.c_char_p
+        L.mb3d_cu_last_error.restype = ctypes.c_char_p
+        L.mb3d_cu_init.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        L.mb3d_cu_free.argtypes = [vp]
+        L.mb3d_cu_free.restype = None
+        L.mb3d_cu_set_stream.argtypes = [vp, vp]
+        L.mb3d_cu_unsupported.argtypes = [sp, ctypes.c_char_p, ctypes.c_size_t]
+        L.mb3d_cu_march.argtypes = [vp, sp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
+        L.mb3d_cu_post.argtypes = [vp, sp, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
+        L.mb3d_cu_render.argtypes = [vp, sp, ctypes.c_int, vp, vp]
+        L.mb3d_cu_de_probe.argtypes = [vp, sp, ctypes.c_int, vp, ctypes.c_uint32, vp, vp]
+        L.mb3d_cu_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
+        _lib = L
+    return _lib
+
+
+EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_free", "mb3d_cu_set_stream",
+            "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
+            "mb3d_cu_stats_get"]
+
+
+def _ptr(buf):
+    """(pointer, is_torch) of a numpy array or a torch tensor."""
+    if isinstance(buf, np.ndarray):
+        assert buf.flags["C_CONTIGUOUS"]
+        return buf.ctypes.data, False
+    return buf.data_ptr(), True
+
+
+def unsupported(scene):
+    """gpu::unsupported: None when the card renders the scene, else the reason."""
+    reason = ctypes.create_string_buffer(256)
+    r = lib().mb3d_cu_unsupported(ctypes.byref(scene), reason, 256)
+    if r < 0:
+        raise CardError(r, lib().mb3d_cu_last_error().decode())
+    return reason.value.decode() if r == 1 else None
+
+
+class Card:
+    """One device context (its own CUDA stream)."""
+
+    def __init__(self, device=0):
+        self._ctx = ctypes.c_void_p()
+        r = lib().mb3d_cu_init(device, ctypes.byref(self._ctx))
+        self._check(r)
+
+    def close(self):
+        if self._ctx:
+            lib().mb3d_cu_free(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _check(r):
+        if r != 0:
+            raise CardError(r, lib().mb3d_cu_last_error().decode())
+
+    def set_stream(self, stream_handle):
+        self._check(lib().mb3d_cu_set_stream(self._ctx, ctypes.c_void_p(stream_handle or None)))
+
+    def march(self, scene, precision=FP32_FP64, row0=0, rows=None, out=None, cancel=None):
+        rows = scene.height - row0 if rows is None else rows
+        if out is None:
+            out = np.zeros(rows * scene.width, dtype=SILIGHT)
+        p, _ = _ptr(out)
+        cp = ctypes.cast(ctypes.byref(cancel), ctypes.c_void_p) if cancel is not None else None
+        self._check(lib().mb3d_cu_march(self._ctx, ctypes.byref(scene), precision, row0, rows, p, cp))
+        return out
+
+    def post_on_card(self, scene, gbuf, passes=POST_SHADOW | POST_DEAO, precision=FP32_FP64, row0=0, rows=None):
+        rows = scene.height - row0 if rows is None else rows
+        p, _ = _ptr(gbuf)
+        self._check(lib().mb3d_cu_post(self._ctx, ctypes.byref(scene), precision, passes, row0, rows, p, None))
+        return gbuf
+
+    def render(self, scene, precision=FP32_FP64, out=None):
+        if out is None:
+            out = np.zeros(scene.height * scene.width, dtype=SILIGHT)
+        p, _ = _ptr(out)
+        self._check(lib().mb3d_cu_render(self._ctx, ctypes.byref(scene), precision, p, None))
+        return out
+
+    def de_probe(self, scene, pos, precision=FP64):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        n = len(pos)
+        de = np.zeros(n, np.float64)
+        its = np.zeros(n, np.int32)
+        self._check(lib().mb3d_cu_de_probe(self._ctx, ctypes.byref(scene), precision, pos.ctypes.data, n,
+                                           de.ctypes.data, its.ctypes.data))
+        return de, its
+
+    def stats(self):
+        s = Stats()
+        self._check(lib().mb3d_cu_stats_get(self._ctx, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+def is_background(g):
+    return (g["zpos_fine"] >> 16) >= 32768
+
+
+def hit_mask(g):
+    """Pixels with a surface (not background, not the start-inside cut)."""
+    return ((g["zpos_fine"] >> 16) < 32768) & (g["si_gradient"] < 32768)
+
+
+def depth_steps(g, scene_params):
+    """mzz (depth in step widths) of each record from its zpos (src/calc.rs:2166-2167)."""
+    zf = (g["zpos_fine"] >> 8).astype(np.float64)
+    zc_mul, zcorr = scene_params
+    return (((8388351.5 - zf) / zc_mul + 1.0) ** 2 - 1.0) / zcorr

@@ -1,0 +1,104 @@
+"""TEST INFRASTRUCTURE: ctypes binding of the parity oracle (liboracle.so,
+the C++ restatement of mb3d-rs's CPU march).  Only the tests, the smoke
+check and the benchmark's CPU-baseline leg load it; the product never does.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = ctypes.CDLL(LIB)
+        vp = ctypes.c_void_p
+        L.oracle_last_error.restype = ctypes.c_char_p
+        L.oracle_params.argtypes = [vp, vp, ctypes.c_int]
+        L.oracle_pixel_seed.argtypes = [ctypes.c_int64, ctypes.c_int64]
+        L.oracle_pixel_seed.restype = ctypes.c_int32
+        L.oracle_formula_iterate.argtypes = [ctypes.c_int, vp, vp, vp, ctypes.c_double, ctypes.c_int]
+        L.oracle_de_at.argtypes = [vp, vp, ctypes.c_int, vp, vp]
+        L.oracle_march.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int, vp]
+        L.oracle_march_pixels.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int]
+        L.oracle_shadows.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int]
+        L.oracle_deao.argtypes = [vp, vp, ctypes.c_int]
+        L.oracle_ao_rays.argtypes = [ctypes.c_int, vp, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _chk(r):
+    if r < 0:
+        raise RuntimeError(lib().oracle_last_error().decode())
+    return r
+
+
+def params(scene):
+    out = np.zeros(64, np.float64)
+    n = _chk(lib().oracle_params(ctypes.addressof(scene), out.ctypes.data, 64))
+    return out[:n]
+
+
+def pixel_seed(y, x):
+    return lib().oracle_pixel_seed(y, x)
+
+
+def formula_iterate(formula, options, v, j, rout=0.0, ade=False):
+    o = np.zeros(16, np.float64)
+    o[: len(options)] = options
+    v = np.array(v, np.float64)
+    j = np.array(j, np.float64)
+    _chk(lib().oracle_formula_iterate(formula, o.ctypes.data, v.ctypes.data, j.ctypes.data, rout, int(ade)))
+    return v, j
+
+
+def de_at(scene, pos):
+    pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+    de = np.zeros(len(pos), np.float64)
+    its = np.zeros(len(pos), np.int32)
+    _chk(lib().oracle_de_at(ctypes.addressof(scene), pos.ctypes.data, len(pos), de.ctypes.data, its.ctypes.data))
+    return de, its
+
+
+def march(scene, dtype, row0=0, rows=None, threads=0, count=False):
+    rows = scene.height - row0 if rows is None else rows
+    out = np.zeros(rows * scene.width, dtype=dtype)
+    cnt = np.zeros(1, np.uint64)
+    _chk(lib().oracle_march(ctypes.addressof(scene), row0, rows, out.ctypes.data, threads,
+                            cnt.ctypes.data if count else None))
+    return (out, int(cnt[0])) if count else out
+
+
+def march_pixels(scene, dtype, xy, threads=0):
+    xy = np.ascontiguousarray(xy, np.int32).reshape(-1, 2)
+    out = np.zeros(len(xy), dtype=dtype)
+    _chk(lib().oracle_march_pixels(ctypes.addressof(scene), xy.ctypes.data, len(xy), out.ctypes.data, threads))
+    return out
+
+
+def shadows(scene, gbuf, threads=0, per_pixel=True):
+    _chk(lib().oracle_shadows(ctypes.addressof(scene), gbuf.ctypes.data, threads, int(per_pixel)))
+    return gbuf
+
+
+def deao(scene, gbuf, threads=0):
+    _chk(lib().oracle_deao(ctypes.addressof(scene), gbuf.ctypes.data, threads))
+    return gbuf
+
+
+def ao_rays(quality):
+    d = np.zeros((64, 3), np.float32)
+    n = lib().oracle_ao_rays(quality, d.ctypes.data, 64)
+    return d[:n]

@@ -1,0 +1,137 @@
+"""Parity of the card's kernels with the oracle (the C++ FP64 restatement of
+the reference CPU march), through the C ABI.
+
+The plain FP64 march is the drop-in: its records agree with the oracle up
+to the last bits of FMA contraction and of the device's log/sin/cos.  The
+mixed march (FP32 bulk, FP64 origin, t and finish) is held to the targets:
+>= 99.9 % hit/miss agreement and <= 1e-4 relative depth error on the
+pixels both hit (median and 99th percentile), normals within the
+reference's own card tolerance (mean cosine > 0.97, src/gpu.rs:4177-4248).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import mb3dcu
+import oracle_py as O
+import scenes
+from gbcompare import compare
+
+pytestmark = pytest.mark.gpu
+
+
+def zc(sc):
+    p = O.params(sc)
+    return p[7], p[6]
+
+
+def test_de_probe_matches_oracle(card):
+    rng = np.random.default_rng(1)
+    for name in ("Integer Power", "Amazing Box", "Bulbox", "Tricorn", "Real Power", "Folding Int Pow"):
+        sc = scenes.preset(name, 96, 72)
+        pts = rng.uniform(-1.6, 1.6, size=(2000, 3))
+        d0, i0 = O.de_at(sc, pts)
+        d1, i1 = card.de_probe(sc, pts, mb3dcu.FP64)
+        assert (i0 == i1).mean() > 0.999, name
+        rel = np.abs(d0 - d1) / np.maximum(np.abs(d0), 1e-300)
+        assert np.median(rel) < 1e-12 and (rel < 1e-6).mean() > 0.999, (name, np.max(rel))
+        d2, i2 = card.de_probe(sc, pts, mb3dcu.FP32_FP64)
+        rel2 = np.abs(d0 - d2) / np.maximum(np.abs(d0), 1e-300)
+        assert np.median(rel2) < 1e-2, (name, np.median(rel2))
+
+
+@pytest.mark.parametrize("name", scenes.PRESETS)
+def test_fp64_march_matches_oracle(card, name):
+    sc = scenes.preset(name, 160, 120)
+    ref = O.march(sc, mb3dcu.SILIGHT)
+    g = card.march(sc, mb3dcu.FP64)
+    r = compare(g, ref, *zc(sc))
+    assert r["hit_agree"] >= 0.999, r
+    assert r["exact"] >= 0.95, r
+    assert r.get("depth_rel_p99", 0.0) < 1e-6, r
+
+
+def test_menger_hybrid_fp64_and_mixed(card):
+    sc = scenes.scaled(scenes.c4_frames(8)[0], 160, 90)
+    ref = O.march(sc, mb3dcu.SILIGHT)
+    g = card.march(sc, mb3dcu.FP64)
+    r = compare(g, ref, *zc(sc))
+    assert r["hit_agree"] >= 0.999 and r["exact"] >= 0.95, r
+    m = card.march(sc, mb3dcu.FP32_FP64)
+    rm = compare(m, ref, *zc(sc))
+    assert rm["hit_agree"] >= 0.99, rm
+
+
+@pytest.mark.parametrize("name", ["Integer Power", "Amazing Box", "Bulbox"])
+def test_mixed_march_matches_oracle(card, name):
+    sc = scenes.preset(name, 320, 240)
+    ref = O.march(sc, mb3dcu.SILIGHT)
+    g = card.march(sc, mb3dcu.FP32_FP64)
+    r = compare(g, ref, *zc(sc))
+    assert r["hit_agree"] >= 0.995, r
+    assert r["depth_rel_median"] <= 1e-4, r
+    assert r["normal_cos_mean"] > 0.97, r
+
+
+def test_c1_full_size_both_precisions(card):
+    sc = scenes.c1_plain_bulb()
+    ref = O.march(sc, mb3dcu.SILIGHT)
+    g64 = card.march(sc, mb3dcu.FP64)
+    r64 = compare(g64, ref, *zc(sc))
+    assert r64["hit_agree"] >= 0.9995, r64
+    g32 = card.march(sc, mb3dcu.FP32_FP64)
+    r32 = compare(g32, ref, *zc(sc))
+    assert r32["hit_agree"] >= 0.999, r32
+    assert r32["depth_rel_p99"] <= 1e-4, r32
+    assert r32["normal_cos_mean"] > 0.97, r32
+
+
+def test_c2_shadows_and_deao(card):
+    sc = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    ref = O.march(sc, mb3dcu.SILIGHT)
+    for prec, agree in ((mb3dcu.FP64, 0.999), (mb3dcu.FP32_FP64, 0.99)):
+        g = card.march(sc, prec)
+        # post passes on the oracle's own G-buffer: the pass compared alone
+        a = card.post_on_card(sc, ref.copy(), mb3dcu.POST_SHADOW | mb3dcu.POST_DEAO, prec)
+        b = O.deao(sc, O.shadows(sc, ref.copy(), per_pixel=True))
+        obj = mb3dcu.hit_mask(ref)
+        sh = ((a["shadow"] & 0x400) == (b["shadow"] & 0x400))[obj].mean()
+        assert sh >= agree, (prec, sh)
+        dao = np.abs(a["amb_shadow"].astype(np.int64) - b["amb_shadow"].astype(np.int64))[obj] / 16383.0
+        assert dao.mean() < 0.01 and (dao > 0.1).mean() < 0.01, (prec, dao.mean(), (dao > 0.1).mean())
+        r = compare(g, ref, *zc(sc))
+        assert r["hit_agree"] >= agree, (prec, r)
+
+
+def test_render_device_buffer_equals_host_buffer(card):
+    import torch
+    sc = scenes.scaled(scenes.c2_hybrid(), 240, 136)
+    host = card.render(sc, mb3dcu.FP32_FP64)
+    dev = torch.zeros(sc.width * sc.height * 20, dtype=torch.uint8, device="cuda")
+    card.render(sc, mb3dcu.FP32_FP64, out=dev)
+    torch.cuda.synchronize()
+    got = np.frombuffer(dev.cpu().numpy().tobytes(), dtype=mb3dcu.SILIGHT)
+    assert got.tobytes() == host.tobytes()
+    # the same picture twice (no state left between calls)
+    assert card.render(sc, mb3dcu.FP32_FP64).tobytes() == host.tobytes()
+
+
+def test_bands_equal_whole_picture(card):
+    sc = scenes.preset("Integer Power", 128, 96)
+    whole = card.march(sc, mb3dcu.FP32_FP64)
+    parts = [card.march(sc, mb3dcu.FP32_FP64, row0=r, rows=32) for r in (0, 32, 64)]
+    assert np.concatenate(parts).tobytes() == whole.tobytes()
+
+
+def test_errors_and_cancel(card):
+    sc = scenes.preset("Integer Power", 64, 48)
+    with pytest.raises(mb3dcu.CardError) as e:
+        card.march(sc, mb3dcu.FP64, row0=40, rows=20)
+    assert e.value.status == mb3dcu.EINVAL
+    flag = ctypes.c_int(1)
+    with pytest.raises(mb3dcu.CardError) as e:
+        card.march(sc, mb3dcu.FP64, cancel=flag)
+    assert e.value.status == mb3dcu.ECANCELED
+    # the context still works after the failures
+    assert mb3dcu.hit_mask(card.march(sc, mb3dcu.FP64)).mean() > 0.05

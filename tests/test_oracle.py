@@ -1,0 +1,151 @@
+"""The oracle against the reference's own known-answer tests (CPU only).
+
+Each test restates one of mb3d-rs's tests for this path; the citation is
+in its docstring.  These pin the oracle, since the reference binary cannot
+run here.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import mb3dcu
+import oracle_py as O
+import scenes
+
+
+def triplex(n, v):
+    """The spherical triplex power (src/formulas.rs:915-921)."""
+    r = math.sqrt(sum(c * c for c in v))
+    th = math.atan2(v[1], v[0]) * n
+    ph = math.atan2(v[2], math.hypot(v[0], v[1])) * n
+    rn = r ** n
+    return [rn * math.cos(th) * math.cos(ph), rn * math.sin(th) * math.cos(ph), -rn * math.sin(ph)]
+
+
+@pytest.mark.parametrize("n", range(2, 9))
+def test_int_powers_match_spherical_triplex(n):
+    """src/formulas.rs:923-941."""
+    p = [0.31, -0.42, 0.27]
+    v, _ = O.formula_iterate(mb3dcu.F_INTPOW, [n, -1.0], p + [0.0], [0, 0, 0, 0])
+    exp = triplex(n, p)
+    for k in range(3):
+        assert abs(v[k] - exp[k]) < 1e-9, (n, k, v[k], exp[k])
+
+
+def test_real_power_matches_int_power8():
+    """src/formulas.rs:943-954."""
+    p = [0.31, -0.42, 0.27]
+    rout = sum(c * c for c in p)
+    a, _ = O.formula_iterate(mb3dcu.F_INTPOW, [8, -1.0], p + [0.0], [0] * 4, rout)
+    b, _ = O.formula_iterate(mb3dcu.F_REALPOWER, [8.0, -1.0], p + [0.0], [0] * 4, rout)
+    assert np.all(np.abs(a[:3] - b[:3]) < 1e-9)
+
+
+def test_box_scales_derivative():
+    """src/formulas.rs:956-966: r < min_r^2, w *= scale / min_r^2."""
+    v, _ = O.formula_iterate(mb3dcu.F_AMAZINGBOX, [2.0, 0.5, 1.0], [0.1, 0.1, 0.1, 1.0], [0] * 4, 0.0, ade=True)
+    assert abs(v[3] - 8.0) < 1e-12
+
+
+def test_a_negative_min_r_acts_as_zero():
+    """src/formulas.rs:863-875."""
+    for ade in (False, True):
+        for p in ([0.1, 0.1, 0.1, 1.0], [0.8, -0.3, 0.2, 1.0], [0.01, 0.02, -0.01, 1.0]):
+            neg, _ = O.formula_iterate(mb3dcu.F_AMAZINGBOX, [1.7, -0.6, 0.3], p, [0] * 4, 0.0, ade)
+            zero, _ = O.formula_iterate(mb3dcu.F_AMAZINGBOX, [1.7, 0.0, 0.3], p, [0] * 4, 0.0, ade)
+            pos, _ = O.formula_iterate(mb3dcu.F_AMAZINGBOX, [1.7, 0.6, 0.3], p, [0] * 4, 0.0, ade)
+            assert np.array_equal(neg, zero)
+            assert not np.array_equal(neg, pos)
+
+
+def test_pixel_seed_steps_along_the_row():
+    """src/calc.rs:2986-2996 (the jump-ahead equals stepping the LCG)."""
+    for y in (0, 7, 1499):
+        s = ((0x24563487 + (y + 1) * 0x324594A1) + 2 ** 31) % 2 ** 32 - 2 ** 31
+        for x in range(3000):
+            assert O.pixel_seed(y, x) == s, (y, x)
+            s = ((s * 214013 + 2531011) + 2 ** 31) % 2 ** 32 - 2 ** 31
+
+
+def test_bulb_distance_estimate_is_sane():
+    """tests/render.rs:47-60."""
+    s = scenes.preset("Integer Power", 96, 72)
+    de, its = O.de_at(s, [[0.0, 0.0, 0.0], [0.3, 0.2, -2.0]])
+    assert its[0] == s.iterations
+    assert its[1] < s.iterations
+    assert 0.2 < de[1] < 1.5
+
+
+def test_analytic_box_de_is_sane():
+    """tests/render.rs:63-71."""
+    s = scenes.preset("Amazing Box", 96, 72)
+    p = O.params(s)
+    assert p[29] == 1.0  # is_custom_de
+    de, _ = O.de_at(s, [[0.0, 0.0, -9.0]])
+    assert 0.5 < de[0] < 6.0
+
+
+@pytest.mark.parametrize("name", scenes.PRESETS)
+def test_every_preset_hits_the_object(name):
+    """tests/render.rs:24-30."""
+    g = O.march(scenes.preset(name, 96, 72), mb3dcu.SILIGHT)
+    cov = 1.0 - mb3dcu.is_background(g).mean()
+    assert 0.05 < cov < 0.995, (name, cov)
+
+
+def test_deterministic_and_thread_independent():
+    """tests/render.rs:11-21 (byte-exact across thread counts)."""
+    s = scenes.preset("Integer Power", 96, 72)
+    a = O.march(s, mb3dcu.SILIGHT, threads=1)
+    b = O.march(s, mb3dcu.SILIGHT, threads=3)
+    assert a.tobytes() == b.tobytes()
+
+
+def test_shadows_darken():
+    """tests/render.rs:118-139: some pixel in shadow; the per-pixel form of the
+    card pass agrees with the row pass on most pixels."""
+    s = scenes.preset("Integer Power", 96, 72)
+    s.shadow_lights = 0x3F
+    s.soft_radius = 2.0
+    g = O.march(s, mb3dcu.SILIGHT)
+    a = O.shadows(s, g.copy(), per_pixel=False)
+    b = O.shadows(s, g.copy(), per_pixel=True)
+    obj = ~mb3dcu.is_background(a)
+    assert ((a["shadow"] & 0x400) != 0)[obj].sum() > 0
+    assert ((a["shadow"] & 0x400) == (b["shadow"] & 0x400))[obj].mean() > 0.95
+
+
+def test_deao_occludes():
+    """tests/render.rs:162-177 (DE AO quality 1: some pixel > 2000)."""
+    s = scenes.preset("Integer Power", 96, 72)
+    s.deao_quality = 1
+    g = O.deao(s, O.march(s, mb3dcu.SILIGHT))
+    obj = ~mb3dcu.is_background(g)
+    assert (g["amb_shadow"][obj] > 2000).sum() > 0
+
+
+def test_deao_ray_counts():
+    """src/deao.rs:462-470."""
+    assert len(O.ao_rays(0)) == 3
+    r1, r3 = len(O.ao_rays(1)), len(O.ao_rays(3))
+    assert 5 <= r1 and r3 <= 33 and r3 > r1
+    assert len(O.ao_rays(2)) == 17
+
+
+def test_catmull_rom_passes_through_keyframes():
+    """src/anim.rs:692-700: weight 1 on keyframe 1 at t=0, on keyframe 2 at t=1."""
+    assert scenes.catmull_rom_weights(0.0) == [0.0, 1.0, 0.0, 0.0]
+    w = scenes.catmull_rom_weights(1.0)
+    assert abs(w[2] - 1.0) < 1e-15 and abs(w[0]) + abs(w[1]) + abs(w[3]) < 1e-15
+    for t in (0.1, 0.5, 0.9):
+        assert abs(sum(scenes.catmull_rom_weights(t)) - 1.0) < 1e-12
+
+
+def test_configs_see_the_object():
+    """The synthetic workloads show the fractal (not empty, not all inside)."""
+    for sc in (scenes.scaled(scenes.c1_plain_bulb(), 160, 120), scenes.scaled(scenes.c2_hybrid(), 160, 90),
+               scenes.scaled(scenes.c4_frames(8)[0], 160, 90)):
+        g = O.march(sc, mb3dcu.SILIGHT)
+        h = mb3dcu.hit_mask(g).mean()
+        assert 0.05 < h < 0.99, h
