@@ -1,0 +1,322 @@
+#!/usr/bin/env python3
+"""Benchmark of the DE ray march with its post passes on B200.
+
+A step is one whole "Calculate 3D" frame of the hybrid workload: 2 Amazing
+Box (scale -1.5) + 1 Integer Power 8 iterations, repeating, 30 iterations,
+1920x1080, a seeded camera on the r=3 sphere, hard shadows from one light
+and DE ambient occlusion with 17 rays: the primary march (single precision
+bulk, double precision origin, ray parameter and finish), the shadow pass
+and the DE AO pass, into a device-resident G-buffer.  The metric is primary
+rays per second (Mrays/s) of the whole frame.  With N GPUs every rank
+renders its own frame (its own camera seed): weak scaling, no collective on
+the data path; the time is the max over ranks.
+
+  value   device-resident G-buffer, kernels timed with CUDA events
+  e2e     the same through the C ABI with a pinned host G-buffer (the copy
+          back inside the call), timed on the host around each call
+  --impl reference   the reference's CPU renderer (its C++ restatement, all
+          host cores) on a bounded sample of rows of the same frame
+
+Between timed steps a 512 MiB buffer is written to flush L2 (outside the
+events of the step).
+"""
+import argparse
+import ctypes
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "mb3d-rs_b200")]
+
+import numpy as np  # noqa: E402
+
+import mb3dcu  # noqa: E402
+import scenes  # noqa: E402
+
+METRIC = "Mrays/s (primary rays, whole frame: march + hard shadows + 17-ray DE AO)"
+WORKLOAD = "c2-hybrid-1920x1080: AmazingBox(-1.5,0.5,1)x2 + IntPow8x1, 30 its, hard shadows, DE AO 17 rays"
+
+# algorithmic FP32 operations per formula iteration (adds, multiplies,
+# divisions and square roots counted once), from the formula code
+FLOPS_PER_IT = {mb3dcu.F_INTPOW: 61, mb3dcu.F_AMAZINGBOX: 30, mb3dcu.F_MENGERIFS: 16, mb3dcu.F_REALPOWER: 30,
+                mb3dcu.F_TRICORN: 14, mb3dcu.F_BULBOX: 40, mb3dcu.F_FOLDINGINTPOW: 73}
+FLOPS_PER_DE = 40  # the DE's set-up and final formula (numerical gradient)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--scale", type=float, default=1.0, help="picture size factor (profiling runs)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample size")
+    return ap.parse_args()
+
+
+def frame(rank, scale):
+    sc = scenes.c2_hybrid(scenes.C2_SEED + rank)
+    if scale != 1.0:
+        sc = scenes.scaled(sc, max(16, int(1920 * scale)), max(16, int(1080 * scale)))
+    return sc
+
+
+# ---------------------------------------------------------------------------
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _oracle():
+    """The oracle (CPU-baseline leg and reference arm only)."""
+    p = os.path.join(ROOT, "oracle")
+    if p not in sys.path:
+        sys.path.insert(0, p)
+    import oracle_py
+    return oracle_py
+
+
+def cpu_rows(sc, seconds, timer_rows=16):
+    """Evenly spaced rows whose CPU render takes about `seconds`."""
+    O = _oracle()
+    h = sc.height
+    probe = np.linspace(0, h - 1, timer_rows).round().astype(np.int32)
+    t = time.perf_counter()
+    O.render_rows(sc, mb3dcu.SILIGHT, probe)
+    dt = max(time.perf_counter() - t, 1e-3)
+    n = int(min(h, max(timer_rows, timer_rows * seconds / dt)))
+    return np.linspace(0, h - 1, n).round().astype(np.int32)
+
+
+def cpu_baseline(sc, seconds):
+    """The oracle (C++ restatement of the reference CPU renderer) on a row sample."""
+    O = _oracle()
+    rows = cpu_rows(sc, seconds)
+    t = time.perf_counter()
+    O.render_rows(sc, mb3dcu.SILIGHT, rows)
+    dt = time.perf_counter() - t
+    rays = len(rows) * sc.width
+    return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{len(rows)} evenly spaced rows of the {sc.width}x{sc.height} frame ({rays} primary rays, "
+                      f"march + hard shadows + DE AO), {dt:.1f} s, all host threads, C++ restatement of the "
+                      f"reference CPU renderer"}
+
+
+def run_reference(args):
+    sc = frame(0, args.scale)
+    rows = cpu_rows(sc, 6.0)
+    O = _oracle()
+    for _ in range(args.warmup):
+        O.render_rows(sc, mb3dcu.SILIGHT, rows[: max(1, len(rows) // 8)])
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        O.render_rows(sc, mb3dcu.SILIGHT, rows)
+        times.append(time.perf_counter() - t)
+    rays = len(rows) * sc.width
+    ms = 1000.0 * statistics.mean(times)
+    v = rays / (ms / 1000.0) / 1e6
+    sample = (f"{len(rows)} evenly spaced rows of the {sc.width}x{sc.height} frame per step ({rays} primary rays, "
+              f"march + hard shadows + DE AO), C++ restatement of the reference CPU renderer (the Rust "
+              f"reference cannot be built here), all host threads")
+    out = {"metric": METRIC, "value": v, "unit": "Mrays/s", "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "width": sc.width, "height": sc.height, "seed": scenes.C2_SEED},
+           "impl": "reference",
+           "cpu_baseline": {"value": v, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": v, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def march_flops(sc, st):
+    its = st["orbit_its"]
+    f = 0
+    for k in range(sc.n_slots):
+        f += its[k] * FLOPS_PER_IT.get(sc.slots[k].formula, 30)
+    return f + st["de_evals"] * FLOPS_PER_DE
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local))
+    prec = mb3dcu.FP32_FP64 if args.precision == "mixed" else mb3dcu.FP64
+    card = mb3dcu.Card(local)
+    stream = torch.cuda.current_stream()
+    card.set_stream(stream.cuda_stream)
+    sc = frame(rank, args.scale)
+    npix = sc.width * sc.height
+    gbuf = torch.empty(npix * 20, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    for _ in range(max(3, args.warmup)):
+        card.render(sc, prec, out=gbuf)
+    # algorithmic work of the march kernel (a counting pass, not timed)
+    card.set_counting(True)
+    card.render(sc, prec, out=gbuf)
+    counted = card.stats()
+    card.set_counting(False)
+    peak32 = card.fma_peak(False)
+    peak64 = card.fma_peak(True)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    clk = Clocks(local)
+    clk.start()
+    step_ms, kern = [], []
+    launches = 0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        card.render(sc, prec, out=gbuf)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        st = card.stats()
+        kern.append(st)
+        launches += st["launches"]
+    barrier()
+    clocks = clk.stop()
+    ms = statistics.mean(step_ms)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * npix / (ms / 1000.0) / 1e6
+
+    # end to end: the C ABI with a pinned host G-buffer (copy back inside the call)
+    host = torch.empty(npix * 20, dtype=torch.uint8, pin_memory=True)
+    hnp = host.numpy()
+    card.set_stream(None)
+    card.render(sc, prec, out=hnp)
+    barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        card.render(sc, prec, out=hnp)
+        e2e_ms.append(1000.0 * (time.perf_counter() - t))
+    barrier()
+    e2e = statistics.mean(e2e_ms)
+    if world > 1:
+        t = torch.tensor([e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e = float(t.item())
+
+    # roofline of the march kernel (single precision bulk): counted flops per
+    # launch over its mean launch time, against the measured FP32 FMA peak
+    k_ms = statistics.mean(k["ms_march"] - k["ms_finish"] for k in kern)
+    stage = {"k_march": k_ms, "k_finish64": statistics.mean(k["ms_finish"] for k in kern),
+             "k_shadow": statistics.mean(k["ms_shadow"] for k in kern),
+             "k_deao": statistics.mean(k["ms_deao"] for k in kern)}
+    flops = march_flops(sc, counted)
+    achieved = flops / (k_ms / 1000.0) / 1e12
+    traffic = load_traffic().get("k_march")
+    roof = {"kernel": "k_march (FP32 bulk march)", "bound": "fp32-alu", "achieved": achieved, "peak": peak32,
+            "unit": "TFLOP/s", "frac": achieved / peak32 if peak32 else None,
+            "peak_source": "measured FP32 FMA chain on this GPU (MEASURED_PEAKS.json has no FP32 figure)",
+            "traffic": traffic, "flops_per_launch": flops, "ms_per_launch": k_ms}
+    out = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32+f64" if prec == mb3dcu.FP32_FP64 else "f64", "data": "synthetic",
+           "config": {"workload": WORKLOAD, "width": sc.width, "height": sc.height, "seed": scenes.C2_SEED,
+                      "precision": args.precision, "parallelism": f"frame per rank x{world}",
+                      "l2": "512 MiB buffer written between timed steps (outside the step events)"},
+           "e2e": {"value": world * npix / (e2e / 1000.0) / 1e6, "unit": "Mrays/s",
+                   "h2d_bytes_per_step": ctypes.sizeof(mb3dcu.Scene), "d2h_bytes_per_step": npix * 20},
+           "gpu_launches": launches, "roofline": roof, "stages_ms": stage,
+           "peaks": {"fp32_fma_tflops": peak32, "fp64_fma_tflops": peak64},
+           "counted": {"de_evals": counted["de_evals"], "orbit_its": counted["orbit_its"]},
+           "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(frame(0, args.scale), args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    card.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -147,7 +147,8 @@ typedef struct mb3d_cu_stats {
     float ms_total;       /* first launch to last, device time */
     uint32_t launches;    /* this library's kernel launches in the call */
     uint32_t fp64_pixels; /* pixels the mixed mode marched in double precision */
-    uint64_t de_evals;    /* DE evaluations (counting builds only, else 0) */
+    uint64_t de_evals;    /* DE evaluations of the march kernel (counting mode only, else 0) */
+    uint64_t orbit_its[6];/* formula iterations per slot, all orbits (counting mode only) */
 } mb3d_cu_stats;
 
 typedef struct mb3d_cu_ctx mb3d_cu_ctx;
@@ -204,6 +205,17 @@ int mb3d_cu_de_probe(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision
 
 /* The counters of the last call on this context. */
 int mb3d_cu_stats_get(const mb3d_cu_ctx *ctx, mb3d_cu_stats *out);
+
+/* Counting mode (on != 0): the march kernel also counts its DE evaluations
+ * and formula iterations into the stats (a slower build of the kernel, for
+ * the roofline's algorithmic work; the reference's ItStats counterpart,
+ * src/calc.rs:140-180). */
+int mb3d_cu_set_counting(mb3d_cu_ctx *ctx, int on);
+
+/* Measurement helper: the FP32 (fp64 = 0) or FP64 (fp64 = 1) fused
+ * multiply-add issue rate of this device, TFLOP/s (2 per FMA), from a
+ * dependent-chain kernel timed with CUDA events. */
+int mb3d_cu_fma_peak(mb3d_cu_ctx *ctx, int fp64, double *tflops);
 
 #ifdef __cplusplus
 }

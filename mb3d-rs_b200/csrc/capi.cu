@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstring>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -31,11 +32,21 @@ struct mb3d_cu_ctx {
     size_t gbuf_cap = 0;
     Hand *d_hand = nullptr;
     size_t hand_cap = 0;
+    Hand *d_slow = nullptr;  // the finish's rare cases
+    size_t slow_cap = 0;
+    uint32_t *d_slist = nullptr;  // surface pixels of the post passes
+    size_t slist_cap = 0;
+    PostStart *d_ps = nullptr;
+    size_t ps_cap = 0;
+    float *d_minra = nullptr;     // the DE AO rays' openness
+    size_t minra_cap = 0;
     unsigned int *d_counters = nullptr;
     double *d_probe = nullptr;
     size_t probe_cap = 0;
     cudaEvent_t ev[8] = {};
     mb3d_cu_stats stats = {};
+    int counting = 0;
+    unsigned long long *d_count = nullptr;
     std::mutex mu;
 };
 
@@ -114,8 +125,13 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     if (c->stream && c->stream != c->own) cudaStreamSynchronize(c->stream);
     cudaFree(c->d_gbuf);
     cudaFree(c->d_hand);
+    cudaFree(c->d_slow);
+    cudaFree(c->d_slist);
+    cudaFree(c->d_ps);
+    cudaFree(c->d_minra);
     cudaFree(c->d_counters);
     cudaFree(c->d_probe);
+    cudaFree(c->d_count);
     for (auto &ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     if (c->own) cudaStreamDestroy(c->own);
@@ -156,44 +172,64 @@ int mb3d_cu_unsupported(const mb3d_cu_scene *sc, char *reason, size_t cap) {
 static int march_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int row0, int rows, mb3d_cu_silight *dg) {
     cudaStream_t s = c->stream;
     size_t npix = (size_t)rows * p.width;
-    c->stats.fp64_pixels = 0;
-    CU_TRY(cudaEventRecord(c->ev[0], s));
-    if (precision == MB3D_CU_FP64 || p.all_fp64) {
-        launch_march64(p, row0, rows, dg, s);
-        c->stats.launches += 1;
-        if (int r = check_launch("k_march64")) return r;
-        CU_TRY(cudaEventRecord(c->ev[1], s));
-        CU_TRY(cudaEventRecord(c->ev[2], s));
-        if (precision != MB3D_CU_FP64) c->stats.fp64_pixels = (uint32_t)npix;
-    } else {
-        if (int r = grow((void **)&c->d_hand, &c->hand_cap, npix * sizeof(Hand))) return r;
-        CU_TRY(cudaMemsetAsync(c->d_counters, 0, 64 * sizeof(unsigned int), s));
-        launch_march32(p, row0, rows, dg, c->d_hand, c->d_counters, c->sms, s);
-        if (int r = check_launch("k_march32")) return r;
-        CU_TRY(cudaEventRecord(c->ev[1], s));
-        launch_finish64(p, row0, c->d_hand, c->d_counters, dg, c->sms, s);
-        if (int r = check_launch("k_finish64")) return r;
-        CU_TRY(cudaEventRecord(c->ev[2], s));
-        c->stats.launches += 2;
+    bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
+    c->stats.fp64_pixels = (precision != MB3D_CU_FP64 && p.all_fp64) ? (uint32_t)npix : 0u;
+    if (int r = grow((void **)&c->d_hand, &c->hand_cap, npix * sizeof(Hand))) return r;
+    CU_TRY(cudaMemsetAsync(c->d_counters, 0, 64 * sizeof(unsigned int), s));
+    if (c->counting) {
+        if (!c->d_count) CU_TRY(cudaMalloc(&c->d_count, 16 * sizeof(unsigned long long)));
+        CU_TRY(cudaMemsetAsync(c->d_count, 0, 16 * sizeof(unsigned long long), s));
     }
+    int items = ((p.width + 7) / 8) * ((rows + 3) / 4);  // warps' worth of work
+    int blocks = c->sms * p.blocks_per_sm;
+    int need = (items + 7) / 8;
+    if (blocks > need) blocks = need > 0 ? need : 1;
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    launch_march(p, mixed, row0, rows, dg, c->d_hand, c->d_counters, c->counting ? c->d_count : nullptr, blocks, s);
+    if (int r = check_launch("k_march")) return r;
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    if (int r = grow((void **)&c->d_slow, &c->slow_cap, npix * sizeof(Hand))) return r;
+    launch_finish(p, mixed, row0, c->d_hand, c->d_counters, c->d_slow, dg, c->sms * p.blocks_per_sm, s);
+    if (int r = check_launch("k_finish")) return r;
+    CU_TRY(cudaEventRecord(c->ev[2], s));
+    c->stats.launches += 3;
     return 0;
 }
 
+// the post passes: the surface pixels listed, their start points found,
+// then one lane per shadow ray and per DE AO ray
 static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int passes, int row0, int rows,
                        mb3d_cu_silight *dg) {
     cudaStream_t s = c->stream;
     bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
+    if (!(passes & MB3D_CU_POST_SHADOW) || p.n_lights == 0) passes &= ~MB3D_CU_POST_SHADOW;
+    if (!(passes & MB3D_CU_POST_DEAO) || p.ao_quality < 0 || p.ao_rays == 0) passes &= ~MB3D_CU_POST_DEAO;
+    size_t npix = (size_t)rows * p.width;
+    if (int r = grow((void **)&c->d_slist, &c->slist_cap, npix * sizeof(uint32_t))) return r;
+    if (int r = grow((void **)&c->d_ps, &c->ps_cap, npix * sizeof(PostStart))) return r;
+    if (passes & MB3D_CU_POST_DEAO)
+        if (int r = grow((void **)&c->d_minra, &c->minra_cap, npix * (size_t)p.ao_rays * sizeof(float))) return r;
+    unsigned int *cnt = c->d_counters + 8;  // [0] surfaces, [1] shadow queue, [2] AO queue
+    CU_TRY(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned int), s));
     CU_TRY(cudaEventRecord(c->ev[3], s));
-    if ((passes & MB3D_CU_POST_SHADOW) && p.n_lights > 0) {
-        launch_shadow(p, row0, rows, dg, mixed, s);
+    launch_surface(p, (int)npix, passes, dg, c->d_slist, cnt, c->sms * 4, s);
+    c->stats.launches += 1;
+    if (passes) {
+        launch_post_start(p, mixed, row0, passes, dg, c->d_slist, cnt, c->d_ps, c->sms * 8, s);
         c->stats.launches += 1;
-        if (int r = check_launch("k_shadow")) return r;
+        if (int r = check_launch("k_post_start")) return r;
+    }
+    if (passes & MB3D_CU_POST_SHADOW) {
+        launch_shadow_rays(p, mixed, row0, c->d_ps, cnt, dg, cnt + 1, c->sms * p.blocks_per_sm, s);
+        c->stats.launches += 1;
+        if (int r = check_launch("k_shadow_rays")) return r;
     }
     CU_TRY(cudaEventRecord(c->ev[4], s));
-    if ((passes & MB3D_CU_POST_DEAO) && p.ao_quality >= 0 && p.ao_rays > 0) {
-        launch_deao(p, row0, rows, dg, mixed, s);
-        c->stats.launches += 1;
-        if (int r = check_launch("k_deao")) return r;
+    if (passes & MB3D_CU_POST_DEAO) {
+        launch_ao_rays(p, mixed, c->d_ps, dg, cnt, c->d_minra, cnt + 2, c->sms * p.blocks_per_sm, s);
+        launch_ao_final(p, c->d_ps, cnt, c->d_minra, dg, c->sms * 8, s);
+        c->stats.launches += 2;
+        if (int r = check_launch("k_ao")) return r;
     }
     CU_TRY(cudaEventRecord(c->ev[5], s));
     return 0;
@@ -202,6 +238,12 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
 static int finish_call(mb3d_cu_ctx *c, bool marched, bool posted) {
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    if (marched && c->counting && c->d_count) {
+        unsigned long long h[16];
+        CU_TRY(cudaMemcpy(h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < 6; k++) c->stats.orbit_its[k] = h[k];
+        c->stats.de_evals = h[6];
+    }
     float ms = 0.f;
     if (marched) {
         cudaEventElapsedTime(&ms, c->ev[0], c->ev[2]);
@@ -220,6 +262,29 @@ static int finish_call(mb3d_cu_ctx *c, bool marched, bool posted) {
     return 0;
 }
 
+// launch tuning: MB3D_CU_TUNE="refill=8,blocks=4,margin=4,back=2"
+static void apply_tuning(DevParams &p) {
+    const char *t = getenv("MB3D_CU_TUNE");
+    if (!t) return;
+    std::string s(t);
+    size_t i = 0;
+    while (i < s.size()) {
+        size_t j = s.find(',', i);
+        if (j == std::string::npos) j = s.size();
+        std::string kv = s.substr(i, j - i);
+        size_t e = kv.find('=');
+        if (e != std::string::npos) {
+            std::string k = kv.substr(0, e);
+            double v = atof(kv.c_str() + e + 1);
+            if (k == "refill" && v >= 1 && v <= 32) p.refill_min = (int)v;
+            else if (k == "blocks" && v >= 1 && v <= 16) p.blocks_per_sm = (int)v;
+            else if (k == "margin" && v >= 1) p.hand_margin = (float)v;
+            else if (k == "back" && v >= 0 && v <= 2) p.hand_back = (int)v;
+        }
+        i = j + 1;
+    }
+}
+
 static int run(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, int passes, bool do_march, uint32_t row0,
                uint32_t rows, mb3d_cu_silight *gbuf, const volatile int *cancel) {
     if (!c || !sc || !gbuf) return fail(MB3D_CU_EINVAL, "NULL argument");
@@ -230,6 +295,7 @@ static int run(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, int passe
     std::string err;
     int r = setup_params(*sc, p, err);
     if (r < 0) return fail(r, err);
+    apply_tuning(p);
     if ((uint64_t)row0 + rows > (uint64_t)p.height || rows == 0) return fail(MB3D_CU_EINVAL, "rows outside the picture");
     if (cancel && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
     std::memset(&c->stats, 0, sizeof(c->stats));
@@ -299,6 +365,35 @@ int mb3d_cu_de_probe(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, con
 int mb3d_cu_stats_get(const mb3d_cu_ctx *c, mb3d_cu_stats *out) {
     if (!c || !out) return fail(MB3D_CU_EINVAL, "NULL argument");
     *out = c->stats;
+    return 0;
+}
+
+int mb3d_cu_set_counting(mb3d_cu_ctx *c, int on) {
+    if (!c) return fail(MB3D_CU_EINVAL, "ctx is NULL");
+    c->counting = on != 0;
+    return 0;
+}
+
+int mb3d_cu_fma_peak(mb3d_cu_ctx *c, int fp64, double *tflops) {
+    if (!c || !tflops) return fail(MB3D_CU_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    if (int e = grow((void **)&c->d_probe, &c->probe_cap, 64)) return e;
+    int blocks = c->sms * 8, iters = fp64 ? 512 : 2048;
+    launch_fma_peak(fp64 != 0, c->d_probe, blocks, iters, c->stream);  // warm-up
+    if (int r = check_launch("k_fma_peak")) return r;
+    float best = 1e30f;
+    for (int rep = 0; rep < 5; rep++) {
+        CU_TRY(cudaEventRecord(c->ev[6], c->stream));
+        launch_fma_peak(fp64 != 0, c->d_probe, blocks, iters, c->stream);
+        CU_TRY(cudaEventRecord(c->ev[7], c->stream));
+        CU_TRY(cudaEventSynchronize(c->ev[7]));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
+        if (ms < best) best = ms;
+    }
+    double flops = 2.0 * 8.0 * 16.0 * (double)iters * (double)blocks * 256.0;
+    *tflops = flops / ((double)best * 1e-3) / 1e12;
     return 0;
 }
 

@@ -1,0 +1,327 @@
+// The distance estimate of the march loop, in double or single precision:
+// only the two values the march decides on (the DE in step widths and the
+// iteration count), with the four orbits of the numerical DE iterated in
+// lock-step.
+//
+// Numerical DE (MB3D DE option 0, src/calc.rs:1515-1543): the hybrid at c,
+// then at c + offset on each axis with the centre's iteration count as the
+// limit and RStop3D as the bailout; DE = R ln R * s / (sqrt(sum (R - R_k)^2)
+// + o006).  In lock-step the offset orbits stop where the centre stops (its
+// count is their limit) or at their own bailout, exactly as the sequential
+// runs do, so the double precision form gives the reference's values.
+//
+// The single precision form keeps the reference's formula, rewritten so that
+// it stays accurate and overflow-free in single precision:
+//     d_k = (v - v_k).(v + v_k) / |v|^2 (scaled by the largest component),
+//     DE  = ln R * s / (sqrt(sum (d_k * h/h_k)^2) + o006 / R),
+// where h_k is the offset each rounded offset point actually got, so that
+// the rounding of the coordinates does not bias the gradient.
+//
+// Analytic DE (options 2 / 11, src/iteration.rs:539-574): one orbit with the
+// running derivative in w; sqrt(R) / |w|.
+#pragma once
+#include "devparams.h"
+#include "formulas.cuh"
+
+namespace mb3dcu {
+
+struct DEr {
+    double de;
+    int it;
+    bool need64;  // single precision cannot resolve the offset here
+};
+
+// The iteration state a full DE leaves for the colouring (the record's
+// fields after calc_de, src/calc.rs:1536-1542: rout and it_result of the
+// centre; rold, otrap and the vector of the last run, the z offset's for the
+// numerical DE) and the centre's smoothed iteration count.
+struct DEstate {
+    double rout, rold, otrap, v[3];
+    float smooth_it;
+};
+
+__device__ __forceinline__ float fsqrt_fast(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
+// ln |v|^2 without overflow
+__device__ __forceinline__ float log_len2_f(const float v[4]) {
+    float m = fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2])));
+    if (!(m > 0.0f)) return -1e30f;
+    float s = __frcp_rn(m);
+    float a = v[0] * s, b = v[1] * s, c = v[2] * s;
+    return __logf(a * a + b * b + c * c) + 2.0f * __logf(m);
+}
+
+template <typename R>
+__device__ __forceinline__ R param_f(const DevParams &p, double d, float f);
+template <>
+__device__ __forceinline__ double param_f<double>(const DevParams &, double d, float) { return d; }
+template <>
+__device__ __forceinline__ float param_f<float>(const DevParams &, double, float f) { return f; }
+
+// One counted-or-not hybrid step on orbit q (run_with's body, src/iteration.rs:289-301)
+template <typename R, int Q, int FM>
+__device__ __forceinline__ void step_orbits(const DevSlot &s, R (&v)[Q][4], R (&j)[Q][3], const R (&rout)[Q]) {
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+        formula_iterate<R, FM>(s, v[q], j[q], rout[q]);
+        if (s.julia_add) {
+            v[q][0] += j[q][0];
+            v[q][1] += j[q][1];
+            v[q][2] += j[q][2];
+        }
+    }
+}
+
+// Counting (bench and roofline only): orbit iterations per slot and DE
+// evaluations, kept per thread and added to global counters at the end.
+struct DECount {
+    unsigned long long its[MB3D_MAX_SLOTS];
+    unsigned long long evals;
+    __device__ void clear() {
+        for (int k = 0; k < MB3D_MAX_SLOTS; k++) its[k] = 0;
+        evals = 0;
+    }
+    __device__ void flush(unsigned long long *g) {
+        for (int k = 0; k < MB3D_MAX_SLOTS; k++)
+            if (its[k]) atomicAdd(&g[k], its[k]);
+        if (evals) atomicAdd(&g[MB3D_MAX_SLOTS], evals);
+    }
+};
+
+// CalcSmoothIterations (src/iteration.rs:140-152) on the centre's lengths,
+// given as ln(rout) and ln(rold) (single precision: from the scaled vector,
+// so that an overflowed length still has its logarithm)
+__device__ __forceinline__ float smooth_iterations_d(const DevParams &p, bool rout_le1, bool rold_lt1, double lr,
+                                                     double lro, int it, int n) {
+    if (rout_le1) return (float)it;
+    if (rold_lt1) {
+        double d = log(lr * 0.5) * (double)p.fhln[n];
+        return (float)((double)it + (double)p.ln_rstop - d);
+    }
+    double d = log(0.5 * lr);
+    double e = d - log(0.5 * lro);
+    return (float)(((double)p.ln_rstop - d) / (e + 1e-100) + (double)it);
+}
+
+template <typename R>
+__device__ __forceinline__ float smooth_of(const DevParams &p, R rout, R rold, const R v[4], int it, int n) {
+    if (sizeof(R) == 8) {
+        double ro = (double)rout, rl = (double)rold;
+        if (ro <= 1.0) return (float)it;
+        return smooth_iterations_d(p, false, rl < 1.0, log(ro), rl < 1.0 ? 0.0 : log(rl), it, n);
+    } else {
+        float ro = (float)rout, rl = (float)rold;
+        if (ro <= 1.0f) return (float)it;
+        float vf[4] = {(float)v[0], (float)v[1], (float)v[2], 0.f};
+        double lr = (ro < 1e30f) ? (double)__logf(ro) : (double)log_len2_f(vf);
+        return smooth_iterations_d(p, false, rl < 1.0f, lr, rl < 1.0f ? 0.0 : (double)__logf(rl), it, n);
+    }
+}
+
+template <typename R, int FM, bool COUNT = false, bool FULL = false>
+__device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], float ms_de_stop, DECount *cnt = nullptr,
+                                       DEstate *st = nullptr, bool calc_sit = false) {
+    if (COUNT) cnt->evals++;
+    DEr out;
+    out.need64 = false;
+    const int max_it = p.max_it;
+    const R rstop = param_f<R>(p, p.d_rstop, p.d_rstop_f);
+    if (p.is_custom_de) {
+        R v[1][4], j[1][3], rout[1];
+        v[0][0] = (R)c[0];
+        v[0][1] = (R)c[1];
+        v[0][2] = (R)c[2];
+        if (p.do_julia) {
+            j[0][0] = param_f<R>(p, p.ju[0], p.ju_f[0]);
+            j[0][1] = param_f<R>(p, p.ju[1], p.ju_f[1]);
+            j[0][2] = param_f<R>(p, p.ju[2], p.ju_f[2]);
+        } else {
+            j[0][0] = v[0][0]; j[0][1] = v[0][1]; j[0][2] = v[0][2];
+        }
+        rout[0] = v[0][0] * v[0][0] + v[0][1] * v[0][1] + v[0][2] * v[0][2];
+        v[0][3] = ((p.de_option & 0x38) == 16) ? rout[0] : R(1);
+        R rold0 = 0, otrap0 = rout[0];
+        int n = 0, btmp = p.slots[0].iterations, it = 0;
+        unsigned int unc = 0;
+        for (;;) {
+            if (FULL) rold0 = rout[0];
+            int guard = 0;
+            while (btmp <= 0) {
+                n += 1;
+                if (n > p.end_to) n = p.repeat_from;
+                btmp = p.slots[n].iterations;
+                if (++guard > 64) goto done_a;
+            }
+            {
+                const DevSlot &s = p.slots[n];
+                step_orbits<R, 1, FM>(s, v, j, rout);
+                if (COUNT) cnt->its[n] += 1;
+                btmp -= 1;
+                if (s.uncounted) {
+                    if (++unc > 100000u) goto done_a;
+                    continue;
+                }
+            }
+            it += 1;
+            rout[0] = v[0][0] * v[0][0] + v[0][1] * v[0][1] + v[0][2] * v[0][2];
+            if (FULL && rout[0] < otrap0) otrap0 = rout[0];
+            if (it >= max_it || rout[0] > rstop) break;
+        }
+    done_a:
+        if (FULL) {
+            st->rout = (double)rout[0];
+            st->rold = (double)rold0;
+            st->otrap = (double)otrap0;
+            st->v[0] = (double)v[0][0]; st->v[1] = (double)v[0][1]; st->v[2] = (double)v[0][2];
+            st->smooth_it = calc_sit ? smooth_of<R>(p, rout[0], rold0, v[0], it, n) : 0.f;
+        }
+        double r;
+        if (sizeof(R) == 8) {
+            double w = (double)v[0][3];
+            r = ((p.de_option & 7) == 4) ? fabs((double)v[0][1]) * log(fabs((double)v[0][1])) / w
+                                         : sqrt((double)rout[0]) / fabs(w);
+        } else {
+            float vf[4] = {(float)v[0][0], (float)v[0][1], (float)v[0][2], (float)v[0][3]};
+            float rf;
+            if ((p.de_option & 7) == 4) {
+                rf = __fdividef(fabsf(vf[1]) * __logf(fabsf(vf[1])), vf[3]);
+            } else {
+                float len = fsqrt_fast((float)rout[0]);
+                if (!((float)rout[0] < 1e30f)) len = __expf(0.5f * log_len2_f(vf));
+                rf = __fdividef(len, fabsf(vf[3]));
+            }
+            r = (double)rf;
+        }
+        out.de = r * (double)p.d_de_scale;
+        out.it = it;
+    } else {
+        // four orbits: 0 = the centre, 1..3 = the offsets on x, y, z
+        R v[4][4], j[4][3], rout[4];
+        float corr[3] = {1.f, 1.f, 1.f};
+        const double off = (double)p.de_offset;
+        if (sizeof(R) == 4) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                float cf = (float)c[k];
+                float o = (float)(c[k] + off);
+                double h = (double)o - (double)cf;
+                if (h <= 0.0) out.need64 = true;
+                corr[k] = (float)(off / fmax(h, 1e-300));
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) v[q][k] = (R)((q == k + 1) ? c[k] + off : c[k]);
+            v[q][3] = R(0);
+            if (p.do_julia) {
+                j[q][0] = param_f<R>(p, p.ju[0], p.ju_f[0]);
+                j[q][1] = param_f<R>(p, p.ju[1], p.ju_f[1]);
+                j[q][2] = param_f<R>(p, p.ju[2], p.ju_f[2]);
+            } else {
+                j[q][0] = v[q][0]; j[q][1] = v[q][1]; j[q][2] = v[q][2];
+            }
+            rout[q] = v[q][0] * v[q][0] + v[q][1] * v[q][1] + v[q][2] * v[q][2];
+        }
+        const R rstop3d = param_f<R>(p, p.rstop3d, p.rstop3d_f);
+        bool live[4] = {true, true, true, true};
+        float lr_frozen[4] = {0.f, 0.f, 0.f, 0.f};
+        R rold0 = 0, rold3 = 0, otrap3 = rout[3];
+        int n = 0, btmp = p.slots[0].iterations, it = 0;
+        unsigned int unc = 0;
+        for (;;) {
+            if (FULL) {
+                rold0 = rout[0];
+                if (live[3]) rold3 = rout[3];
+            }
+            int guard = 0;
+            while (btmp <= 0) {
+                n += 1;
+                if (n > p.end_to) n = p.repeat_from;
+                btmp = p.slots[n].iterations;
+                if (++guard > 64) goto done_n;
+            }
+            {
+                const DevSlot &s = p.slots[n];
+                step_orbits<R, 4, FM>(s, v, j, rout);
+                if (COUNT) cnt->its[n] += 4;
+                btmp -= 1;
+                if (s.uncounted) {
+                    if (++unc > 100000u) goto done_n;
+                    continue;
+                }
+            }
+            it += 1;
+            rout[0] = v[0][0] * v[0][0] + v[0][1] * v[0][1] + v[0][2] * v[0][2];
+#pragma unroll
+            for (int q = 1; q < 4; q++) {
+                if (live[q]) {
+                    rout[q] = v[q][0] * v[q][0] + v[q][1] * v[q][1] + v[q][2] * v[q][2];
+                    if (FULL && q == 3 && rout[3] < otrap3) otrap3 = rout[3];
+                    if (rout[q] > rstop3d) {
+                        live[q] = false;
+                        if (sizeof(R) == 4) {
+                            float vf[4] = {(float)v[q][0], (float)v[q][1], (float)v[q][2], 0.f};
+                            lr_frozen[q] = log_len2_f(vf);
+                        }
+                    }
+                }
+            }
+            if (it >= max_it || rout[0] > rstop) break;
+            // (a stopped offset orbit keeps being iterated in the lock-step;
+            // its values are no longer used)
+        }
+    done_n:
+        if (FULL) {
+            st->rout = (double)rout[0];
+            st->rold = (double)rold3;
+            st->otrap = (double)otrap3;
+            st->v[0] = (double)v[3][0]; st->v[1] = (double)v[3][1]; st->v[2] = (double)v[3][2];
+            st->smooth_it = calc_sit ? smooth_of<R>(p, rout[0], rold0, v[0], it, n) : 0.f;
+        }
+        if (sizeof(R) == 8) {
+            double R0 = (double)rout[0];
+            if (R0 < 1e-200) {
+                out.de = 0.0;
+            } else {
+                double g0 = (R0 - (double)rout[1]) * (R0 - (double)rout[1]);
+                double g1 = (R0 - (double)rout[2]) * (R0 - (double)rout[2]);
+                double g2 = (R0 - (double)rout[3]) * (R0 - (double)rout[3]);
+                out.de = R0 * log(R0) * (double)p.d_de_scale / (sqrt(g0 + g1 + g2) + (double)p.de_offset006);
+            }
+        } else {
+            float m0 = fmaxf(fabsf((float)v[0][0]), fmaxf(fabsf((float)v[0][1]), fabsf((float)v[0][2])));
+            if (!(m0 > 0.0f)) {
+                out.de = 0.0;
+            } else {
+                float sc = m0 > 1e15f ? __frcp_rn(m0) : 1.0f;
+                float c0 = (float)v[0][0] * sc, c1 = (float)v[0][1] * sc, c2 = (float)v[0][2] * sc;
+                float Rs = c0 * c0 + c1 * c1 + c2 * c2;
+                float lr = __logf(Rs) - 2.0f * __logf(sc);
+                float inv = __frcp_rn(Rs);
+                float g = 0.0f;
+#pragma unroll
+                for (int q = 1; q < 4; q++) {
+                    float d;
+                    if (live[q]) {
+                        float a0 = ((float)v[0][0] - (float)v[q][0]) * sc, b0 = ((float)v[0][0] + (float)v[q][0]) * sc;
+                        float a1 = ((float)v[0][1] - (float)v[q][1]) * sc, b1 = ((float)v[0][1] + (float)v[q][1]) * sc;
+                        float a2 = ((float)v[0][2] - (float)v[q][2]) * sc, b2 = ((float)v[0][2] + (float)v[q][2]) * sc;
+                        d = (a0 * b0 + a1 * b1 + a2 * b2) * inv;
+                    } else {
+                        d = 1.0f - __expf(lr_frozen[q] - lr);
+                    }
+                    d *= corr[q - 1];
+                    g += d * d;
+                }
+                out.de = (double)__fdividef(lr * p.d_de_scale, fsqrt_fast(g) + p.de_offset006 * __expf(-lr));
+            }
+        }
+        out.it = it;
+    }
+    double mn = (double)ms_de_stop * 0.25;
+    if (out.de < mn || isnan(out.de)) out.de = mn;
+    return out;
+}
+
+}  // namespace mb3dcu

@@ -18,6 +18,8 @@ struct DevSlot {
     int32_t ade;
     int32_t julia_add;
     int32_t ipow;       // the integer power (IntPow, FoldingIntPow)
+    int32_t kind;       // FKIND_* bit of the formula (IntPow 8 apart from the other powers)
+    int32_t pad;
     double o[6];        // options
     float of[6];        // options, single precision
 };
@@ -29,11 +31,16 @@ struct DevParams {
     int32_t sm_normals, color_option, color_on_it, dfog_on_it;
     int32_t normals_on_de, first_step_random, do_julia, width;
     int32_t height, all_fp64, n_lights, shadow_soft;
+    int32_t fmask;        // FKIND_* bits of the formulas the scene uses
+    int32_t finish_slow;  // every surface in the FP64 marcher (smoothed normals, colour on iteration, ...)
     float d_de_scale, de_stop, z_step_div, mh04zsd;
     float de_stop_factor, ln_rstop, de_offset, de_offset006;
     float mcts_m, ms_de_sub, d_col_plus, col_var;
     float fovx_off, fovx_mul, pl_optic_z, mct_color_mul;
     float fhln[6];
+    float hand_margin;  // the mixed march hands over from where DE >= this x DE stop
+    int32_t hand_back;  // ... at most this many steps back
+    int32_t refill_min, blocks_per_sm;  // wavefront: idle lanes that trigger a refill; resident blocks
     float d_rstop_f, rstop3d_f, soft_radius, hs_max_len_mul;
     double d_rstop, rstop3d, zcorr, zc_mul;
     double zend, step_width, fov_y, coord_eps;
@@ -48,4 +55,5 @@ struct DevParams {
     int32_t ao_quality, ao_rays, ao_first_step_random, pad1;
     float ao_d_step_mul, ao_d_min_a_dif, ao_corr_weight, ao_max_len;
     float ao_dirs[MB3D_MAX_AO_RAYS][3];
+    double ao_rot[3][3];  // camera rows, step width long (normalise_matrix_to(sw, vgrads))
 };

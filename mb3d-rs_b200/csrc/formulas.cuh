@@ -25,7 +25,7 @@ template <> struct Num<double> {
 // single precision: 1e-40 is a denormal, flushed to zero in the bulk march;
 // the smallest normal single keeps the division defined on the z axis
 template <> struct Num<float> {
-    static __device__ __forceinline__ float sqrt_(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float sqrt_(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
     static __device__ __forceinline__ float div_(float a, float b) { return __fdividef(a, b); }
     static __device__ __forceinline__ float eps() { return 1.2e-38f; }
     static __device__ __forceinline__ float opt(const DevSlot &s, int k) { return s.of[k]; }
@@ -188,9 +188,40 @@ __device__ __forceinline__ void f_menger(R s, R cx, R cy, R cz, R v[4], bool ade
     v[2] = z;
 }
 
-template <typename R>
+// The formula set a kernel is compiled for (FKIND_* bits): the kernels are
+// built for a few sets (the scene's set must be inside the kernel's), so
+// that a kernel holds only the formulas its scenes use and its loop fits
+// the instruction cache.  FKIND_ALL holds every built-in formula.
+#define FKIND_IP8 1
+#define FKIND_IPN 2
+#define FKIND_BOX 4
+#define FKIND_MENGER 8
+#define FKIND_REAL 16
+#define FKIND_TRI 32
+#define FKIND_BULBOX 64
+#define FKIND_FIP 128
+#define FKIND_ALL 255
+
+template <typename R, int FM = FKIND_ALL>
 __device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], const R j[3], R rout) {
     const bool ade = s.ade != 0;
+    if (FM == FKIND_IP8) {
+        f_int_pow<R>(8, Num<R>::opt(s, 1), v, j);
+        return;
+    }
+    if ((FM & FKIND_IP8) && s.kind == FKIND_IP8) {
+        f_int_pow<R>(8, Num<R>::opt(s, 1), v, j);
+        return;
+    }
+    if ((FM & FKIND_BOX) && s.kind == FKIND_BOX) {
+        f_amazing_box<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), Num<R>::opt(s, 2), v, j, ade);
+        return;
+    }
+    if ((FM & FKIND_MENGER) && s.kind == FKIND_MENGER) {
+        f_menger<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), Num<R>::opt(s, 2), Num<R>::opt(s, 3), v, ade);
+        return;
+    }
+    if (FM != FKIND_ALL) return;
     switch (s.formula) {
         case MB3D_CU_F_INTPOW: f_int_pow<R>(s.ipow, Num<R>::opt(s, 1), v, j); break;
         case MB3D_CU_F_AMAZINGBOX:

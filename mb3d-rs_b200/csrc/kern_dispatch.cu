@@ -1,0 +1,72 @@
+// The launches by formula set, and the FMA throughput kernel of the
+// measurement helper.
+#include <cuda_runtime.h>
+#include "kernels.h"
+#include "formulas.cuh"
+
+namespace mb3dcu {
+
+int kernel_set(int fmask) {
+    const int sets[3] = {KSET_IP8, KSET_IP8BOX, KSET_MENGERBOX};
+    for (int s : sets)
+        if ((fmask & ~s) == 0) return s;
+    return KSET_ALL;
+}
+
+static const LaunchTable &table(int fmask) {
+    static const LaunchTable t1 = table_ip8(), t5 = table_ip8box(), t12 = table_mengerbox(), ta = table_all();
+    switch (kernel_set(fmask)) {
+        case KSET_IP8: return t1;
+        case KSET_IP8BOX: return t5;
+        case KSET_MENGERBOX: return t12;
+        default: return ta;
+    }
+}
+
+void launch_march(const DevParams &p, bool mixed, int row0, int rows, mb3d_cu_silight *out, Hand *list,
+                  unsigned int *counters, unsigned long long *gcount, int blocks, cudaStream_t s) {
+    table(p.fmask).march(p, mixed, row0, rows, out, list, counters, gcount, blocks, s);
+}
+void launch_finish(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                   mb3d_cu_silight *out, int blocks, cudaStream_t s) {
+    table(p.fmask).finish(p, mixed, row0, list, counters, slow, out, blocks, s);
+}
+void launch_post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
+                       const uint32_t *list, const unsigned int *count, PostStart *ps, int blocks, cudaStream_t s) {
+    table(p.fmask).post_start(p, mixed, row0, passes, gbuf, list, count, ps, blocks, s);
+}
+void launch_shadow_rays(const DevParams &p, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
+                        mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s) {
+    table(p.fmask).shadow_rays(p, mixed, row0, ps, count, gbuf, queue, blocks, s);
+}
+void launch_ao_rays(const DevParams &p, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,
+                    const unsigned int *count, float *min_ra, unsigned int *queue, int blocks, cudaStream_t s) {
+    table(p.fmask).ao_rays(p, mixed, ps, gbuf, count, min_ra, queue, blocks, s);
+}
+void launch_de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s) {
+    table(p.fmask).de_probe(p, pos, n, de, its, mixed, s);
+}
+
+// FMA throughput: 8 independent chains per thread (the issue peak of the
+// FP32 or FP64 pipe); the store keeps the chains alive.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fma_peak(T *out, int iters, T a, T b) {
+    T x0 = threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            x0 = x0 * a + b; x1 = x1 * a + b; x2 = x2 * a + b; x3 = x3 * a + b;
+            x4 = x4 * a + b; x5 = x5 * a + b; x6 = x6 * a + b; x7 = x7 * a + b;
+        }
+    }
+    T s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+    if (s == (T)-1.2345) out[0] = s;  // (never true: keeps the work)
+}
+
+int launch_fma_peak(bool fp64, void *out, int blocks, int iters, cudaStream_t s) {
+    if (fp64) k_fma_peak<double><<<blocks, 256, 0, s>>>((double *)out, iters, 0.999999, 1e-7);
+    else k_fma_peak<float><<<blocks, 256, 0, s>>>((float *)out, iters, 0.999999f, 1e-7f);
+    return 1;
+}
+
+}  // namespace mb3dcu

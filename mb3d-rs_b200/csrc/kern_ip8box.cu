@@ -1,0 +1,9 @@
+// The kernels built for one formula set (KSET_IP8BOX); see kernels_impl.cuh.
+#include "kernels_impl.cuh"
+
+namespace mb3dcu {
+LaunchTable table_ip8box() {
+    typedef Launch<KSET_IP8BOX> L;
+    return LaunchTable{&L::march, &L::finish, &L::post_start, &L::shadow_rays, &L::ao_rays, &L::de_probe};
+}
+}  // namespace mb3dcu

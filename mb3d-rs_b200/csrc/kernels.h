@@ -12,24 +12,73 @@ struct Hand {
     double mzz;        // depth in step widths
     double last_step;
     double last_de;
+    double dtmp;       // the DE at the surface (plain march)
+    double c[3];       // the position (plain march: accumulated as the reference does)
     uint32_t pix;      // index in the band's G-buffer
     uint32_t flags;    // HAND_*
     float step_count;  // the dynamic fog's count so far
     float rsf;         // the step factor (rsf_mul)
     int32_t seed;
-    uint32_t pad;
+    int32_t it;        // the iteration count at the surface (plain march)
 };
 #define HAND_FULL 1u     // march the whole pixel in double precision
 #define HAND_STEPPED 2u  // the hand-over came right after a step
 #define HAND_FIRST 4u    // the random first step is still to come
+#define HAND_REMARCH 8u  // march on in double precision from this state
 
-int launch_march64(const DevParams &p, int row0, int rows, mb3d_cu_silight *out, cudaStream_t s);
-int launch_march32(const DevParams &p, int row0, int rows, mb3d_cu_silight *out, Hand *list, unsigned int *counters,
-                   int sms, cudaStream_t s);
-int launch_finish64(const DevParams &p, int row0, const Hand *list, const unsigned int *counters, mb3d_cu_silight *out,
-                    int sms, cudaStream_t s);
-int launch_shadow(const DevParams &p, int row0, int rows, mb3d_cu_silight *gbuf, bool mixed, cudaStream_t s);
-int launch_deao(const DevParams &p, int row0, int rows, mb3d_cu_silight *gbuf, bool mixed, cudaStream_t s);
-int launch_de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s);
+// Where a post pass starts on a surface pixel.
+struct PostStart {
+    double sh_c[3];  // the shadow rays' start (0.1 step in front of the surface)
+    double sh_mzz;
+    double ao_c[3];  // the DE AO rays' start (on the surface)
+    float ao_ms;     // the DE stop there
+    uint32_t pix;
+    uint32_t flags;  // bit l: the surface faces away from light l
+    uint32_t pad;
+};
+
+// The formula sets the kernels are built for (FKIND_* bits, formulas.cuh):
+// the smallest one that holds the scene's formulas is used.
+#define KSET_IP8 1
+#define KSET_IP8BOX 5
+#define KSET_MENGERBOX 12
+#define KSET_ALL 255
+int kernel_set(int fmask);
+
+// the launches of one formula set's kernels (kern_*.cu)
+struct LaunchTable {
+    void (*march)(const DevParams &, bool mixed, int row0, int rows, mb3d_cu_silight *out, Hand *list,
+                  unsigned int *counters, unsigned long long *gcount, int blocks, cudaStream_t s);
+    void (*finish)(const DevParams &, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                   mb3d_cu_silight *out, int blocks, cudaStream_t s);
+    void (*post_start)(const DevParams &, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
+                       const uint32_t *list, const unsigned int *count, PostStart *ps, int blocks, cudaStream_t s);
+    void (*shadow_rays)(const DevParams &, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
+                        mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s);
+    void (*ao_rays)(const DevParams &, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,
+                    const unsigned int *count, float *min_ra, unsigned int *queue, int blocks, cudaStream_t s);
+    void (*de_probe)(const DevParams &, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s);
+};
+LaunchTable table_ip8();
+LaunchTable table_ip8box();
+LaunchTable table_mengerbox();
+LaunchTable table_all();
+
+void launch_march(const DevParams &p, bool mixed, int row0, int rows, mb3d_cu_silight *out, Hand *list,
+                  unsigned int *counters, unsigned long long *gcount, int blocks, cudaStream_t s);
+void launch_finish(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                   mb3d_cu_silight *out, int blocks, cudaStream_t s);
+void launch_surface(const DevParams &p, int npix, int passes, mb3d_cu_silight *gbuf, uint32_t *list,
+                    unsigned int *count, int blocks, cudaStream_t s);
+void launch_post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
+                       const uint32_t *list, const unsigned int *count, PostStart *ps, int blocks, cudaStream_t s);
+void launch_shadow_rays(const DevParams &p, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
+                        mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s);
+void launch_ao_rays(const DevParams &p, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,
+                    const unsigned int *count, float *min_ra, unsigned int *queue, int blocks, cudaStream_t s);
+void launch_ao_final(const DevParams &p, const PostStart *ps, const unsigned int *count, const float *min_ra,
+                     mb3d_cu_silight *gbuf, int blocks, cudaStream_t s);
+void launch_de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s);
+int launch_fma_peak(bool fp64, void *out, int blocks, int iters, cudaStream_t s);
 
 }  // namespace mb3dcu

@@ -97,7 +97,9 @@ __device__ __forceinline__ void pixel_ray(const DevParams &p, int x, int y, doub
     for (int k = 0; k < 3; k++) c[k] = p.ystart[k] + p.vgrads[0][k] * xd + p.vgrads[1][k] * yd;
 }
 
-// the iteration record (TIteration3Dext, src/iteration.rs:57-105)
+// the iteration record (TIteration3Dext, src/iteration.rs:57-105); FM is
+// the formula set the kernel is built for
+template <int FM>
 struct It64 {
     double v[4], c[3], j[3];
     double rout, rold, otrap, rstop;
@@ -133,7 +135,7 @@ struct It64 {
                 if (++guard > 64) return n;
             }
             const DevSlot &s = p.slots[n];
-            formula_iterate<double>(s, v, j, rout);
+            formula_iterate<double, FM>(s, v, j, rout);
             if (s.julia_add) {
                 v[0] += j[0];
                 v[1] += j[1];
@@ -183,17 +185,20 @@ struct It64 {
     }
 };
 
+template <int FM>
 struct M64 {
     const DevParams &p;
-    It64 it;
+    It64<FM> it;
     float ms_de_stop;
     double mzz;
     double vfov[3];
     int max_its_result;
     float s_roughness;
     int seed;
+    int add_steps;  // binary search steps (the march's; 8 for shadows, 5 for DE AO)
 
     __device__ M64(const DevParams &pp) : p(pp) {
+        add_steps = p.de_add_steps;
         it.max_it = p.max_it;
         it.rstop = p.d_rstop;
         it.calc_sit = false;
@@ -254,7 +259,7 @@ struct M64 {
 
     // RMdoBinSearch (src/calc.rs:1706-1734)
     __device__ void bin_search(double &de, double last_step_width) {
-        int itmp = p.de_add_steps;
+        int itmp = add_steps;
         double dt1 = last_step_width * -0.5;
         while (fabs(de - (double)ms_de_stop) > 0.001) {
             mzz += dt1;
@@ -275,7 +280,7 @@ struct M64 {
         float yp = (float)it.max_it - 0.99f;
         int saved = it.max_it;
         it.max_it += 1;
-        int itmp = p.de_add_steps;
+        int itmp = add_steps;
         it.calc_sit = true;
         double dt1 = 0.0, dmul = 1.0;
         bool first = true;
@@ -312,7 +317,7 @@ struct M64 {
         it.max_it = saved;
     }
 
-    __device__ static void store_normal(G &si, const double n[3]) {  // MakeWNormalsFromDVec
+    __device__ static __forceinline__ void store_normal(G &si, const double n[3]) {  // MakeWNormalsFromDVec
         double d = 32767.0 / sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2] + 1e-100);
         short o[3];
 #pragma unroll
@@ -501,7 +506,7 @@ struct M64 {
     // surface_found (src/calc.rs:2471-2511)
     __device__ void surface_found(G &si, double dtmp, double last_step) {
         bool de_limited = it.it_result < max_its_result || dtmp < (double)ms_de_stop;
-        if (p.de_add_steps != 0) {
+        if (add_steps != 0) {
             if (de_limited) bin_search(dtmp, last_step);
             else bin_search_it();
         }

@@ -91,8 +91,8 @@ int unsupported_reason(const mb3d_cu_scene &sc, std::string &why) {
         why = "no formula with iterations > 0";
         return MB3D_CU_EINVAL;
     }
-    if (sc.deao_quality >= 0 && sc.deao_dither != 0) {
-        why = "DE ambient occlusion with dithering is not on the card";
+    if (sc.deao_quality >= 0 && (sc.deao_dither != 0 || sc.deao_first_step_random != 0)) {
+        why = "DE ambient occlusion with dithering or a random first step is not on the card";
         return 1;
     }
     return 0;
@@ -289,6 +289,16 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
         d.ade = custom;
         d.julia_add = sc.julia && fs[i] == MB3D_CU_F_MENGERIFS;
         d.ipow = f_ipow(sc.slots[i]);
+        switch (fs[i]) {
+            case MB3D_CU_F_INTPOW: d.kind = d.ipow == 8 ? 1 : 2; break;
+            case MB3D_CU_F_AMAZINGBOX: d.kind = 4; break;
+            case MB3D_CU_F_MENGERIFS: d.kind = 8; break;
+            case MB3D_CU_F_REALPOWER: d.kind = 16; break;
+            case MB3D_CU_F_TRICORN: d.kind = 32; break;
+            case MB3D_CU_F_BULBOX: d.kind = 64; break;
+            default: d.kind = 128; break;
+        }
+        if (its[i] > 0) p.fmask |= d.kind;
         for (int k = 0; k < 6; k++) {
             d.o[k] = sc.slots[i].options[k];
             d.of[k] = (float)sc.slots[i].options[k];
@@ -304,6 +314,11 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     double prec = custom ? sw / (coord * eps32) : (double)p.de_offset / (coord * eps32);
     p.all_fp64 = custom ? (prec < 64.0) : (prec < 3.0);
     p.coord_eps = coord * eps32;
+    p.hand_margin = 4.0f;
+    p.hand_back = 2;
+    p.finish_slow = (p.sm_normals > 0 || !p.normals_on_de || p.color_on_it != 0) ? 1 : 0;
+    p.refill_min = 16;
+    p.blocks_per_sm = 3;
 
     // shadow lights (render::shadow_job): HSvecs = RotateVectorReverse(-sw * LN, M)
     p.n_lights = 0;
@@ -337,6 +352,10 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     p.soft_radius = sc.soft_radius;
     p.hs_max_len_mul = sc.hs_max_len_mul;
 
+    for (int i = 0; i < 3; i++) {
+        double d = sw / std::sqrt(p.vgrads[i][0] * p.vgrads[i][0] + p.vgrads[i][1] * p.vgrads[i][1] + p.vgrads[i][2] * p.vgrads[i][2]);
+        for (int k = 0; k < 3; k++) p.ao_rot[i][k] = p.vgrads[i][k] * d;
+    }
     // DE AO rays (deao::build_rays)
     p.ao_quality = sc.deao_quality;
     p.ao_max_len = sc.deao_max_len;

@@ -17,7 +17,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmb3dcu.so")
+LIB_PATH = os.environ.get("MB3D_CU_LIB") or os.path.join(HERE, "libmb3dcu.so")
 
 OK, EINVAL, ENOMEM, ENODEV, EIO, ECANCELED, ETIMEDOUT, EOVERFLOW, ENOTSUP = 0, -22, -12, -19, -5, -125, -110, -75, -95
 
@@ -66,7 +66,7 @@ class Scene(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("ms_march", ctypes.c_float), ("ms_finish", ctypes.c_float), ("ms_shadow", ctypes.c_float),
                 ("ms_deao", ctypes.c_float), ("ms_total", ctypes.c_float), ("launches", ctypes.c_uint32),
-                ("fp64_pixels", ctypes.c_uint32), ("de_evals", ctypes.c_uint64)]
+                ("fp64_pixels", ctypes.c_uint32), ("de_evals", ctypes.c_uint64), ("orbit_its", ctypes.c_uint64 * 6)]
 
 
 # the G-buffer record (mb3d_cu_silight, 20 bytes)
@@ -105,13 +105,15 @@ def lib():
         L.mb3d_cu_render.argtypes = [vp, sp, ctypes.c_int, vp, vp]
         L.mb3d_cu_de_probe.argtypes = [vp, sp, ctypes.c_int, vp, ctypes.c_uint32, vp, vp]
         L.mb3d_cu_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
+        L.mb3d_cu_set_counting.argtypes = [vp, ctypes.c_int]
+        L.mb3d_cu_fma_peak.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 
 
 EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_free", "mb3d_cu_set_stream",
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
-            "mb3d_cu_stats_get"]
+            "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak"]
 
 
 def _ptr(buf):
@@ -192,7 +194,17 @@ class Card:
     def stats(self):
         s = Stats()
         self._check(lib().mb3d_cu_stats_get(self._ctx, ctypes.byref(s)))
-        return {k: getattr(s, k) for k, _ in Stats._fields_}
+        d = {k: getattr(s, k) for k, _ in Stats._fields_}
+        d["orbit_its"] = list(s.orbit_its)
+        return d
+
+    def set_counting(self, on):
+        self._check(lib().mb3d_cu_set_counting(self._ctx, int(on)))
+
+    def fma_peak(self, fp64=False):
+        t = ctypes.c_double()
+        self._check(lib().mb3d_cu_fma_peak(self._ctx, int(fp64), ctypes.byref(t)))
+        return t.value
 
 
 def is_background(g):

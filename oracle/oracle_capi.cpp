@@ -188,6 +188,48 @@ int oracle_deao(const mb3d_cu_scene *sc, mb3d_cu_silight *gbuf, int threads) {
     return 0;
 }
 
+/* The whole CPU render of a band of rows, as the reference's CPU path does
+ * it (src/render.rs:459-799, then the post passes src/render.rs:2119-2496,
+ * src/deao.rs:109): the march, the hard shadows with the row pass (with
+ * its open-air shortcut) and the DE AO of the listed rows; threads take
+ * rows t, t+T, ... of the list.  Used as the timed CPU baseline. */
+int oracle_render_rows(const mb3d_cu_scene *sc, const int32_t *row_list, int rows, mb3d_cu_silight *out, int threads) {
+    Params p;
+    if (!make_params(*sc, p, g_err)) return -22;
+    Params ps = p, pa = p;
+    ps.de_add_steps = 8;
+    pa.de_add_steps = 5;
+    std::vector<HsLight> lights;
+    shadow_lights(*sc, ps, lights);
+    int w = p.width;
+    rows_threaded(threads, rows, [&](int r) {
+        int y = row_list[r];
+        std::vector<SiLight> row(w);
+        {
+            Marcher m(&p, 0);
+            for (int x = 0; x < w; x++) {
+                m.seed = pixel_seed(y, x);
+                row[x] = m.march_pixel(x, y);
+            }
+        }
+        int32_t seed = (int32_t)((int64_t)0x24563487u + ((int64_t)y + 1) * (int64_t)0x324594A1);
+        if (!lights.empty()) {
+            Marcher m(&ps, seed);
+            if (sc->shadow_soft)
+                m.soft_shadow_row(y, row.data(), w, lights[0], sc->soft_radius, sc->hs_max_len_mul);
+            else
+                m.hard_shadow_row(y, row.data(), w, lights, sc->hs_max_len_mul, false);
+        }
+        if (sc->deao_quality >= 0) {
+            Marcher m(&pa, seed);
+            int32_t rnd = seed;
+            deao_row(m, y, row.data(), w, sc->deao_quality, sc->deao_max_len, sc->deao_first_step_random != 0, rnd);
+        }
+        for (int x = 0; x < w; x++) to_c(row[x], out[(size_t)r * w + x]);
+    });
+    return 0;
+}
+
 /* The DE AO ray directions of a quality level (deao::build_rays,
  * src/deao.rs:75-104): their count, directions into dirs (3 floats each). */
 int oracle_ao_rays(int quality, float *dirs, int cap) {

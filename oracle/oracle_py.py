@@ -35,6 +35,7 @@ def lib():
         L.oracle_shadows.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int]
         L.oracle_deao.argtypes = [vp, vp, ctypes.c_int]
         L.oracle_ao_rays.argtypes = [ctypes.c_int, vp, ctypes.c_int]
+        L.oracle_render_rows.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -102,3 +103,11 @@ def ao_rays(quality):
     d = np.zeros((64, 3), np.float32)
     n = lib().oracle_ao_rays(quality, d.ctypes.data, 64)
     return d[:n]
+
+
+def render_rows(scene, dtype, rows, threads=0):
+    """March + shadows + DE AO of the listed rows (the reference CPU path)."""
+    rows = np.ascontiguousarray(rows, np.int32)
+    out = np.zeros(len(rows) * scene.width, dtype=dtype)
+    _chk(lib().oracle_render_rows(ctypes.addressof(scene), rows.ctypes.data, len(rows), out.ctypes.data, threads))
+    return out
