@@ -217,6 +217,29 @@ int mb3d_cu_set_counting(mb3d_cu_ctx *ctx, int on);
  * dependent-chain kernel timed with CUDA events. */
 int mb3d_cu_fma_peak(mb3d_cu_ctx *ctx, int fp64, double *tflops);
 
+/* The march without any device allocation, for callers that cannot
+ * allocate GPU memory: a renderer whose device memory belongs to another
+ * allocator (an engine's fixed pool, PyTorch's caching allocator), which may
+ * not call cudaMalloc/cudaFree behind that allocator's back, and render
+ * loops that cannot take the device-wide synchronisation cudaMalloc and
+ * cudaFree imply.  It has no counterpart in the reference (mb3d-rs's card
+ * backend allocates its wgpu buffers per render).
+ *
+ * It marches rows row0 .. row0+rows of the picture into `gbuf`, which must
+ * be device memory (rows * width records), on `stream` (a cudaStream_t, NULL
+ * for the default stream), and returns when the work is queued.  Its
+ * scratch (the lists the march hands its surfaces over in) is a static
+ * device array of this library, MB3D_CU_NOALLOC_MAX_PIXELS pixels' worth
+ * (10.5 MB, held by every GPU that loads the library until the process
+ * exits); a band larger than that is rejected (MB3D_CU_EINVAL).  The first
+ * call on a device looks up the array's device address, so make that first
+ * call before any stream capture.  Every call shares the one array: calls
+ * that overlap on the GPU (two streams, or two host threads) race and must
+ * be ordered by the caller.  Results are those of mb3d_cu_march. */
+#define MB3D_CU_NOALLOC_MAX_PIXELS 65536
+int mb3d_cu_march_noalloc(const mb3d_cu_scene *scene, int precision, uint32_t row0, uint32_t rows,
+                          mb3d_cu_silight *gbuf, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -368,6 +368,87 @@ int mb3d_cu_stats_get(const mb3d_cu_ctx *c, mb3d_cu_stats *out) {
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// the allocation-free march: its scratch is this file's static device array
+// (the march's hand-over list, the finish's slow list, the queue counters)
+
+#define NOALLOC_COUNTER_BYTES 256
+#define NOALLOC_BYTES (2 * (size_t)MB3D_CU_NOALLOC_MAX_PIXELS * sizeof(Hand) + NOALLOC_COUNTER_BYTES)
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_BYTES];
+
+struct NoallocDevice {
+    void *scratch = nullptr;  // the array's device address on this device
+    int sms = 0;
+};
+static std::mutex g_noalloc_mu;
+static NoallocDevice g_noalloc_dev[64];
+
+// once per device, with the device current: the device address of the
+// static array (its host-side name is only a stand-in) and the SM count
+static int noalloc_setup(int dev, NoallocDevice &out) {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (dev < 0 || dev >= 64) return fail(MB3D_CU_ENODEV, "device index out of range");
+    NoallocDevice &d = g_noalloc_dev[dev];
+    if (!d.scratch) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(MB3D_CU_EIO, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        int sms = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess || sms <= 0) return fail(MB3D_CU_EIO, std::string("SM count: ") + cudaGetErrorString(e));
+        d.sms = sms;
+        d.scratch = ptr;
+    }
+    out = d;
+    return 0;
+}
+
+int mb3d_cu_march_noalloc(const mb3d_cu_scene *sc, int precision, uint32_t row0, uint32_t rows,
+                          mb3d_cu_silight *gbuf, void *stream) {
+    if (!sc || !gbuf) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (precision != MB3D_CU_FP64 && precision != MB3D_CU_FP32_FP64) return fail(MB3D_CU_EINVAL, "unknown precision");
+    DevParams p;
+    std::string err;
+    int r = setup_params(*sc, p, err);
+    if (r < 0) return fail(r, err);
+    if (rows == 0 || (uint64_t)row0 + rows > (uint64_t)p.height) return fail(MB3D_CU_EINVAL, "rows outside the picture");
+    uint64_t npix = (uint64_t)rows * (uint64_t)p.width;
+    if (npix > MB3D_CU_NOALLOC_MAX_PIXELS)
+        return fail(MB3D_CU_EINVAL, "band of " + std::to_string(npix) + " pixels is over the allocation-free limit of " +
+                                        std::to_string(MB3D_CU_NOALLOC_MAX_PIXELS) + " (march it in smaller bands)");
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, gbuf) != cudaSuccess ||
+        !(a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged)) {
+        cudaGetLastError();
+        return fail(MB3D_CU_EINVAL, "gbuf must be device memory");
+    }
+    int dev = a.device;
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != dev) {
+        if (cudaSetDevice(dev) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    }
+    NoallocDevice d;
+    if (int e = noalloc_setup(dev, d)) return e;
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned char *base = (unsigned char *)d.scratch;
+    Hand *list = (Hand *)base;
+    Hand *slow = list + MB3D_CU_NOALLOC_MAX_PIXELS;
+    unsigned int *counters = (unsigned int *)(slow + MB3D_CU_NOALLOC_MAX_PIXELS);
+    // the queues and list lengths start at zero; the lists need no clearing
+    CU_TRY(cudaMemsetAsync(counters, 0, NOALLOC_COUNTER_BYTES, s));
+    bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
+    int items = ((p.width + 7) / 8) * (((int)rows + 3) / 4);
+    int blocks = d.sms * p.blocks_per_sm;
+    int need = (items + 7) / 8;
+    if (blocks > need) blocks = need > 0 ? need : 1;
+    launch_march(p, mixed, (int)row0, (int)rows, gbuf, list, counters, nullptr, blocks, s);
+    if (int e = check_launch("k_march")) return e;
+    launch_finish(p, mixed, (int)row0, list, counters, slow, gbuf, d.sms * p.blocks_per_sm, s);
+    if (int e = check_launch("k_finish")) return e;
+    return 0;
+}
+
 int mb3d_cu_set_counting(mb3d_cu_ctx *c, int on) {
     if (!c) return fail(MB3D_CU_EINVAL, "ctx is NULL");
     c->counting = on != 0;

@@ -107,13 +107,28 @@ def lib():
         L.mb3d_cu_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
         L.mb3d_cu_set_counting.argtypes = [vp, ctypes.c_int]
         L.mb3d_cu_fma_peak.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.mb3d_cu_march_noalloc.argtypes = [sp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
         _lib = L
     return _lib
 
 
 EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_free", "mb3d_cu_set_stream",
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
-            "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak"]
+            "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc"]
+
+NOALLOC_MAX_PIXELS = 65536
+
+
+def march_noalloc(scene, out, precision=FP32_FP64, row0=0, rows=None, stream=None):
+    """mb3d_cu_march_noalloc: the march into a device buffer `out` (a torch
+    CUDA tensor of rows * width * 20 bytes) with no device allocation; the
+    work is queued on `stream` (a cudaStream_t handle, None: default)."""
+    rows = scene.height - row0 if rows is None else rows
+    r = lib().mb3d_cu_march_noalloc(ctypes.byref(scene), precision, row0, rows, out.data_ptr(),
+                                    ctypes.c_void_p(stream) if stream else None)
+    if r != 0:
+        raise CardError(r, lib().mb3d_cu_last_error().decode())
+    return out
 
 
 def _ptr(buf):
