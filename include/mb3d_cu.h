@@ -203,6 +203,31 @@ int mb3d_cu_render(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, 
 int mb3d_cu_de_probe(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, const double *pos, uint32_t n,
                      double *de, int32_t *its);
 
+/* Launch settings of the wavefront kernels (picked by mb3d_cu_autotune). */
+typedef struct mb3d_cu_tune {
+    int32_t blocks_per_sm; /* resident blocks of 256 threads per SM the persistent kernels start with */
+    int32_t refill_min;    /* idle lanes of a warp that make it take new rays (the compaction interval) */
+    int32_t streams;       /* frames in flight at once in a frame batch */
+    int32_t pad;
+} mb3d_cu_tune;
+
+/* All frames of an animation (every frame the same size and formulas, its
+ * own camera; `frames` is an array of n_frames scenes) marched with their
+ * post passes into `out` (n_frames * width * height records, host or
+ * device), the launches of all frames captured in one CUDA graph and the
+ * frames spread over tune->streams streams so that one frame's tail
+ * overlaps the next frame's work.  Replaces the per-frame loop of
+ * frames::render_frames on the card (src/frames.rs:467).  tune may be NULL
+ * (the defaults). */
+int mb3d_cu_render_frames(mb3d_cu_ctx *ctx, const mb3d_cu_scene *frames, uint32_t n_frames, int precision,
+                          const mb3d_cu_tune *tune, mb3d_cu_silight *out);
+
+/* The launch settings that render a sample of the frames (every
+ * n_frames / sample-th) fastest, from a small grid of candidates, each timed
+ * with CUDA events after a warm-up. */
+int mb3d_cu_autotune(mb3d_cu_ctx *ctx, const mb3d_cu_scene *frames, uint32_t n_frames, uint32_t sample,
+                     int precision, mb3d_cu_tune *out);
+
 /* The counters of the last call on this context. */
 int mb3d_cu_stats_get(const mb3d_cu_ctx *ctx, mb3d_cu_stats *out);
 

@@ -44,6 +44,20 @@ struct mb3d_cu_ctx {
     double *d_probe = nullptr;
     size_t probe_cap = 0;
     cudaEvent_t ev[8] = {};
+    // the frame batches: extra streams, their scratch sets, the output staging
+    struct Scratch {
+        Hand *hand = nullptr, *slow = nullptr;
+        uint32_t *slist = nullptr;
+        PostStart *ps = nullptr;
+        float *minra = nullptr;
+        unsigned int *counters = nullptr;
+        size_t npix = 0, nray = 0;
+    };
+    std::vector<cudaStream_t> fstreams;
+    std::vector<cudaEvent_t> fevents;
+    std::vector<Scratch> fscratch;
+    mb3d_cu_silight *d_frames = nullptr;
+    size_t frames_cap = 0;
     mb3d_cu_stats stats = {};
     int counting = 0;
     unsigned long long *d_count = nullptr;
@@ -134,6 +148,17 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_count);
     for (auto &ev : c->ev)
         if (ev) cudaEventDestroy(ev);
+    for (auto &s : c->fscratch) {
+        cudaFree(s.hand);
+        cudaFree(s.slow);
+        cudaFree(s.slist);
+        cudaFree(s.ps);
+        cudaFree(s.minra);
+        cudaFree(s.counters);
+    }
+    for (auto s : c->fstreams) cudaStreamDestroy(s);
+    for (auto e : c->fevents) cudaEventDestroy(e);
+    cudaFree(c->d_frames);
     if (c->own) cudaStreamDestroy(c->own);
     delete c;
 }
@@ -446,6 +471,180 @@ int mb3d_cu_march_noalloc(const mb3d_cu_scene *sc, int precision, uint32_t row0,
     if (int e = check_launch("k_march")) return e;
     launch_finish(p, mixed, (int)row0, list, counters, slow, gbuf, d.sms * p.blocks_per_sm, s);
     if (int e = check_launch("k_finish")) return e;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// frame batches (one CUDA graph over all frames, frames spread over streams)
+
+// one frame's whole pipeline on stream s with scratch set sc (no events,
+// no synchronisation: what the graph captures)
+static int enqueue_frame(mb3d_cu_ctx *c, mb3d_cu_ctx::Scratch &sc, const DevParams &p, bool mixed, int passes,
+                         mb3d_cu_silight *dg, cudaStream_t s) {
+    int rows = p.height;
+    size_t npix = (size_t)rows * p.width;
+    CU_TRY(cudaMemsetAsync(sc.counters, 0, 64 * sizeof(unsigned int), s));
+    int items = ((p.width + 7) / 8) * ((rows + 3) / 4);
+    int blocks = c->sms * p.blocks_per_sm;
+    int need = (items + 7) / 8;
+    if (blocks > need) blocks = need > 0 ? need : 1;
+    launch_march(p, mixed, 0, rows, dg, sc.hand, sc.counters, nullptr, blocks, s);
+    launch_finish(p, mixed, 0, sc.hand, sc.counters, sc.slow, dg, c->sms * p.blocks_per_sm, s);
+    if (passes) {
+        unsigned int *cnt = sc.counters + 8;
+        launch_surface(p, (int)npix, passes, dg, sc.slist, cnt, c->sms * 4, s);
+        launch_post_start(p, mixed, 0, passes, dg, sc.slist, cnt, sc.ps, c->sms * 8, s);
+        if (passes & MB3D_CU_POST_SHADOW) launch_shadow_rays(p, mixed, 0, sc.ps, cnt, dg, cnt + 1, c->sms * p.blocks_per_sm, s);
+        if (passes & MB3D_CU_POST_DEAO) {
+            launch_ao_rays(p, mixed, sc.ps, dg, cnt, sc.minra, cnt + 2, c->sms * p.blocks_per_sm, s);
+            launch_ao_final(p, sc.ps, cnt, sc.minra, dg, c->sms * 8, s);
+        }
+    }
+    return check_launch("frame launches");
+}
+
+static int ensure_frame_resources(mb3d_cu_ctx *c, int streams, size_t npix, size_t nray) {
+    while ((int)c->fstreams.size() < streams) {
+        cudaStream_t s;
+        cudaEvent_t e;
+        CU_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        CU_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->fstreams.push_back(s);
+        c->fevents.push_back(e);
+        c->fscratch.push_back(mb3d_cu_ctx::Scratch());
+    }
+    if (c->fevents.size() < (size_t)streams + 1) {
+        cudaEvent_t e;
+        CU_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        c->fevents.push_back(e);
+    }
+    for (int i = 0; i < streams; i++) {
+        auto &sc = c->fscratch[i];
+        if (sc.npix < npix || sc.nray < nray) {
+            cudaFree(sc.hand); cudaFree(sc.slow); cudaFree(sc.slist); cudaFree(sc.ps); cudaFree(sc.minra); cudaFree(sc.counters);
+            sc = mb3d_cu_ctx::Scratch();
+            CU_TRY(cudaMalloc(&sc.hand, npix * sizeof(Hand)));
+            CU_TRY(cudaMalloc(&sc.slow, npix * sizeof(Hand)));
+            CU_TRY(cudaMalloc(&sc.slist, npix * sizeof(uint32_t)));
+            CU_TRY(cudaMalloc(&sc.ps, npix * sizeof(PostStart)));
+            CU_TRY(cudaMalloc(&sc.minra, (nray > 0 ? nray : 1) * sizeof(float)));
+            CU_TRY(cudaMalloc(&sc.counters, 64 * sizeof(unsigned int)));
+            sc.npix = npix;
+            sc.nray = nray;
+        }
+    }
+    return 0;
+}
+
+static int render_frames_locked(mb3d_cu_ctx *c, const mb3d_cu_scene *frames, uint32_t n, int precision,
+                                const mb3d_cu_tune *tune, mb3d_cu_silight *out, float *ms_out) {
+    if (!frames || n == 0 || !out) return fail(MB3D_CU_EINVAL, "no frames");
+    if (precision != MB3D_CU_FP64 && precision != MB3D_CU_FP32_FP64) return fail(MB3D_CU_EINVAL, "unknown precision");
+    std::vector<DevParams> P(n);
+    std::string err;
+    for (uint32_t f = 0; f < n; f++) {
+        if (frames[f].width != frames[0].width || frames[f].height != frames[0].height)
+            return fail(MB3D_CU_EINVAL, "the frames of a batch must have one size");
+        int r = setup_params(frames[f], P[f], err);
+        if (r < 0) return fail(r, "frame " + std::to_string(f) + ": " + err);
+        if (tune) {
+            if (tune->blocks_per_sm >= 1 && tune->blocks_per_sm <= 16) P[f].blocks_per_sm = tune->blocks_per_sm;
+            if (tune->refill_min >= 1 && tune->refill_min <= 32) P[f].refill_min = tune->refill_min;
+        }
+    }
+    const DevParams &p0 = P[0];
+    int streams = tune && tune->streams >= 1 ? (tune->streams > 8 ? 8 : tune->streams) : 2;
+    size_t npix = (size_t)p0.width * p0.height;
+    int passes = (frames[0].shadow_lights && p0.n_lights > 0 ? MB3D_CU_POST_SHADOW : 0) |
+                 (p0.ao_quality >= 0 && p0.ao_rays > 0 ? MB3D_CU_POST_DEAO : 0);
+    size_t nray = (passes & MB3D_CU_POST_DEAO) ? npix * (size_t)p0.ao_rays : 0;
+    if (int e = ensure_frame_resources(c, streams, npix, nray)) return e;
+    bool dev = is_device_ptr(out);
+    mb3d_cu_silight *dg = out;
+    if (!dev) {
+        if (int e = grow((void **)&c->d_frames, &c->frames_cap, (size_t)n * npix * sizeof(mb3d_cu_silight))) return e;
+        dg = c->d_frames;
+    }
+    cudaStream_t s0 = c->stream;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CU_TRY(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    cudaEvent_t fork = c->fevents[streams];
+    if (cudaEventRecord(fork, s0) != cudaSuccess) rc = fail(MB3D_CU_EIO, "capture: fork");
+    for (int i = 0; i < streams && !rc; i++)
+        if (cudaStreamWaitEvent(c->fstreams[i], fork, 0) != cudaSuccess) rc = fail(MB3D_CU_EIO, "capture: wait");
+    for (uint32_t f = 0; f < n && !rc; f++) {
+        bool mixed = precision != MB3D_CU_FP64 && !P[f].all_fp64;
+        int i = (int)(f % (uint32_t)streams);
+        rc = enqueue_frame(c, c->fscratch[i], P[f], mixed, passes, dg + (size_t)f * npix, c->fstreams[i]);
+        c->stats.launches += 2 + (passes ? 2 : 0) + ((passes & MB3D_CU_POST_SHADOW) ? 1 : 0) + ((passes & MB3D_CU_POST_DEAO) ? 2 : 0);
+    }
+    for (int i = 0; i < streams && !rc; i++) {
+        if (cudaEventRecord(c->fevents[i], c->fstreams[i]) != cudaSuccess || cudaStreamWaitEvent(s0, c->fevents[i], 0) != cudaSuccess)
+            rc = fail(MB3D_CU_EIO, "capture: join");
+    }
+    cudaError_t ee = cudaStreamEndCapture(s0, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ee != cudaSuccess) return fail(MB3D_CU_EIO, std::string("capture: ") + cudaGetErrorString(ee));
+    ee = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ee != cudaSuccess) return fail(MB3D_CU_EIO, std::string("graph instantiate: ") + cudaGetErrorString(ee));
+    cudaEventRecord(c->ev[6], s0);
+    ee = cudaGraphLaunch(exec, s0);
+    cudaEventRecord(c->ev[7], s0);
+    if (ee == cudaSuccess) ee = cudaStreamSynchronize(s0);
+    cudaGraphExecDestroy(exec);
+    if (ee != cudaSuccess) return fail(MB3D_CU_EIO, std::string("frames: ") + cudaGetErrorString(ee));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[6], c->ev[7]);
+    c->stats.ms_total = ms;
+    if (ms_out) *ms_out = ms;
+    if (!dev) CU_TRY(cudaMemcpy(out, dg, (size_t)n * npix * sizeof(mb3d_cu_silight), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int mb3d_cu_render_frames(mb3d_cu_ctx *c, const mb3d_cu_scene *frames, uint32_t n, int precision,
+                          const mb3d_cu_tune *tune, mb3d_cu_silight *out) {
+    if (!c) return fail(MB3D_CU_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    return render_frames_locked(c, frames, n, precision, tune, out, nullptr);
+}
+
+int mb3d_cu_autotune(mb3d_cu_ctx *c, const mb3d_cu_scene *frames, uint32_t n, uint32_t sample, int precision,
+                     mb3d_cu_tune *out) {
+    if (!c || !frames || n == 0 || !out) return fail(MB3D_CU_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    if (sample == 0 || sample > n) sample = n < 8 ? n : 8;
+    std::vector<mb3d_cu_scene> pick;
+    for (uint32_t k = 0; k < sample; k++) pick.push_back(frames[(size_t)k * n / sample]);
+    size_t npix = (size_t)frames[0].width * frames[0].height;
+    mb3d_cu_silight *buf = nullptr;
+    if (int e = grow((void **)&c->d_frames, &c->frames_cap, pick.size() * npix * sizeof(mb3d_cu_silight))) return e;
+    buf = c->d_frames;
+    const int blocks[3] = {2, 3, 4}, refills[3] = {8, 16, 24}, streams[3] = {1, 2, 4};
+    float best = 1e30f;
+    mb3d_cu_tune bt = {3, 16, 2, 0};
+    for (int b : blocks)
+        for (int r : refills)
+            for (int s : streams) {
+                mb3d_cu_tune t = {b, r, s, 0};
+                float ms = 0.f;
+                if (int e = render_frames_locked(c, pick.data(), (uint32_t)pick.size(), precision, &t, buf, &ms)) return e;
+                if (int e = render_frames_locked(c, pick.data(), (uint32_t)pick.size(), precision, &t, buf, &ms)) return e;
+                if (ms < best) {
+                    best = ms;
+                    bt = t;
+                }
+            }
+    *out = bt;
+    c->stats.ms_total = best;
     return 0;
 }
 

@@ -63,6 +63,11 @@ class Scene(ctypes.Structure):
     ]
 
 
+class Tune(ctypes.Structure):
+    _fields_ = [("blocks_per_sm", ctypes.c_int32), ("refill_min", ctypes.c_int32), ("streams", ctypes.c_int32),
+                ("pad", ctypes.c_int32)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("ms_march", ctypes.c_float), ("ms_finish", ctypes.c_float), ("ms_shadow", ctypes.c_float),
                 ("ms_deao", ctypes.c_float), ("ms_total", ctypes.c_float), ("launches", ctypes.c_uint32),
@@ -107,6 +112,8 @@ def lib():
         L.mb3d_cu_stats_get.argtypes = [vp, ctypes.POINTER(Stats)]
         L.mb3d_cu_set_counting.argtypes = [vp, ctypes.c_int]
         L.mb3d_cu_fma_peak.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.mb3d_cu_render_frames.argtypes = [vp, sp, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(Tune), vp]
+        L.mb3d_cu_autotune.argtypes = [vp, sp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(Tune)]
         L.mb3d_cu_march_noalloc.argtypes = [sp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
         _lib = L
     return _lib
@@ -114,7 +121,8 @@ def lib():
 
 EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_free", "mb3d_cu_set_stream",
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
-            "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc"]
+            "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
+            "mb3d_cu_autotune"]
 
 NOALLOC_MAX_PIXELS = 65536
 
@@ -212,6 +220,23 @@ class Card:
         d = {k: getattr(s, k) for k, _ in Stats._fields_}
         d["orbit_its"] = list(s.orbit_its)
         return d
+
+    def render_frames(self, frames, precision=FP32_FP64, tune=None, out=None):
+        """All frames (a list of scenes of one size) in one CUDA graph."""
+        arr = (Scene * len(frames))(*frames)
+        npix = frames[0].width * frames[0].height
+        if out is None:
+            out = np.zeros(len(frames) * npix, dtype=SILIGHT)
+        p, _ = _ptr(out)
+        self._check(lib().mb3d_cu_render_frames(self._ctx, arr, len(frames), precision,
+                                                ctypes.byref(tune) if tune is not None else None, p))
+        return out
+
+    def autotune(self, frames, sample=8, precision=FP32_FP64):
+        arr = (Scene * len(frames))(*frames)
+        t = Tune()
+        self._check(lib().mb3d_cu_autotune(self._ctx, arr, len(frames), sample, precision, ctypes.byref(t)))
+        return t
 
     def set_counting(self, on):
         self._check(lib().mb3d_cu_set_counting(self._ctx, int(on)))

@@ -149,3 +149,14 @@ def test_configs_see_the_object():
         g = O.march(sc, mb3dcu.SILIGHT)
         h = mb3dcu.hit_mask(g).mean()
         assert 0.05 < h < 0.99, h
+
+
+def test_deep_zoom_fixture_point():
+    """The deep zoom's point is on the surface and its camera outside the set."""
+    import json
+    import os
+    f = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "c3_point.json")))
+    assert f["camera_outside"]
+    sc = scenes.c3_deep_zoom(f["point"], f["view_dir"], 64, 36)
+    de, its = O.de_at(sc, [f["point"]])
+    assert de[0] < 1e-8
