@@ -129,14 +129,81 @@ typedef struct mb3d_cu_silight {
     uint16_t otrap;
 } mb3d_cu_silight;
 
-/* Monte Carlo options (the fixed-spp subset of src/mc.rs). */
+/* ---- the Monte Carlo renderer (src/mc.rs) ---- */
+
+/* A march request of the Monte Carlo tracer (McReq, src/mc.rs:402-437):
+ * kind 0 a ray of CalcRay from pos along dir (one step width long) up to
+ * len steps, zz the depth along the view, zz2 the ray's length so far,
+ * zzplus the depth per step, probe: a primary ray that first checks
+ * whether it starts inside the set; kind 1 a shadow ray of CalcHSMC
+ * (len its length, zz the depth of its start, zz2/zzplus the depth along
+ * it).  Kind 2 (through transparent objects) is not on the card. */
+typedef struct mb3d_cu_mc_req {
+    double pos[3], dir[3];
+    double zz, zz2, zzplus, len;
+    int32_t seed;
+    uint8_t kind, probe, inside, pad;
+} mb3d_cu_mc_req;
+
+/* The result of a march (McRes, src/mc.rs:439-467): kind 0 open air (or a
+ * shadow ray, with len the length left), 1 a surface, 2 a primary ray that
+ * starts inside the set. */
+typedef struct mb3d_cu_mc_res {
+    double pos[3], normals[3];
+    double zz, zz2, len;
+    float dyn_fog, ms_de_stop;
+    int32_t seed;
+    uint16_t si_grad, otrap;
+    uint8_t kind, de_limited, inside, pad;
+    uint32_t pad2;
+} mb3d_cu_mc_res;
+
+/* The light values the Monte Carlo shading reads: the part of mb3d-rs's
+ * LightVals (src/lighting.rs:605-690, LightVals::build src/lighting.rs:
+ * 978-1190) for global (directional) lights that are not visible in the
+ * picture, the surface palette, the ambient and depth colours and the fogs,
+ * as the host renderer holds them (light and ambient colours 0..255,
+ * palette colours 0..1, or squared with internal gamma 2). */
+typedef struct mb3d_cu_mc_light {
+    int32_t n_lights;     /* 0..6 (LightVals.lights, lights that are on) */
+    int32_t sqr;          /* internal gamma 2 */
+    float ln[6][3];       /* LightVal.ln: the light's direction, view space */
+    float col[6][3];      /* LightVal.col */
+    float lmax_l[6];      /* LightVal.lmax_l */
+    int32_t pow_func[6];  /* LightVal.pow_func: the specular power, a power of two */
+    float amb_col[3], amb_col2[3], depth_col[3], depth_col2[3], dyn_fog_col[3], dyn_fog_col2[3];
+    float s_depth, s_shad, s_shad_gr, s_shad_zmul, s_dyn_fog_mul;
+    float s_diff, s_spec, s_col_zmul, s_c_start, s_c_mul;
+    int32_t col_cycling, col_on_otrap, far_fog, depth_func, no_col_ipol, dfog_options;
+    int32_t col_pos[10];
+    float col_dif[10][3], col_spe[10][3], col_spe_a[10], s_c_div[10];
+} mb3d_cu_mc_light;
+
+/* What one mb3d_cu_mc_render call traces: rays ray0 .. ray0+rays-1 of every
+ * pixel of the rectangle (x0, y0, w, h) (w = 0: the whole picture).  A
+ * ray's number fixes its random numbers (seed_of, src/mc.rs:1107-1116) and
+ * its place in the Halton sequence; rays 0..3 go through the first pass's
+ * fixed quarter-pixel positions (src/mc.rs:2493-2494), later rays through
+ * a random point of the pixel.  depth is MCDepth (McSettings.depth, the
+ * ambient bounces), secant McSettings.options bit 1 (the 4-step secant
+ * search instead of the 10-step binary search). */
 typedef struct mb3d_cu_mc_opts {
-    int32_t spp;          /* rays per pixel */
-    int32_t depth;        /* diffuse bounces (mc_depth) */
-    uint64_t seed;        /* frame seed */
-    float soft_shadow_radius;
-    float pad;
+    int32_t rays, ray0;
+    int32_t depth, secant;
+    float soft_shadow_radius; /* McSettings.soft_shadow_radius */
+    int32_t x0, y0, w, h;
+    int32_t pad;
 } mb3d_cu_mc_opts;
+
+/* Per pixel outputs of mb3d_cu_mc_render (device or host buffers, w*h
+ * pixels row-major; any but radiance may be NULL). */
+typedef struct mb3d_cu_mc_out {
+    float *radiance;  /* w*h*3: the mean light of the rays (McRecord.col, linear) */
+    float *albedo;    /* w*h*3: the first surface's diffuse colour (ray ray0) */
+    float *normal;    /* w*h*3: its unit normal, world space */
+    float *depth;     /* w*h: its distance along the view in world units (0: none) */
+    uint8_t *hit;     /* w*h: a ray of the pixel met the object (McRecord.hit) */
+} mb3d_cu_mc_out;
 
 /* Per-render counters the last call measured on the device. */
 typedef struct mb3d_cu_stats {
@@ -149,6 +216,8 @@ typedef struct mb3d_cu_stats {
     uint32_t fp64_pixels; /* pixels the mixed mode marched in double precision */
     uint64_t de_evals;    /* DE evaluations of the march kernel (counting mode only, else 0) */
     uint64_t orbit_its[6];/* formula iterations per slot, all orbits (counting mode only) */
+    uint32_t mc_inside_rays; /* Monte Carlo rays that started inside the set (left dark) */
+    uint32_t mc_fp64_rays;   /* Monte Carlo rays whose single precision DE fell back to double */
 } mb3d_cu_stats;
 
 typedef struct mb3d_cu_ctx mb3d_cu_ctx;
@@ -241,6 +310,36 @@ int mb3d_cu_set_counting(mb3d_cu_ctx *ctx, int on);
  * multiply-add issue rate of this device, TFLOP/s (2 per FMA), from a
  * dependent-chain kernel timed with CUDA events. */
 int mb3d_cu_fma_peak(mb3d_cu_ctx *ctx, int fp64, double *tflops);
+
+/* The light values of MB3D's start-up light preset (Lighting::default,
+ * src/lighting.rs:290-391) with the scene's lights (on flags and angles),
+ * as LightVals::build makes them (src/lighting.rs:978-1190): for hosts
+ * that do not have their own.  Host code only. */
+int mb3d_cu_mc_light_default(const mb3d_cu_scene *scene, mb3d_cu_mc_light *out);
+
+/* Replaces gpu::mc_batch (src/gpu.rs:3022): the n marches of the Monte
+ * Carlo tracer in `reqs` (McMarch::run, src/mc.rs:488-501: kind 0 ray,
+ * src/mc.rs:665-865; kind 1 shadow ray without transparency,
+ * src/mc.rs:869-914) into `res`; `secant` as mb3d_cu_mc_opts.secant.
+ * Buffers host or device.  The scene is taken as the Monte Carlo renderer
+ * takes it (mc_scene, src/mc.rs:2842-2850; no smoothed normals). */
+int mb3d_cu_mc_batch(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, int secant,
+                     const mb3d_cu_mc_req *reqs, uint32_t n, mb3d_cu_mc_res *res);
+
+/* The Monte Carlo tracer's rays traced whole on the card: Tracer::ray
+ * (src/mc.rs:2467-2627) with CalcRay (src/mc.rs:1904-2348), the direct
+ * light of CalcPhongLight and CalcHSMC (src/mc.rs:1513-1768), the ambient
+ * and depth colours (CalcBGLight, CalcVisLights) and the ambient bounces,
+ * for scenes without reflections, transparency, cutting planes, depth of
+ * field, volumetric light, water and clouds.  Each pixel's record is the
+ * mean of its rays' light clamped to 0..400 (Tracer::pixel,
+ * src/mc.rs:2766-2834, for a fixed number of rays).  Rays that start inside
+ * the set are left dark and counted (stats.mc_inside_rays).
+ * Work items are single rays; a pixel's rays are summed in 32.32 fixed
+ * point, so the result does not depend on the order the card takes them. */
+int mb3d_cu_mc_render(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_mc_light *light,
+                      const mb3d_cu_mc_opts *opts, int precision, const mb3d_cu_mc_out *out,
+                      const volatile int *cancel);
 
 /* The march without any device allocation, for callers that cannot
  * allocate GPU memory: a renderer whose device memory belongs to another

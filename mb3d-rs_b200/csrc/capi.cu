@@ -3,6 +3,7 @@
 // capi/src/lib.rs:18-40).  There is no CPU fallback: a failure is a
 // negative status and the caller decides what to do.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstring>
 #include <cstdio>
 #include <cstdlib>
@@ -13,6 +14,7 @@
 #include "devparams.h"
 #include "kernels.h"
 #include "setup.h"
+#include "mcsetup.h"
 
 using namespace mb3dcu;
 
@@ -61,6 +63,11 @@ struct mb3d_cu_ctx {
     mb3d_cu_stats stats = {};
     int counting = 0;
     unsigned long long *d_count = nullptr;
+    // the Monte Carlo tracer: the Halton table, the pixel sums and the
+    // staging of its requests, results and per pixel outputs
+    uint2 *d_halton = nullptr;
+    unsigned char *d_mc = nullptr;
+    size_t mc_cap = 0;
     std::mutex mu;
 };
 
@@ -146,6 +153,8 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_counters);
     cudaFree(c->d_probe);
     cudaFree(c->d_count);
+    cudaFree(c->d_halton);
+    cudaFree(c->d_mc);
     for (auto &ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     for (auto &s : c->fscratch) {
@@ -674,6 +683,195 @@ int mb3d_cu_fma_peak(mb3d_cu_ctx *c, int fp64, double *tflops) {
     }
     double flops = 2.0 * 8.0 * 16.0 * (double)iters * (double)blocks * 256.0;
     *tflops = flops / ((double)best * 1e-3) / 1e12;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// the Monte Carlo tracer
+
+int mb3d_cu_mc_light_default(const mb3d_cu_scene *sc, mb3d_cu_mc_light *out) {
+    if (!sc || !out) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (sc->width <= 0 || sc->height <= 0 || !(sc->zoom > 0.0)) return fail(MB3D_CU_EINVAL, "bad picture size or zoom");
+    return mc_light_default(*sc, *out);
+}
+
+static int mc_halton(mb3d_cu_ctx *c) {
+    if (c->d_halton) return 0;
+    const std::vector<uint32_t> &t = mc_halton_table();
+    CU_TRY(cudaMalloc(&c->d_halton, t.size() * sizeof(uint32_t)));
+    CU_TRY(cudaMemcpy(c->d_halton, t.data(), t.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+static size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+int mb3d_cu_mc_batch(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, int secant, const mb3d_cu_mc_req *reqs,
+                     uint32_t n, mb3d_cu_mc_res *res) {
+    if (!c || !sc || (n && (!reqs || !res))) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (precision != MB3D_CU_FP64 && precision != MB3D_CU_FP32_FP64) return fail(MB3D_CU_EINVAL, "unknown precision");
+    if (n == 0) return 0;
+    bool dreq = is_device_ptr(reqs), dres = is_device_ptr(res);
+    if (!dreq)
+        for (uint32_t i = 0; i < n; i++) {
+            if (reqs[i].kind > 1) return fail(MB3D_CU_ENOTSUP, "march kind 2 (through transparent objects) is not on the card");
+            if (reqs[i].inside) return fail(MB3D_CU_ENOTSUP, "inside rendering is not on the card");
+        }
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    DevParams p;
+    McDev m;
+    mb3d_cu_mc_light lv;
+    std::memset(&lv, 0, sizeof(lv));
+    std::string err;
+    int r = mc_setup(*sc, lv, 0, secant, 1.0f, p, m, err);
+    if (r < 0) return fail(r, err);
+    apply_tuning(p);
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    size_t oreq = 256, ores = oreq + align256((size_t)n * sizeof(mb3d_cu_mc_req));
+    size_t need = ores + align256((size_t)n * sizeof(mb3d_cu_mc_res));
+    if (int e = grow((void **)&c->d_mc, &c->mc_cap, need)) return e;
+    unsigned long long *cnt = (unsigned long long *)c->d_mc;
+    const mb3d_cu_mc_req *dq = reqs;
+    mb3d_cu_mc_res *dr = dres ? res : (mb3d_cu_mc_res *)(c->d_mc + ores);
+    cudaStream_t s = c->stream;
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    if (!dreq) {
+        CU_TRY(cudaMemcpyAsync(c->d_mc + oreq, reqs, (size_t)n * sizeof(mb3d_cu_mc_req), cudaMemcpyHostToDevice, s));
+        dq = (const mb3d_cu_mc_req *)(c->d_mc + oreq);
+    }
+    CU_TRY(cudaMemsetAsync(c->d_mc, 0, 256, s));
+    McAcc acc;
+    std::memset(&acc, 0, sizeof(acc));
+    acc.counters = cnt;
+    bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
+    launch_mc(p, m, mixed, true, acc, dq, dr, (unsigned int *)(cnt + 8), n, c->sms * 4, s);
+    c->stats.launches = 1;
+    if (int e = check_launch("k_mc (batch)")) return e;
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    if (!dres) CU_TRY(cudaMemcpyAsync(res, dr, (size_t)n * sizeof(mb3d_cu_mc_res), cudaMemcpyDeviceToHost, s));
+    unsigned long long h[4];
+    CU_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    c->stats.ms_march = ms;
+    c->stats.de_evals = h[0];
+    c->stats.mc_fp64_rays = (uint32_t)h[3];
+    return 0;
+}
+
+int mb3d_cu_mc_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_light *lv, const mb3d_cu_mc_opts *o,
+                      int precision, const mb3d_cu_mc_out *out, const volatile int *cancel) {
+    if (!c || !sc || !lv || !o || !out || !out->radiance) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (precision != MB3D_CU_FP64 && precision != MB3D_CU_FP32_FP64) return fail(MB3D_CU_EINVAL, "unknown precision");
+    if (o->rays < 1 || o->ray0 < 0 || (int64_t)o->ray0 + o->rays > 0x7FFFFFFF) return fail(MB3D_CU_EINVAL, "bad ray numbers");
+    if (o->depth < 0 || o->depth > 64) return fail(MB3D_CU_EINVAL, "depth must be 0..64");
+    int x0 = o->x0, y0 = o->y0, w = o->w, h = o->h;
+    if (w == 0) {
+        x0 = 0;
+        y0 = 0;
+        w = sc->width;
+        h = sc->height;
+    }
+    if (w <= 0 || h <= 0 || x0 < 0 || y0 < 0 || (int64_t)x0 + w > sc->width || (int64_t)y0 + h > sc->height)
+        return fail(MB3D_CU_EINVAL, "rectangle outside the picture");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    DevParams p;
+    McDev m;
+    std::string err;
+    int r = mc_setup(*sc, *lv, o->depth, o->secant, o->soft_shadow_radius, p, m, err);
+    if (r < 0) return fail(r, err);
+    apply_tuning(p);
+    if (int e = mc_halton(c)) return e;
+    if (cancel && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    size_t npix = (size_t)w * (size_t)h;
+    uint32_t tiles_x = (uint32_t)((w + 7) / 8), tiles_y = (uint32_t)((h + 3) / 4);
+    size_t npad = (size_t)tiles_x * tiles_y * 32;
+    m.rays = o->rays;
+    m.ray0 = o->ray0;
+    m.x0 = x0;
+    m.y0 = y0;
+    m.w = w;
+    m.h = h;
+    m.npad = (uint32_t)npad;
+    m.tiles_x = tiles_x;
+    m.halton = c->d_halton;
+    // the pixel sums, hits, counters, and staging for host outputs
+    bool d_rad = is_device_ptr(out->radiance);
+    bool d_alb = out->albedo && is_device_ptr(out->albedo);
+    bool d_nrm = out->normal && is_device_ptr(out->normal);
+    bool d_dep = out->depth && is_device_ptr(out->depth);
+    bool d_hit = out->hit && is_device_ptr(out->hit);
+    size_t o_cnt = 0, o_sum = 256, o_hit = o_sum + align256(npix * 24), o_rad = o_hit + align256(npix * 4);
+    size_t o_alb = o_rad + align256(npix * 12), o_nrm = o_alb + align256(npix * 12), o_dep = o_nrm + align256(npix * 12);
+    size_t o_hb = o_dep + align256(npix * 4), need = o_hb + align256(npix);
+    if (int e = grow((void **)&c->d_mc, &c->mc_cap, need)) return e;
+    unsigned char *B = c->d_mc;
+    McAcc acc;
+    acc.counters = (unsigned long long *)(B + o_cnt);
+    acc.sum = (unsigned long long *)(B + o_sum);
+    acc.hit = (unsigned int *)(B + o_hit);
+    acc.albedo = out->albedo ? (d_alb ? out->albedo : (float *)(B + o_alb)) : nullptr;
+    acc.normal = out->normal ? (d_nrm ? out->normal : (float *)(B + o_nrm)) : nullptr;
+    acc.depth = out->depth ? (d_dep ? out->depth : (float *)(B + o_dep)) : nullptr;
+    float *rad = d_rad ? out->radiance : (float *)(B + o_rad);
+    uint8_t *hb = out->hit ? (d_hit ? out->hit : (uint8_t *)(B + o_hb)) : nullptr;
+    cudaStream_t s = c->stream;
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    CU_TRY(cudaMemsetAsync(B, 0, o_rad, s));  // counters, sums, hits
+    if (acc.albedo) CU_TRY(cudaMemsetAsync(acc.albedo, 0, npix * 12, s));
+    if (acc.normal) CU_TRY(cudaMemsetAsync(acc.normal, 0, npix * 12, s));
+    if (acc.depth) CU_TRY(cudaMemsetAsync(acc.depth, 0, npix * 4, s));
+    bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
+    // the rays in batches of at most 2^30 items, the cancel flag polled between them
+    uint32_t per = (uint32_t)std::max<size_t>(1, ((size_t)1 << 30) / npad);
+    uint32_t launches = 0;
+    for (int b0 = 0; b0 < o->rays; b0 += (int)per) {
+        int nb = std::min<int>((int)per, o->rays - b0);
+        McDev mb = m;
+        mb.ray0 = o->ray0 + b0;
+        // (the first surface of ray ray0 only)
+        McAcc ab = acc;
+        if (b0 > 0) ab.albedo = ab.normal = ab.depth = nullptr;
+        unsigned int *queue = (unsigned int *)(acc.counters + 8) + launches;
+        launch_mc(p, mb, mixed, false, ab, nullptr, nullptr, queue, (uint32_t)((size_t)nb * npad), c->sms * 4, s);
+        launches++;
+        if (int e = check_launch("k_mc")) return e;
+        if (cancel && b0 + (int)per < o->rays) {
+            CU_TRY(cudaStreamSynchronize(s));
+            if (*cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
+        }
+        if (launches >= 16 && b0 + (int)per < o->rays) {
+            // (the queue counters hold 16 launches; start them again)
+            CU_TRY(cudaMemsetAsync(acc.counters + 8, 0, 64, s));
+            launches = 0;
+        }
+    }
+    launch_mc_final(acc, (uint32_t)npix, o->rays, rad, hb, s);
+    if (int e = check_launch("k_mc_final")) return e;
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    if (!d_rad) CU_TRY(cudaMemcpyAsync(out->radiance, rad, npix * 12, cudaMemcpyDeviceToHost, s));
+    if (out->albedo && !d_alb) CU_TRY(cudaMemcpyAsync(out->albedo, acc.albedo, npix * 12, cudaMemcpyDeviceToHost, s));
+    if (out->normal && !d_nrm) CU_TRY(cudaMemcpyAsync(out->normal, acc.normal, npix * 12, cudaMemcpyDeviceToHost, s));
+    if (out->depth && !d_dep) CU_TRY(cudaMemcpyAsync(out->depth, acc.depth, npix * 4, cudaMemcpyDeviceToHost, s));
+    if (out->hit && !d_hit) CU_TRY(cudaMemcpyAsync(out->hit, hb, npix, cudaMemcpyDeviceToHost, s));
+    unsigned long long hc[4];
+    CU_TRY(cudaMemcpyAsync(hc, acc.counters, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    c->stats.ms_march = ms;
+    c->stats.launches = (uint32_t)((o->rays + per - 1) / per) + 1;
+    c->stats.de_evals = hc[0];
+    c->stats.mc_inside_rays = (uint32_t)hc[2];
+    c->stats.mc_fp64_rays = (uint32_t)hc[3];
+    if (cancel && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
     return 0;
 }
 

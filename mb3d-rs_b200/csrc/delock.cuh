@@ -120,11 +120,11 @@ __device__ __forceinline__ float smooth_of(const DevParams &p, R rout, R rold, c
 
 template <typename R, int FM, bool COUNT = false, bool FULL = false>
 __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], float ms_de_stop, DECount *cnt = nullptr,
-                                       DEstate *st = nullptr, bool calc_sit = false) {
+                                       DEstate *st = nullptr, bool calc_sit = false, int max_add = 0) {
     if (COUNT) cnt->evals++;
     DEr out;
     out.need64 = false;
-    const int max_it = p.max_it;
+    const int max_it = p.max_it + max_add;  // (max_add: doBinSearchIt's one more iteration)
     const R rstop = param_f<R>(p, p.d_rstop, p.d_rstop_f);
     if (p.is_custom_de) {
         R v[1][4], j[1][3], rout[1];

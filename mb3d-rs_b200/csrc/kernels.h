@@ -4,6 +4,7 @@
 #include <stdint.h>
 #include "../../include/mb3d_cu.h"
 #include "devparams.h"
+#include "mc.h"
 
 namespace mb3dcu {
 
@@ -80,5 +81,18 @@ void launch_ao_final(const DevParams &p, const PostStart *ps, const unsigned int
                      mb3d_cu_silight *gbuf, int blocks, cudaStream_t s);
 void launch_de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s);
 int launch_fma_peak(bool fp64, void *out, int blocks, int iters, cudaStream_t s);
+
+// the Monte Carlo kernels of one formula set (kern_mc_*.cu)
+struct McTable {
+    void (*run)(const DevParams &, const McDev &, bool mixed, bool batch, const McAcc &, const mb3d_cu_mc_req *reqs,
+                mb3d_cu_mc_res *res, unsigned int *queue, uint32_t n_items, int blocks, cudaStream_t s);
+};
+McTable mc_table_ip8();
+McTable mc_table_ip8box();
+McTable mc_table_mengerbox();
+McTable mc_table_all();
+void launch_mc(const DevParams &p, const McDev &m, bool mixed, bool batch, const McAcc &acc, const mb3d_cu_mc_req *reqs,
+               mb3d_cu_mc_res *res, unsigned int *queue, uint32_t n_items, int blocks, cudaStream_t s);
+void launch_mc_final(const McAcc &acc, uint32_t npix, int rays, float *radiance, uint8_t *hit, cudaStream_t s);
 
 }  // namespace mb3dcu

@@ -1,0 +1,30 @@
+// The Monte Carlo tracer's launch parameters, shared by the host code and
+// the kernels (mc.cuh).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/mb3d_cu.h"
+
+namespace mb3dcu {
+
+// the render constants of CalcMCT (src/mc.rs:3120-3237) the card needs
+struct McDev {
+    mb3d_cu_mc_light lv;
+    double hs_vecs[6][3];  // HSvecs: -step width x the light direction, world
+    double amb_max_l, zz_stmit_dif;
+    float fovy1d, soft_shadow_radius, hs_max_lmul, pad;
+    int32_t max_amb_depth, secant, rays, ray0;
+    int32_t x0, y0, w, h;
+    uint32_t npad, tiles_x;  // the rectangle's pixels in 8x4 tiles (npad = tiles x 32)
+    const uint2 *halton;     // halton_seq (src/mc.rs:117-128): (hrx | hry << 16, hdx | hdy << 16)
+};
+
+// per pixel accumulators of a render
+struct McAcc {
+    unsigned long long *sum;  // 3 per pixel, light in 32.32 fixed point
+    unsigned int *hit;        // 1 per pixel
+    float *albedo, *normal, *depth;  // the first surface of ray ray0 (device, may be null)
+    unsigned long long *counters;    // [0] DE evaluations, [1] centre iterations, [2] inside starts, [3] FP64 fallbacks
+};
+
+}  // namespace mb3dcu

@@ -71,7 +71,71 @@ class Tune(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("ms_march", ctypes.c_float), ("ms_finish", ctypes.c_float), ("ms_shadow", ctypes.c_float),
                 ("ms_deao", ctypes.c_float), ("ms_total", ctypes.c_float), ("launches", ctypes.c_uint32),
-                ("fp64_pixels", ctypes.c_uint32), ("de_evals", ctypes.c_uint64), ("orbit_its", ctypes.c_uint64 * 6)]
+                ("fp64_pixels", ctypes.c_uint32), ("de_evals", ctypes.c_uint64), ("orbit_its", ctypes.c_uint64 * 6),
+                ("mc_inside_rays", ctypes.c_uint32), ("mc_fp64_rays", ctypes.c_uint32)]
+
+
+# ---- the Monte Carlo tracer (src/mc.rs) ----
+class McReq(ctypes.Structure):
+    """McReq (src/mc.rs:402-437): a march of the Monte Carlo tracer."""
+    _fields_ = [("pos", ctypes.c_double * 3), ("dir", ctypes.c_double * 3), ("zz", ctypes.c_double),
+                ("zz2", ctypes.c_double), ("zzplus", ctypes.c_double), ("len", ctypes.c_double),
+                ("seed", ctypes.c_int32), ("kind", ctypes.c_uint8), ("probe", ctypes.c_uint8),
+                ("inside", ctypes.c_uint8), ("pad", ctypes.c_uint8)]
+
+
+class McRes(ctypes.Structure):
+    """McRes (src/mc.rs:439-467): the result of a march."""
+    _fields_ = [("pos", ctypes.c_double * 3), ("normals", ctypes.c_double * 3), ("zz", ctypes.c_double),
+                ("zz2", ctypes.c_double), ("len", ctypes.c_double), ("dyn_fog", ctypes.c_float),
+                ("ms_de_stop", ctypes.c_float), ("seed", ctypes.c_int32), ("si_grad", ctypes.c_uint16),
+                ("otrap", ctypes.c_uint16), ("kind", ctypes.c_uint8), ("de_limited", ctypes.c_uint8),
+                ("inside", ctypes.c_uint8), ("pad", ctypes.c_uint8), ("pad2", ctypes.c_uint32)]
+
+
+class McLight(ctypes.Structure):
+    """The LightVals part the Monte Carlo shading reads (mb3d_cu_mc_light)."""
+    _fields_ = [("n_lights", ctypes.c_int32), ("sqr", ctypes.c_int32),
+                ("ln", (ctypes.c_float * 3) * 6), ("col", (ctypes.c_float * 3) * 6),
+                ("lmax_l", ctypes.c_float * 6), ("pow_func", ctypes.c_int32 * 6),
+                ("amb_col", ctypes.c_float * 3), ("amb_col2", ctypes.c_float * 3),
+                ("depth_col", ctypes.c_float * 3), ("depth_col2", ctypes.c_float * 3),
+                ("dyn_fog_col", ctypes.c_float * 3), ("dyn_fog_col2", ctypes.c_float * 3),
+                ("s_depth", ctypes.c_float), ("s_shad", ctypes.c_float), ("s_shad_gr", ctypes.c_float),
+                ("s_shad_zmul", ctypes.c_float), ("s_dyn_fog_mul", ctypes.c_float),
+                ("s_diff", ctypes.c_float), ("s_spec", ctypes.c_float), ("s_col_zmul", ctypes.c_float),
+                ("s_c_start", ctypes.c_float), ("s_c_mul", ctypes.c_float),
+                ("col_cycling", ctypes.c_int32), ("col_on_otrap", ctypes.c_int32), ("far_fog", ctypes.c_int32),
+                ("depth_func", ctypes.c_int32), ("no_col_ipol", ctypes.c_int32), ("dfog_options", ctypes.c_int32),
+                ("col_pos", ctypes.c_int32 * 10), ("col_dif", (ctypes.c_float * 3) * 10),
+                ("col_spe", (ctypes.c_float * 3) * 10), ("col_spe_a", ctypes.c_float * 10),
+                ("s_c_div", ctypes.c_float * 10)]
+
+
+class McOpts(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_int32), ("ray0", ctypes.c_int32), ("depth", ctypes.c_int32),
+                ("secant", ctypes.c_int32), ("soft_shadow_radius", ctypes.c_float), ("x0", ctypes.c_int32),
+                ("y0", ctypes.c_int32), ("w", ctypes.c_int32), ("h", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class McOut(ctypes.Structure):
+    _fields_ = [("radiance", ctypes.c_void_p), ("albedo", ctypes.c_void_p), ("normal", ctypes.c_void_p),
+                ("depth", ctypes.c_void_p), ("hit", ctypes.c_void_p)]
+
+
+def mc_opts(rays, depth=3, ray0=0, secant=True, soft_shadow_radius=1.0, rect=None):
+    """McSettings' defaults (src/scene.rs:607-624): depth 3, options 2 (secant)."""
+    x0, y0, w, h = rect if rect is not None else (0, 0, 0, 0)
+    return McOpts(rays, ray0, depth, int(bool(secant)), soft_shadow_radius, x0, y0, w, h, 0)
+
+
+def mc_light_default(scene):
+    """LightVals of MB3D's start-up lighting with the scene's lights."""
+    lv = McLight()
+    r = lib().mb3d_cu_mc_light_default(ctypes.byref(scene), ctypes.byref(lv))
+    if r != 0:
+        raise CardError(r, lib().mb3d_cu_last_error().decode())
+    return lv
 
 
 # the G-buffer record (mb3d_cu_silight, 20 bytes)
@@ -115,6 +179,10 @@ def lib():
         L.mb3d_cu_render_frames.argtypes = [vp, sp, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(Tune), vp]
         L.mb3d_cu_autotune.argtypes = [vp, sp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(Tune)]
         L.mb3d_cu_march_noalloc.argtypes = [sp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
+        L.mb3d_cu_mc_light_default.argtypes = [sp, ctypes.POINTER(McLight)]
+        L.mb3d_cu_mc_batch.argtypes = [vp, sp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_uint32, vp]
+        L.mb3d_cu_mc_render.argtypes = [vp, sp, ctypes.POINTER(McLight), ctypes.POINTER(McOpts), ctypes.c_int,
+                                        ctypes.POINTER(McOut), vp]
         _lib = L
     return _lib
 
@@ -122,7 +190,7 @@ def lib():
 EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_free", "mb3d_cu_set_stream",
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
-            "mb3d_cu_autotune"]
+            "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render"]
 
 NOALLOC_MAX_PIXELS = 65536
 
@@ -237,6 +305,33 @@ class Card:
         t = Tune()
         self._check(lib().mb3d_cu_autotune(self._ctx, arr, len(frames), sample, precision, ctypes.byref(t)))
         return t
+
+    def mc_batch(self, scene, reqs, precision=FP64, secant=True):
+        """gpu::mc_batch: the marches `reqs` (a ctypes array of McReq)."""
+        n = len(reqs)
+        res = (McRes * n)()
+        self._check(lib().mb3d_cu_mc_batch(self._ctx, ctypes.byref(scene), precision, int(bool(secant)),
+                                           ctypes.addressof(reqs), n, ctypes.addressof(res)))
+        return res
+
+    def mc_render(self, scene, opts, light=None, precision=FP32_FP64, out=None, cancel=None):
+        """The Monte Carlo rays of opts on the card: a dict of radiance, albedo,
+        normal (h, w, 3), depth (h, w) and hit (h, w); `out` may give torch CUDA
+        tensors (float32; hit uint8) for any of them, used in place."""
+        light = mc_light_default(scene) if light is None else light
+        w, h = (opts.w, opts.h) if opts.w else (scene.width, scene.height)
+        res = dict(out or {})
+        for k, shape, dt in (("radiance", (h, w, 3), np.float32), ("albedo", (h, w, 3), np.float32),
+                             ("normal", (h, w, 3), np.float32), ("depth", (h, w), np.float32),
+                             ("hit", (h, w), np.uint8)):
+            if k not in res:
+                res[k] = np.zeros(shape, dt)
+        ptrs = McOut(*[_ptr(res[k])[0] if res[k] is not None else None
+                       for k in ("radiance", "albedo", "normal", "depth", "hit")])
+        cp = ctypes.cast(ctypes.byref(cancel), ctypes.c_void_p) if cancel is not None else None
+        self._check(lib().mb3d_cu_mc_render(self._ctx, ctypes.byref(scene), ctypes.byref(light), ctypes.byref(opts),
+                                            precision, ctypes.byref(ptrs), cp))
+        return res
 
     def set_counting(self, on):
         self._check(lib().mb3d_cu_set_counting(self._ctx, int(on)))

@@ -17,36 +17,6 @@ static inline double to_radians(double d) { return d * (PI / 180.0); }
 
 // ---------------------------------------------------------------------------
 // math helpers (src/math.rs:28-134, 218-246)
-static inline void add_weight(double a[3], const double b[3], double w) {
-    a[0] += b[0] * w;
-    a[1] += b[1] * w;
-    a[2] += b[2] * w;
-}
-static inline double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
-static inline void rotate_vector_reverse(const double v[3], const Mat3 m, double out[3]) {
-    double r0 = v[0] * m[0][0] + v[1] * m[1][0] + v[2] * m[2][0];
-    double r1 = v[0] * m[0][1] + v[1] * m[1][1] + v[2] * m[2][1];
-    double r2 = v[0] * m[0][2] + v[1] * m[1][2] + v[2] * m[2][2];
-    out[0] = r0;
-    out[1] = r1;
-    out[2] = r2;
-}
-static void normalise_matrix_to(double n, const Mat3 m, Mat3 r) {
-    for (int i = 0; i < 3; i++) {
-        double d = n / std::sqrt(dot3(m[i], m[i]));
-        for (int j = 0; j < 3; j++) r[i][j] = m[i][j] * d;
-    }
-}
-// BuildViewVectorDFOV (src/math.rs:127-134)
-static void build_view_vector_dfov(double xa, double ya, double out[3]) {
-    double sx = std::sin(xa), cx = std::cos(xa);
-    double sy = std::sin(ya), cy = std::cos(ya);
-    double v[3] = {-sy, sx, cx * cy};
-    double n = 1.0 / std::sqrt(dot3(v, v));
-    out[0] = v[0] * n;
-    out[1] = v[1] * n;
-    out[2] = v[2] * n;
-}
 // create_xy_vecs_from_normals (src/math.rs:218-233)
 static void create_xy_vecs_from_normals(const double n[3], double vx[3], double vy[3]) {
     double d = n[1] * n[1] + n[0] * n[0];

@@ -80,6 +80,37 @@ inline int16_t sat_i16(double x) {
 }
 inline int32_t wrap_lcg(int32_t s, uint32_t a, uint32_t c) { return (int32_t)((uint32_t)s * a + c); }
 
+// ---- math helpers (src/math.rs:28-134) ----
+inline void add_weight(double a[3], const double b[3], double w) {
+    a[0] += b[0] * w;
+    a[1] += b[1] * w;
+    a[2] += b[2] * w;
+}
+inline double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline void rotate_vector_reverse(const double v[3], const Mat3 m, double out[3]) {
+    double r0 = v[0] * m[0][0] + v[1] * m[1][0] + v[2] * m[2][0];
+    double r1 = v[0] * m[0][1] + v[1] * m[1][1] + v[2] * m[2][1];
+    double r2 = v[0] * m[0][2] + v[1] * m[1][2] + v[2] * m[2][2];
+    out[0] = r0;
+    out[1] = r1;
+    out[2] = r2;
+}
+inline void normalise_matrix_to(double n, const Mat3 m, Mat3 r) {
+    for (int i = 0; i < 3; i++) {
+        double d = n / std::sqrt(dot3(m[i], m[i]));
+        for (int j = 0; j < 3; j++) r[i][j] = m[i][j] * d;
+    }
+}
+// BuildViewVectorDFOV (src/math.rs:127-134)
+inline void build_view_vector_dfov(double xa, double ya, double out[3]) {
+    double sx = std::sin(xa), cx = std::cos(xa);
+    double sy = std::sin(ya), cy = std::cos(ya);
+    double v[3] = {-sy, sx, cx * cy};
+    double n = 1.0 / std::sqrt(dot3(v, v));
+    out[0] = v[0] * n;
+    out[1] = v[1] * n;
+    out[2] = v[2] * n;
+}
 // ---- formulas (src/formulas.rs) ----
 enum FormulaKind { F_INTPOW = 0, F_REALPOWER = 1, F_TRICORN = 3, F_AMAZINGBOX = 4, F_BULBOX = 5, F_FOLDINGINTPOW = 6, F_MENGER = 100 };
 

@@ -36,6 +36,12 @@ def lib():
         L.oracle_deao.argtypes = [vp, vp, ctypes.c_int]
         L.oracle_ao_rays.argtypes = [ctypes.c_int, vp, ctypes.c_int]
         L.oracle_render_rows.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int]
+        L.oracle_mc_render.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int]
+        L.oracle_mc_batch.argtypes = [vp, ctypes.c_int, vp, ctypes.c_uint32, vp, ctypes.c_int]
+        L.oracle_mc_halton.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
+        L.oracle_mc_halton.restype = None
+        L.oracle_mc_seed_of.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
+        L.oracle_mc_seed_of.restype = ctypes.c_int32
         _lib = L
     return _lib
 
@@ -111,3 +117,39 @@ def render_rows(scene, dtype, rows, threads=0):
     out = np.zeros(len(rows) * scene.width, dtype=dtype)
     _chk(lib().oracle_render_rows(ctypes.addressof(scene), rows.ctypes.data, len(rows), out.ctypes.data, threads))
     return out
+
+
+def mc_render(scene, light, opts, threads=0):
+    """The Monte Carlo oracle (oracle/mc.cpp): radiance, albedo, normal
+    (h, w, 3), depth, hit (h, w) and the count of rays that started inside."""
+    w, h = (opts.w, opts.h) if opts.w else (scene.width, scene.height)
+    rad = np.zeros((h, w, 3))
+    alb = np.zeros((h, w, 3))
+    nrm = np.zeros((h, w, 3))
+    dep = np.zeros((h, w))
+    hit = np.zeros((h, w), np.uint8)
+    inside = ctypes.c_uint64()
+    _chk(lib().oracle_mc_render(ctypes.addressof(scene), ctypes.addressof(light), ctypes.addressof(opts),
+                                rad.ctypes.data, alb.ctypes.data, nrm.ctypes.data, dep.ctypes.data, hit.ctypes.data,
+                                ctypes.byref(inside), threads))
+    return dict(radiance=rad, albedo=alb, normal=nrm, depth=dep, hit=hit, inside=inside.value)
+
+
+def mc_batch(scene, reqs, secant=True, threads=0):
+    """McMarch::run on the requests (a ctypes array of mb3dcu.McReq)."""
+    import mb3dcu
+    res = (mb3dcu.McRes * len(reqs))()
+    _chk(lib().oracle_mc_batch(ctypes.addressof(scene), int(bool(secant)), ctypes.addressof(reqs), len(reqs),
+                               ctypes.addressof(res), threads))
+    return res
+
+
+def mc_halton(i, x1, y):
+    rec = (ctypes.c_uint16 * 4)()
+    sh = (ctypes.c_float * 2)()
+    lib().oracle_mc_halton(i, x1, y, rec, sh)
+    return list(rec), list(sh)
+
+
+def mc_seed_of(x, y, b):
+    return lib().oracle_mc_seed_of(x, y, b)

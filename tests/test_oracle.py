@@ -160,3 +160,64 @@ def test_deep_zoom_fixture_point():
     sc = scenes.c3_deep_zoom(f["point"], f["view_dir"], 64, 36)
     de, its = O.de_at(sc, [f["point"]])
     assert de[0] < 1e-8
+
+
+def _seed_of(x, y, b):
+    """seed_of (src/mc.rs:1107-1116) in Python."""
+    def mix(h):
+        h &= 0xFFFFFFFF
+        h ^= h >> 16
+        h = (h * 0x7FEB352D) & 0xFFFFFFFF
+        h ^= h >> 15
+        h = (h * 0x846CA68B) & 0xFFFFFFFF
+        return h ^ (h >> 16)
+    v = mix(((x * 0x9E3779B1) & 0xFFFFFFFF) ^ mix(((y * 0x85EBCA77) & 0xFFFFFFFF) ^ mix(b + 0x165667B1)))
+    return v - (1 << 32) if v >= 1 << 31 else v
+
+
+def test_mc_seed_and_halton():
+    """seed_of and halton_seq (src/mc.rs:103-128, 1107-1116) as Python
+    restates them; the first Halton numbers of bases 2 and 3 are the van der
+    Corput fractions 1/2, 1/4, 3/4 and 1/3, 2/3, 1/9."""
+    for x, y, b in ((1, 0, 0), (1920, 1079, 3), (17, 5, 1023), (-3, 7, 2 ** 31)):
+        assert O.mc_seed_of(x, y, b & 0xFFFFFFFF) == _seed_of(x, y, b), (x, y, b)
+    for i, (f2, f3) in enumerate(((0.5, 1 / 3), (0.25, 2 / 3), (0.75, 1 / 9))):
+        rec, _ = O.mc_halton(i, 1, 0)
+        assert rec[0] == round(f2 * 65535) and rec[1] == round(f3 * 65535)
+    _, sh = O.mc_halton(0, 5, 9)
+    assert all(0.0 <= s < 1.0 for s in sh)
+
+
+def test_mc_light_values_of_the_startup_lighting():
+    """LightVals::build (src/lighting.rs:978-1190) of Lighting::default
+    (src/lighting.rs:290-391): light 0 colour $A0E8FF as r, g, b; specular
+    function 53 & 7 -> power 2 << 5; diffuse 120 x 0.02; specular 50 x 0.02;
+    depth fog 27 x 0.8e-6; the palette at 0, 10922, 21844, 32200 + 84 k."""
+    sc = scenes.c2_hybrid()
+    lv = mb3dcu.mc_light_default(sc)
+    assert lv.n_lights == 1
+    assert list(lv.col[0]) == [255.0, 232.0, 160.0]
+    assert lv.pow_func[0] == 64
+    assert abs(lv.s_diff - 2.4) < 1e-6 and abs(lv.s_spec - 1.0) < 1e-7
+    assert abs(lv.s_depth - 2.16e-5) < 1e-11
+    assert list(lv.col_pos) == [0, 10922, 21844] + [32200 + 84 * k for k in range(7)]
+    assert abs(lv.col_dif[0][0] - 0xE1 / 255) < 1e-7  # 5873889 = $59A0E1: r = $E1
+    assert abs(lv.lmax_l[0] - 800.0 * (255 + 232 + 160 + 128)) < 1e-3
+    ln = np.array(list(lv.ln[0]))
+    assert abs(np.linalg.norm(ln) - 1.0) < 1e-6
+
+
+def test_mc_oracle_is_deterministic_and_sane():
+    """The Monte Carlo oracle: thread-independent, lights the object, every
+    pixel's light finite and within the clamp."""
+    sc = scenes.scaled(scenes.c2_hybrid(), 64, 36)
+    lv = mb3dcu.mc_light_default(sc)
+    o = mb3dcu.mc_opts(4, depth=3)
+    a = O.mc_render(sc, lv, o, threads=1)
+    b = O.mc_render(sc, lv, o, threads=4)
+    assert a["radiance"].tobytes() == b["radiance"].tobytes()
+    assert 0.05 < a["hit"].mean() < 0.99
+    assert np.isfinite(a["radiance"]).all() and a["radiance"].min() >= 0.0 and a["radiance"].max() <= 400.0
+    # the first surface's normal is a unit vector where there is one
+    n = np.linalg.norm(a["normal"], axis=2)
+    assert np.all(np.abs(n[a["depth"] > 0] - 1.0) < 1e-9)
