@@ -341,6 +341,55 @@ int mb3d_cu_mc_render(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_c
                       const mb3d_cu_mc_opts *opts, int precision, const mb3d_cu_mc_out *out,
                       const volatile int *cancel);
 
+/* ---- the learned denoiser of the Monte Carlo pictures ----
+ * A 5-level U-Net of 3x3 convolutions (32/48/64/80/96 channels) that
+ * takes the noisy colour and the albedo, normal and depth guides of a
+ * picture and returns the denoised colour: the card's counterpart of the
+ * Open Image Denoise call of mb3d-rs (oidn::Input, src/oidn.rs:170-180;
+ * denoise_mc, src/oidn.rs:262-277), which the reference does not train.
+ * Its weights are BF16 (FP32 master copies), its convolutions run on the
+ * tensor cores with FP32 accumulation, and it is trained on the card on
+ * pictures the path tracer renders (mb3d_cu_dn_train_step).  Inputs are
+ * float arrays of n pictures of h x w pixels (colour, albedo, normal: 3
+ * floats per pixel; depth: 1), host or device; albedo, normal and depth may
+ * be NULL (zero guides).  depth_scale scales the depth to about 0..1. */
+typedef struct mb3d_cu_dn mb3d_cu_dn;
+
+/* The number of parameters (FP32 master weights and biases). */
+size_t mb3d_cu_dn_param_count(void);
+
+/* A denoiser on the context's device, its weights He-initialised from seed. */
+int mb3d_cu_dn_create(mb3d_cu_ctx *ctx, uint64_t seed, mb3d_cu_dn **out);
+void mb3d_cu_dn_free(mb3d_cu_dn *dn);
+
+/* The FP32 parameters (mb3d_cu_dn_param_count floats, host or device). */
+int mb3d_cu_dn_get_params(mb3d_cu_dn *dn, float *params);
+int mb3d_cu_dn_set_params(mb3d_cu_dn *dn, const float *params);
+
+/* The denoised colour of the pictures into out (n * h * w * 3 floats). */
+int mb3d_cu_dn_denoise(mb3d_cu_dn *dn, int n, int h, int w, const float *radiance, const float *albedo,
+                       const float *normal, const float *depth, float depth_scale, float *out);
+
+/* One Adam step (learning rate lr) on the L1 loss in log space against
+ * target (n * h * w * 3 floats); *loss (may be NULL) receives the loss
+ * before the step. */
+int mb3d_cu_dn_train_step(mb3d_cu_dn *dn, int n, int h, int w, const float *radiance, const float *albedo,
+                          const float *normal, const float *depth, float depth_scale, const float *target, float lr,
+                          float *loss);
+
+/* The loss and its gradient with respect to every parameter (grad:
+ * mb3d_cu_dn_param_count floats, host or device), without a step. */
+int mb3d_cu_dn_gradient(mb3d_cu_dn *dn, int n, int h, int w, const float *radiance, const float *albedo,
+                        const float *normal, const float *depth, float depth_scale, const float *target, float *loss,
+                        float *grad);
+
+/* Test hook: one 3x3 convolution (NHWC, cin and cout multiples of 16,
+ * cout <= 96, weights [cout][3][3][cin]) and its gradients for the output
+ * gradient dy, through the same kernels, on float host arrays (BF16
+ * inside). */
+int mb3d_cu_dn_conv_check(mb3d_cu_ctx *ctx, int n, int h, int w, int cin, int cout, const float *x, const float *wt,
+                          const float *b, const float *dy, float *y, float *dx, float *dw, float *db);
+
 /* The march without any device allocation, for callers that cannot
  * allocate GPU memory: a renderer whose device memory belongs to another
  * allocator (an engine's fixed pool, PyTorch's caching allocator), which may

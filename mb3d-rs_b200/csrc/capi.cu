@@ -105,6 +105,14 @@ static int check_launch(const char *what) {
     return 0;
 }
 
+// the context's pieces the denoiser (dn.cu) uses
+namespace mb3dcu {
+int dn_fail(int code, const std::string &msg) { return fail(code, msg); }
+bool dn_is_device_ptr(const void *p) { return is_device_ptr(p); }
+cudaStream_t dn_stream(mb3d_cu_ctx *c) { return c->stream; }
+int dn_device(mb3d_cu_ctx *c) { return c->device; }
+}  // namespace mb3dcu
+
 extern "C" {
 
 const char *mb3d_cu_version(void) { return "mb3d_cu 0.1.0 (sm_100a)"; }
@@ -744,7 +752,7 @@ int mb3d_cu_mc_batch(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, int
     std::memset(&acc, 0, sizeof(acc));
     acc.counters = cnt;
     bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
-    launch_mc(p, m, mixed, true, acc, dq, dr, (unsigned int *)(cnt + 8), n, c->sms * 4, s);
+    launch_mc(p, m, mixed, true, acc, dq, dr, (unsigned int *)(cnt + 8), n, c->sms, s);
     c->stats.launches = 1;
     if (int e = check_launch("k_mc (batch)")) return e;
     CU_TRY(cudaEventRecord(c->ev[1], s));
@@ -838,7 +846,7 @@ int mb3d_cu_mc_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_
         McAcc ab = acc;
         if (b0 > 0) ab.albedo = ab.normal = ab.depth = nullptr;
         unsigned int *queue = (unsigned int *)(acc.counters + 8) + launches;
-        launch_mc(p, mb, mixed, false, ab, nullptr, nullptr, queue, (uint32_t)((size_t)nb * npad), c->sms * 4, s);
+        launch_mc(p, mb, mixed, false, ab, nullptr, nullptr, queue, (uint32_t)((size_t)nb * npad), c->sms, s);
         launches++;
         if (int e = check_launch("k_mc")) return e;
         if (cancel && b0 + (int)per < o->rays) {

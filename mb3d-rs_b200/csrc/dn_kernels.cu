@@ -1,0 +1,550 @@
+// The denoiser's kernels: 3x3 convolutions as implicit GEMMs on the BF16
+// tensor cores with FP32 accumulation (forward, and backward to the input
+// through the flipped weights), the weight and bias gradients, and the
+// elementwise pieces of the U-Net (pooling, upsampling, ReLU masks, input
+// packing, the loss, Adam).
+//
+// Activations are NHWC bf16 tensors whose channel counts are multiples of
+// 16; a convolution reads `cin` channels at offset `in_off` of a tensor of
+// `in_c` channels and writes `cout` channels at `out_off` of one of `out_c`
+// channels, so the decoder's concatenations are slots of one tensor.
+// Weights are [cout][tap][cin] (tap = ky * 3 + kx), bf16.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "dn.h"
+
+namespace mb3dcu {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid) {
+    // zero-fills the 16 bytes when !valid (src-size 0)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void ldsm_x4(uint32_t r[4], const void *p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x4_t(uint32_t r[4], const void *p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// ---------------------------------------------------------------------------
+// 3x3 convolution, stride 1, zero padding 1, as an implicit GEMM:
+//   M = pixels (128 per block), N = output channels (BN per block, grid.y
+//   tiles), K = 9 taps x cin in chunks of 16 (4-stage cp.async pipeline).
+// Each of the 4 warps computes 32 pixels x BN channels with m16n8k16 MMAs
+// from ldmatrix fragments; shared rows are 48 bytes apart (conflict-free).
+constexpr int CV_BM = 128, CV_STAGES = 4, CV_LD = 24;  // row stride in bf16 (48 B)
+
+template <int BN>
+__global__ void __launch_bounds__(128) k_conv3x3(ConvArgs a) {
+    __shared__ __align__(128) __nv_bfloat16 sa[CV_STAGES][CV_BM * CV_LD];
+    __shared__ __align__(128) __nv_bfloat16 sb[CV_STAGES][BN * CV_LD];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * CV_BM, n0 = blockIdx.y * BN;
+    const int hw = a.h * a.w;
+    const int kchunks = 9 * (a.cin >> 4);
+    const int cin16 = a.cin >> 4;
+    // this thread's two A rows (pixel, half) and their coordinates
+    int arow[2], ahalf[2], an[2], ay[2], ax[2];
+    bool avalid[2];
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        int e = tid + i * 128;  // 256 16-byte pieces: 128 rows x 2 halves
+        arow[i] = e >> 1;
+        ahalf[i] = e & 1;
+        int m = m0 + arow[i];
+        avalid[i] = m < a.m;
+        int mm = avalid[i] ? m : 0;
+        an[i] = mm / hw;
+        int r = mm - an[i] * hw;
+        ay[i] = r / a.w;
+        ax[i] = r - ay[i] * a.w;
+    }
+    auto load_stage = [&](int kc, int buf) {
+        int tap = kc / cin16, ci0 = (kc - tap * cin16) << 4;
+        int dy = tap / 3 - 1, dx = tap - (tap / 3) * 3 - 1;
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            int y = ay[i] + dy, x = ax[i] + dx;
+            bool v = avalid[i] && (unsigned)y < (unsigned)a.h && (unsigned)x < (unsigned)a.w;
+            const __nv_bfloat16 *src = v ? a.in + ((size_t)(an[i] * a.h + y) * a.w + x) * a.in_c + a.in_off + ci0 + ahalf[i] * 8
+                                         : a.in;
+            cp_async16(&sa[buf][arow[i] * CV_LD + ahalf[i] * 8], src, v);
+        }
+        for (int e = tid; e < BN * 2; e += 128) {
+            int row = e >> 1, half = e & 1;
+            int n = n0 + row;
+            bool v = n < a.cout;
+            const __nv_bfloat16 *src = v ? a.wt + ((size_t)n * 9 + tap) * a.cin + ci0 + half * 8 : a.wt;
+            cp_async16(&sb[buf][row * CV_LD + half * 8], src, v);
+        }
+    };
+    constexpr int NT = BN / 8;
+    float acc[2][NT][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < NT; j++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) acc[i][j][k] = 0.0f;
+#pragma unroll
+    for (int s = 0; s < CV_STAGES - 1; s++) {
+        if (s < kchunks) load_stage(s, s);
+        cp_async_commit();
+    }
+    for (int kc = 0; kc < kchunks; kc++) {
+        cp_async_wait<CV_STAGES - 2>();
+        __syncthreads();
+        int nxt = kc + CV_STAGES - 1;
+        if (nxt < kchunks) load_stage(nxt, nxt % CV_STAGES);
+        cp_async_commit();
+        const int buf = kc % CV_STAGES;
+        uint32_t af[2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; mt++) {
+            int r = warp * 32 + mt * 16 + (lane & 15);
+            ldsm_x4(af[mt], &sa[buf][r * CV_LD + (lane >> 4) * 8]);
+        }
+#pragma unroll
+        for (int j = 0; j < NT / 2; j++) {
+            uint32_t bf[4];
+            int r = j * 16 + (lane & 7) + ((lane >> 4) << 3);
+            ldsm_x4(bf, &sb[buf][r * CV_LD + ((lane >> 3) & 1) * 8]);
+#pragma unroll
+            for (int mt = 0; mt < 2; mt++) {
+                mma16816(acc[mt][2 * j], af[mt], bf[0], bf[1]);
+                mma16816(acc[mt][2 * j + 1], af[mt], bf[2], bf[3]);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    // epilogue: bias, ReLU, bf16 pairs into the output slot
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+            int m = m0 + warp * 32 + mt * 16 + g + half * 8;
+            if (m >= a.m) continue;
+            __nv_bfloat16 *o = a.out + (size_t)m * a.out_c + a.out_off;
+#pragma unroll
+            for (int nt = 0; nt < NT; nt++) {
+                int n = n0 + nt * 8 + 2 * t;
+                if (n >= a.cout) continue;
+                float v0 = acc[mt][nt][half * 2], v1 = acc[mt][nt][half * 2 + 1];
+                if (a.bias) {
+                    v0 += a.bias[n];
+                    v1 += a.bias[n + 1];
+                }
+                if (a.relu) {
+                    v0 = fmaxf(v0, 0.0f);
+                    v1 = fmaxf(v1, 0.0f);
+                }
+                if (a.accumulate) {
+                    __nv_bfloat162 old = *reinterpret_cast<const __nv_bfloat162 *>(o + n);
+                    v0 += __bfloat162float(old.x);
+                    v1 += __bfloat162float(old.y);
+                }
+                *reinterpret_cast<__nv_bfloat162 *>(o + n) = __floats2bfloat162_rn(v0, v1);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradient: dW[co][tap][ci] += sum over pixels p of
+// dz[p][co] * x[p + tap][ci] (zero outside the picture).  GEMM with
+// M = cout (CO = cout/16 m16 tiles), N = 16 input channels of one tap
+// (blockIdx.x = tap x cin/16), K = the pixels of the block's chunk
+// (blockIdx.y); each warp takes every 4th 16-pixel step of the chunk with its
+// own double-buffered shared slice, the warps' sums meet in shared memory and
+// go to dW with one FP32 atomicAdd per element.
+constexpr int WG_PIX = 2048;  // pixels per block
+
+template <int CO>
+__global__ void __launch_bounds__(128) k_conv3x3_wgrad(WgradArgs a) {
+    constexpr int COUT = CO * 16;
+    constexpr int LDZ = COUT + 8;  // dz rows (16 B pad: conflict-free ldmatrix)
+    constexpr int LDX = 16 + 8;
+    __shared__ __align__(128) __nv_bfloat16 sz[4][2][16 * LDZ];
+    __shared__ __align__(128) __nv_bfloat16 sx[4][2][16 * LDX];
+    __shared__ float red[4][COUT * 16 / 4];  // (reused per warp pair below)
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cin16 = a.cin >> 4;
+    const int tap = blockIdx.x / cin16, ci0 = (blockIdx.x - tap * cin16) << 4;
+    const int dy = tap / 3 - 1, dx = tap - (tap / 3) * 3 - 1;
+    const int p_begin = blockIdx.y * WG_PIX, p_end = min(p_begin + WG_PIX, a.m);
+    const int hw = a.h * a.w;
+    float acc[CO][2][4];
+#pragma unroll
+    for (int i = 0; i < CO; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) acc[i][j][k] = 0.0f;
+    // one 16-pixel step: dz rows (COUT*2 B each) and x rows (32 B each)
+    auto load = [&](int p0, int buf) {
+        for (int e = lane; e < 16 * (COUT / 8); e += 32) {
+            int row = e / (COUT / 8), piece = e - row * (COUT / 8);
+            int p = p0 + row;
+            bool v = p < p_end;
+            const __nv_bfloat16 *src = v ? a.dz + (size_t)p * a.dz_c + a.dz_off + piece * 8 : a.dz;
+            cp_async16(&sz[warp][buf][row * LDZ + piece * 8], src, v);
+        }
+        {
+            int row = lane >> 1, half = lane & 1;
+            int p = p0 + row;
+            bool v = p < p_end;
+            if (v) {
+                int n = p / hw, r = p - n * hw, y = r / a.w, x = r - y * a.w;
+                y += dy;
+                x += dx;
+                v = (unsigned)y < (unsigned)a.h && (unsigned)x < (unsigned)a.w;
+                if (v) p = (n * a.h + y) * a.w + x;
+            }
+            const __nv_bfloat16 *src = v ? a.x + (size_t)p * a.x_c + a.x_off + ci0 + half * 8 : a.x;
+            cp_async16(&sx[warp][buf][row * LDX + half * 8], src, v);
+        }
+    };
+    int step = 0;
+    int p0 = p_begin + warp * 16;
+    if (p0 < p_end) load(p0, 0);
+    cp_async_commit();
+    for (; p0 < p_end; p0 += 64, step++) {
+        const int buf = step & 1;
+        if (p0 + 64 < p_end) load(p0 + 64, buf ^ 1);
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncwarp();
+        // B fragments: x rows = k (pixels), 16 channels = two n8 tiles
+        uint32_t bx[4];
+        {
+            int r = (lane & 7) + (((lane >> 3) & 1) << 3);  // k rows 0..15
+            int c = (lane >> 4) * 8;                          // n block
+            ldsm_x4_t(bx, &sx[warp][buf][r * LDX + c]);
+        }
+#pragma unroll
+        for (int i = 0; i < CO; i++) {
+            // A = dz^T: m = co (16), k = pixels (16)
+            uint32_t af[4];
+            int r = (lane & 7) + ((lane >> 4) << 3);  // pixel rows
+            int c = i * 16 + ((lane >> 3) & 1) * 8;    // co block
+            ldsm_x4_t(af, &sz[warp][buf][r * LDZ + c]);
+            mma16816(acc[i][0], af, bx[0], bx[1]);
+            mma16816(acc[i][1], af, bx[2], bx[3]);
+        }
+        __syncwarp();
+    }
+    cp_async_wait<0>();
+    // the warps' sums: warp 0..3 add into shared memory, then atomics
+    __syncthreads();
+    float *rs = &red[0][0];  // COUT x 16 floats
+    for (int e = tid; e < COUT * 16; e += 128) rs[e] = 0.0f;
+    __syncthreads();
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int i = 0; i < CO; i++)
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                int co = i * 16 + g + (k >> 1) * 8, ci = j * 8 + 2 * t + (k & 1);
+                atomicAdd(&rs[co * 16 + ci], acc[i][j][k]);
+            }
+    __syncthreads();
+    for (int e = tid; e < COUT * 16; e += 128) {
+        int co = e >> 4, ci = e & 15;
+        if (co < a.cout) atomicAdd(&a.dw[((size_t)co * 9 + tap) * a.cin + ci0 + ci], rs[e]);
+    }
+}
+
+// bias gradient: db[c] += sum over the block's pixels of dz[p][c]
+__global__ void k_bias_grad(const __nv_bfloat16 *dz, int dz_c, int dz_off, int cout, int m, float *db) {
+    __shared__ float s[128];
+    const int c = threadIdx.x;
+    float acc = 0.0f;
+    if (c < cout) {
+        int p_end = min((int)(blockIdx.x + 1) * WG_PIX, m);
+        for (int p = blockIdx.x * WG_PIX; p < p_end; p++) acc += __bfloat162float(dz[(size_t)p * dz_c + dz_off + c]);
+    }
+    s[c] = acc;
+    __syncthreads();
+    if (c < cout) atomicAdd(&db[c], s[c]);
+}
+
+// ---------------------------------------------------------------------------
+// elementwise pieces (one thread per element or per 2x2 group)
+
+// dz = dy * (y > 0) in place (the ReLU's backward), on a channel slot
+__global__ void k_relu_mask(__nv_bfloat16 *d, const __nv_bfloat16 *y, int c_tot, int off, int cn, size_t m) {
+    size_t n = m * (size_t)cn;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        size_t p = i / cn, c = i - p * cn;
+        size_t k = p * c_tot + off + c;
+        if (!(__bfloat162float(y[k]) > 0.0f)) d[k] = __float2bfloat16(0.0f);
+    }
+}
+
+// 2x2 max pooling: out (h/2, w/2, cn) from a slot of in (h, w)
+__global__ void k_pool2(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w, __nv_bfloat16 *out) {
+    int h2 = h >> 1, w2 = w >> 1;
+    size_t total = (size_t)n * h2 * w2 * cn;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int c = (int)(i % cn);
+        size_t q = i / cn;
+        int x = (int)(q % w2), y = (int)((q / w2) % h2), b = (int)(q / ((size_t)w2 * h2));
+        size_t base = (((size_t)b * h + 2 * y) * w + 2 * x) * in_c + in_off + c;
+        float v = __bfloat162float(in[base]);
+        v = fmaxf(v, __bfloat162float(in[base + in_c]));
+        v = fmaxf(v, __bfloat162float(in[base + (size_t)w * in_c]));
+        v = fmaxf(v, __bfloat162float(in[base + (size_t)w * in_c + in_c]));
+        out[i] = __float2bfloat16(v);
+    }
+}
+
+// its backward: the gradient to the first of the four inputs that holds the
+// maximum, added to the slot of din
+__global__ void k_pool2_bwd(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w,
+                            const __nv_bfloat16 *dout, __nv_bfloat16 *din) {
+    int h2 = h >> 1, w2 = w >> 1;
+    size_t total = (size_t)n * h2 * w2 * cn;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int c = (int)(i % cn);
+        size_t q = i / cn;
+        int x = (int)(q % w2), y = (int)((q / w2) % h2), b = (int)(q / ((size_t)w2 * h2));
+        size_t base = (((size_t)b * h + 2 * y) * w + 2 * x) * in_c + in_off + c;
+        size_t k[4] = {base, base + in_c, base + (size_t)w * in_c, base + (size_t)w * in_c + in_c};
+        float best = __bfloat162float(in[k[0]]);
+        int arg = 0;
+#pragma unroll
+        for (int j = 1; j < 4; j++) {
+            float v = __bfloat162float(in[k[j]]);
+            if (v > best) {
+                best = v;
+                arg = j;
+            }
+        }
+        float g = __bfloat162float(dout[i]);
+        din[k[arg]] = __float2bfloat16(__bfloat162float(din[k[arg]]) + g);
+    }
+}
+
+// nearest 2x upsampling of in (h/2, w/2, cn) into a slot of out (h, w)
+__global__ void k_up2(const __nv_bfloat16 *in, int cn, int n, int h, int w, __nv_bfloat16 *out, int out_c, int out_off) {
+    size_t total = (size_t)n * h * w * cn;
+    int h2 = h >> 1, w2 = w >> 1;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int c = (int)(i % cn);
+        size_t q = i / cn;
+        int x = (int)(q % w), y = (int)((q / w) % h), b = (int)(q / ((size_t)w * h));
+        out[q * out_c + out_off + c] = in[(((size_t)b * h2 + (y >> 1)) * w2 + (x >> 1)) * cn + c];
+    }
+}
+
+// its backward: the sum of the four gradients
+__global__ void k_up2_bwd(const __nv_bfloat16 *dout, int out_c, int out_off, int cn, int n, int h, int w,
+                          __nv_bfloat16 *din) {
+    int h2 = h >> 1, w2 = w >> 1;
+    size_t total = (size_t)n * h2 * w2 * cn;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int c = (int)(i % cn);
+        size_t q = i / cn;
+        int x = (int)(q % w2), y = (int)((q / w2) % h2), b = (int)(q / ((size_t)w2 * h2));
+        size_t base = (((size_t)b * h + 2 * y) * w + 2 * x) * out_c + out_off + c;
+        float s = __bfloat162float(dout[base]) + __bfloat162float(dout[base + out_c]) +
+                  __bfloat162float(dout[base + (size_t)w * out_c]) + __bfloat162float(dout[base + (size_t)w * out_c + out_c]);
+        din[i] = __float2bfloat16(s);
+    }
+}
+
+// the network's input: log(1 + radiance), albedo, normal, depth / its
+// maximum, zero channels 10..15; pixels outside (w_src, h_src) are zero.
+// Sources are float (h_src, w_src, 3) per image, images one after another.
+__global__ void k_pack_input(const float *rad, const float *alb, const float *nrm, const float *dep, float depth_scale,
+                             int n, int h_src, int w_src, int h, int w, __nv_bfloat16 *out) {
+    size_t total = (size_t)n * h * w;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int x = (int)(i % w), y = (int)((i / w) % h), b = (int)(i / ((size_t)w * h));
+        float v[16];
+#pragma unroll
+        for (int c = 0; c < 16; c++) v[c] = 0.0f;
+        if (y < h_src && x < w_src) {
+            size_t s = ((size_t)b * h_src + y) * w_src + x;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                v[c] = log1pf(fmaxf(rad[3 * s + c], 0.0f));
+                if (alb) v[3 + c] = alb[3 * s + c];
+                if (nrm) v[6 + c] = nrm[3 * s + c];
+            }
+            if (dep) v[9] = dep[s] * depth_scale;
+        }
+        __nv_bfloat16 *o = out + i * 16;
+#pragma unroll
+        for (int c = 0; c < 16; c += 2) *reinterpret_cast<__nv_bfloat162 *>(o + c) = __floats2bfloat162_rn(v[c], v[c + 1]);
+    }
+}
+
+// the network's output (log space, 16 channels) as radiance (h_src, w_src, 3)
+__global__ void k_unpack_output(const __nv_bfloat16 *pred, int n, int h, int w, int h_src, int w_src, float *out) {
+    size_t total = (size_t)n * h_src * w_src;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int x = (int)(i % w_src), y = (int)((i / w_src) % h_src), b = (int)(i / ((size_t)w_src * h_src));
+        size_t p = ((size_t)b * h + y) * w + x;
+#pragma unroll
+        for (int c = 0; c < 3; c++) out[3 * i + c] = fmaxf(expm1f(__bfloat162float(pred[p * 16 + c])), 0.0f);
+    }
+}
+
+// L1 loss in log space on channels 0..2 of the valid pixels: its sum into
+// *loss, its gradient (1/count per element, the sign) into dpred
+__global__ void k_l1_loss(const __nv_bfloat16 *pred, const float *target, int n, int h, int w, int h_src, int w_src,
+                          float inv_count, __nv_bfloat16 *dpred, float *loss) {
+    __shared__ float s[256];
+    size_t total = (size_t)n * h * w;
+    float acc = 0.0f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int x = (int)(i % w), y = (int)((i / w) % h), b = (int)(i / ((size_t)w * h));
+        __nv_bfloat16 *d = dpred + i * 16;
+        for (int c = 0; c < 16; c++) d[c] = __float2bfloat16(0.0f);
+        if (y < h_src && x < w_src) {
+            size_t t = ((size_t)b * h_src + y) * w_src + x;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                float e = __bfloat162float(pred[i * 16 + c]) - log1pf(fmaxf(target[3 * t + c], 0.0f));
+                acc += fabsf(e);
+                d[c] = __float2bfloat16(e > 0.0f ? inv_count : (e < 0.0f ? -inv_count : 0.0f));
+            }
+        }
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, s[0] * inv_count);
+}
+
+// Adam on the FP32 master parameters; then the bf16 weights of the forward
+// ([co][tap][ci]) and of the backward to the input ([ci][8 - tap][co])
+__global__ void k_adam(float *param, const float *grad, float *m1, float *m2, size_t n, float lr, float b1, float b2,
+                       float eps, float c1, float c2) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        float g = grad[i];
+        float a = b1 * m1[i] + (1.0f - b1) * g;
+        float b = b2 * m2[i] + (1.0f - b2) * g * g;
+        m1[i] = a;
+        m2[i] = b;
+        param[i] -= lr * (a * c1) / (sqrtf(b * c2) + eps);
+    }
+}
+
+__global__ void k_cast_weights(const float *w, int cout, int cin, __nv_bfloat16 *wf, __nv_bfloat16 *wb) {
+    size_t total = (size_t)cout * 9 * cin;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int ci = (int)(i % cin), tap = (int)((i / cin) % 9), co = (int)(i / ((size_t)cin * 9));
+        __nv_bfloat16 v = __float2bfloat16(w[i]);
+        wf[i] = v;
+        if (wb) wb[((size_t)ci * 9 + (8 - tap)) * cout + co] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+
+static int grid_for(size_t n, int per = 256) {
+    size_t b = (n + per - 1) / per;
+    return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+int dn_conv(const ConvArgs &a, cudaStream_t s) {
+    if (a.cin % 16 || a.cout <= 0 || a.in_c % 8 || a.in_off % 8 || a.out_c % 2 || a.out_off % 2) return -1;
+    int bn = a.cout <= 16 ? 16 : a.cout <= 32 ? 32 : a.cout <= 48 ? 48 : a.cout <= 64 ? 64 : a.cout <= 80 ? 80 : 96;
+    if (a.cout > 96) {
+        // wide outputs: tiles of 64 or 48 (whichever wastes fewer columns)
+        int w64 = (64 - a.cout % 64) % 64, w48 = (48 - a.cout % 48) % 48;
+        bn = w64 <= w48 ? 64 : 48;
+    }
+    dim3 grid((a.m + CV_BM - 1) / CV_BM, (a.cout + bn - 1) / bn);
+    switch (bn) {
+        case 16: k_conv3x3<16><<<grid, 128, 0, s>>>(a); break;
+        case 32: k_conv3x3<32><<<grid, 128, 0, s>>>(a); break;
+        case 48: k_conv3x3<48><<<grid, 128, 0, s>>>(a); break;
+        case 64: k_conv3x3<64><<<grid, 128, 0, s>>>(a); break;
+        case 80: k_conv3x3<80><<<grid, 128, 0, s>>>(a); break;
+        default: k_conv3x3<96><<<grid, 128, 0, s>>>(a); break;
+    }
+    return 0;
+}
+
+int dn_wgrad(const WgradArgs &a, float *db, cudaStream_t s) {
+    if (a.cin % 16 || a.cout % 16 || a.cout > 96 || a.dz_c % 8 || a.dz_off % 8 || a.x_c % 8 || a.x_off % 8) return -1;
+    dim3 grid(9 * (a.cin / 16), (a.m + WG_PIX - 1) / WG_PIX);
+    switch (a.cout / 16) {
+        case 1: k_conv3x3_wgrad<1><<<grid, 128, 0, s>>>(a); break;
+        case 2: k_conv3x3_wgrad<2><<<grid, 128, 0, s>>>(a); break;
+        case 3: k_conv3x3_wgrad<3><<<grid, 128, 0, s>>>(a); break;
+        case 4: k_conv3x3_wgrad<4><<<grid, 128, 0, s>>>(a); break;
+        case 5: k_conv3x3_wgrad<5><<<grid, 128, 0, s>>>(a); break;
+        default: k_conv3x3_wgrad<6><<<grid, 128, 0, s>>>(a); break;
+    }
+    if (db) k_bias_grad<<<(a.m + WG_PIX - 1) / WG_PIX, 128, 0, s>>>(a.dz, a.dz_c, a.dz_off, a.cout, a.m, db);
+    return 0;
+}
+
+void dn_relu_mask(__nv_bfloat16 *d, const __nv_bfloat16 *y, int c_tot, int off, int cn, size_t m, cudaStream_t s) {
+    k_relu_mask<<<grid_for(m * cn), 256, 0, s>>>(d, y, c_tot, off, cn, m);
+}
+void dn_pool2(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w, __nv_bfloat16 *out,
+              cudaStream_t s) {
+    k_pool2<<<grid_for((size_t)n * (h / 2) * (w / 2) * cn), 256, 0, s>>>(in, in_c, in_off, cn, n, h, w, out);
+}
+void dn_pool2_bwd(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w, const __nv_bfloat16 *dout,
+                  __nv_bfloat16 *din, cudaStream_t s) {
+    k_pool2_bwd<<<grid_for((size_t)n * (h / 2) * (w / 2) * cn), 256, 0, s>>>(in, in_c, in_off, cn, n, h, w, dout, din);
+}
+void dn_up2(const __nv_bfloat16 *in, int cn, int n, int h, int w, __nv_bfloat16 *out, int out_c, int out_off, cudaStream_t s) {
+    k_up2<<<grid_for((size_t)n * h * w * cn), 256, 0, s>>>(in, cn, n, h, w, out, out_c, out_off);
+}
+void dn_up2_bwd(const __nv_bfloat16 *dout, int out_c, int out_off, int cn, int n, int h, int w, __nv_bfloat16 *din,
+                cudaStream_t s) {
+    k_up2_bwd<<<grid_for((size_t)n * (h / 2) * (w / 2) * cn), 256, 0, s>>>(dout, out_c, out_off, cn, n, h, w, din);
+}
+void dn_pack_input(const float *rad, const float *alb, const float *nrm, const float *dep, float depth_scale, int n,
+                   int h_src, int w_src, int h, int w, __nv_bfloat16 *out, cudaStream_t s) {
+    k_pack_input<<<grid_for((size_t)n * h * w), 256, 0, s>>>(rad, alb, nrm, dep, depth_scale, n, h_src, w_src, h, w, out);
+}
+void dn_unpack_output(const __nv_bfloat16 *pred, int n, int h, int w, int h_src, int w_src, float *out, cudaStream_t s) {
+    k_unpack_output<<<grid_for((size_t)n * h_src * w_src), 256, 0, s>>>(pred, n, h, w, h_src, w_src, out);
+}
+void dn_l1_loss(const __nv_bfloat16 *pred, const float *target, int n, int h, int w, int h_src, int w_src,
+                __nv_bfloat16 *dpred, float *loss, cudaStream_t s) {
+    float inv = 1.0f / (float)((size_t)n * h_src * w_src * 3);
+    k_l1_loss<<<grid_for((size_t)n * h * w), 256, 0, s>>>(pred, target, n, h, w, h_src, w_src, inv, dpred, loss);
+}
+void dn_adam(float *param, const float *grad, float *m1, float *m2, size_t n, float lr, int t, cudaStream_t s) {
+    const float b1 = 0.9f, b2 = 0.999f;
+    float c1 = 1.0f / (1.0f - powf(b1, (float)t)), c2 = 1.0f / (1.0f - powf(b2, (float)t));
+    k_adam<<<grid_for(n), 256, 0, s>>>(param, grad, m1, m2, n, lr, b1, b2, 1e-8f, c1, c2);
+}
+void dn_cast_weights(const float *w, int cout, int cin, __nv_bfloat16 *wf, __nv_bfloat16 *wb, cudaStream_t s) {
+    k_cast_weights<<<grid_for((size_t)cout * 9 * cin), 256, 0, s>>>(w, cout, cin, wf, wb);
+}
+
+}  // namespace mb3dcu

@@ -122,7 +122,7 @@ struct McLane {
     int x1, y, b;
     uint32_t pix;
     int32_t seed;
-    double pos[3], vfov[3], normals[3], dir[3];
+    double vfov[3], normals[3], dir[3];
     double mzz;
     bool hit, calc_amb_shadow, rit1, probe, aov;
     int rit, guard;
@@ -206,7 +206,7 @@ struct McRun {
         double nv = 1.0 / sqrt(dot3d(v, v));
         for (int k = 0; k < 3; k++) v[k] *= nv;
         rot_rev(v, p.vgrads, L.vfov);
-        for (int k = 0; k < 3; k++) L.pos[k] = p.ystart[k] + p.vgrads[1][k] * (double)yy + p.vgrads[0][k] * (double)xx;
+        for (int k = 0; k < 3; k++) L.c[k] = p.ystart[k] + p.vgrads[1][k] * (double)yy + p.vgrads[0][k] * (double)xx;
         for (int k = 0; k < 3; k++) {
             L.tl[k] = 0.0f;
             L.ta[k] = 1.0f;
@@ -367,7 +367,7 @@ struct McRun {
 
     // Runs the lane's logic on the result r (st) of the DE it asked for,
     // up to the next DE it asks for (or the end of its item).
-    __device__ void advance(McLane &L, const DEr &r, const DEstate &st, McAcc &acc, mb3d_cu_mc_res *res) const {
+    __device__ __forceinline__ void advance(McLane &L, const DEr &r, const DEstate &st, McAcc &acc, mb3d_cu_mc_res *res) const {
         const double sw = p.step_width;
         const double zero3[3] = {0.0, 0.0, 0.0};
         for (int turn = 0; turn < 64; turn++) {
@@ -397,8 +397,7 @@ struct McRun {
                 L.rit1 = L.rit == 1;
                 L.zz2 = L.rit1 ? L.zz : 0.0;
                 L.bg_dec = 1.0f;
-                L.zzplus = dot3d(L.dir, L.vfov) / (sw * sw);
-                for (int k = 0; k < 3; k++) L.c[k] = L.pos[k];
+                L.zzplus = dot3d(L.dir, L.vfov) / (sw * sw);  // (the march starts at c)
                 L.ms = de_stop(L.zz);
                 ask(L, W_M0);
                 return;
@@ -616,18 +615,33 @@ struct McRun {
                 L.phase = L_NSAMP;
                 break;
             case L_NSAMP: {
-                // the one-sided sample on axis k = 2, 0, 1
-                int k = L.nq == 0 ? 2 : L.nq - 1;
+                // the one-sided sample on axis k = 2, 0, 1 (q = 0, 1, 2)
                 double off = (double)fminf(p.de_stop, 1.0f) * (1.0 + L.mzz * (double)p.de_stop_factor) * (double)L.sca * p.step_width;
-                L.tsave = L.c[k];
-                L.c[k] = L.tsave + off;
+                if (L.nq == 0) {
+                    L.tsave = L.c[2];
+                    L.c[2] = L.tsave + off;
+                } else if (L.nq == 1) {
+                    L.tsave = L.c[0];
+                    L.c[0] = L.tsave + off;
+                } else {
+                    L.tsave = L.c[1];
+                    L.c[1] = L.tsave + off;
+                }
                 ask(L, W_NK);
                 return;
             }
             case W_NK: {
-                int k = L.nq == 0 ? 2 : L.nq - 1;
-                L.n[k] = (r.de - L.no) * (double)L.sca;
-                L.c[k] = L.tsave;
+                double g = (r.de - L.no) * (double)L.sca;
+                if (L.nq == 0) {
+                    L.n[2] = g;
+                    L.c[2] = L.tsave;
+                } else if (L.nq == 1) {
+                    L.n[0] = g;
+                    L.c[0] = L.tsave;
+                } else {
+                    L.n[1] = g;
+                    L.c[1] = L.tsave;
+                }
                 L.nq += 1;
                 if (L.nq < 3) {
                     L.phase = L_NSAMP;
@@ -655,7 +669,6 @@ struct McRun {
                     L.phase = L_ITEM_END;
                 } else {
                     // CalcRay in open air: the background
-                    for (int k = 0; k < 3; k++) L.pos[k] = L.c[k];
                     L.t_dyn_fog = L.m_dyn_fog;
                     const mb3d_cu_mc_light &lv = m.lv;
                     L.zpos_dyn_fog = (float)(p.zend * sw + m.zz_stmit_dif);
@@ -698,11 +711,10 @@ struct McRun {
                     L.phase = L_ITEM_END;
                 } else {
                     // CalcRay on a surface, up to the lights
-                    for (int k = 0; k < 3; k++) L.pos[k] = L.c[k];
                     L.t_dyn_fog = L.m_dyn_fog;
                     L.hit = true;
                     L.mzz = fabs(L.zz);
-                    for (int k = 0; k < 3; k++) L.cc[k] = L.pos[k];
+                    for (int k = 0; k < 3; k++) L.cc[k] = L.c[k];
                     uint32_t cr_zpos = mc_zpos_of(p, L.zz2);
                     if (L.rit1) L.main_zpos = cr_zpos;
                     calc_color(L, (float)(L.mzz * sw + m.zz_stmit_dif));
@@ -854,7 +866,7 @@ struct McRun {
                 for (int k = 0; k < 3; k++)
                     nv[k] = (double)((float)(o0[k] * d3c * dd) + (float)(o1[k] * d4s * dd)) + L.normals[k] * w;
                 mc_norm_to(sw, nv, L.dir);
-                for (int k = 0; k < 3; k++) L.pos[k] = L.cc[k];
+                for (int k = 0; k < 3; k++) L.c[k] = L.cc[k];
                 L.calc_amb_shadow = true;
                 for (int k = 0; k < 3; k++) L.ta[k] = L.ta[k] * (L.obj_dif[k] * 1.0f);
                 L.probe = false;
@@ -886,8 +898,11 @@ struct McRun {
 // The persistent kernel.  BATCH: the items are the march requests `reqs`
 // (results into `res`); else item i is ray ray0 + i / npad of pixel i % npad
 // (8x4 tiles), so that neighbouring lanes trace neighbouring pixels.
+#ifndef MB3D_MC_MIN_BLOCKS
+#define MB3D_MC_MIN_BLOCKS 6  // (measured best: spills to L1 beat fewer resident warps)
+#endif
 template <typename R, int FM, bool BATCH>
-__global__ void __launch_bounds__(128) k_mc(const __grid_constant__ DevParams p, const __grid_constant__ McDev m,
+__global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_constant__ DevParams p, const __grid_constant__ McDev m,
                                             McAcc acc, const mb3d_cu_mc_req *reqs, mb3d_cu_mc_res *res,
                                             unsigned int *queue, uint32_t n_items) {
     McRun<BATCH> run(p, m);
@@ -937,17 +952,16 @@ __global__ void __launch_bounds__(128) k_mc(const __grid_constant__ DevParams p,
                     L.y = m.y0 + ly;
                     L.b = m.ray0 + (int)(item / m.npad);
                     L.aov = L.b == m.ray0;
-                    L.phase = L_RAY;
-                    run.advance(L, r, st, acc, res);
+                    L.phase = L_RAY;  // (its logic runs below, its first DE on the next trip)
                 }
             }
         }
-        bool wants = L.phase >= W_M0;
-        unsigned int busy = __ballot_sync(0xffffffffu, wants);
+        unsigned int busy = __ballot_sync(0xffffffffu, L.phase != L_IDLE);
         if (busy == 0) {
             if (!open) break;
             continue;
         }
+        const bool wants = L.phase >= W_M0;
         if (wants) {
             if (single) {
                 r = de_lock<float, FM, false, true>(p, L.c, L.ms, nullptr, &st, L.sit, L.max_add);
@@ -960,8 +974,8 @@ __global__ void __launch_bounds__(128) k_mc(const __grid_constant__ DevParams p,
             }
             evals++;
             its += (unsigned long long)r.it;
-            run.advance(L, r, st, acc, res);
         }
+        if (L.phase != L_IDLE) run.advance(L, r, st, acc, res);
     }
     if (acc.counters) {
         atomicAdd(&acc.counters[0], evals);

@@ -179,6 +179,17 @@ def lib():
         L.mb3d_cu_render_frames.argtypes = [vp, sp, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(Tune), vp]
         L.mb3d_cu_autotune.argtypes = [vp, sp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(Tune)]
         L.mb3d_cu_march_noalloc.argtypes = [sp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.mb3d_cu_dn_param_count.restype = ctypes.c_size_t
+        L.mb3d_cu_dn_create.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(vp)]
+        L.mb3d_cu_dn_free.argtypes = [vp]
+        L.mb3d_cu_dn_free.restype = None
+        L.mb3d_cu_dn_get_params.argtypes = [vp, vp]
+        L.mb3d_cu_dn_set_params.argtypes = [vp, vp]
+        L.mb3d_cu_dn_denoise.argtypes = [vp] + [ctypes.c_int] * 3 + [vp] * 4 + [ctypes.c_float, vp]
+        L.mb3d_cu_dn_train_step.argtypes = [vp] + [ctypes.c_int] * 3 + [vp] * 4 + [ctypes.c_float, vp, ctypes.c_float, fp]
+        L.mb3d_cu_dn_gradient.argtypes = [vp] + [ctypes.c_int] * 3 + [vp] * 4 + [ctypes.c_float, vp, fp, vp]
+        L.mb3d_cu_dn_conv_check.argtypes = [vp] + [ctypes.c_int] * 5 + [vp] * 8
         L.mb3d_cu_mc_light_default.argtypes = [sp, ctypes.POINTER(McLight)]
         L.mb3d_cu_mc_batch.argtypes = [vp, sp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_uint32, vp]
         L.mb3d_cu_mc_render.argtypes = [vp, sp, ctypes.POINTER(McLight), ctypes.POINTER(McOpts), ctypes.c_int,
@@ -190,7 +201,10 @@ def lib():
 EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_free", "mb3d_cu_set_stream",
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
-            "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render"]
+            "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render",
+            "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
+            "mb3d_cu_dn_set_params", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
+            "mb3d_cu_dn_conv_check"]
 
 NOALLOC_MAX_PIXELS = 65536
 
@@ -356,3 +370,104 @@ def depth_steps(g, scene_params):
     zf = (g["zpos_fine"] >> 8).astype(np.float64)
     zc_mul, zcorr = scene_params
     return (((8388351.5 - zf) / zc_mul + 1.0) ** 2 - 1.0) / zcorr
+
+
+def _fptr(a):
+    """A float32 buffer's pointer (numpy array or torch CUDA tensor), or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.dtype == np.float32 and a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    assert a.is_contiguous()
+    return a.data_ptr()
+
+
+class Denoiser:
+    """The Monte Carlo pictures' denoiser (mb3d_cu_dn_*): a BF16 U-Net on the
+    card, the counterpart of mb3d-rs's Open Image Denoise call
+    (denoise_mc, src/oidn.rs:262-277).  Arrays are (n, h, w, 3) float32 (depth
+    (n, h, w)), numpy or torch CUDA tensors."""
+
+    def __init__(self, card, seed=1):
+        self.card = card
+        self._d = ctypes.c_void_p()
+        card._check(lib().mb3d_cu_dn_create(card._ctx, seed, ctypes.byref(self._d)))
+        self.n_params = lib().mb3d_cu_dn_param_count()
+
+    def close(self):
+        if self._d:
+            lib().mb3d_cu_dn_free(self._d)
+            self._d = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def get_params(self):
+        p = np.zeros(self.n_params, np.float32)
+        self.card._check(lib().mb3d_cu_dn_get_params(self._d, p.ctypes.data))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.n_params
+        self.card._check(lib().mb3d_cu_dn_set_params(self._d, p.ctypes.data))
+
+    @staticmethod
+    def _shape(radiance):
+        s = tuple(radiance.shape)
+        return (1,) + s[:2] if len(s) == 3 else s[:3]
+
+    def denoise(self, radiance, albedo=None, normal=None, depth=None, depth_scale=None, out=None):
+        n, h, w = self._shape(radiance)
+        if depth_scale is None:
+            depth_scale = _depth_scale(depth)
+        if out is None:
+            out = np.zeros((n, h, w, 3), np.float32) if isinstance(radiance, np.ndarray) else radiance.new_zeros((n, h, w, 3))
+        self.card._check(lib().mb3d_cu_dn_denoise(self._d, n, h, w, _fptr(radiance), _fptr(albedo), _fptr(normal),
+                                                  _fptr(depth), depth_scale, _fptr(out)))
+        return out
+
+    def train_step(self, radiance, target, albedo=None, normal=None, depth=None, depth_scale=None, lr=1e-3):
+        n, h, w = self._shape(radiance)
+        if depth_scale is None:
+            depth_scale = _depth_scale(depth)
+        loss = ctypes.c_float()
+        self.card._check(lib().mb3d_cu_dn_train_step(self._d, n, h, w, _fptr(radiance), _fptr(albedo), _fptr(normal),
+                                                     _fptr(depth), depth_scale, _fptr(target), lr, ctypes.byref(loss)))
+        return loss.value
+
+    def gradient(self, radiance, target, albedo=None, normal=None, depth=None, depth_scale=1.0):
+        n, h, w = self._shape(radiance)
+        loss = ctypes.c_float()
+        g = np.zeros(self.n_params, np.float32)
+        self.card._check(lib().mb3d_cu_dn_gradient(self._d, n, h, w, _fptr(radiance), _fptr(albedo), _fptr(normal),
+                                                   _fptr(depth), depth_scale, _fptr(target), ctypes.byref(loss),
+                                                   g.ctypes.data))
+        return loss.value, g
+
+
+def _depth_scale(depth):
+    """1 / the largest depth (the guides' depth about 0..1)."""
+    if depth is None:
+        return 1.0
+    m = float(depth.max())
+    return 1.0 / m if m > 0 else 1.0
+
+
+def conv_check(card, x, w, b, dy):
+    """mb3d_cu_dn_conv_check: y, dx, dw, db of one 3x3 convolution."""
+    n, h, ww, cin = x.shape
+    cout = w.shape[0]
+    x, w, b, dy = (np.ascontiguousarray(a, np.float32) for a in (x, w, b, dy))
+    y = np.zeros((n, h, ww, cout), np.float32)
+    dx = np.zeros_like(x)
+    dw = np.zeros_like(w)
+    db = np.zeros_like(b)
+    card._check(lib().mb3d_cu_dn_conv_check(card._ctx, n, h, ww, cin, cout, x.ctypes.data, w.ctypes.data, b.ctypes.data,
+                                            dy.ctypes.data, y.ctypes.data, dx.ctypes.data, dw.ctypes.data,
+                                            db.ctypes.data))
+    return y, dx, dw, db

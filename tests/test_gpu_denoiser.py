@@ -1,0 +1,95 @@
+"""The denoiser's kernels and network against the numpy FP64 oracle
+(oracle/unet.py), and its training on the card.
+
+One convolution: the forward output, the input gradient and the weight and
+bias gradients of the BF16 tensor-core kernels equal the FP64 results on the
+same BF16-rounded operands up to FP32 accumulation and the BF16 rounding of
+the outputs (y, dx: 1/128 of the largest value; dw, db: 1e-3 relative).
+The whole network's parameter gradient: per layer, cosine > 0.99 and
+relative error < 0.1 against the FP64 oracle run on the same parameters
+(the card stores every activation and activation gradient in BF16).
+"""
+import numpy as np
+import pytest
+
+import mb3dcu
+import unet
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("cin,cout", [(16, 32), (32, 32), (48, 64), (80, 48), (32, 96), (112, 16), (176, 80)])
+def test_conv_kernels_match_fp64(card, cin, cout):
+    rng = np.random.default_rng(cin * 1000 + cout)
+    n, h, w = 2, 9, 13  # ragged: partial pixel tiles, every border
+    x = unet.bf16(rng.standard_normal((n, h, w, cin)))
+    wt = unet.bf16(rng.standard_normal((cout, 9, cin)) * np.sqrt(2.0 / (9 * cin)))
+    b = rng.standard_normal(cout).astype(np.float32)
+    dy = unet.bf16(rng.standard_normal((n, h, w, cout)))
+    if cout > 96:
+        pytest.skip("the weight gradient kernel takes cout <= 96")
+    y, dx, dw, db = mb3dcu.conv_check(card, x, wt, b, dy)
+    ye = unet.conv(x.astype(np.float64), wt.astype(np.float64), b.astype(np.float64))
+    dxe, dwe, dbe = unet.conv_bwd(x.astype(np.float64), wt.astype(np.float64), dy.astype(np.float64))
+    assert np.abs(y - ye).max() <= np.abs(ye).max() / 128, (cin, cout)
+    assert np.abs(dx - dxe).max() <= np.abs(dxe).max() / 128, (cin, cout)
+    assert np.abs(dw - dwe).max() <= 1e-3 * np.abs(dwe).max(), (cin, cout)
+    assert np.abs(db - dbe).max() <= 1e-3 * np.abs(dbe).max(), (cin, cout)
+
+
+def _batch(rng, n, h, w):
+    rad = rng.gamma(1.0, 0.4, (n, h, w, 3)).astype(np.float32)
+    alb = rng.uniform(0, 1, (n, h, w, 3)).astype(np.float32)
+    nrm = rng.standard_normal((n, h, w, 3)).astype(np.float32)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    dep = rng.uniform(0.2, 1.0, (n, h, w)).astype(np.float32)
+    tgt = (rad * rng.uniform(0.5, 1.5, rad.shape)).astype(np.float32)
+    return rad, alb, nrm, dep, tgt
+
+
+def test_network_gradient_matches_fp64_oracle(card):
+    rng = np.random.default_rng(5)
+    dn = mb3dcu.Denoiser(card, seed=3)
+    try:
+        p = dn.get_params()
+        # non-zero biases, so that every ReLU sees both signs
+        p = p + np.where(np.arange(p.size) % 7 == 0, 0.01, 0.0).astype(np.float32)
+        dn.set_params(p)
+        rad, alb, nrm, dep, tgt = _batch(rng, 2, 32, 48)
+        loss, g = dn.gradient(rad, tgt, alb, nrm, dep, depth_scale=1.0)
+        x = unet.pack_input(rad.astype(np.float64), alb, nrm, dep, 1.0)
+        pred, cache = unet.forward(p, x)
+        le, dpred = unet.l1_loss(pred, tgt.astype(np.float64))
+        ge = unet.backward(p, cache, dpred)
+        assert abs(loss - le) <= 0.02 * le, (loss, le)
+        o = 0
+        for i, (cin, cout, _) in enumerate(unet.layers()):
+            k = cout * 9 * cin + cout
+            a, e = g[o:o + k].astype(np.float64), ge[o:o + k]
+            o += k
+            if i == 18:  # the output layer: only channels 0..2 have a gradient
+                a = a.reshape(-1)
+            cos = a @ e / (np.linalg.norm(a) * np.linalg.norm(e) + 1e-30)
+            rel = np.linalg.norm(a - e) / (np.linalg.norm(e) + 1e-30)
+            assert cos > 0.99 and rel < 0.1, (i, cos, rel)
+    finally:
+        dn.close()
+
+
+def test_training_lowers_the_loss(card):
+    rng = np.random.default_rng(9)
+    dn = mb3dcu.Denoiser(card, seed=4)
+    try:
+        rad, alb, nrm, dep, tgt = _batch(rng, 4, 64, 64)
+        first = dn.train_step(rad, tgt, alb, nrm, dep, lr=2e-3)
+        for _ in range(60):
+            last = dn.train_step(rad, tgt, alb, nrm, dep, lr=2e-3)
+        assert last < 0.7 * first, (first, last)
+        out = dn.denoise(rad, alb, nrm, dep)
+        assert out.shape == rad.shape and np.isfinite(out).all() and out.min() >= 0.0
+        # a picture whose size is not a multiple of 16
+        odd = dn.denoise(rad[:1, :50, :37].copy(), alb[:1, :50, :37].copy(), nrm[:1, :50, :37].copy(),
+                         dep[:1, :50, :37].copy())
+        assert odd.shape == (1, 50, 37, 3) and np.isfinite(odd).all()
+    finally:
+        dn.close()

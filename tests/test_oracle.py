@@ -221,3 +221,39 @@ def test_mc_oracle_is_deterministic_and_sane():
     # the first surface's normal is a unit vector where there is one
     n = np.linalg.norm(a["normal"], axis=2)
     assert np.all(np.abs(n[a["depth"] > 0] - 1.0) < 1e-9)
+
+
+def test_unet_oracle_backward_matches_finite_differences():
+    """The denoiser oracle's backward pass (oracle/unet.py) against central
+    differences of its forward pass, FP64, on a 1 x 16 x 16 input."""
+    import unet
+    rng = np.random.default_rng(2)
+    n_par = sum(co * 9 * ci + co for ci, co, _ in unet.layers())
+    p = np.zeros(n_par)
+    o = 0
+    for ci, co, _ in unet.layers():
+        p[o:o + co * 9 * ci] = rng.standard_normal(co * 9 * ci) * np.sqrt(2.0 / (9 * ci))
+        o += co * 9 * ci
+        p[o:o + co] = rng.standard_normal(co) * 0.05
+        o += co
+    rad = rng.gamma(1.0, 0.4, (1, 16, 16, 3))
+    x = unet.pack_input(rad, rng.uniform(0, 1, (1, 16, 16, 3)), rng.standard_normal((1, 16, 16, 3)),
+                        rng.uniform(0, 1, (1, 16, 16)), 1.0)
+    tgt = rad * 1.3
+
+    def loss(q):
+        # a smooth loss (squared error) keeps the check away from L1's kinks
+        pred, _ = unet.forward(q, x)
+        e = pred[..., :3] - np.log1p(tgt)
+        return 0.5 * np.sum(e * e)
+
+    pred, cache = unet.forward(p, x)
+    dpred = np.zeros_like(pred)
+    dpred[..., :3] = pred[..., :3] - np.log1p(tgt)
+    g = unet.backward(p, cache, dpred)
+    idx = rng.choice(n_par, 40, replace=False)
+    for i in idx:
+        e = np.zeros(n_par)
+        e[i] = 1e-6
+        num = (loss(p + e) - loss(p - e)) / 2e-6
+        assert abs(num - g[i]) <= 1e-4 * max(1.0, abs(num)), (i, num, g[i])
