@@ -279,3 +279,49 @@ def scaled(sc, width, height):
     n.width, n.height = width, height
     n.de_stop = max(sc.de_stop * f, 0.001)
     return n
+
+
+def c5_mc(width=1920, height=1080):
+    """The Monte Carlo workload: the C2 hybrid scene, 1920x1080, up to 4
+    ambient bounces (MCDepth 4), light 1 plus the ambient sky."""
+    return c2_hybrid(width=width, height=height)
+
+
+C5_DEPTH = 4
+TRAIN_SEED = 0x5EED0005
+
+
+def random_training_scene(seed, width=256, height=256):
+    """A seeded scene for the denoiser's training pictures: one of four
+    formula families with random parameters (box/bulb hybrid, bulb, box,
+    Menger/box), a random camera on a sphere around the origin looking at
+    it, a random zoom and a random light direction."""
+    st = seed & 0xFFFFFFFFFFFFFFFF
+    u = []
+    for _ in range(12):
+        st, v = splitmix64(st)
+        u.append(v / 2.0 ** 64)
+    sc = default_scene()
+    sc.width, sc.height = width, height
+    fam = int(u[0] * 4)
+    power = 3 + int(u[1] * 6)
+    bscale = (1.3 + 1.2 * u[2]) * (-1.0 if u[3] < 0.6 else 1.0)
+    min_r, fold = 0.25 + 0.5 * u[4], 0.8 + 0.4 * u[5]
+    if fam == 0:
+        set_slots(sc, [amazing_box(bscale, min_r, fold, 1 + int(u[6] * 2)), intpow(power, -1.0, 1)])
+        radius = 2.6 + 1.2 * u[7]
+    elif fam == 1:
+        set_slots(sc, [intpow(power, -1.0, 1)])
+        radius = 2.0 + 1.0 * u[7]
+    elif fam == 2:
+        set_slots(sc, [amazing_box(bscale, min_r, fold, 1)])
+        radius = 3.0 + 3.0 * u[7] if bscale < 0 else 5.0 + 3.0 * u[7]
+    else:
+        set_slots(sc, [menger_ifs(3.0, 1.0, 1.0, 0.5, 1), amazing_box(2.0, 0.5, 1.0, 1)])
+        radius = 1.8 + 2.2 * u[7]
+    sc.iterations = 12 + int(u[8] * 19)
+    place_camera(sc, sphere_point(st, radius))
+    sc.zoom = 1.0 + 1.5 * u[9]
+    sc.lights[0].x_angle = (u[10] - 0.5) * PI
+    sc.lights[0].y_angle = (u[11] - 0.5) * PI * 0.66
+    return sc
