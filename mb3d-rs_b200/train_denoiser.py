@@ -120,6 +120,20 @@ def train(card, data, steps, batch=8, piece=128, lr_max=2e-3, seed=1, log=print)
     return dn, time.time() - t0, losses
 
 
+def val_loss(dn, data, lo, hi):
+    """The L1 loss in log space of the denoised held-out pictures (4 and 16
+    rays) against their targets."""
+    torch = _torch()
+    tot = []
+    for i in range(lo, hi, 8):
+        j = min(i + 8, hi)
+        for k in ("r4", "r16"):
+            den = dn.denoise(data[k][i:j].contiguous(), data["alb"][i:j].contiguous(), data["nrm"][i:j].contiguous(),
+                             data["dep"][i:j, ..., 0].contiguous(), depth_scale=1.0)
+            tot.append(float((torch.log1p(den) - torch.log1p(data["tgt"][i:j].clamp(min=0))).abs().mean()))
+    return float(np.mean(tot))
+
+
 def tonemap(x):
     return x / (1.0 + x)
 
@@ -142,7 +156,7 @@ def fallback_tiles(noisy_a, noisy_b, den, tile=16, k=3.0):
         for x in range(0, w - tile + 1, tile):
             sl = (slice(y, y + tile), slice(x, x + tile))
             a, b, d, m = (tonemap(v[sl]) for v in (noisy_a, noisy_b, den, noisy))
-            sigma = np.sqrt(np.mean((a - b) ** 2) / 4.0 / (tile * tile * 3)) + 1e-4
+            sigma = np.sqrt(np.mean((a - b) ** 2) / 4.0 / (tile * tile * 3)) + 1e-3
             n += 1
             if abs(float(np.mean(d - m))) > k * sigma:
                 bad += 1
@@ -208,6 +222,7 @@ def main():
     ap.add_argument("--target-rays", type=int, default=64)
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, nargs="+", default=[2e-3])
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--report", default=None)
     ap.add_argument("--ref-rays", type=int, default=1024)
@@ -215,17 +230,32 @@ def main():
     card = mb3dcu.Card(0)
     report = {}
     if a.what == "train":
-        data, t_data, skipped = make_dataset(card, a.crops, a.target_rays, scenes.C5_DEPTH)
-        print(f"dataset: {a.crops} crops in {t_data:.0f} s ({skipped} empty scenes skipped)", flush=True)
-        dn, t_train, losses = train(card, data, a.steps, batch=a.batch)
-        print(f"trained {a.steps} steps in {t_train:.0f} s, loss {np.mean(losses[:100]):.4f} -> "
-              f"{np.mean(losses[-200:]):.4f}", flush=True)
+        n_val = max(8, a.crops // 25)
+        data, t_data, skipped = make_dataset(card, a.crops + n_val, a.target_rays, scenes.C5_DEPTH)
+        print(f"dataset: {a.crops} + {n_val} held-out crops in {t_data:.0f} s ({skipped} empty scenes skipped)",
+              flush=True)
+        train_part = {k: v[:a.crops] for k, v in data.items()}
+        best = None
+        runs = []
+        for lr in a.lr:
+            dn, t_train, losses = train(card, train_part, a.steps, batch=a.batch, lr_max=lr)
+            vl = val_loss(dn, data, a.crops, a.crops + n_val)
+            print(f"lr {lr}: {a.steps} steps in {t_train:.0f} s, loss {np.mean(losses[:100]):.4f} -> "
+                  f"{np.mean(losses[-200:]):.4f}, held-out {vl:.4f}", flush=True)
+            runs.append(dict(lr=lr, s_train=t_train, loss_first=float(np.mean(losses[:100])),
+                             loss_last=float(np.mean(losses[-200:])), val_loss=vl))
+            if best is None or vl < best[0]:
+                if best is not None:
+                    best[1].close()
+                best = (vl, dn)
+            else:
+                dn.close()
+        dn = best[1]
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
         dn.get_params().astype("<f4").tofile(a.out)
-        report.update(crops=a.crops, target_rays=a.target_rays, steps=a.steps, batch=a.batch, s_data=t_data,
-                      s_train=t_train, loss_first=float(np.mean(losses[:100])),
-                      loss_last=float(np.mean(losses[-200:])))
-        del data
+        report.update(crops=a.crops, held_out=n_val, target_rays=a.target_rays, steps=a.steps, batch=a.batch,
+                      s_data=t_data, runs=runs)
+        del data, train_part
     else:
         dn = mb3dcu.Denoiser(card)
         dn.set_params(np.fromfile(a.out, "<f4"))
