@@ -59,7 +59,21 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="picture size factor (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample size")
+    ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo / denoiser figures")
+    ap.add_argument("--mc-ref-rays", type=int, default=1024)
     return ap.parse_args()
+
+
+def max_over_ranks(x, world, device):
+    """The largest value of x over the ranks (the step time of a weak-scaled
+    run is its slowest rank's)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def frame(rank, scale):
@@ -190,6 +204,81 @@ def march_flops(sc, st):
     return f + st["de_evals"] * FLOPS_PER_DE
 
 
+def depth_of(g, sc):
+    """mzz (depth in step widths) of G-buffer records from their zpos
+    (CalcPPZvals, src/calc.rs:673-676, inverted)."""
+    sw = 2.1345 / (sc.zoom * sc.width)
+    zcorr = np.sin(max(np.deg2rad(sc.fov_y), 1.0) / sc.height)
+    zc_mul = 32767.0 * 256.0 / (np.sqrt((sc.z_end - sc.z_start) * zcorr / sw + 1.0) - 0.999999999)
+    zf = (g["zpos_fine"] >> 8).astype(np.float64)
+    return (((8388352.0 - zf) / zc_mul + 1.0) ** 2 - 1.0) / zcorr
+
+
+def parity_vs_fp64(sc, mixed, fp64):
+    """The mixed march's G-buffer against the plain FP64 march's (the drop-in,
+    itself held to the FP64 oracle by the parity tests)."""
+    a, b = mixed, fp64
+    ha, hb = mb3dcu.hit_mask(a), mb3dcu.hit_mask(b)
+    both = ha & hb
+    da, db = depth_of(a[both], sc), depth_of(b[both], sc)
+    rel = np.abs(da - db) / np.maximum(np.abs(db), 1e-30)
+    return {"hit_agree": float((ha == hb).mean()), "depth_rel_median": float(np.median(rel)),
+            "depth_rel_p99": float(np.percentile(rel, 99)), "depth_within_1e-4": float((rel <= 1e-4).mean()),
+            "pixels_both_hit": int(both.sum())}
+
+
+def mc_figures(card, ref_rays):
+    """The Monte Carlo workload (the hybrid scene at 1920x1080, 4 ambient
+    bounces) on its middle 480x270 rectangle: the 16-ray trace and its
+    denoised picture against an independent plain trace of ref_rays rays."""
+    import torch
+    import train_denoiser as T
+    if not os.path.exists(T.WEIGHTS):
+        return {"unavailable": "no trained weights (mb3d-rs_b200/weights/denoiser.f32)"}
+    sc = scenes.c5_mc()
+    lv = mb3dcu.mc_light_default(sc)
+    rect = (720, 405, 480, 270)
+
+    def trace(rays, ray0=0):
+        r = card.mc_render(sc, mb3dcu.mc_opts(rays, depth=scenes.C5_DEPTH, ray0=ray0, rect=rect), lv,
+                           mb3dcu.FP32_FP64)
+        return r, card.stats()
+
+    card.set_stream(torch.cuda.current_stream().cuda_stream)  # (the denoiser between the timing events)
+    dn = mb3dcu.Denoiser(card)
+    dn.set_params(np.fromfile(T.WEIGHTS, "<f4"))
+    ref, st_ref = trace(ref_rays, 1 << 20)
+    out = {"workload": "c5: hybrid scene 1920x1080, MCDepth 4, light 1 + sky; rectangle 480x270 at (720, 405)",
+           "ref_rays": ref_rays, "ms_ref": st_ref["ms_total"],
+           "mpaths_per_s": rect[2] * rect[3] * ref_rays / st_ref["ms_total"] / 1e3,
+           "de_evals_per_s": st_ref["de_evals"] / st_ref["ms_total"] * 1e3, "levels": []}
+    for rays in (4, 16):
+        r, st = trace(rays)
+        dmax = float(r["depth"].max()) or 1.0
+        ins = [torch.from_numpy(r[k]).cuda()[None] for k in ("radiance", "albedo", "normal", "depth")]
+        dn.denoise(*ins, depth_scale=1.0 / dmax)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        den = dn.denoise(*ins, depth_scale=1.0 / dmax)
+        e1.record()
+        torch.cuda.synchronize()
+        ms_dn = e0.elapsed_time(e1)
+        den = den[0].cpu().numpy()
+        ha, _ = trace(rays // 2, 0)
+        hb, _ = trace(rays // 2, rays // 2)
+        comp, fb = T.fallback_tiles(ha["radiance"], hb["radiance"], den)
+        out["levels"].append({"rays": rays, "ms_trace": st["ms_total"], "ms_denoise": ms_dn,
+                              "psnr_noisy": T.psnr(r["radiance"], ref["radiance"]),
+                              "psnr_denoised": T.psnr(den, ref["radiance"]),
+                              "psnr_with_fallback": T.psnr(comp, ref["radiance"]), "fallback_rate": fb})
+    l16 = out["levels"][1]
+    out["time_ratio_16_denoised_vs_ref"] = (l16["ms_trace"] + l16["ms_denoise"]) / out["ms_ref"]
+    out["psnr_metric"] = "PSNR of x/(1+x) tone-mapped linear records against the plain trace of ref_rays rays"
+    dn.close()
+    card.set_stream(None)
+    return out
+
+
 def load_traffic():
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
@@ -257,11 +346,7 @@ def main():
         launches += st["launches"]
     barrier()
     clocks = clk.stop()
-    ms = statistics.mean(step_ms)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(statistics.mean(step_ms), world, "cuda")
     value = world * npix / (ms / 1000.0) / 1e6
 
     # end to end: the C ABI with a pinned host G-buffer (copy back inside the call)
@@ -278,11 +363,7 @@ def main():
         card.render(sc, prec, out=hnp)
         e2e_ms.append(1000.0 * (time.perf_counter() - t))
     barrier()
-    e2e = statistics.mean(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e = float(t.item())
+    e2e = max_over_ranks(statistics.mean(e2e_ms), world, "cuda")
 
     # roofline of the march kernel (single precision bulk): counted flops per
     # launch over its mean launch time, against the measured FP32 FMA peak
@@ -309,6 +390,32 @@ def main():
            "peaks": {"fp32_fma_tflops": peak32, "fp64_fma_tflops": peak64},
            "counted": {"de_evals": counted["de_evals"], "orbit_its": counted["orbit_its"]},
            "clocks": clocks}
+    if rank == 0:
+        # the plain FP64 march (the drop-in) on the same frame, and the mixed
+        # march's agreement with it
+        mixed_g = np.frombuffer(gbuf.cpu().numpy().tobytes(), dtype=mb3dcu.SILIGHT).copy()
+        card.set_stream(stream.cuda_stream)
+        other = mb3dcu.FP64 if prec == mb3dcu.FP32_FP64 else mb3dcu.FP32_FP64
+        card.render(sc, other, out=gbuf)
+        o_ms = []
+        for _ in range(max(3, args.steps // 2)):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            card.render(sc, other, out=gbuf)
+            e1.record(stream)
+            e1.synchronize()
+            o_ms.append(e0.elapsed_time(e1))
+        other_g = np.frombuffer(gbuf.cpu().numpy().tobytes(), dtype=mb3dcu.SILIGHT).copy()
+        om = statistics.mean(o_ms)
+        if prec == mb3dcu.FP32_FP64:
+            out["fp64_march"] = {"value": npix / (om / 1000.0) / 1e6, "unit": "Mrays/s", "ms_per_step": om,
+                                 "mixed_over_fp64": om / ms}
+            out["parity_vs_fp64"] = parity_vs_fp64(sc, mixed_g, other_g)
+        card.set_stream(None)
+        if not args.no_mc and args.scale == 1.0:
+            out["mc"] = mc_figures(card, args.mc_ref_rays)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(frame(0, args.scale), args.cpu_seconds)
     if rank == 0:
