@@ -13,7 +13,9 @@
  *  - a context is used by one thread at a time; contexts on different
  *    threads may run concurrently (each has its own CUDA stream);
  *  - buffers may be host or device memory (the library finds out which);
- *    host buffers are copied in and out inside the call.
+ *    host buffers are copied in and out inside the call; device buffers are
+ *    read and written on the context's stream (mb3d_cu_set_stream), so a
+ *    caller that fills them on another stream orders the two streams first.
  *
  * Precision modes: MB3D_CU_FP64 is the plain double precision march, the
  * drop-in for the reference's FP64 CPU march.  MB3D_CU_FP32_FP64 marches in

@@ -68,6 +68,8 @@ struct mb3d_cu_ctx {
     uint2 *d_halton = nullptr;
     unsigned char *d_mc = nullptr;
     size_t mc_cap = 0;
+    unsigned char *d_mcs = nullptr;  // the split render's paths, requests, results, list
+    size_t mcs_cap = 0;
     std::mutex mu;
 };
 
@@ -163,6 +165,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_count);
     cudaFree(c->d_halton);
     cudaFree(c->d_mc);
+    cudaFree(c->d_mcs);
     for (auto &ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     for (auto &s : c->fscratch) {
@@ -752,7 +755,7 @@ int mb3d_cu_mc_batch(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, int
     std::memset(&acc, 0, sizeof(acc));
     acc.counters = cnt;
     bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
-    launch_mc(p, m, mixed, true, acc, dq, dr, (unsigned int *)(cnt + 8), n, c->sms, s);
+    launch_mc(p, m, mixed, true, acc, dq, dr, (unsigned int *)(cnt + 8), n, nullptr, c->sms, s);
     c->stats.launches = 1;
     if (int e = check_launch("k_mc (batch)")) return e;
     CU_TRY(cudaEventRecord(c->ev[1], s));
@@ -835,9 +838,10 @@ int mb3d_cu_mc_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_
     if (acc.normal) CU_TRY(cudaMemsetAsync(acc.normal, 0, npix * 12, s));
     if (acc.depth) CU_TRY(cudaMemsetAsync(acc.depth, 0, npix * 4, s));
     bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
-    // the rays in batches of at most 2^30 items, the cancel flag polled between them
+    // the rays in groups of at most 2^30 items, the cancel flag polled between them
     uint32_t per = (uint32_t)std::max<size_t>(1, ((size_t)1 << 30) / npad);
     uint32_t launches = 0;
+    const bool mega = getenv("MB3D_CU_MC_MEGA") != nullptr;  // (the one-kernel form, for comparison)
     for (int b0 = 0; b0 < o->rays; b0 += (int)per) {
         int nb = std::min<int>((int)per, o->rays - b0);
         McDev mb = m;
@@ -845,18 +849,51 @@ int mb3d_cu_mc_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_
         // (the first surface of ray ray0 only)
         McAcc ab = acc;
         if (b0 > 0) ab.albedo = ab.normal = ab.depth = nullptr;
-        unsigned int *queue = (unsigned int *)(acc.counters + 8) + launches;
-        launch_mc(p, mb, mixed, false, ab, nullptr, nullptr, queue, (uint32_t)((size_t)nb * npad), c->sms, s);
-        launches++;
-        if (int e = check_launch("k_mc")) return e;
+        const uint32_t n_items = (uint32_t)((size_t)nb * npad);
+        if (mega) {
+            unsigned int *queue = (unsigned int *)(B + 64);
+            CU_TRY(cudaMemsetAsync(queue, 0, 4, s));
+            launch_mc(p, mb, mixed, false, ab, nullptr, nullptr, queue, n_items, nullptr, c->sms, s);
+            launches++;
+            if (int e = check_launch("k_mc")) return e;
+        } else {
+            // the split render: the paths' logic (k_mc_logic) and their marches
+            // (k_mc in batch mode on the list of waiting paths) in turns
+            const uint32_t slots = std::min<uint32_t>(n_items, 1u << 21);
+            const size_t lb = mc_lane_bytes();
+            size_t s_req = align256((size_t)slots * lb), s_res = s_req + align256((size_t)slots * sizeof(mb3d_cu_mc_req));
+            size_t s_list = s_res + align256((size_t)slots * sizeof(mb3d_cu_mc_res));
+            size_t s_need = s_list + align256((size_t)slots * 4);
+            if (int e = grow((void **)&c->d_mcs, &c->mcs_cap, s_need)) return e;
+            unsigned char *S = c->d_mcs;
+            mb3d_cu_mc_req *reqs = (mb3d_cu_mc_req *)(S + s_req);
+            mb3d_cu_mc_res *res = (mb3d_cu_mc_res *)(S + s_res);
+            uint32_t *list = (uint32_t *)(S + s_list);
+            unsigned int *ctrl = (unsigned int *)(B + 128);  // next item, list length, march queue
+            CU_TRY(cudaMemsetAsync(S, 0, (size_t)slots * lb, s));  // (every path idle)
+            CU_TRY(cudaMemsetAsync(ctrl, 0, 12, s));
+            for (int turn = 0;; turn++) {
+                if (turn > 4000000) return fail(MB3D_CU_EIO, "Monte Carlo turns did not end");
+                CU_TRY(cudaMemsetAsync(ctrl + 1, 0, 8, s));
+                launch_mc_logic(p, mb, ab, S, reqs, res, slots, ctrl, n_items, list, ctrl + 1, c->sms, s);
+                if (int e = check_launch("k_mc_logic")) return e;
+                unsigned int h[2];
+                CU_TRY(cudaMemcpyAsync(h, ctrl, 8, cudaMemcpyDeviceToHost, s));
+                CU_TRY(cudaStreamSynchronize(s));
+                launches++;
+                if (h[1] == 0) {
+                    if (h[0] >= n_items) break;
+                    continue;  // (only padding items were taken this turn)
+                }
+                launch_mc(p, mb, mixed, true, ab, reqs, res, ctrl + 2, h[1], list, c->sms, s);
+                launches++;
+                if (int e = check_launch("k_mc (split)")) return e;
+                if (cancel && (turn & 15) == 15 && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
+            }
+        }
         if (cancel && b0 + (int)per < o->rays) {
             CU_TRY(cudaStreamSynchronize(s));
             if (*cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
-        }
-        if (launches >= 16 && b0 + (int)per < o->rays) {
-            // (the queue counters hold 16 launches; start them again)
-            CU_TRY(cudaMemsetAsync(acc.counters + 8, 0, 64, s));
-            launches = 0;
         }
     }
     launch_mc_final(acc, (uint32_t)npix, o->rays, rad, hb, s);
@@ -875,7 +912,7 @@ int mb3d_cu_mc_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
     c->stats.ms_total = ms;
     c->stats.ms_march = ms;
-    c->stats.launches = (uint32_t)((o->rays + per - 1) / per) + 1;
+    c->stats.launches = launches + 1;
     c->stats.de_evals = hc[0];
     c->stats.mc_inside_rays = (uint32_t)hc[2];
     c->stats.mc_fp64_rays = (uint32_t)hc[3];

@@ -44,7 +44,8 @@ void launch_ao_rays(const DevParams &p, bool mixed, const PostStart *ps, const m
     table(p.fmask).ao_rays(p, mixed, ps, gbuf, count, min_ra, queue, blocks, s);
 }
 void launch_mc(const DevParams &p, const McDev &m, bool mixed, bool batch, const McAcc &acc, const mb3d_cu_mc_req *reqs,
-               mb3d_cu_mc_res *res, unsigned int *queue, uint32_t n_items, int sms, cudaStream_t s) {
+               mb3d_cu_mc_res *res, unsigned int *queue, uint32_t n_items, const uint32_t *list, int sms,
+               cudaStream_t s) {
     static const McTable t1 = mc_table_ip8(), t5 = mc_table_ip8box(), t12 = mc_table_mengerbox(), ta = mc_table_all();
     const McTable *t = &ta;
     switch (kernel_set(p.fmask)) {
@@ -53,7 +54,7 @@ void launch_mc(const DevParams &p, const McDev &m, bool mixed, bool batch, const
         case KSET_MENGERBOX: t = &t12; break;
         default: break;
     }
-    t->run(p, m, mixed, batch, acc, reqs, res, queue, n_items, sms, s);
+    t->run(p, m, mixed, batch, acc, reqs, res, queue, n_items, list, sms, s);
 }
 void launch_de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s) {
     table(p.fmask).de_probe(p, pos, n, de, its, mixed, s);

@@ -85,14 +85,21 @@ int launch_fma_peak(bool fp64, void *out, int blocks, int iters, cudaStream_t s)
 // the Monte Carlo kernels of one formula set (kern_mc_*.cu)
 struct McTable {
     void (*run)(const DevParams &, const McDev &, bool mixed, bool batch, const McAcc &, const mb3d_cu_mc_req *reqs,
-                mb3d_cu_mc_res *res, unsigned int *queue, uint32_t n_items, int sms, cudaStream_t s);
+                mb3d_cu_mc_res *res, unsigned int *queue, uint32_t n_items, const uint32_t *list, int sms,
+                cudaStream_t s);
 };
 McTable mc_table_ip8();
 McTable mc_table_ip8box();
 McTable mc_table_mengerbox();
 McTable mc_table_all();
 void launch_mc(const DevParams &p, const McDev &m, bool mixed, bool batch, const McAcc &acc, const mb3d_cu_mc_req *reqs,
-               mb3d_cu_mc_res *res, unsigned int *queue, uint32_t n_items, int sms, cudaStream_t s);
+               mb3d_cu_mc_res *res, unsigned int *queue, uint32_t n_items, const uint32_t *list, int sms,
+               cudaStream_t s);
+// the split render's logic kernel (kern_mc_all.cu) and the bytes of a path's state
+size_t mc_lane_bytes();
+void launch_mc_logic(const DevParams &p, const McDev &m, const McAcc &acc, void *lanes, mb3d_cu_mc_req *reqs,
+                     const mb3d_cu_mc_res *res, uint32_t n_slots, unsigned int *next, uint32_t n_items, uint32_t *list,
+                     unsigned int *n_list, int sms, cudaStream_t s);
 void launch_mc_final(const McAcc &acc, uint32_t npix, int rays, float *radiance, uint8_t *hit, cudaStream_t s);
 
 }  // namespace mb3dcu

@@ -106,7 +106,8 @@ __device__ __forceinline__ void mc_do_color(const DevParams &p, const DEstate &s
 enum McPhase : int {
     L_IDLE = 0, L_RAY, L_CALC_RAY, L_MSTEP, L_SEC, L_BIS, L_BIT, L_BIT_END, L_NORM, L_NTRY, L_NSAMP, L_MHIT, L_MOPEN,
     L_LIGHT, L_SSTEP, L_SDONE, L_PHONG_END, L_RAY_END, L_ITEM_END,
-    W_M0, W_MSTEP, W_SEC, W_BIS, W_BIT1, W_BIT2, W_N0, W_NK, W_S0, W_SSTEP
+    W_M0, W_MSTEP, W_SEC, W_BIS, W_BIT1, W_BIT2, W_N0, W_NK, W_S0, W_SSTEP,
+    A_RAY, A_SHADOW  // (split render: the path waits for the march kernel's result)
 };
 
 // Everything one lane carries.
@@ -373,10 +374,18 @@ struct McRun {
         for (int turn = 0; turn < 64; turn++) {
             switch (L.phase) {
             case L_RAY:
+                if (BATCH) {  // (render logic: not in the march kernels)
+                    L.phase = L_IDLE;
+                    return;
+                }
                 ray_begin(L);
                 L.phase = L_CALC_RAY;
                 break;
             case L_CALC_RAY: {
+                if (BATCH) {  // (render logic: not in the march kernels)
+                    L.phase = L_IDLE;
+                    return;
+                }
                 // CalcRay's entry
                 if (fabsf(L.ta[0]) * 0.3f + fabsf(L.ta[1]) * 0.59f + fabsf(L.ta[2]) * 0.11f < 1e-4f) {
                     L.phase = L_RAY_END;
@@ -743,6 +752,10 @@ struct McRun {
                 }
                 break;
             case L_LIGHT: {
+                if (BATCH) {  // (render logic: not in the march kernels)
+                    L.phase = L_IDLE;
+                    return;
+                }
                 if (L.li >= m.lv.n_lights) {
                     L.phase = L_PHONG_END;
                     break;
@@ -834,6 +847,10 @@ struct McRun {
                 }
                 break;
             case L_PHONG_END: {
+                if (BATCH) {  // (render logic: not in the march kernels)
+                    L.phase = L_IDLE;
+                    return;
+                }
                 const float ws = (0.25f + 1.0f) * 0.8f;
                 for (int k = 0; k < 3; k++) {
                     float spec = (L.obj_spe[k] * ws) * L.lsd[0][k];
@@ -875,6 +892,10 @@ struct McRun {
                 break;
             }
             case L_RAY_END:
+                if (BATCH) {  // (render logic: not in the march kernels)
+                    L.phase = L_IDLE;
+                    return;
+                }
                 // the ray's light into its pixel's sum
                 for (int k = 0; k < 3; k++) {
                     float sv = fminf(fmaxf(L.tl[k], 0.0f), 400.0f);
@@ -904,7 +925,7 @@ struct McRun {
 template <typename R, int FM, bool BATCH>
 __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_constant__ DevParams p, const __grid_constant__ McDev m,
                                             McAcc acc, const mb3d_cu_mc_req *reqs, mb3d_cu_mc_res *res,
-                                            unsigned int *queue, uint32_t n_items) {
+                                            unsigned int *queue, uint32_t n_items, const uint32_t *list) {
     McRun<BATCH> run(p, m);
     McLane L;
     L.phase = L_IDLE;
@@ -924,7 +945,8 @@ __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_con
         if (item != UINT32_MAX) {
             L.item = item;
             if (BATCH) {
-                const mb3d_cu_mc_req &q = reqs[item];
+                if (list) L.item = list[item];  // (the split render: a path's slot)
+                const mb3d_cu_mc_req &q = reqs[L.item];
                 for (int k = 0; k < 3; k++) L.c[k] = q.pos[k];
                 L.seed = q.seed;
                 L.zz = q.zz;
@@ -961,7 +983,7 @@ __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_con
             if (!open) break;
             continue;
         }
-        const bool wants = L.phase >= W_M0;
+        const bool wants = L.phase >= W_M0 && L.phase <= W_SSTEP;
         if (wants) {
             if (single) {
                 r = de_lock<float, FM, false, true>(p, L.c, L.ms, nullptr, &st, L.sit, L.max_add);
@@ -985,6 +1007,132 @@ __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_con
 }
 
 #ifdef MB3D_MC_COMMON
+// The split render's logic: every path (one per slot, its state in `lanes`)
+// takes in the result of its last march, runs Tracer::ray's logic up to
+// its next march, writes that march's request into its slot and puts the
+// slot on the march list; a path whose ray ended takes the next ray item
+// (warp-aggregated atomicAdd on `next`), so the slots stay full.
+__global__ void __launch_bounds__(128) k_mc_logic(const __grid_constant__ DevParams p, const __grid_constant__ McDev m,
+                                                  McAcc acc, McLane *lanes, mb3d_cu_mc_req *reqs,
+                                                  const mb3d_cu_mc_res *res, uint32_t n_slots, unsigned int *next,
+                                                  uint32_t n_items, uint32_t *list, unsigned int *n_list) {
+    McRun<false> run(p, m);
+    DEr r;
+    r.de = 0.0;
+    r.it = 0;
+    r.need64 = false;
+    DEstate st;
+    st.rout = 0.0; st.rold = 0.0; st.otrap = 0.0;
+    st.v[0] = 0.0; st.v[1] = 0.0; st.v[2] = 0.0;
+    st.smooth_it = 0.0f;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n_slots; base += gridDim.x * blockDim.x) {
+        const uint32_t slot = base + threadIdx.x;
+        const bool mine = slot < n_slots;
+        McLane L;
+        L.phase = L_IDLE;
+        bool queued = false;
+        if (mine) {
+            L = lanes[slot];
+            if (L.phase == A_RAY) {
+                const mb3d_cu_mc_res &o = res[slot];
+                L.seed = o.seed;
+                if (o.kind == 2) {
+                    if (acc.counters) atomicAdd(&acc.counters[2], 1ull);
+                    L.hit = true;  // (Tracer::ray takes the start inside for a hit)
+                    for (int k = 0; k < 3; k++) L.tl[k] = 0.0f;
+                    L.phase = L_RAY_END;
+                } else {
+                    for (int k = 0; k < 3; k++) L.c[k] = o.pos[k];
+                    L.zz = o.zz;
+                    L.zz2 = o.zz2;
+                    L.m_dyn_fog = o.dyn_fog;
+                    if (o.kind == 1) {
+                        for (int k = 0; k < 3; k++) L.normals[k] = o.normals[k];
+                        L.ms = o.ms_de_stop;
+                        L.si_grad = o.si_grad;
+                        L.otrap = o.otrap;
+                        L.de_limited = o.de_limited != 0;
+                        L.phase = L_MHIT;
+                    } else {
+                        L.phase = L_MOPEN;
+                    }
+                }
+            } else if (L.phase == A_SHADOW) {
+                L.max_l = res[slot].len;
+                L.phase = L_SDONE;
+            }
+        }
+        // the logic up to the next march; a finished ray takes the next item
+        for (int turn = 0; turn < 8; turn++) {
+            bool want_item = mine && L.phase == L_IDLE;
+            unsigned int ask = __ballot_sync(0xffffffffu, want_item);
+            if (ask) {
+                int leader = __ffs(ask) - 1;
+                uint32_t b0 = 0;
+                if (lane == leader) b0 = atomicAdd(next, (unsigned int)__popc(ask));
+                b0 = __shfl_sync(0xffffffffu, b0, leader);
+                if (want_item) {
+                    uint32_t item = b0 + (uint32_t)__popc(ask & ((1u << lane) - 1u));
+                    if (item < n_items) {
+                        uint32_t within = item % m.npad;
+                        int x, ly;
+                        item_pixel(within, (int)m.tiles_x, x, ly);
+                        if (x < m.w && ly < m.h) {
+                            L.pix = (uint32_t)ly * (uint32_t)m.w + (uint32_t)x;
+                            L.x1 = m.x0 + x + 1;
+                            L.y = m.y0 + ly;
+                            L.b = m.ray0 + (int)(item / m.npad);
+                            L.aov = L.b == m.ray0;
+                            L.item = item;
+                            L.phase = L_RAY;
+                        }
+                        // (a padding item outside the rectangle: the slot asks again)
+                    } else {
+                        want_item = false;
+                        L.phase = L_IDLE;  // (no rays left: the slot stays empty)
+                        L.item = UINT32_MAX;
+                    }
+                }
+            }
+            if (mine && L.phase != L_IDLE && L.phase != W_M0 && L.phase != W_S0) run.advance(L, r, st, acc, nullptr);
+            bool more = mine && L.phase == L_IDLE && L.item != UINT32_MAX;
+            if (!__any_sync(0xffffffffu, more)) break;
+        }
+        if (mine) {
+            mb3d_cu_mc_req &q = reqs[slot];
+            if (L.phase == W_M0) {
+                for (int k = 0; k < 3; k++) {
+                    q.pos[k] = L.c[k];
+                    q.dir[k] = L.dir[k];
+                }
+                q.zz = L.zz; q.zz2 = L.zz2; q.zzplus = L.zzplus; q.len = L.max_l;
+                q.seed = L.seed; q.kind = 0; q.probe = L.probe ? 1 : 0; q.inside = 0; q.pad = 0;
+                L.phase = A_RAY;
+                queued = true;
+            } else if (L.phase == W_S0) {
+                for (int k = 0; k < 3; k++) {
+                    q.pos[k] = L.c[k];
+                    q.dir[k] = L.sdir[k];
+                }
+                q.zz = L.zz; q.zz2 = L.zz2; q.zzplus = L.zzplus; q.len = L.max_l;
+                q.seed = L.seed; q.kind = 1; q.probe = 0; q.inside = 0; q.pad = 0;
+                L.phase = A_SHADOW;
+                queued = true;
+            }
+            lanes[slot] = L;
+        }
+        unsigned int qm = __ballot_sync(0xffffffffu, queued);
+        if (qm) {
+            int leader = __ffs(qm) - 1;
+            uint32_t b0 = 0;
+            if (lane == leader) b0 = atomicAdd(n_list, (unsigned int)__popc(qm));
+            b0 = __shfl_sync(0xffffffffu, b0, leader);
+            if (queued) list[b0 + (uint32_t)__popc(qm & ((1u << lane) - 1u))] = slot;
+        }
+    }
+}
+
 // the records: the mean light of each pixel's rays, and the hit flags
 __global__ void k_mc_final(McAcc acc, uint32_t npix, int rays, float *radiance, uint8_t *hit) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {

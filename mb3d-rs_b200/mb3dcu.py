@@ -243,8 +243,19 @@ class Card:
 
     def __init__(self, device=0):
         self._ctx = ctypes.c_void_p()
+        self._stream = None
         r = lib().mb3d_cu_init(device, ctypes.byref(self._ctx))
         self._check(r)
+
+    def _order(self, *bufs):
+        """Device buffers from torch: the library's stream does not wait for
+        torch's, so torch's pending work on them (fills, copies, gathers)
+        finishes first, unless the card already runs on torch's stream."""
+        if any(b is not None and not isinstance(b, np.ndarray) for b in bufs):
+            import torch
+            cs = torch.cuda.current_stream()
+            if self._stream != cs.cuda_stream:
+                cs.synchronize()
 
     def close(self):
         if self._ctx:
@@ -264,12 +275,14 @@ class Card:
 
     def set_stream(self, stream_handle):
         self._check(lib().mb3d_cu_set_stream(self._ctx, ctypes.c_void_p(stream_handle or None)))
+        self._stream = stream_handle or None
 
     def march(self, scene, precision=FP32_FP64, row0=0, rows=None, out=None, cancel=None):
         rows = scene.height - row0 if rows is None else rows
         if out is None:
             out = np.zeros(rows * scene.width, dtype=SILIGHT)
         p, _ = _ptr(out)
+        self._order(out)
         cp = ctypes.cast(ctypes.byref(cancel), ctypes.c_void_p) if cancel is not None else None
         self._check(lib().mb3d_cu_march(self._ctx, ctypes.byref(scene), precision, row0, rows, p, cp))
         return out
@@ -277,6 +290,7 @@ class Card:
     def post_on_card(self, scene, gbuf, passes=POST_SHADOW | POST_DEAO, precision=FP32_FP64, row0=0, rows=None):
         rows = scene.height - row0 if rows is None else rows
         p, _ = _ptr(gbuf)
+        self._order(gbuf)
         self._check(lib().mb3d_cu_post(self._ctx, ctypes.byref(scene), precision, passes, row0, rows, p, None))
         return gbuf
 
@@ -284,6 +298,7 @@ class Card:
         if out is None:
             out = np.zeros(scene.height * scene.width, dtype=SILIGHT)
         p, _ = _ptr(out)
+        self._order(out)
         self._check(lib().mb3d_cu_render(self._ctx, ctypes.byref(scene), precision, p, None))
         return out
 
@@ -310,6 +325,7 @@ class Card:
         if out is None:
             out = np.zeros(len(frames) * npix, dtype=SILIGHT)
         p, _ = _ptr(out)
+        self._order(out)
         self._check(lib().mb3d_cu_render_frames(self._ctx, arr, len(frames), precision,
                                                 ctypes.byref(tune) if tune is not None else None, p))
         return out
@@ -342,6 +358,7 @@ class Card:
                 res[k] = np.zeros(shape, dt)
         ptrs = McOut(*[_ptr(res[k])[0] if res[k] is not None else None
                        for k in ("radiance", "albedo", "normal", "depth", "hit")])
+        self._order(*res.values())
         cp = ctypes.cast(ctypes.byref(cancel), ctypes.c_void_p) if cancel is not None else None
         self._check(lib().mb3d_cu_mc_render(self._ctx, ctypes.byref(scene), ctypes.byref(light), ctypes.byref(opts),
                                             precision, ctypes.byref(ptrs), cp))
@@ -427,6 +444,7 @@ class Denoiser:
             depth_scale = _depth_scale(depth)
         if out is None:
             out = np.zeros((n, h, w, 3), np.float32) if isinstance(radiance, np.ndarray) else radiance.new_zeros((n, h, w, 3))
+        self.card._order(radiance, albedo, normal, depth, out)
         self.card._check(lib().mb3d_cu_dn_denoise(self._d, n, h, w, _fptr(radiance), _fptr(albedo), _fptr(normal),
                                                   _fptr(depth), depth_scale, _fptr(out)))
         return out
@@ -436,6 +454,7 @@ class Denoiser:
         if depth_scale is None:
             depth_scale = _depth_scale(depth)
         loss = ctypes.c_float()
+        self.card._order(radiance, target, albedo, normal, depth)
         self.card._check(lib().mb3d_cu_dn_train_step(self._d, n, h, w, _fptr(radiance), _fptr(albedo), _fptr(normal),
                                                      _fptr(depth), depth_scale, _fptr(target), lr, ctypes.byref(loss)))
         return loss.value
@@ -444,6 +463,7 @@ class Denoiser:
         n, h, w = self._shape(radiance)
         loss = ctypes.c_float()
         g = np.zeros(self.n_params, np.float32)
+        self.card._order(radiance, target, albedo, normal, depth)
         self.card._check(lib().mb3d_cu_dn_gradient(self._d, n, h, w, _fptr(radiance), _fptr(albedo), _fptr(normal),
                                                    _fptr(depth), depth_scale, _fptr(target), ctypes.byref(loss),
                                                    g.ctypes.data))

@@ -93,3 +93,23 @@ def test_training_lowers_the_loss(card):
         assert odd.shape == (1, 50, 37, 3) and np.isfinite(odd).all()
     finally:
         dn.close()
+
+
+def test_device_inputs_made_by_torch_are_ready(card):
+    """Inputs that torch has only just computed on its own stream: the binding
+    orders torch's stream before the library's, so the denoised picture is
+    the one of the finished inputs (the same as from host arrays)."""
+    import torch
+    rng = np.random.default_rng(11)
+    dn = mb3dcu.Denoiser(card, seed=2)
+    try:
+        rad, alb, nrm, dep, _ = _batch(rng, 2, 64, 96)
+        want = dn.denoise(rad, alb, nrm, dep, depth_scale=1.0)
+        big = torch.randn(4096, 4096, device="cuda")
+        for _ in range(4):
+            big = big @ big  # (keeps torch's stream busy)
+        t = [torch.from_numpy(a).cuda(non_blocking=True) * 1.0 + 0.0 * big[0, 0] for a in (rad, alb, nrm, dep)]
+        got = dn.denoise(*t, depth_scale=1.0)
+        assert np.array_equal(got.cpu().numpy(), want)
+    finally:
+        dn.close()

@@ -15,6 +15,7 @@ variant of the same estimator: held to the oracle by the picture's mean
 and by its noise.
 """
 import ctypes
+import os  # noqa: F401
 
 import numpy as np
 import pytest
@@ -180,3 +181,17 @@ def test_mc_errors(card):
     with pytest.raises(mb3dcu.CardError) as e:
         card.mc_render(sc, mb3dcu.mc_opts(2), lv, cancel=flag)
     assert e.value.status == mb3dcu.ECANCELED
+
+
+def test_split_render_equals_one_kernel_render(card, monkeypatch):
+    """The split render (logic kernel + list-fed march kernel, the default)
+    traces the same rays as the one-kernel form: the same records."""
+    sc = scenes.scaled(scenes.c2_hybrid(), 160, 90)
+    lv = mb3dcu.mc_light_default(sc)
+    for prec in (mb3dcu.FP64, mb3dcu.FP32_FP64):
+        split = card.mc_render(sc, mb3dcu.mc_opts(8, depth=4), lv, prec)
+        monkeypatch.setenv("MB3D_CU_MC_MEGA", "1")
+        one = card.mc_render(sc, mb3dcu.mc_opts(8, depth=4), lv, prec)
+        monkeypatch.delenv("MB3D_CU_MC_MEGA")
+        for k in ("radiance", "albedo", "normal", "depth", "hit"):
+            assert split[k].tobytes() == one[k].tobytes(), (prec, k)
