@@ -247,7 +247,7 @@ def mc_figures(card, ref_rays):
     card.set_stream(torch.cuda.current_stream().cuda_stream)  # (the denoiser between the timing events)
     dn = mb3dcu.Denoiser(card)
     dn.set_params(np.fromfile(T.WEIGHTS, "<f4"))
-    ref, st_ref = trace(ref_rays, 1 << 20)
+    ref, st_ref = trace(ref_rays, 4096)  # (independent rays, each with its own Halton record)
     out = {"workload": "c5: hybrid scene 1920x1080, MCDepth 4, light 1 + sky; rectangle 480x270 at (720, 405)",
            "ref_rays": ref_rays, "ms_ref": st_ref["ms_total"],
            "mpaths_per_s": rect[2] * rect[3] * ref_rays / st_ref["ms_total"] / 1e3,

@@ -319,6 +319,9 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
         }
         out.it = it;
     }
+    // (single precision that overflowed, e.g. a vanishing gradient sum with
+    // exp(-ln R) underflowing: the double precision DE decides)
+    if (sizeof(R) == 4 && !isfinite(out.de)) out.need64 = true;
     double mn = (double)ms_de_stop * 0.25;
     if (out.de < mn || isnan(out.de)) out.de = mn;
     return out;

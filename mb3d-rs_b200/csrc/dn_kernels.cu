@@ -374,7 +374,8 @@ __global__ void k_up2_bwd(const __nv_bfloat16 *dout, int out_c, int out_off, int
 }
 
 // the network's input: log(1 + radiance), albedo, normal, depth / its
-// maximum, zero channels 10..15; pixels outside (w_src, h_src) are zero.
+// maximum, zero channels 10..15; pixels outside (w_src, h_src) and values
+// that are not finite are zero.
 // Sources are float (h_src, w_src, 3) per image, images one after another.
 __global__ void k_pack_input(const float *rad, const float *alb, const float *nrm, const float *dep, float depth_scale,
                              int n, int h_src, int w_src, int h, int w, __nv_bfloat16 *out) {
@@ -394,6 +395,9 @@ __global__ void k_pack_input(const float *rad, const float *alb, const float *nr
             }
             if (dep) v[9] = dep[s] * depth_scale;
         }
+#pragma unroll
+        for (int c = 0; c < 10; c++)
+            if (!isfinite(v[c])) v[c] = 0.0f;  // (a non-finite guide would poison the gradients)
         __nv_bfloat16 *o = out + i * 16;
 #pragma unroll
         for (int c = 0; c < 16; c += 2) *reinterpret_cast<__nv_bfloat162 *>(o + c) = __floats2bfloat162_rn(v[c], v[c + 1]);

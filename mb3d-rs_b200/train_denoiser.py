@@ -71,10 +71,11 @@ def make_dataset(card, n_crops, target_rays, depth, size=256, seed=scenes.TRAIN_
         t = render_set(card, sc, target_rays, 16, depth, torch, False)
         data["r4"][i] = a["radiance"]
         data["r16"][i] = (a["radiance"] * 4 + b["radiance"] * 12) / 16
-        data["alb"][i] = a["albedo"]
-        data["nrm"][i] = a["normal"]
-        dmax = a["depth"].max()
-        data["dep"][i, ..., 0] = a["depth"] / dmax if dmax > 0 else a["depth"]
+        data["alb"][i] = torch.nan_to_num(a["albedo"], 0.0, 0.0, 0.0)
+        data["nrm"][i] = torch.nan_to_num(a["normal"], 0.0, 0.0, 0.0)
+        d = torch.nan_to_num(a["depth"], 0.0, 0.0, 0.0)
+        dmax = d.max()
+        data["dep"][i, ..., 0] = d / dmax if dmax > 0 else d
         data["tgt"][i] = t["radiance"]
         i += 1
         if i % 200 == 0:
@@ -176,7 +177,7 @@ def evaluate(card, dn, rect=(720, 405, 480, 270), ref_rays=1024, log=print):
         r = card.mc_render(sc, o, lv, mb3dcu.FP32_FP64)
         return r, card.stats()["ms_total"]
 
-    ref, ms_ref = trace(ref_rays, ray0=1 << 20)  # (rays of their own: independent of the inputs)
+    ref, ms_ref = trace(ref_rays, ray0=4096)  # (rays of their own, each with its own Halton record (< 65536))
     res = {"rect": list(rect), "ref_rays": ref_rays, "ms_ref": ms_ref, "levels": []}
     for rays in (4, 8, 16, 32, 64):
         r, ms = trace(rays)
