@@ -892,17 +892,15 @@ struct McRun {
                 break;
             }
             case L_RAY_END:
-                if (BATCH) {  // (render logic: not in the march kernels)
-                    L.phase = L_IDLE;
-                    return;
+                if (!BATCH) {  // (render logic: not in the march kernels)
+                    // the ray's light into its pixel's sum
+                    for (int k = 0; k < 3; k++) {
+                        float sv = fminf(fmaxf(L.tl[k], 0.0f), 400.0f);
+                        unsigned long long q = (unsigned long long)rint((double)sv * 4294967296.0);
+                        if (q) atomicAdd(&acc.sum[3 * L.pix + k], q);
+                    }
+                    if (L.hit) atomicOr(&acc.hit[L.pix], 1u);
                 }
-                // the ray's light into its pixel's sum
-                for (int k = 0; k < 3; k++) {
-                    float sv = fminf(fmaxf(L.tl[k], 0.0f), 400.0f);
-                    unsigned long long q = (unsigned long long)rint((double)sv * 4294967296.0);
-                    if (q) atomicAdd(&acc.sum[3 * L.pix + k], q);
-                }
-                if (L.hit) atomicOr(&acc.hit[L.pix], 1u);
                 L.phase = L_IDLE;
                 return;
             case L_ITEM_END:
@@ -919,8 +917,17 @@ struct McRun {
 // The persistent kernel.  BATCH: the items are the march requests `reqs`
 // (results into `res`); else item i is ray ray0 + i / npad of pixel i % npad
 // (8x4 tiles), so that neighbouring lanes trace neighbouring pixels.
+// the double precision DE where single precision cannot resolve it: out of
+// line in the single precision kernel (rare; keeps the loop's code small)
+template <int FM>
+__device__ __noinline__ DEr mc_de64(const DevParams &p, double c0, double c1, double c2, float ms, DEstate *st, bool sit,
+                                    int max_add) {
+    const double c[3] = {c0, c1, c2};
+    return de_lock<double, FM, false, true>(p, c, ms, nullptr, st, sit, max_add);
+}
+
 #ifndef MB3D_MC_MIN_BLOCKS
-#define MB3D_MC_MIN_BLOCKS 6  // (measured best: spills to L1 beat fewer resident warps)
+#define MB3D_MC_MIN_BLOCKS 3  // (measured best of 2..6 on the 1920x1080 Monte Carlo workload)
 #endif
 template <typename R, int FM, bool BATCH>
 __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_constant__ DevParams p, const __grid_constant__ McDev m,
@@ -988,7 +995,7 @@ __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_con
             if (single) {
                 r = de_lock<float, FM, false, true>(p, L.c, L.ms, nullptr, &st, L.sit, L.max_add);
                 if (r.need64) {
-                    r = de_lock<double, FM, false, true>(p, L.c, L.ms, nullptr, &st, L.sit, L.max_add);
+                    r = mc_de64<FM>(p, L.c[0], L.c[1], L.c[2], L.ms, &st, L.sit, L.max_add);
                     fb++;
                 }
             } else {
