@@ -1,0 +1,51 @@
+"""Small fixed workloads for profiling runs (ncu), one per hot kernel family.
+
+    python mb3d-rs_b200/profile_cases.py mc        # Monte Carlo: C2 scene 480x270, 4 rays, MCDepth 4, mixed
+    python mb3d-rs_b200/profile_cases.py denoise   # the denoiser on one 1920x1080 picture (6 passes)
+
+The Calculate 3D kernels are profiled through bench.py (--scale 0.25).
+"""
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import numpy as np  # noqa: E402
+
+import mb3dcu  # noqa: E402
+import scenes  # noqa: E402
+
+
+def mc():
+    card = mb3dcu.Card(0)
+    sc = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    lv = mb3dcu.mc_light_default(sc)
+    card.mc_render(sc, mb3dcu.mc_opts(4, depth=4), lv, mb3dcu.FP32_FP64)
+    st = card.stats()
+    print("ok", st["ms_total"], st["de_evals"])
+
+
+def denoise():
+    import torch
+    card = mb3dcu.Card(0)
+    dn = mb3dcu.Denoiser(card)
+    h, w = 1080, 1920
+    rng = np.random.default_rng(0)
+    rad = torch.from_numpy(rng.gamma(1.0, 0.4, (1, h, w, 3)).astype(np.float32)).cuda()
+    alb = torch.rand((1, h, w, 3), device="cuda")
+    nrm = torch.rand((1, h, w, 3), device="cuda")
+    dep = torch.rand((1, h, w), device="cuda")
+    out = dn.denoise(rad, alb, nrm, dep, depth_scale=1.0)
+    torch.cuda.synchronize()
+    card.set_stream(torch.cuda.current_stream().cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        dn.denoise(rad, alb, nrm, dep, depth_scale=1.0, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    print("ok denoise 1920x1080 ms", e0.elapsed_time(e1) / 5)
+
+
+if __name__ == "__main__":
+    {"mc": mc, "denoise": denoise}[sys.argv[1]]()
