@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample size")
     ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo / denoiser figures")
     ap.add_argument("--mc-ref-rays", type=int, default=1024)
+    ap.add_argument("--no-configs", action="store_true", help="skip the plain bulb, deep zoom and flight figures")
     return ap.parse_args()
 
 
@@ -279,6 +280,71 @@ def mc_figures(card, ref_rays):
     return out
 
 
+def _timed_render(card, sc, prec, gbuf, flush, stream, reps):
+    import torch
+    card.render(sc, prec, out=gbuf)
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        card.render(sc, prec, out=gbuf)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return statistics.mean(ms)
+
+
+def config_figures(card, flush, stream, reps=3):
+    """The other workloads, one GPU, device-resident outputs: the plain
+    Mandelbulb (640x480) and the deep zoom (1920x1080) in both precisions
+    with the mixed march's agreement with the FP64 one; the 240-frame
+    1280x720 Menger/Amazing Box flight through one CUDA graph with the
+    launch settings the autotuner picked on 8 sample frames."""
+    import torch
+    card.set_stream(stream.cuda_stream)
+    out = {}
+    for name, sc in (("c1_plain_bulb_640x480", scenes.c1_plain_bulb()), ("c3_deep_zoom_1920x1080", scenes.c3())):
+        npix = sc.width * sc.height
+        gbuf = torch.empty(npix * 20, dtype=torch.uint8, device="cuda")
+        ms_m = _timed_render(card, sc, mb3dcu.FP32_FP64, gbuf, flush, stream, reps)
+        g_m = np.frombuffer(gbuf.cpu().numpy().tobytes(), dtype=mb3dcu.SILIGHT).copy()
+        fp64_pix = card.stats()["fp64_pixels"]
+        ms_d = _timed_render(card, sc, mb3dcu.FP64, gbuf, flush, stream, reps)
+        g_d = np.frombuffer(gbuf.cpu().numpy().tobytes(), dtype=mb3dcu.SILIGHT).copy()
+        out[name] = {"mixed_mrays_s": npix / (ms_m / 1000.0) / 1e6, "mixed_ms": ms_m,
+                     "fp64_mrays_s": npix / (ms_d / 1000.0) / 1e6, "fp64_ms": ms_d, "mixed_over_fp64": ms_d / ms_m,
+                     "mixed_fp64_fallback_pixels": fp64_pix, "parity_vs_fp64": parity_vs_fp64(sc, g_m, g_d)}
+        del gbuf
+    frames = scenes.c4_frames(240)
+    npix = frames[0].width * frames[0].height
+    gbuf = torch.empty(len(frames) * npix * 20, dtype=torch.uint8, device="cuda")
+    t0 = time.perf_counter()
+    tune = card.autotune(frames, 8)
+    tune_s = time.perf_counter() - t0
+    card.render_frames(frames, mb3dcu.FP32_FP64, tune, out=gbuf)
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        card.render_frames(frames, mb3dcu.FP32_FP64, tune, out=gbuf)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    st = card.stats()
+    m = statistics.mean(ms)
+    out["c4_flight_240x1280x720"] = {
+        "mrays_s": len(frames) * npix / (m / 1000.0) / 1e6, "ms_all_frames": m, "ms_per_frame": m / len(frames),
+        "tune": {"blocks_per_sm": tune.blocks_per_sm, "refill_min": tune.refill_min, "streams": tune.streams},
+        "autotune_s": tune_s, "launches_per_call": st["launches"]}
+    del gbuf
+    card.set_stream(None)
+    return out
+
+
 def load_traffic():
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
@@ -414,6 +480,8 @@ def main():
                                  "mixed_over_fp64": om / ms}
             out["parity_vs_fp64"] = parity_vs_fp64(sc, mixed_g, other_g)
         card.set_stream(None)
+        if not args.no_configs and args.scale == 1.0:
+            out["configs"] = config_figures(card, flush, stream)
         if not args.no_mc and args.scale == 1.0:
             out["mc"] = mc_figures(card, args.mc_ref_rays)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -215,7 +215,9 @@ typedef struct mb3d_cu_stats {
     float ms_deao;
     float ms_total;       /* first launch to last, device time */
     uint32_t launches;    /* this library's kernel launches in the call */
-    uint32_t fp64_pixels; /* pixels the mixed mode marched in double precision */
+    uint32_t fp64_pixels; /* mixed mode: the pixels marched in double precision from the start plane or finished
+                           * by the per-thread double precision marcher (all of them where the zoom needs double
+                           * precision throughout); 0 in the FP64 mode */
     uint64_t de_evals;    /* DE evaluations of the march kernel (counting mode only, else 0) */
     uint64_t orbit_its[6];/* formula iterations per slot, all orbits (counting mode only) */
     uint32_t mc_inside_rays; /* Monte Carlo rays that started inside the set (left dark) */

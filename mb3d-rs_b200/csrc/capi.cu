@@ -43,6 +43,8 @@ struct mb3d_cu_ctx {
     float *d_minra = nullptr;     // the DE AO rays' openness
     size_t minra_cap = 0;
     unsigned int *d_counters = nullptr;
+    unsigned int *h_counters = nullptr;  // (pinned) the march's list lengths, read back with each call
+    bool read_slow = false;
     double *d_probe = nullptr;
     size_t probe_cap = 0;
     cudaEvent_t ev[8] = {};
@@ -141,7 +143,8 @@ int mb3d_cu_init(int device, mb3d_cu_ctx **out) {
     }
     c->stream = c->own;
     for (auto &ev : c->ev) cudaEventCreate(&ev);
-    if (cudaMalloc(&c->d_counters, 64 * sizeof(unsigned int)) != cudaSuccess) {
+    if (cudaMalloc(&c->d_counters, 64 * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMallocHost(&c->h_counters, 16 * sizeof(unsigned int)) != cudaSuccess) {
         mb3d_cu_free(c);
         return fail(MB3D_CU_ENOMEM, "device memory");
     }
@@ -161,6 +164,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_ps);
     cudaFree(c->d_minra);
     cudaFree(c->d_counters);
+    cudaFreeHost(c->h_counters);
     cudaFree(c->d_probe);
     cudaFree(c->d_count);
     cudaFree(c->d_halton);
@@ -238,6 +242,10 @@ static int march_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int r
     if (int r = check_launch("k_finish")) return r;
     CU_TRY(cudaEventRecord(c->ev[2], s));
     c->stats.launches += 3;
+    // the slow list's length: the mixed mode's pixels finished by the
+    // per-thread double precision marcher
+    c->read_slow = mixed;
+    if (mixed) CU_TRY(cudaMemcpyAsync(c->h_counters, c->d_counters, 4 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
     return 0;
 }
 
@@ -283,6 +291,8 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
 static int finish_call(mb3d_cu_ctx *c, bool marched, bool posted) {
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    if (marched && c->read_slow) c->stats.fp64_pixels = c->h_counters[2];
+    c->read_slow = false;
     if (marched && c->counting && c->d_count) {
         unsigned long long h[16];
         CU_TRY(cudaMemcpy(h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost));

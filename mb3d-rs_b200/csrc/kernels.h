@@ -23,8 +23,7 @@ struct Hand {
     int32_t it;        // the iteration count at the surface (plain march)
 };
 #define HAND_FULL 1u     // march the whole pixel in double precision
-#define HAND_STEPPED 2u  // the hand-over came right after a step
-#define HAND_FIRST 4u    // the random first step is still to come
+#define HAND_HALF 2u     // the state is right after the half step back (with its step factor rsf)
 #define HAND_REMARCH 8u  // march on in double precision from this state
 
 // Where a post pass starts on a surface pixel.

@@ -30,6 +30,9 @@
 #ifndef MB3D_MIN_BLOCKS
 #define MB3D_MIN_BLOCKS 3
 #endif
+#ifndef MB3D_MIN_BLOCKS_MARCH
+#define MB3D_MIN_BLOCKS_MARCH MB3D_MIN_BLOCKS
+#endif
 
 namespace mb3dcu {
 
@@ -102,7 +105,10 @@ __device__ __forceinline__ float de_stop_at(const DevParams &p, double zz) {
 // surfaces are handed to the finish where they were found.  R = float: the
 // single precision bulk march; a surface is handed over from the last point
 // where the DE was still >= hand_margin x the DE stop (at most hand_back
-// steps back) and the finish marches on from there in double precision.
+// steps back) and the finish marches on from there in double precision; a
+// ray whose single precision DE cannot decide (need64) is handed over from
+// where it is, and only one that needs double precision at the start plane
+// is marched whole by the per-thread finish.
 
 #define PH_IDLE 0
 #define PH_START 1
@@ -110,7 +116,7 @@ __device__ __forceinline__ float de_stop_at(const DevParams &p, double zz) {
 #define PH_HALF 3
 
 template <typename R, int FM, bool COUNT>
-__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_march(const __grid_constant__ DevParams p, int row0, int rows,
+__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_MARCH) k_march(const __grid_constant__ DevParams p, int row0, int rows,
                                                mb3d_cu_silight *out, Hand *list, unsigned int *counters,
                                                unsigned long long *gcount) {
     const bool MIXED = sizeof(R) == 4;
@@ -147,7 +153,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_march(const __grid_con
             if (!open) break;
             continue;
         }
-        bool hand = false, full = false, done_bg = false;
+        bool hand = false, full = false, done_bg = false, resume = false;
         double cur_de = 0.0;
         int cur_it = 0;
         if (phase != PH_IDLE) {
@@ -158,7 +164,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_march(const __grid_con
             bool skip_half = false, decide = true;
             if (MIXED && r.need64) {
                 hand = true;
-                full = true;
+                full = phase == PH_START;
+                resume = !full;
                 decide = false;
             } else if (phase == PH_START) {
                 if (it >= p.max_it || dtmp < (double)ms) {
@@ -245,6 +252,12 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_march(const __grid_con
                     h.it = cur_it;
                     h.step_count = step_count;
                     h.c[0] = c[0]; h.c[1] = c[1]; h.c[2] = c[2];
+                } else if (resume) {
+                    h.flags = HAND_REMARCH | (phase == PH_HALF ? HAND_HALF : 0u);
+                    h.mzz = mzz;
+                    h.last_step = last_step;
+                    h.last_de = last_de;
+                    h.step_count = step_count;
                 } else if (nb < 0) {
                     h.flags = HAND_FULL;  // no state to go back to: all in double
                 } else {
@@ -299,15 +312,16 @@ __global__ void __launch_bounds__(128) k_finish_slow(const __grid_constant__ Dev
             if (h.flags & HAND_REMARCH) {
                 for (int k = 0; k < 3; k++) m.it.c[k] = c0[k] + m.vfov[k] * h.mzz;
                 double dtmp = m.calc_de();
-                float rsf = 1.0f;
-                if (h.mzz > 0.0) {
+                const bool half = (h.flags & HAND_HALF) != 0;
+                float rsf = half ? h.rsf : 1.0f;
+                if (h.mzz > 0.0 && !half) {
                     if (dtmp > h.last_de + h.last_step) dtmp = h.last_de + h.last_step;
                     if (h.last_de > dtmp + 1e-30) {
                         double t = h.last_step / (h.last_de - dtmp);
                         rsf = t < 1.0 ? (float)fmax(0.5, t) : 1.0f;
                     }
                 }
-                m.march_from(si, dtmp, h.last_step, rsf, false, h.step_count);
+                m.march_from(si, dtmp, h.last_step, rsf, false, h.step_count, half);
             } else {
                 // a surface, exactly where it was found
                 m.it.c[0] = h.c[0]; m.it.c[1] = h.c[1]; m.it.c[2] = h.c[2];
@@ -320,12 +334,14 @@ __global__ void __launch_bounds__(128) k_finish_slow(const __grid_constant__ Dev
     }
 }
 
-// The finish of every handed-over ray as a wavefront, double precision for
-// the march and the binary search, RN for the normals (double: the plain
-// march; single: the mixed one): the rest of the reference's loop from the
-// hand-over state (src/calc.rs:2539-2640), RMdoBinSearch (:1706-1734),
+// The finish of every handed-over ray as a wavefront, in double precision:
+// the rest of the reference's loop from the hand-over state
+// (src/calc.rs:2539-2640), RMdoBinSearch (:1706-1734) on a DE-limited
+// surface, RMdoBinSearchIt (:1737-1791) on one the iteration count limits,
 // RMCalculateNormals (:1813-1906, unsmoothed), the colour and the depth
-// (:2496-2507).  One DE per trip; the rare cases go to the slow list.
+// (:2496-2507).  One DE per trip; the rare cases (a ray marched whole, the
+// smoothed normals, normals on the iteration count, colour on an iteration)
+// go to the slow list.
 #define F_IDLE 0
 #define F_REMARCH 1
 #define F_STEP 2
@@ -334,24 +350,29 @@ __global__ void __launch_bounds__(128) k_finish_slow(const __grid_constant__ Dev
 #define F_NC 5
 #define F_NSP 6
 #define F_NSM 7
+#define F_BSI1 8  // RMdoBinSearchIt: the DE at the stepped position
+#define F_BSI2 9  // ... and 0.001 behind it
 
-template <typename RN, int FM>
+template <int FM>
 __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_constant__ DevParams p, int row0, const Hand *list,
                                                 unsigned int *counters, Hand *slow, mb3d_cu_silight *out) {
     const uint32_t n_items = counters[0];
+    // RMdoBinSearchIt's target count and its limit (the search iterates once more)
+    const float bsi_yp = (float)p.max_it - 0.99f, bsi_top = (float)(p.max_it + 1) - 0.1f;
     int phase = F_IDLE;
     bool open = true;
     uint32_t pix = 0;
     double c[3] = {0, 0, 0}, vf[3] = {0, 0, 0}, ct[3] = {0, 0, 0}, nrm[3] = {0, 0, 0};
-    double mzz = 0, last_step = 0, last_de = 0, dt1 = 0, noffset = 0, a_plus = 0, dtmp = 0;
-    float ms = 0.f, rsf = 1.f, step_count = 0.f, nn = 0.f;
+    double mzz = 0, last_step = 0, last_de = 0, dt1 = 0, noffset = 0, a_plus = 0, dtmp = 0, dmul = 1.0;
+    float ms = 0.f, rsf = 1.f, step_count = 0.f, nn = 0.f, b_last_si = 0.f, b_last_dif = 0.f;
     int itmp = 0, k_ax = 0;
+    bool it_limited = false, b_first = false;
     unsigned int guard = 0;
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
         uint32_t item = warp_take(phase == F_IDLE, &counters[3], n_items, p.refill_min, open);
         bool to_slow = false;
         Hand hs;
-        int entry = 0;  // 1: a march state to evaluate, 2: a surface already evaluated
+        int entry = 0;  // 2: a surface already evaluated (the plain march)
         int it_in = 0;
         if (item != UINT32_MAX) {
             Hand h = list[item];
@@ -370,9 +391,15 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
                 last_de = h.last_de;
                 rsf = 1.0f;
                 guard = 0;
+                it_limited = false;
                 if (h.flags & HAND_REMARCH) {
                     for (int k = 0; k < 3; k++) c[k] = c0[k] + vf[k] * mzz;
-                    phase = F_REMARCH;
+                    if (h.flags & HAND_HALF) {
+                        rsf = h.rsf;
+                        phase = F_HALF;
+                    } else {
+                        phase = F_REMARCH;
+                    }
                 } else {
                     c[0] = h.c[0]; c[1] = h.c[1]; c[2] = h.c[2];
                     dtmp = h.dtmp;
@@ -383,7 +410,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
             }
         }
         if (item != UINT32_MAX && to_slow) phase = F_IDLE;
-        // ---- one DE for the lanes whose phase asks for one
+        // ---- one DE for the lanes whose phase asks for one (the iteration
+        // count search: with the smoothed count and one more iteration)
         DEr r;
         r.de = 0.0;
         r.it = 0;
@@ -392,14 +420,9 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
         st.rout = st.rold = st.otrap = 0.0;
         st.v[0] = st.v[1] = st.v[2] = 0.0;
         st.smooth_it = 0.f;
-        bool normal_phase = phase >= F_NC;
         if (phase != F_IDLE && entry != 2) {
-            if (sizeof(RN) == 8 || !normal_phase) {
-                r = de_lock<double, FM, false, true>(p, c, ms, nullptr, &st, phase == F_NC);
-            } else {
-                r = de_lock<RN, FM, false, true>(p, c, ms, nullptr, &st, phase == F_NC);
-                if (r.need64) r = de_lock<double, FM, false, true>(p, c, ms, nullptr, &st, phase == F_NC);
-            }
+            const bool bsi = phase >= F_BSI1;
+            r = de_lock<double, FM, false, true>(p, c, ms, nullptr, &st, phase == F_NC || bsi, bsi ? 1 : 0);
         }
         if (entry == 2) {
             r.de = dtmp;
@@ -408,7 +431,9 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
         // ---- the per-lane machine
         bool done_bg = false, done_surf = false;
         if (phase != F_IDLE) {
-            int go = 0;  // 1: decide the march step, 2: the surface, 3: bisection loop, 4: normals begin
+            // 1: decide the march step, 2: the surface, 3: bisection loop,
+            // 5: iteration count search loop, 4: normals begin
+            int go = 0;
             bool skip_half = false;
             if (++guard > 4000000u) {
                 done_bg = true;  // (a cap the reference's guards never reach)
@@ -436,6 +461,35 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
                 if (r.it >= p.max_it) dt1 = -fabs(dt1);
                 else dt1 = (dtmp - (double)ms) < 0.0 ? fabs(dt1) * -0.55 : fabs(dt1) * 0.55;
                 go = 3;
+            } else if (phase == F_BSI1) {
+                float si_now = st.smooth_it;
+                if (!b_first && b_last_dif < fabsf(bsi_yp - si_now)) {
+                    // worse than the last position: back there, smaller steps
+                    mzz -= dt1;
+                    add_w(c, vf, -dt1);
+                    si_now = b_last_si;
+                    dmul *= dt1 > 0.0 ? 0.5 : 0.7;
+                }
+                b_last_dif = fabsf(bsi_yp - si_now);
+                b_last_si = si_now;
+                if (si_now > bsi_top) {
+                    dt1 = -3.0;
+                    go = 5;
+                } else {
+                    mzz -= 0.001;
+                    add_w(c, vf, -0.001);
+                    phase = F_BSI2;
+                }
+            } else if (phase == F_BSI2) {
+                float s2 = st.smooth_it;
+                float rr = b_last_si - s2;
+                if (fabsf(rr) < 1e-30f) dt1 = (b_last_si < s2 ? 1.0 : 0.0) - 0.5;
+                else if (rr < 0.0f) dt1 = (double)__fdiv_rn(bsi_yp - s2, rr * 500.0f);
+                else dt1 = (double)__fdiv_rn(bsi_yp - s2, rr * 1000.0f);
+                if (dt1 > 4.0) dt1 = sqrt(dt1) * 2.0;
+                else if (dt1 < -9.0) dt1 = sqrt(-dt1) * -3.0;
+                dt1 = dt1 * dmul + 0.0005;
+                go = 5;
             } else if (phase == F_NC) {
                 nn = st.smooth_it;
                 k_ax = 0;
@@ -491,21 +545,18 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
                 }
             }
             if (go == 2) {
-                // surface_found: the binary search on the DE, or the slow list
-                if (!(r.it < p.max_it || dtmp < (double)ms)) {
-                    to_slow = true;
-                    hs.pix = pix;
-                    hs.flags = 0;
-                    hs.mzz = mzz;
-                    hs.last_step = last_step;
-                    hs.last_de = last_de;
-                    hs.dtmp = dtmp;
-                    hs.it = r.it;
-                    hs.step_count = step_count;
-                    hs.c[0] = c[0]; hs.c[1] = c[1]; hs.c[2] = c[2];
-                    phase = F_IDLE;
-                } else if (p.de_add_steps == 0) {
+                // surface_found: the binary search on the DE or on the
+                // iteration count, then the normals
+                it_limited = !(r.it < p.max_it || dtmp < (double)ms);
+                if (p.de_add_steps == 0) {
                     go = 4;
+                } else if (it_limited) {
+                    itmp = p.de_add_steps;
+                    dt1 = 0.0;
+                    dmul = 1.0;
+                    b_first = true;
+                    add_w(c, vf, 0.0);  // (the search's first step is 0)
+                    phase = F_BSI1;
                 } else {
                     itmp = p.de_add_steps;
                     dt1 = last_step * -0.5;
@@ -523,6 +574,16 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
                     else phase = F_BISECT;
                 }
             }
+            if (go == 5) {
+                b_first = false;
+                if (--itmp < 0) {
+                    go = 4;
+                } else {
+                    mzz += dt1;
+                    add_w(c, vf, dt1);
+                    phase = F_BSI1;
+                }
+            }
             if (go == 4) {
                 noffset = (double)fminf(p.de_stop, 1.0f) * (1.0 + mzz * (double)p.de_stop_factor) * 0.15;
                 ct[0] = c[0]; ct[1] = c[1]; ct[2] = c[2];
@@ -535,8 +596,13 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
             si.amb_shadow = 5000;
             if (done_surf) {
                 M64<FM>::store_normal(si, nrm);
-                float l = (float)log((double)fmaxf(p.de_stop, ms) * p.step_width);
-                float v = 32767.0f - (nn + p.d_col_plus + p.col_var * l) * p.mcts_m;
+                float v;
+                if (it_limited) {
+                    v = 32767.0f - nn * p.mcts_m;
+                } else {
+                    float l = (float)log((double)fmaxf(p.de_stop, ms) * p.step_width);
+                    v = 32767.0f - (nn + p.d_col_plus + p.col_var * l) * p.mcts_m;
+                }
                 si.si_gradient = clip15(v);
                 // RMdoColor with the last DE's state, at the surface point
                 const double PI = 3.14159265358979323846;
@@ -1039,8 +1105,7 @@ struct Launch {
     }
     static void finish(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters,
                        Hand *slow, mb3d_cu_silight *out, int blocks, cudaStream_t s) {
-        if (mixed) k_finish<float, FM><<<blocks, 256, 0, s>>>(p, row0, list, counters, slow, out);
-        else k_finish<double, FM><<<blocks, 256, 0, s>>>(p, row0, list, counters, slow, out);
+        k_finish<FM><<<blocks, 256, 0, s>>>(p, row0, list, counters, slow, out);
         k_finish_slow<FM><<<blocks, 128, 0, s>>>(p, row0, slow, counters + 2, out);
     }
     static void post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,

@@ -540,13 +540,17 @@ struct M64 {
 
     // march_from (src/calc.rs:2533-2655), from the state (dtmp, last_step,
     // rsf_mul, first_step, step_count) so that the mixed march can hand a
-    // ray over to it in the middle
-    __device__ void march_from(G &si, double dtmp, double last_step, float rsf_mul, bool first_step, float step_count) {
+    // ray over to it in the middle (after_half: the state is right after the
+    // half step back, whose DE decides without another one)
+    __device__ void march_from(G &si, double dtmp, double last_step, float rsf_mul, bool first_step, float step_count,
+                               bool after_half = false) {
         double last_de;
         unsigned int guard = 0;
         for (;;) {
             if (++guard > 2000000u) break;
-            if (it.it_result >= max_its_result) {
+            bool half = !after_half && it.it_result >= max_its_result;
+            after_half = false;
+            if (half) {
                 double dt1 = -0.5 * last_step;
                 mzz += dt1;
                 step(dt1);

@@ -2,6 +2,8 @@
 
     python mb3d-rs_b200/profile_cases.py mc        # Monte Carlo: C2 scene 480x270, 4 rays, MCDepth 4, mixed
     python mb3d-rs_b200/profile_cases.py denoise   # the denoiser on one 1920x1080 picture (6 passes)
+    python mb3d-rs_b200/profile_cases.py c1        # the plain bulb 640x480: one mixed, one FP64 render
+    python mb3d-rs_b200/profile_cases.py c4        # frame 37 of the 240-frame flight: one mixed, one FP64 render
 
 The Calculate 3D kernels are profiled through bench.py (--scale 0.25).
 """
@@ -47,5 +49,21 @@ def denoise():
     print("ok denoise 1920x1080 ms", e0.elapsed_time(e1) / 5)
 
 
+def _both(sc):
+    card = mb3dcu.Card(0)
+    for prec in (mb3dcu.FP32_FP64, mb3dcu.FP64):
+        card.render(sc, prec)
+        st = card.stats()
+        print("ok", prec, "ms", st["ms_total"], "finish", st["ms_finish"], "fp64 pixels", st["fp64_pixels"])
+
+
+def c1():
+    _both(scenes.c1_plain_bulb())
+
+
+def c4():
+    _both(scenes.c4_frames(240)[37])
+
+
 if __name__ == "__main__":
-    {"mc": mc, "denoise": denoise}[sys.argv[1]]()
+    {"mc": mc, "denoise": denoise, "c1": c1, "c4": c4}[sys.argv[1]]()

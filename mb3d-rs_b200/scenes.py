@@ -193,7 +193,9 @@ def c2_hybrid(seed=C2_SEED, width=1920, height=1080):
 # the surface point of the deep zoom: where the FP64 march of the middle ray
 # from the seeded camera met the Mandelbulb (tests/golden/make_fixtures.py)
 C3_SEED = 0x5EED0003
-C3_POINT = None  # filled by c3_point() from the fixture file when present
+# (tests/golden/c3_point.json, made by tests/golden/make_fixtures.py)
+C3_POINT = [-0.8697553607530222, 0.22843892661237097, 0.3317609632059464]
+C3_VIEW = [0.9074121027226582, -0.2383293694925562, -0.34612481487134783]
 
 
 def c3_deep_zoom(point, view_dir, width=1920, height=1080):
@@ -214,6 +216,11 @@ def c3_deep_zoom(point, view_dir, width=1920, height=1080):
     sc.z_start = point[2] - 1e-5
     sc.z_end = sc.z_start + 1e-3
     return sc
+
+
+def c3(width=1920, height=1080):
+    """The deep zoom workload at the committed surface point."""
+    return c3_deep_zoom(C3_POINT, C3_VIEW, width, height)
 
 
 C4_SEED = 0x5EED0004

@@ -185,7 +185,13 @@ def test_mc_errors(card):
 
 def test_split_render_equals_one_kernel_render(card, monkeypatch):
     """The split render (logic kernel + list-fed march kernel, the default)
-    traces the same rays as the one-kernel form: the same records."""
+    traces the same rays as the one-kernel form: in double precision the
+    same records.  In the mixed mode the single precision DE is compiled
+    into two different kernels, where the code generator may fuse its
+    multiplies and adds differently: the last bits of a ray's positions,
+    and with them of most pixels' light, differ (as they do against the
+    oracle), and a grazing ray can part.  There the two are held to the same
+    picture."""
     sc = scenes.scaled(scenes.c2_hybrid(), 160, 90)
     lv = mb3dcu.mc_light_default(sc)
     for prec in (mb3dcu.FP64, mb3dcu.FP32_FP64):
@@ -193,5 +199,13 @@ def test_split_render_equals_one_kernel_render(card, monkeypatch):
         monkeypatch.setenv("MB3D_CU_MC_MEGA", "1")
         one = card.mc_render(sc, mb3dcu.mc_opts(8, depth=4), lv, prec)
         monkeypatch.delenv("MB3D_CU_MC_MEGA")
-        for k in ("radiance", "albedo", "normal", "depth", "hit"):
-            assert split[k].tobytes() == one[k].tobytes(), (prec, k)
+        if prec == mb3dcu.FP64:
+            for k in ("radiance", "albedo", "normal", "depth", "hit"):
+                assert split[k].tobytes() == one[k].tobytes(), (prec, k)
+        else:
+            assert (split["hit"] == one["hit"]).mean() >= 0.999
+            a = split["radiance"].astype(np.float64)
+            b = one["radiance"].astype(np.float64)
+            assert abs(a.mean() - b.mean()) <= 0.01 * a.mean()
+            psnr = 10 * np.log10(a.max() ** 2 / np.mean((a - b) ** 2))
+            assert psnr > 30.0, psnr
