@@ -262,13 +262,13 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
     if (int r = grow((void **)&c->d_ps, &c->ps_cap, npix * sizeof(PostStart))) return r;
     if (passes & MB3D_CU_POST_DEAO)
         if (int r = grow((void **)&c->d_minra, &c->minra_cap, npix * (size_t)p.ao_rays * sizeof(float))) return r;
-    unsigned int *cnt = c->d_counters + 8;  // [0] surfaces, [1] shadow queue, [2] AO queue
+    unsigned int *cnt = c->d_counters + 8;  // [0] surfaces, [1] shadow queue, [2] AO queue, [3] start queue
     CU_TRY(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned int), s));
     CU_TRY(cudaEventRecord(c->ev[3], s));
     launch_surface(p, (int)npix, passes, dg, c->d_slist, cnt, c->sms * 4, s);
     c->stats.launches += 1;
     if (passes) {
-        launch_post_start(p, mixed, row0, passes, dg, c->d_slist, cnt, c->d_ps, c->sms * 8, s);
+        launch_post_start(p, mixed, row0, passes, dg, c->d_slist, cnt, cnt + 3, c->d_ps, c->sms * p.blocks_per_sm, s);
         c->stats.launches += 1;
         if (int r = check_launch("k_post_start")) return r;
     }
@@ -523,7 +523,7 @@ static int enqueue_frame(mb3d_cu_ctx *c, mb3d_cu_ctx::Scratch &sc, const DevPara
     if (passes) {
         unsigned int *cnt = sc.counters + 8;
         launch_surface(p, (int)npix, passes, dg, sc.slist, cnt, c->sms * 4, s);
-        launch_post_start(p, mixed, 0, passes, dg, sc.slist, cnt, sc.ps, c->sms * 8, s);
+        launch_post_start(p, mixed, 0, passes, dg, sc.slist, cnt, cnt + 3, sc.ps, c->sms * p.blocks_per_sm, s);
         if (passes & MB3D_CU_POST_SHADOW) launch_shadow_rays(p, mixed, 0, sc.ps, cnt, dg, cnt + 1, c->sms * p.blocks_per_sm, s);
         if (passes & MB3D_CU_POST_DEAO) {
             launch_ao_rays(p, mixed, sc.ps, dg, cnt, sc.minra, cnt + 2, c->sms * p.blocks_per_sm, s);

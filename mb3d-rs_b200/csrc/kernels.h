@@ -52,7 +52,8 @@ struct LaunchTable {
     void (*finish)(const DevParams &, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
                    mb3d_cu_silight *out, int blocks, cudaStream_t s);
     void (*post_start)(const DevParams &, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
-                       const uint32_t *list, const unsigned int *count, PostStart *ps, int blocks, cudaStream_t s);
+                       const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps,
+                       int blocks, cudaStream_t s);
     void (*shadow_rays)(const DevParams &, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
                         mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s);
     void (*ao_rays)(const DevParams &, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,
@@ -71,7 +72,8 @@ void launch_finish(const DevParams &p, bool mixed, int row0, const Hand *list, u
 void launch_surface(const DevParams &p, int npix, int passes, mb3d_cu_silight *gbuf, uint32_t *list,
                     unsigned int *count, int blocks, cudaStream_t s);
 void launch_post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
-                       const uint32_t *list, const unsigned int *count, PostStart *ps, int blocks, cudaStream_t s);
+                       const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps, int blocks,
+                       cudaStream_t s);
 void launch_shadow_rays(const DevParams &p, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
                         mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s);
 void launch_ao_rays(const DevParams &p, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,

@@ -11,7 +11,7 @@
 //                cleared, DE AO zeroed) and the list of surface pixels.
 //  k_post_start  per surface pixel: the surface found again from the stored
 //                depth, once for the shadow pass (8 binary search steps) and
-//                once for the DE AO (5 steps).
+//                once for the DE AO (5 steps); a persistent wavefront.
 //  k_shadow_rays one lane per (surface pixel, light) ray, persistent, refill.
 //  k_ao_rays     one lane per (surface pixel, AO direction) ray, likewise.
 //  k_ao_final    per surface pixel: the AO rays' correction and mean.
@@ -674,126 +674,236 @@ __global__ void k_surface(const __grid_constant__ DevParams p, int npix, int pas
 #endif
 
 
-// bin_search (src/calc.rs:1706-1734) on the single precision DE, from the
-// position c at depth mzz along vf; false when the pixel is not limited by
-// the DE (the iteration count search then runs in double precision)
-template <int FM>
-__device__ bool bin_search32(const DevParams &p, double c[3], const double vf[3], double &mzz, float &ms, double de,
-                             double last_step_width, int steps) {
-    int itmp = steps;
-    double dt1 = last_step_width * -0.5;
-    while (fabs(de - (double)ms) > 0.001) {
-        mzz += dt1;
-        add_w(c, vf, dt1);
-        ms = de_stop_at(p, mzz);
-        if (--itmp <= 0) break;
-        DEr r = de_lock<float, FM>(p, c, ms);
-        if (r.need64) return false;
-        de = r.de;
-        if (r.it >= p.max_it) {
-            dt1 = -fabs(dt1);
+// The post passes' start points as a wavefront: per surface pixel, the
+// surface found again from the stored depth -- hs_surface_start
+// (src/calc.rs:2741-2764: RMdoBinSearch with 8 steps, or RMdoBinSearchIt
+// where the iteration count limits the surface) for the shadow pass, then
+// surface_point (src/calc.rs:2157-2191: a 5-step search to 0.004, or
+// RMdoBinSearchIt) for the DE AO.  One DE per lane and trip; a lane whose
+// item is done takes the next surface pixel.  MIXED: a search limited by the
+// DE runs in single precision first; where single precision cannot decide
+// (need64, or the iteration count limits the surface) the task starts over
+// from the stored depth in double precision, as the plain march does it.
+#define Q_IDLE 0
+#define Q_D0 1    // the DE at the stored depth
+#define Q_BIS 2   // RMdoBinSearch (the shadow start)
+#define Q_LIM 3   // the DE AO start's short search
+#define Q_BSI1 4  // RMdoBinSearchIt: the DE at the stepped position
+#define Q_BSI2 5  // ... and 0.001 behind it
+
+template <int FM, bool MIXED>
+__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __grid_constant__ DevParams p, int row0, int passes,
+                                                    const mb3d_cu_silight *gbuf, const uint32_t *list,
+                                                    const unsigned int *count, unsigned int *queue, PostStart *ps) {
+    const uint32_t n_items = count[0];
+    const bool do_sh = (passes & MB3D_CU_POST_SHADOW) && p.n_lights > 0;
+    const bool do_ao = (passes & MB3D_CU_POST_DEAO) && p.ao_rays > 0;
+    const float bsi_yp = (float)p.max_it - 0.99f, bsi_top = (float)(p.max_it + 1) - 0.1f;
+    int phase = Q_IDLE;
+    bool open = true;
+    uint32_t idx = 0;
+    double c0[3] = {0, 0, 0}, vf[3] = {0, 0, 0}, c[3] = {0, 0, 0};
+    double mzz0 = 0, digit = 0, mzz = 0, dt1 = 0, dmul = 1.0, dcur = 0;
+    float ms = 0.f, b_last_si = 0.f, b_last_dif = 0.f;
+    int itmp = 0;
+    bool ao = false, p64 = !MIXED, b_first = false;
+    for (unsigned int trip = 0; trip < 400000000u; trip++) {
+        uint32_t item = warp_take(phase == Q_IDLE, queue, n_items, p.refill_min, open);
+        bool begin = false;
+        if (item != UINT32_MAX) {
+            idx = item;
+            uint32_t pix = list[item];
+            int x = (int)(pix % (uint32_t)p.width), y = row0 + (int)(pix / (uint32_t)p.width);
+            G si;
+            si.load(gbuf[pix]);
+            pixel_ray(p, x, y, c0, vf);
+            double zf = (double)(si.zpos_fine >> 8);
+            double q1 = (8388351.5 - zf) / p.zc_mul + 1.0, q2 = (8388351.9 - zf) / p.zc_mul + 1.0;
+            mzz0 = (q1 * q1 - 1.0) / p.zcorr;
+            digit = (q2 * q2 - 1.0) / p.zcorr - mzz0;
+            uint32_t flags = 0;
+            if (do_sh) {
+                double nv0[3] = {si.n0 / 32767.0, si.n1 / 32767.0, si.n2 / 32767.0}, nvec[3];
+                rot_rev(nv0, p.vgrads, nvec);
+                for (int l = 0; l < p.n_lights; l++)
+                    if (dot3d(nvec, p.light_vec[l]) > 0.0) flags |= 1u << l;
+            }
+            ps[idx].pix = pix;
+            ps[idx].flags = flags;
+            ps[idx].pad = 0;
+            ao = !do_sh;
+            p64 = !MIXED;
+            begin = do_sh || do_ao;
+        }
+        // ---- a task starts (or starts over in double precision) at the stored depth
+#define POST_BEGIN()                                   \
+    do {                                               \
+        mzz = mzz0;                                    \
+        c[0] = c0[0]; c[1] = c0[1]; c[2] = c0[2];      \
+        add_w(c, vf, mzz);                             \
+        ms = de_stop_at(p, mzz);                       \
+        phase = Q_D0;                                  \
+    } while (0)
+        if (begin) POST_BEGIN();
+        unsigned int busy = __ballot_sync(0xffffffffu, phase != Q_IDLE);
+        if (busy == 0) {
+            if (!open) break;
             continue;
         }
-        dt1 = (de - (double)ms) < 0.0 ? fabs(dt1) * -0.55 : fabs(dt1) * 0.55;
-    }
-    return true;
-}
-
-// hs_surface_start (src/calc.rs:2741-2764) and surface_point
-// (src/calc.rs:2157-2191) of a surface pixel, in single precision (MIXED)
-// or as the plain FP64 marcher does them
-template <int FM, bool MIXED>
-__global__ void __launch_bounds__(128) k_post_start(const __grid_constant__ DevParams p, int row0, int passes,
-                                                    const mb3d_cu_silight *gbuf, const uint32_t *list,
-                                                    const unsigned int *count, PostStart *ps) {
-    unsigned int n = count[0];
-    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        uint32_t pix = list[i];
-        int x = (int)(pix % (uint32_t)p.width), y = row0 + (int)(pix / (uint32_t)p.width);
-        G si;
-        si.load(gbuf[pix]);
-        PostStart o;
-        o.pix = pix;
-        o.flags = 0;
-        double c0[3], vf[3];
-        pixel_ray(p, x, y, c0, vf);
-        double zf = (double)(si.zpos_fine >> 8);
-        double q1 = (8388351.5 - zf) / p.zc_mul + 1.0, q2 = (8388351.9 - zf) / p.zc_mul + 1.0;
-        double mzz0 = (q1 * q1 - 1.0) / p.zcorr;
-        double digit = (q2 * q2 - 1.0) / p.zcorr - mzz0;
-        if ((passes & MB3D_CU_POST_SHADOW) && p.n_lights > 0) {
-            bool done = false;
-            double c[3], mzz = mzz0;
-            if (MIXED) {
-                for (int k = 0; k < 3; k++) c[k] = c0[k] + vf[k] * mzz;
-                float ms = de_stop_at(p, mzz);
-                DEr r = de_lock<float, FM>(p, c, ms);
-                if (!r.need64 && (r.it < p.max_it || r.de < (double)ms)) {
-                    done = bin_search32<FM>(p, c, vf, mzz, ms, r.de, digit, 8);
-                }
+        // ---- one DE for the lanes whose phase asks for one
+        DEr r;
+        r.de = 0.0;
+        r.it = 0;
+        r.need64 = false;
+        DEstate st;
+        st.smooth_it = 0.f;
+        if (phase != Q_IDLE) {
+            if (MIXED && !p64) {
+                r = de_lock<float, FM>(p, c, ms);
+            } else {
+                const bool bsi = phase >= Q_BSI1;
+                r = de_lock<double, FM, false, true>(p, c, ms, nullptr, &st, bsi, bsi ? 1 : 0);
             }
-            if (!done) {
-                // (the shadow pass always takes 8 binary search steps)
-                M64<FM> m(p);
-                m.add_steps = 8;
-                m.hs_surface_start(x, y, si);
-                mzz = m.mzz;
-                c[0] = m.it.c[0]; c[1] = m.it.c[1]; c[2] = m.it.c[2];
-            }
-            // 0.1 step in front of the surface (src/calc.rs:2799-2802)
-            mzz = p.shadow_soft ? mzz - 0.1 : fmax(mzz - 0.1, 0.0);
-            add_w(c, vf, -0.1);
-            o.sh_c[0] = c[0]; o.sh_c[1] = c[1]; o.sh_c[2] = c[2];
-            o.sh_mzz = mzz;
-            double nv0[3] = {si.n0 / 32767.0, si.n1 / 32767.0, si.n2 / 32767.0}, nvec[3];
-            rot_rev(nv0, p.vgrads, nvec);
-            for (int l = 0; l < p.n_lights; l++)
-                if (dot3d(nvec, p.light_vec[l]) > 0.0) o.flags |= 1u << l;
-        }
-        if ((passes & MB3D_CU_POST_DEAO) && p.ao_rays > 0) {
-            bool done = false;
-            double c[3], mzz = mzz0;
-            float ms = 0.f;
-            if (MIXED) {
-                for (int k = 0; k < 3; k++) c[k] = c0[k] + vf[k] * mzz;
-                ms = de_stop_at(p, mzz);
-                DEr r = de_lock<float, FM>(p, c, ms);
-                if (!r.need64) {
-                    double d = fmin(r.de, (double)ms * 2.0);
-                    if (r.it < p.max_it || d < (double)ms) {
-                        double dt1 = digit;
-                        int itmp = 5;
-                        done = true;
-                        while (itmp > 0 && fabs(d - (double)ms) > 0.004) {
-                            mzz += dt1;
-                            add_w(c, vf, dt1);
-                            ms = de_stop_at(p, mzz);
-                            itmp -= 1;
-                            if (itmp > 0) {
-                                DEr r2 = de_lock<float, FM>(p, c, ms);
-                                if (r2.need64) {
-                                    done = false;
-                                    break;
-                                }
-                                d = r2.de;
-                                dt1 = d < (double)ms ? fabs(dt1) * -0.55 : fabs(dt1) * 0.55;
-                            }
-                        }
+            // ---- the per-lane machine.  go: 1 the shadow search's test, 2 the
+            // DE AO search's test, 3 the iteration count search's next step,
+            // 4 the task is done
+            int go = 0;
+            const int bsi_steps = ao ? 5 : 8;
+            if (phase == Q_D0) {
+                if (!ao) {
+                    const bool limited = r.it < p.max_it || r.de < (double)ms;
+                    if (!p64 && (r.need64 || !limited)) {
+                        p64 = true;
+                        POST_BEGIN();
+                    } else if (limited) {
+                        dcur = r.de;
+                        itmp = 8;
+                        dt1 = digit * -0.5;
+                        go = 1;
+                    } else {
+                        phase = Q_BSI1;
+                    }
+                } else {
+                    dcur = fmin(r.de, (double)ms * 2.0);
+                    const bool limited = r.it < p.max_it || dcur < (double)ms;
+                    if (!p64 && (r.need64 || !limited)) {
+                        p64 = true;
+                        POST_BEGIN();
+                    } else if (limited) {
+                        itmp = 5;
+                        dt1 = digit;
+                        go = 2;
+                    } else {
+                        phase = Q_BSI1;
                     }
                 }
+                if (phase == Q_BSI1) {
+                    // RMdoBinSearchIt from here (its first step is 0)
+                    itmp = bsi_steps;
+                    dt1 = 0.0;
+                    dmul = 1.0;
+                    b_first = true;
+                    add_w(c, vf, 0.0);
+                }
+            } else if (phase == Q_BIS || phase == Q_LIM) {
+                if (MIXED && !p64 && r.need64) {
+                    p64 = true;
+                    POST_BEGIN();
+                } else {
+                    dcur = r.de;
+                    if (phase == Q_BIS) {
+                        if (r.it >= p.max_it) dt1 = -fabs(dt1);
+                        else dt1 = (dcur - (double)ms) < 0.0 ? fabs(dt1) * -0.55 : fabs(dt1) * 0.55;
+                        go = 1;
+                    } else {
+                        dt1 = dcur < (double)ms ? fabs(dt1) * -0.55 : fabs(dt1) * 0.55;
+                        go = 2;
+                    }
+                }
+            } else if (phase == Q_BSI1) {
+                float si_now = st.smooth_it;
+                if (!b_first && b_last_dif < fabsf(bsi_yp - si_now)) {
+                    mzz -= dt1;
+                    add_w(c, vf, -dt1);
+                    si_now = b_last_si;
+                    dmul *= dt1 > 0.0 ? 0.5 : 0.7;
+                }
+                b_last_dif = fabsf(bsi_yp - si_now);
+                b_last_si = si_now;
+                if (si_now > bsi_top) {
+                    dt1 = -3.0;
+                    go = 3;
+                } else {
+                    mzz -= 0.001;
+                    add_w(c, vf, -0.001);
+                    phase = Q_BSI2;
+                }
+            } else if (phase == Q_BSI2) {
+                float s2 = st.smooth_it;
+                float rr = b_last_si - s2;
+                if (fabsf(rr) < 1e-30f) dt1 = (b_last_si < s2 ? 1.0 : 0.0) - 0.5;
+                else if (rr < 0.0f) dt1 = (double)__fdiv_rn(bsi_yp - s2, rr * 500.0f);
+                else dt1 = (double)__fdiv_rn(bsi_yp - s2, rr * 1000.0f);
+                if (dt1 > 4.0) dt1 = sqrt(dt1) * 2.0;
+                else if (dt1 < -9.0) dt1 = sqrt(-dt1) * -3.0;
+                dt1 = dt1 * dmul + 0.0005;
+                go = 3;
             }
-            if (!done) {
-                // (the DE AO takes 5 binary search steps)
-                M64<FM> m(p);
-                m.add_steps = 5;
-                m.surface_point(x, y, si, 5, 0.004);
-                c[0] = m.it.c[0]; c[1] = m.it.c[1]; c[2] = m.it.c[2];
-                ms = m.ms_de_stop;
+            if (go == 1) {  // RMdoBinSearch's loop test and step
+                if (fabs(dcur - (double)ms) <= 0.001) {
+                    go = 4;
+                } else {
+                    mzz += dt1;
+                    add_w(c, vf, dt1);
+                    ms = de_stop_at(p, mzz);
+                    if (--itmp <= 0) go = 4;
+                    else phase = Q_BIS;
+                }
+            } else if (go == 2) {  // surface_point's loop test and step
+                if (!(itmp > 0 && fabs(dcur - (double)ms) > 0.004)) {
+                    go = 4;
+                } else {
+                    mzz += dt1;
+                    add_w(c, vf, dt1);
+                    ms = de_stop_at(p, mzz);
+                    itmp -= 1;
+                    if (itmp > 0) phase = Q_LIM;
+                    else go = 4;
+                }
+            } else if (go == 3) {
+                b_first = false;
+                if (--itmp < 0) {
+                    // surface_point's DE stop after the iteration count search
+                    if (ao) ms = (float)((double)p.de_stop * (1.0 + fabs(mzz) * (double)p.de_stop_factor));
+                    go = 4;
+                } else {
+                    mzz += dt1;
+                    add_w(c, vf, dt1);
+                    phase = Q_BSI1;
+                }
             }
-            o.ao_c[0] = c[0]; o.ao_c[1] = c[1]; o.ao_c[2] = c[2];
-            o.ao_ms = ms;
+            if (go == 4) {
+                if (!ao) {
+                    // 0.1 step in front of the surface (src/calc.rs:2799-2802)
+                    mzz = p.shadow_soft ? mzz - 0.1 : fmax(mzz - 0.1, 0.0);
+                    add_w(c, vf, -0.1);
+                    ps[idx].sh_c[0] = c[0]; ps[idx].sh_c[1] = c[1]; ps[idx].sh_c[2] = c[2];
+                    ps[idx].sh_mzz = mzz;
+                    if (do_ao) {
+                        ao = true;
+                        p64 = !MIXED;
+                        POST_BEGIN();
+                    } else {
+                        phase = Q_IDLE;
+                    }
+                } else {
+                    ps[idx].ao_c[0] = c[0]; ps[idx].ao_c[1] = c[1]; ps[idx].ao_c[2] = c[2];
+                    ps[idx].ao_ms = ms;
+                    phase = Q_IDLE;
+                }
+            }
         }
-        ps[i] = o;
+#undef POST_BEGIN
     }
 }
 
@@ -1109,9 +1219,10 @@ struct Launch {
         k_finish_slow<FM><<<blocks, 128, 0, s>>>(p, row0, slow, counters + 2, out);
     }
     static void post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
-                           const uint32_t *list, const unsigned int *count, PostStart *ps, int blocks, cudaStream_t s) {
-        if (mixed) k_post_start<FM, true><<<blocks, 128, 0, s>>>(p, row0, passes, gbuf, list, count, ps);
-        else k_post_start<FM, false><<<blocks, 128, 0, s>>>(p, row0, passes, gbuf, list, count, ps);
+                           const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps,
+                           int blocks, cudaStream_t s) {
+        if (mixed) k_post_start<FM, true><<<blocks, 256, 0, s>>>(p, row0, passes, gbuf, list, count, queue, ps);
+        else k_post_start<FM, false><<<blocks, 256, 0, s>>>(p, row0, passes, gbuf, list, count, queue, ps);
     }
     static void shadow_rays(const DevParams &p, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
                             mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s) {

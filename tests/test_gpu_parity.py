@@ -108,6 +108,23 @@ def test_c2_shadows_and_deao(card):
         assert r["hit_agree"] >= agree, (prec, r)
 
 
+def test_menger_shadows_iteration_limited_surfaces(card):
+    """The shadow pass where the iteration count limits the surfaces (the
+    Menger IFS hybrid of the animation): its start points come from
+    RMdoBinSearchIt, in double precision in both modes."""
+    sc = scenes.scaled(scenes.c4_frames(8)[3], 160, 90)
+    ref = O.march(sc, mb3dcu.SILIGHT)
+    obj = mb3dcu.hit_mask(ref)
+    assert obj.mean() > 0.2
+    b = O.shadows(sc, ref.copy(), per_pixel=True)
+    for prec, agree in ((mb3dcu.FP64, 0.999), (mb3dcu.FP32_FP64, 0.99)):
+        a = card.post_on_card(sc, ref.copy(), mb3dcu.POST_SHADOW, prec)
+        sh = ((a["shadow"] & 0x400) == (b["shadow"] & 0x400))[obj].mean()
+        assert sh >= agree, (prec, sh)
+        if prec == mb3dcu.FP64:
+            assert (a["shadow"] == b["shadow"])[obj].mean() >= 0.999
+
+
 def test_render_device_buffer_equals_host_buffer(card):
     import torch
     sc = scenes.scaled(scenes.c2_hybrid(), 240, 136)
