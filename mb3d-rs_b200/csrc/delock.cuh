@@ -58,12 +58,31 @@ __device__ __forceinline__ double param_f<double>(const DevParams &, double d, f
 template <>
 __device__ __forceinline__ float param_f<float>(const DevParams &, double, float f) { return f; }
 
-// One counted-or-not hybrid step on orbit q (run_with's body, src/iteration.rs:289-301)
+// One counted-or-not hybrid step on the Q orbits (run_with's body,
+// src/iteration.rs:289-301).  The slot's formula is chosen once for all
+// orbits, so that their independent chains share one block of code.
 template <typename R, int Q, int FM>
 __device__ __forceinline__ void step_orbits(const DevSlot &s, R (&v)[Q][4], R (&j)[Q][3], const R (&rout)[Q]) {
+    if ((FM & FKIND_IP8) && (FM == FKIND_IP8 || s.kind == FKIND_IP8)) {
+        const R zmul = Num<R>::opt(s, 1);
+#pragma unroll
+        for (int q = 0; q < Q; q++) f_int_pow<R>(8, zmul, v[q], j[q]);
+    } else if ((FM & FKIND_BOX) && s.kind == FKIND_BOX) {
+        const R scale = Num<R>::opt(s, 0), min_r = Num<R>::opt(s, 1), fold = Num<R>::opt(s, 2);
+        const bool ade = s.ade != 0;
+#pragma unroll
+        for (int q = 0; q < Q; q++) f_amazing_box<R>(scale, min_r, fold, v[q], j[q], ade);
+    } else if ((FM & FKIND_MENGER) && s.kind == FKIND_MENGER) {
+        const R sc = Num<R>::opt(s, 0), cx = Num<R>::opt(s, 1), cy = Num<R>::opt(s, 2), cz = Num<R>::opt(s, 3);
+        const bool ade = s.ade != 0;
+#pragma unroll
+        for (int q = 0; q < Q; q++) f_menger<R>(sc, cx, cy, cz, v[q], ade);
+    } else if (FM == FKIND_ALL) {
+#pragma unroll
+        for (int q = 0; q < Q; q++) formula_iterate<R, FM>(s, v[q], j[q], rout[q]);
+    }
 #pragma unroll
     for (int q = 0; q < Q; q++) {
-        formula_iterate<R, FM>(s, v[q], j[q], rout[q]);
         if (s.julia_add) {
             v[q][0] += j[q][0];
             v[q][1] += j[q][1];
@@ -200,13 +219,15 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
         float corr[3] = {1.f, 1.f, 1.f};
         const double off = (double)p.de_offset;
         if (sizeof(R) == 4) {
+            // (o - cf is exact in single precision where the two are within a
+            // factor of 2 of each other, i.e. wherever |c| >= the offset)
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 float cf = (float)c[k];
                 float o = (float)(c[k] + off);
-                double h = (double)o - (double)cf;
-                if (h <= 0.0) out.need64 = true;
-                corr[k] = (float)(off / fmax(h, 1e-300));
+                float h = o - cf;
+                if (!(h > 0.0f)) out.need64 = true;
+                corr[k] = __fdividef(p.de_offset, fmaxf(h, 1e-30f));
             }
         }
 #pragma unroll

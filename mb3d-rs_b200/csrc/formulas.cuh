@@ -52,7 +52,7 @@ __device__ __forceinline__ void f_amazing_box(R scale, R min_r, R fold, R v[4], 
     if (r < sqr_min_r) mul = Num<R>::div_(scale, sqr_min_r);
     else if (R(1) < r) mul = scale;
     else mul = Num<R>::div_(scale, r);
-    if (ade) v[3] *= mul;
+    v[3] = ade ? v[3] * mul : v[3];
     v[2] = z * mul + j[2];
     v[1] = y * mul + j[1];
     v[0] = x * mul + j[0];
@@ -182,7 +182,7 @@ __device__ __forceinline__ void f_menger(R s, R cx, R cy, R cz, R v[4], bool ade
     y = s * y - cy * s1;
     z = s * z;
     if (z > R(0.5) * cz * s1) z -= cz * s1;
-    if (ade) v[3] *= fabs(s);
+    v[3] = ade ? v[3] * fabs(s) : v[3];
     v[0] = x;
     v[1] = y;
     v[2] = z;
