@@ -253,7 +253,7 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
         for (;;) {
             if (FULL) {
                 rold0 = rout[0];
-                if (live[3]) rold3 = rout[3];
+                rold3 = live[3] ? rout[3] : rold3;
             }
             int guard = 0;
             while (btmp <= 0) {
@@ -274,19 +274,20 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
             }
             it += 1;
             rout[0] = v[0][0] * v[0][0] + v[0][1] * v[0][1] + v[0][2] * v[0][2];
+            // (a stopped offset orbit keeps its last length, by selects; in
+            // single precision the log of its length is taken from the vector
+            // when it stops, since the squared length may overflow there)
 #pragma unroll
             for (int q = 1; q < 4; q++) {
-                if (live[q]) {
-                    rout[q] = v[q][0] * v[q][0] + v[q][1] * v[q][1] + v[q][2] * v[q][2];
-                    if (FULL && q == 3 && rout[3] < otrap3) otrap3 = rout[3];
-                    if (rout[q] > rstop3d) {
-                        live[q] = false;
-                        if (sizeof(R) == 4) {
-                            float vf[4] = {(float)v[q][0], (float)v[q][1], (float)v[q][2], 0.f};
-                            lr_frozen[q] = log_len2_f(vf);
-                        }
-                    }
+                const R rn = v[q][0] * v[q][0] + v[q][1] * v[q][1] + v[q][2] * v[q][2];
+                const bool stop = live[q] && rn > rstop3d;
+                if (FULL && q == 3) otrap3 = (live[3] && rn < otrap3) ? rn : otrap3;
+                rout[q] = live[q] ? rn : rout[q];
+                if (sizeof(R) == 4 && stop) {
+                    float vf[4] = {(float)v[q][0], (float)v[q][1], (float)v[q][2], 0.f};
+                    lr_frozen[q] = log_len2_f(vf);
                 }
+                live[q] = live[q] && !stop;
             }
             if (it >= max_it || rout[0] > rstop) break;
             // (a stopped offset orbit keeps being iterated in the lock-step;

@@ -49,9 +49,17 @@ __device__ __forceinline__ void f_amazing_box(R scale, R min_r, R fold, R v[4], 
     R m = fmax(min_r, Num<R>::eps());
     R sqr_min_r = m * m;
     R mul;
-    if (r < sqr_min_r) mul = Num<R>::div_(scale, sqr_min_r);
-    else if (R(1) < r) mul = scale;
-    else mul = Num<R>::div_(scale, r);
+    if (sizeof(R) == 4) {
+        // (branch-free in the single precision bulk: the quotient is formed
+        // for the chosen divisor, then selected)
+        const bool below = r < sqr_min_r;
+        R q = Num<R>::div_(scale, below ? sqr_min_r : r);
+        mul = (!below && R(1) < r) ? scale : q;
+    } else {
+        if (r < sqr_min_r) mul = Num<R>::div_(scale, sqr_min_r);
+        else if (R(1) < r) mul = scale;
+        else mul = Num<R>::div_(scale, r);
+    }
     v[3] = ade ? v[3] * mul : v[3];
     v[2] = z * mul + j[2];
     v[1] = y * mul + j[1];
