@@ -183,7 +183,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_MARCH) k_march(const __gr
             } else if (phase == PH_STEP) {
                 if (dtmp > last_de + last_step) dtmp = last_de + last_step;
                 if (last_de > dtmp + 1e-30) {
-                    double t = last_step / (last_de - dtmp);
+                    double t = MIXED ? (double)__fdividef((float)last_step, (float)(last_de - dtmp)) : last_step / (last_de - dtmp);
                     rsf = t < 1.0 ? (float)fmax(0.5, t) : 1.0f;
                 } else {
                     rsf = 1.0f;
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_MARCH) k_march(const __gr
                     double s1 = (double)(fmaxf(ms, 0.4f) * p.mh04zsd);
                     bool count = p.dfog_on_it == 0 || it == p.dfog_on_it;
                     if (s1 < d) {
-                        if (count) step_count += (float)(s1 / d);
+                        if (count) step_count += MIXED ? __fdividef((float)s1, (float)d) : (float)(s1 / d);
                         d = s1;
                     } else if (count) {
                         step_count += 1.0f;
@@ -990,7 +990,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_shadow_rays(const __gr
                 } else {
                     if (dn > last_de + st) dn = last_de + st;
                     if (last_de > dn + 1e-30) {
-                        float t = (float)(st / (last_de - dn));
+                        float t = sizeof(R) == 4 ? __fdividef((float)st, (float)(last_de - dn)) : (float)(st / (last_de - dn));
                         rsf = t < 1.0f ? fmaxf(t, 0.5f) : 1.0f;
                     } else {
                         rsf = 1.0f;
@@ -1142,7 +1142,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_c
             double c[3] = {ic[0] + sv[0] * dt1, ic[1] + sv[1] * dt1, ic[2] + sv[2] * dt1};
             DEr r = ray_de<R, FM>(p, c, ms_s);
             double dt2 = r.de;
-            s_tmp = fmin(s_tmp, (dt2 - msd + dt1 * md_d10) / dt1);
+            s_tmp = fmin(s_tmp, sizeof(R) == 4 ? (double)__fdividef((float)(dt2 - msd + dt1 * md_d10), (float)dt1)
+                                               : (dt2 - msd + dt1 * md_d10) / dt1);
             bool end = s_tmp < 0.02 || b_end || ++guard > 100000;
             if (!end) dt1 += fmax(dt2, dt1 * dsm);
             if (end) {
