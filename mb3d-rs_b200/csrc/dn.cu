@@ -478,6 +478,7 @@ int mb3d_cu_dn_denoise(mb3d_cu_dn *d, int n, int hs, int ws, const float *rad, c
     if (!dev) cudaMemcpyAsync(out, o, px * 3 * sizeof(float), cudaMemcpyDeviceToHost, s);
     if (int e = check("denoiser forward")) return e;
     if (cudaStreamSynchronize(s) != cudaSuccess) return check("denoiser forward");
+    if (dn_conv_error(s)) return dn_fail(MB3D_CU_EIO, "denoiser forward: a convolution's pipeline wait ran out");
     return 0;
 }
 
@@ -490,6 +491,7 @@ int mb3d_cu_dn_gradient(mb3d_cu_dn *d, int n, int hs, int ws, const float *rad, 
     cudaStream_t s = dn_stream(d->ctx);
     cudaMemcpyAsync(grad, d->grad, d->nparam * 4, cudaMemcpyDefault, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return check("denoiser gradient");
+    if (dn_conv_error(s)) return dn_fail(MB3D_CU_EIO, "denoiser gradient: a convolution's pipeline wait ran out");
     return 0;
 }
 
@@ -505,6 +507,7 @@ int mb3d_cu_dn_train_step(mb3d_cu_dn *d, int n, int hs, int ws, const float *rad
     cast_all(d, s);
     if (int e = check("denoiser update")) return e;
     if (!loss && cudaStreamSynchronize(s) != cudaSuccess) return check("denoiser update");
+    if (dn_conv_error(s)) return dn_fail(MB3D_CU_EIO, "denoiser update: a convolution's pipeline wait ran out");
     return 0;
 }
 
@@ -561,6 +564,7 @@ int mb3d_cu_dn_conv_check(mb3d_cu_ctx *ctx, int n, int h, int w, int cin, int co
     cudaFree(dwt); cudaFree(dbias); cudaFree(ddw); cudaFree(ddb);
     if (r) return dn_fail(MB3D_CU_EINVAL, "convolution launch arguments");
     if (e != cudaSuccess) return dn_fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    if (dn_conv_error(s)) return dn_fail(MB3D_CU_EIO, "convolution: a pipeline wait ran out");
     for (size_t i = 0; i < hy.size(); i++) y[i] = __bfloat162float(hy[i]);
     for (size_t i = 0; i < hdx.size(); i++) dx[i] = __bfloat162float(hdx[i]);
     return 0;

@@ -28,7 +28,12 @@ struct WgradArgs {
     int x_c, x_off, cin;
 };
 
+// (the tensor-core convolution; requires cin % 16 == 0, in_c, in_off, out_c
+// and out_off multiples of 8; -1 on bad arguments)
 int dn_conv(const ConvArgs &a, cudaStream_t s);
+// nonzero (and cleared) when a convolution's pipeline wait ran out since the
+// last call; synchronises s
+int dn_conv_error(cudaStream_t s);
 int dn_wgrad(const WgradArgs &a, float *db, cudaStream_t s);
 void dn_relu_mask(__nv_bfloat16 *d, const __nv_bfloat16 *y, int c_tot, int off, int cn, size_t m, cudaStream_t s);
 void dn_pool2(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w, __nv_bfloat16 *out,

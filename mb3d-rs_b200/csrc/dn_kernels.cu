@@ -1,8 +1,7 @@
-// The denoiser's kernels: 3x3 convolutions as implicit GEMMs on the BF16
-// tensor cores with FP32 accumulation (forward, and backward to the input
-// through the flipped weights), the weight and bias gradients, and the
-// elementwise pieces of the U-Net (pooling, upsampling, ReLU masks, input
-// packing, the loss, Adam).
+// The denoiser's kernels besides the convolution itself (dn_tc.cu): the
+// weight and bias gradients of a 3x3 convolution on the BF16 tensor cores
+// with FP32 accumulation, and the elementwise pieces of the U-Net (pooling,
+// upsampling, ReLU masks, input packing, the loss, Adam).
 //
 // Activations are NHWC bf16 tensors whose channel counts are multiples of
 // 16; a convolution reads `cin` channels at offset `in_off` of a tensor of
@@ -41,130 +40,6 @@ __device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32
         "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
         : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// ---------------------------------------------------------------------------
-// 3x3 convolution, stride 1, zero padding 1, as an implicit GEMM:
-//   M = pixels (128 per block), N = output channels (BN per block, grid.y
-//   tiles), K = 9 taps x cin in chunks of 16 (4-stage cp.async pipeline).
-// Each of the 4 warps computes 32 pixels x BN channels with m16n8k16 MMAs
-// from ldmatrix fragments; shared rows are 48 bytes apart (conflict-free).
-constexpr int CV_BM = 128, CV_STAGES = 4, CV_LD = 24;  // row stride in bf16 (48 B)
-
-template <int BN>
-__global__ void __launch_bounds__(128) k_conv3x3(ConvArgs a) {
-    __shared__ __align__(128) __nv_bfloat16 sa[CV_STAGES][CV_BM * CV_LD];
-    __shared__ __align__(128) __nv_bfloat16 sb[CV_STAGES][BN * CV_LD];
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * CV_BM, n0 = blockIdx.y * BN;
-    const int hw = a.h * a.w;
-    const int kchunks = 9 * (a.cin >> 4);
-    const int cin16 = a.cin >> 4;
-    // this thread's two A rows (pixel, half) and their coordinates
-    int arow[2], ahalf[2], an[2], ay[2], ax[2];
-    bool avalid[2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-        int e = tid + i * 128;  // 256 16-byte pieces: 128 rows x 2 halves
-        arow[i] = e >> 1;
-        ahalf[i] = e & 1;
-        int m = m0 + arow[i];
-        avalid[i] = m < a.m;
-        int mm = avalid[i] ? m : 0;
-        an[i] = mm / hw;
-        int r = mm - an[i] * hw;
-        ay[i] = r / a.w;
-        ax[i] = r - ay[i] * a.w;
-    }
-    auto load_stage = [&](int kc, int buf) {
-        int tap = kc / cin16, ci0 = (kc - tap * cin16) << 4;
-        int dy = tap / 3 - 1, dx = tap - (tap / 3) * 3 - 1;
-#pragma unroll
-        for (int i = 0; i < 2; i++) {
-            int y = ay[i] + dy, x = ax[i] + dx;
-            bool v = avalid[i] && (unsigned)y < (unsigned)a.h && (unsigned)x < (unsigned)a.w;
-            const __nv_bfloat16 *src = v ? a.in + ((size_t)(an[i] * a.h + y) * a.w + x) * a.in_c + a.in_off + ci0 + ahalf[i] * 8
-                                         : a.in;
-            cp_async16(&sa[buf][arow[i] * CV_LD + ahalf[i] * 8], src, v);
-        }
-        for (int e = tid; e < BN * 2; e += 128) {
-            int row = e >> 1, half = e & 1;
-            int n = n0 + row;
-            bool v = n < a.cout;
-            const __nv_bfloat16 *src = v ? a.wt + ((size_t)n * 9 + tap) * a.cin + ci0 + half * 8 : a.wt;
-            cp_async16(&sb[buf][row * CV_LD + half * 8], src, v);
-        }
-    };
-    constexpr int NT = BN / 8;
-    float acc[2][NT][4];
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < NT; j++)
-#pragma unroll
-            for (int k = 0; k < 4; k++) acc[i][j][k] = 0.0f;
-#pragma unroll
-    for (int s = 0; s < CV_STAGES - 1; s++) {
-        if (s < kchunks) load_stage(s, s);
-        cp_async_commit();
-    }
-    for (int kc = 0; kc < kchunks; kc++) {
-        cp_async_wait<CV_STAGES - 2>();
-        __syncthreads();
-        int nxt = kc + CV_STAGES - 1;
-        if (nxt < kchunks) load_stage(nxt, nxt % CV_STAGES);
-        cp_async_commit();
-        const int buf = kc % CV_STAGES;
-        uint32_t af[2][4];
-#pragma unroll
-        for (int mt = 0; mt < 2; mt++) {
-            int r = warp * 32 + mt * 16 + (lane & 15);
-            ldsm_x4(af[mt], &sa[buf][r * CV_LD + (lane >> 4) * 8]);
-        }
-#pragma unroll
-        for (int j = 0; j < NT / 2; j++) {
-            uint32_t bf[4];
-            int r = j * 16 + (lane & 7) + ((lane >> 4) << 3);
-            ldsm_x4(bf, &sb[buf][r * CV_LD + ((lane >> 3) & 1) * 8]);
-#pragma unroll
-            for (int mt = 0; mt < 2; mt++) {
-                mma16816(acc[mt][2 * j], af[mt], bf[0], bf[1]);
-                mma16816(acc[mt][2 * j + 1], af[mt], bf[2], bf[3]);
-            }
-        }
-    }
-    cp_async_wait<0>();
-    // epilogue: bias, ReLU, bf16 pairs into the output slot
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++) {
-#pragma unroll
-        for (int half = 0; half < 2; half++) {
-            int m = m0 + warp * 32 + mt * 16 + g + half * 8;
-            if (m >= a.m) continue;
-            __nv_bfloat16 *o = a.out + (size_t)m * a.out_c + a.out_off;
-#pragma unroll
-            for (int nt = 0; nt < NT; nt++) {
-                int n = n0 + nt * 8 + 2 * t;
-                if (n >= a.cout) continue;
-                float v0 = acc[mt][nt][half * 2], v1 = acc[mt][nt][half * 2 + 1];
-                if (a.bias) {
-                    v0 += a.bias[n];
-                    v1 += a.bias[n + 1];
-                }
-                if (a.relu) {
-                    v0 = fmaxf(v0, 0.0f);
-                    v1 = fmaxf(v1, 0.0f);
-                }
-                if (a.accumulate) {
-                    __nv_bfloat162 old = *reinterpret_cast<const __nv_bfloat162 *>(o + n);
-                    v0 += __bfloat162float(old.x);
-                    v1 += __bfloat162float(old.y);
-                }
-                *reinterpret_cast<__nv_bfloat162 *>(o + n) = __floats2bfloat162_rn(v0, v1);
-            }
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -475,26 +350,6 @@ __global__ void k_cast_weights(const float *w, int cout, int cin, __nv_bfloat16 
 static int grid_for(size_t n, int per = 256) {
     size_t b = (n + per - 1) / per;
     return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
-}
-
-int dn_conv(const ConvArgs &a, cudaStream_t s) {
-    if (a.cin % 16 || a.cout <= 0 || a.in_c % 8 || a.in_off % 8 || a.out_c % 2 || a.out_off % 2) return -1;
-    int bn = a.cout <= 16 ? 16 : a.cout <= 32 ? 32 : a.cout <= 48 ? 48 : a.cout <= 64 ? 64 : a.cout <= 80 ? 80 : 96;
-    if (a.cout > 96) {
-        // wide outputs: tiles of 64 or 48 (whichever wastes fewer columns)
-        int w64 = (64 - a.cout % 64) % 64, w48 = (48 - a.cout % 48) % 48;
-        bn = w64 <= w48 ? 64 : 48;
-    }
-    dim3 grid((a.m + CV_BM - 1) / CV_BM, (a.cout + bn - 1) / bn);
-    switch (bn) {
-        case 16: k_conv3x3<16><<<grid, 128, 0, s>>>(a); break;
-        case 32: k_conv3x3<32><<<grid, 128, 0, s>>>(a); break;
-        case 48: k_conv3x3<48><<<grid, 128, 0, s>>>(a); break;
-        case 64: k_conv3x3<64><<<grid, 128, 0, s>>>(a); break;
-        case 80: k_conv3x3<80><<<grid, 128, 0, s>>>(a); break;
-        default: k_conv3x3<96><<<grid, 128, 0, s>>>(a); break;
-    }
-    return 0;
 }
 
 int dn_wgrad(const WgradArgs &a, float *db, cudaStream_t s) {
