@@ -9,7 +9,7 @@ namespace mb3dcu {
 // a 3x3 convolution: m = n * h * w pixels of NHWC tensors
 struct ConvArgs {
     const __nv_bfloat16 *in;  // in_c channels per pixel; cin of them from in_off
-    const __nv_bfloat16 *wt;  // [cout][9][cin]
+    const __nv_bfloat16 *wt;  // [cin/16][9 taps][2 halves][cout][8] (dn_cast_weights)
     const float *bias;        // cout, or null
     __nv_bfloat16 *out;       // out_c channels per pixel; cout of them at out_off
     int n, h, w, m;
@@ -28,8 +28,8 @@ struct WgradArgs {
     int x_c, x_off, cin;
 };
 
-// (the tensor-core convolution; requires cin % 16 == 0, in_c, in_off, out_c
-// and out_off multiples of 8; -1 on bad arguments)
+// (the tensor-core convolution; requires cin and cout multiples of 16, cout
+// <= 256, in_c, in_off, out_c and out_off multiples of 8; -1 on bad arguments)
 int dn_conv(const ConvArgs &a, cudaStream_t s);
 // nonzero (and cleared) when a convolution's pipeline wait ran out since the
 // last call; synchronises s

@@ -176,20 +176,30 @@ __global__ void k_relu_mask(__nv_bfloat16 *d, const __nv_bfloat16 *y, int c_tot,
     }
 }
 
-// 2x2 max pooling: out (h/2, w/2, cn) from a slot of in (h, w)
+// 2x2 max pooling: out (h/2, w/2, cn) from a slot of in (h, w); one thread
+// per output pixel and 8 channels (16-byte loads and stores; cn, in_c and
+// in_off are multiples of 8)
 __global__ void k_pool2(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w, __nv_bfloat16 *out) {
-    int h2 = h >> 1, w2 = w >> 1;
-    size_t total = (size_t)n * h2 * w2 * cn;
+    int h2 = h >> 1, w2 = w >> 1, c8n = cn >> 3;
+    size_t total = (size_t)n * h2 * w2 * c8n;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        int c = (int)(i % cn);
-        size_t q = i / cn;
+        int c8 = (int)(i % c8n);
+        size_t q = i / c8n;
         int x = (int)(q % w2), y = (int)((q / w2) % h2), b = (int)(q / ((size_t)w2 * h2));
-        size_t base = (((size_t)b * h + 2 * y) * w + 2 * x) * in_c + in_off + c;
-        float v = __bfloat162float(in[base]);
-        v = fmaxf(v, __bfloat162float(in[base + in_c]));
-        v = fmaxf(v, __bfloat162float(in[base + (size_t)w * in_c]));
-        v = fmaxf(v, __bfloat162float(in[base + (size_t)w * in_c + in_c]));
-        out[i] = __float2bfloat16(v);
+        size_t base = (((size_t)b * h + 2 * y) * w + 2 * x) * in_c + in_off + c8 * 8;
+        uint4 v0 = *reinterpret_cast<const uint4 *>(in + base);
+        uint4 v1 = *reinterpret_cast<const uint4 *>(in + base + in_c);
+        uint4 v2 = *reinterpret_cast<const uint4 *>(in + base + (size_t)w * in_c);
+        uint4 v3 = *reinterpret_cast<const uint4 *>(in + base + (size_t)w * in_c + in_c);
+        const __nv_bfloat162 *a0 = reinterpret_cast<const __nv_bfloat162 *>(&v0);
+        const __nv_bfloat162 *a1 = reinterpret_cast<const __nv_bfloat162 *>(&v1);
+        const __nv_bfloat162 *a2 = reinterpret_cast<const __nv_bfloat162 *>(&v2);
+        const __nv_bfloat162 *a3 = reinterpret_cast<const __nv_bfloat162 *>(&v3);
+        uint4 r;
+        __nv_bfloat162 *o = reinterpret_cast<__nv_bfloat162 *>(&r);
+#pragma unroll
+        for (int k = 0; k < 4; k++) o[k] = __hmax2(__hmax2(a0[k], a1[k]), __hmax2(a2[k], a3[k]));
+        *reinterpret_cast<uint4 *>(out + q * cn + c8 * 8) = r;
     }
 }
 
@@ -220,15 +230,22 @@ __global__ void k_pool2_bwd(const __nv_bfloat16 *in, int in_c, int in_off, int c
     }
 }
 
-// nearest 2x upsampling of in (h/2, w/2, cn) into a slot of out (h, w)
+// nearest 2x upsampling of in (h/2, w/2, cn) into a slot of out (h, w); one
+// thread per input pixel and 8 channels, its 2x2 block of outputs (cn, out_c
+// and out_off are multiples of 8)
 __global__ void k_up2(const __nv_bfloat16 *in, int cn, int n, int h, int w, __nv_bfloat16 *out, int out_c, int out_off) {
-    size_t total = (size_t)n * h * w * cn;
-    int h2 = h >> 1, w2 = w >> 1;
+    int h2 = h >> 1, w2 = w >> 1, c8n = cn >> 3;
+    size_t total = (size_t)n * h2 * w2 * c8n;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
-        int c = (int)(i % cn);
-        size_t q = i / cn;
-        int x = (int)(q % w), y = (int)((q / w) % h), b = (int)(q / ((size_t)w * h));
-        out[q * out_c + out_off + c] = in[(((size_t)b * h2 + (y >> 1)) * w2 + (x >> 1)) * cn + c];
+        int c8 = (int)(i % c8n);
+        size_t q = i / c8n;
+        int x = (int)(q % w2), y = (int)((q / w2) % h2), b = (int)(q / ((size_t)w2 * h2));
+        uint4 v = *reinterpret_cast<const uint4 *>(in + q * cn + c8 * 8);
+        size_t o = (((size_t)b * h + 2 * y) * w + 2 * x) * out_c + out_off + c8 * 8;
+        *reinterpret_cast<uint4 *>(out + o) = v;
+        *reinterpret_cast<uint4 *>(out + o + out_c) = v;
+        *reinterpret_cast<uint4 *>(out + o + (size_t)w * out_c) = v;
+        *reinterpret_cast<uint4 *>(out + o + (size_t)w * out_c + out_c) = v;
     }
 }
 
@@ -320,8 +337,7 @@ __global__ void k_l1_loss(const __nv_bfloat16 *pred, const float *target, int n,
     if (threadIdx.x == 0) atomicAdd(loss, s[0] * inv_count);
 }
 
-// Adam on the FP32 master parameters; then the bf16 weights of the forward
-// ([co][tap][ci]) and of the backward to the input ([ci][8 - tap][co])
+// Adam on the FP32 master parameters
 __global__ void k_adam(float *param, const float *grad, float *m1, float *m2, size_t n, float lr, float b1, float b2,
                        float eps, float c1, float c2) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -334,13 +350,19 @@ __global__ void k_adam(float *param, const float *grad, float *m1, float *m2, si
     }
 }
 
+// the bf16 weights of a convolution in the layout its kernel reads (dn.h):
+// [cin/16][tap][8-channel half][cout][8] for the forward, from w[co][tap][ci];
+// the backward to the input (input and output channels swapped, the taps
+// mirrored) likewise, [cout/16][tap][half][cin][8]
 __global__ void k_cast_weights(const float *w, int cout, int cin, __nv_bfloat16 *wf, __nv_bfloat16 *wb) {
     size_t total = (size_t)cout * 9 * cin;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         int ci = (int)(i % cin), tap = (int)((i / cin) % 9), co = (int)(i / ((size_t)cin * 9));
         __nv_bfloat16 v = __float2bfloat16(w[i]);
-        wf[i] = v;
-        if (wb) wb[((size_t)ci * 9 + (8 - tap)) * cout + co] = v;
+        // the forward: input channel ci, output channel co
+        wf[((((size_t)(ci >> 4) * 9 + tap) * 2 + ((ci >> 3) & 1)) * cout + co) * 8 + (ci & 7)] = v;
+        // the backward to the input: input channel co, output channel ci, the tap mirrored
+        if (wb) wb[((((size_t)(co >> 4) * 9 + (8 - tap)) * 2 + ((co >> 3) & 1)) * cin + ci) * 8 + (co & 7)] = v;
     }
 }
 
@@ -372,14 +394,14 @@ void dn_relu_mask(__nv_bfloat16 *d, const __nv_bfloat16 *y, int c_tot, int off, 
 }
 void dn_pool2(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w, __nv_bfloat16 *out,
               cudaStream_t s) {
-    k_pool2<<<grid_for((size_t)n * (h / 2) * (w / 2) * cn), 256, 0, s>>>(in, in_c, in_off, cn, n, h, w, out);
+    k_pool2<<<grid_for((size_t)n * (h / 2) * (w / 2) * (cn / 8)), 256, 0, s>>>(in, in_c, in_off, cn, n, h, w, out);
 }
 void dn_pool2_bwd(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w, const __nv_bfloat16 *dout,
                   __nv_bfloat16 *din, cudaStream_t s) {
     k_pool2_bwd<<<grid_for((size_t)n * (h / 2) * (w / 2) * cn), 256, 0, s>>>(in, in_c, in_off, cn, n, h, w, dout, din);
 }
 void dn_up2(const __nv_bfloat16 *in, int cn, int n, int h, int w, __nv_bfloat16 *out, int out_c, int out_off, cudaStream_t s) {
-    k_up2<<<grid_for((size_t)n * h * w * cn), 256, 0, s>>>(in, cn, n, h, w, out, out_c, out_off);
+    k_up2<<<grid_for((size_t)n * (h / 2) * (w / 2) * (cn / 8)), 256, 0, s>>>(in, cn, n, h, w, out, out_c, out_off);
 }
 void dn_up2_bwd(const __nv_bfloat16 *dout, int out_c, int out_off, int cn, int n, int h, int w, __nv_bfloat16 *din,
                 cudaStream_t s) {

@@ -1,17 +1,27 @@
 // The denoiser's 3x3 convolution (stride 1, zero padding 1) on the fifth
-// generation tensor cores: an implicit GEMM with
-//   M = 128 pixels of a bw x bh box of one image (bw * bh = 128),
-//   N = the output channels (one tile of up to 256; more in grid.y tiles),
-//   K = 9 taps x cin, in chunks of 16 channels of one tap (32 bytes).
-// Per chunk one TMA load brings the box's 16 channels at the tap's offset
-// (the picture's border comes as the TMA's zero fill) and one the weights'
-// 16 K-columns; both land in shared memory in the 32-byte swizzled K-major
-// layout that tcgen05.mma reads, and one tcgen05.mma (M=128, N=BN, K=16,
-// BF16 x BF16 -> FP32) adds the chunk into the accumulator in tensor memory.
-// Roles in the block of 128 threads: thread 0 issues the TMA loads, thread 32
-// the MMAs (each MMA's commit frees its stage); then all four warps read the
-// accumulator (warp w holds TMEM lanes 32w..32w+31, i.e. pixels), add the
-// bias, apply the ReLU and store bf16 NHWC.
+// generation tensor cores, as an implicit GEMM:
+//   M = 128 output pixels, a box 8 wide and 16 high of one image,
+//   N = the output channels (up to 256, one tile),
+//   K = 9 taps x cin.
+// For each group of 16 input channels the TMA brings the tile's input box
+// with its one-pixel halo, 10 x 18 pixels, as two 8-channel halves in shared
+// memory ([y][x][8 channels], 16 bytes a pixel; the picture's border is the
+// TMA's zero fill).  That is the A operand of all nine taps: for tap (dy, dx)
+// the 8 output pixels of a row are 8 consecutive pixels of the box, so the
+// tap's operand is the box seen from start ((dy + 1) * 10 + dx + 1) * 16 with
+// 8-row groups 160 bytes apart and the two channel halves one box apart, in
+// the no-swizzle K-major layout tcgen05.mma reads.  The weights come in the
+// matching layout ([group][tap][half][cout][8], made by dn_cast_weights); they
+// stay in shared memory for the whole kernel where they fit, else each group's
+// block comes with its input box.  Nine tcgen05.mma (M=128, N=BN, K=16,
+// BF16 x BF16 -> FP32) per group add into the accumulator in tensor memory.
+// The blocks are persistent (one per SM) and take every grid-th tile.  Roles
+// in a block of 192 threads: lane 0 of warp 0 issues the TMA loads through a
+// ring of stages, lane 0 of warp 1 the MMAs (each group's commit frees its
+// stage; tile i accumulates in TMEM buffer i % 2, so that the epilogue of one
+// tile overlaps the MMAs of the next), and warps 2..5 read the accumulator
+// (warp w holds TMEM lanes 32 (w % 4) .. + 31, i.e. pixels), add the bias,
+// apply the ReLU, store bf16 NHWC and free the buffer.
 // Every wait is bounded (about a second of clock cycles); a wait that runs out
 // sets the error word and the block stops issuing, and frees its tensor memory.
 #include <cuda.h>
@@ -24,18 +34,29 @@ namespace mb3dcu {
 
 namespace {
 
-constexpr int TC_STAGES = 6;
-constexpr int TC_M = 128;
-constexpr long long TC_WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9-2 GHz
+constexpr int TC_M = 128, TILE_W = 8, TILE_H = 16, HALO_W = TILE_W + 2, HALO_H = TILE_H + 2;
+// one 8-channel half of an input box: the bytes the TMA brings, and its
+// place in shared memory, padded to the 128-byte alignment a TMA destination
+// needs
+constexpr uint32_t BOX_BYTES = HALO_W * HALO_H * 16;
+constexpr uint32_t HALF_BYTES = (BOX_BYTES + 127) / 128 * 128;
+constexpr uint32_t A_BYTES = 2 * HALF_BYTES;
+constexpr int MAX_STAGES = 16;
+constexpr uint32_t SMEM_BUDGET = 200 * 1024;           // the dynamic shared memory a block takes
+constexpr uint32_t RESIDENT_MAX = 112 * 1024;          // weights up to this stay in shared memory
+constexpr long long TC_WAIT_CYCLES = 2000000000LL;     // ~1 s at 1.9-2 GHz
 
 struct ConvTc {
+    const __nv_bfloat16 *wt;
     const float *bias;
     __nv_bfloat16 *out;
     int n, h, w;
     int in_off, cin;
     int out_c, out_off, cout;
     int relu, accumulate;
-    int bw, bh, tiles_x, tiles_y;
+    int tiles_x, tiles_y;
+    int stages, resident;
+    uint32_t w_bytes, stage_bytes;
     int *err;
 };
 
@@ -47,15 +68,16 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
-// bounded wait for the phase with parity `parity` to complete
+// bounded wait for the phase with parity `parity` to complete (the thread
+// sleeps in the barrier up to 20 us per try, woken by the phase's completion)
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int *abort) {
     long long t0 = clock64();
     for (;;) {
         uint32_t ok;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(ok)
-            : "r"(bar), "r"(parity)
+            : "r"(bar), "r"(parity), "r"(20000)
             : "memory");
         if (ok) return true;
         if (*abort || clock64() - t0 > TC_WAIT_CYCLES) return false;
@@ -70,21 +92,19 @@ __device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map
         "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
         : "memory");
 }
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int c0, int c1, uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            dst),
-        "l"((uint64_t)map), "r"(c0), "r"(c1), "r"(bar)
-        : "memory");
+// a contiguous block (16-byte aligned, a multiple of 16 bytes)
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
 }
 
-// shared memory descriptor of a K-major operand in the 32-byte swizzle:
-// rows of 32 bytes (16 bf16), 8-row groups 256 bytes apart
-__device__ __forceinline__ uint64_t desc_sw32(uint32_t addr) {
-    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16)  // leading byte offset (unused when swizzled)
-           | ((uint64_t)(256 >> 4) << 32)                           // stride byte offset: 8 rows x 32 B
-           | ((uint64_t)1 << 46)                                    // descriptor version
-           | ((uint64_t)6 << 61);                                   // layout: 32-byte swizzle
+// shared memory descriptor of a K-major operand without swizzle: core
+// matrices of 8 rows x 16 bytes (rows 16 bytes apart), `lbo` bytes between the
+// two 8-element halves of K, `sbo` bytes between 8-row groups
+__device__ __forceinline__ uint64_t desc_plain(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);  // version 1, layout 0 (no swizzle)
 }
 
 // instruction descriptor: FP32 accumulator, BF16 A and B, both K-major
@@ -96,40 +116,87 @@ __device__ __forceinline__ uint32_t idesc_bf16() {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+// 16 accumulator columns of one pixel: bias, ReLU, (the old value), bf16
+__device__ __forceinline__ void store16(__nv_bfloat16 *o, int nb, const uint32_t (&r)[16], const ConvTc &a) {
+    float v[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        v[k] = __uint_as_float(r[k]);
+        if (a.bias && nb + k < a.cout) v[k] += a.bias[nb + k];
+        if (a.relu) v[k] = fmaxf(v[k], 0.0f);
+    }
+    if (nb + 16 <= a.cout) {
+        __align__(16) __nv_bfloat162 p[8];
+        uint4 *dst = reinterpret_cast<uint4 *>(o + nb);
+        if (a.accumulate) {
+            uint4 old0 = dst[0], old1 = dst[1];
+            const __nv_bfloat162 *q0 = reinterpret_cast<const __nv_bfloat162 *>(&old0);
+            const __nv_bfloat162 *q1 = reinterpret_cast<const __nv_bfloat162 *>(&old1);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                v[2 * k] += __low2float(q0[k]);
+                v[2 * k + 1] += __high2float(q0[k]);
+                v[8 + 2 * k] += __low2float(q1[k]);
+                v[8 + 2 * k + 1] += __high2float(q1[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; k++) p[k] = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
+        dst[0] = *reinterpret_cast<const uint4 *>(&p[0]);
+        dst[1] = *reinterpret_cast<const uint4 *>(&p[4]);
+    } else {
+        for (int k = 0; k < 16 && nb + k < a.cout; k++) {
+            float x = v[k];
+            if (a.accumulate) x += __bfloat162float(o[nb + k]);
+            o[nb + k] = __float2bfloat16_rn(x);
+        }
+    }
+}
+
+__device__ __forceinline__ void tile_of(const ConvTc &a, int g, int &img, int &x0, int &y0) {
+    const int tx = g % a.tiles_x;
+    g /= a.tiles_x;
+    const int ty = g % a.tiles_y;
+    img = g / a.tiles_y;
+    x0 = tx * TILE_W;
+    y0 = ty * TILE_H;
+}
+
 template <int BN>
-__global__ void __launch_bounds__(128) k_conv3x3_tc(const __grid_constant__ CUtensorMap ta,
-                                                   const __grid_constant__ CUtensorMap tb, const ConvTc a) {
-    constexpr uint32_t A_BYTES = TC_M * 32, B_BYTES = BN * 32;
-    constexpr uint32_t COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+__global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ CUtensorMap ta, const ConvTc a) {
+    constexpr uint32_t COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;  // one accumulator
+    constexpr uint32_t B_TAP = BN * 32;                                               // one tap's weights
     extern __shared__ __align__(1024) uint8_t dyn[];
-    __shared__ __align__(8) uint64_t full[TC_STAGES], empty[TC_STAGES], done;
+    __shared__ __align__(8) uint64_t full[MAX_STAGES], empty[MAX_STAGES], acc_full[2], acc_empty[2], wbar;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
-    // (the dynamic area is aligned to 1024 bytes by hand)
+    // (the dynamic area is aligned to 1024 bytes by hand): the resident
+    // weights, then the stages (input box, and the group's weights when they
+    // are not resident)
     uint8_t *base = dyn + ((1024u - (smem_addr(dyn) & 1023u)) & 1023u);
-    const uint32_t sa0 = smem_addr(base), sb0 = sa0 + TC_STAGES * A_BYTES;
-
+    const uint32_t w0 = smem_addr(base), st0 = w0 + (a.resident ? a.w_bytes : 0u);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    int t = blockIdx.x;
-    const int tx = t % a.tiles_x;
-    t /= a.tiles_x;
-    const int ty = t % a.tiles_y, img = t / a.tiles_y;
-    const int x0 = tx * a.bw, y0 = ty * a.bh, n0 = blockIdx.y * BN;
-    const int cin16 = a.cin >> 4, kchunks = 9 * cin16;
+    const int groups = a.cin >> 4, ns = a.stages;
+    const int total = a.n * a.tiles_y * a.tiles_x;
+    const uint32_t grp_bytes = 9 * B_TAP;
 
     if (tid == 0) {
-        for (int s = 0; s < TC_STAGES; s++) {
+        for (int s = 0; s < ns; s++) {
             mbar_init(smem_addr(&full[s]), 1);
             mbar_init(smem_addr(&empty[s]), 1);
         }
-        mbar_init(smem_addr(&done), 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_addr(&acc_full[b]), 1);
+            mbar_init(smem_addr(&acc_empty[b]), 4);
+        }
+        mbar_init(smem_addr(&wbar), 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
-                     "r"(COLS)
+                     "r"(2 * COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -138,115 +205,123 @@ __global__ void __launch_bounds__(128) k_conv3x3_tc(const __grid_constant__ CUte
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
 
-    if (tid == 0) {
-        // the TMA producer
-        for (int kc = 0; kc < kchunks; kc++) {
-            const int s = kc % TC_STAGES;
-            if (kc >= TC_STAGES && !mbar_wait(smem_addr(&empty[s]), ((kc / TC_STAGES) - 1) & 1, &abort_flag)) {
-                abort_flag = 1;
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            // the TMA producer
+            if (a.resident) {
+                mbar_expect_tx(smem_addr(&wbar), a.w_bytes);
+                bulk_load(w0, a.wt, a.w_bytes, smem_addr(&wbar));
             }
-            const int tap = kc / cin16, ci0 = (kc - tap * cin16) << 4;
-            const int dy = tap / 3 - 1, dx = tap - (tap / 3) * 3 - 1;
-            const uint32_t bar = smem_addr(&full[s]);
-            mbar_expect_tx(bar, A_BYTES + B_BYTES);
-            tma_load_4d(sa0 + s * A_BYTES, &ta, a.in_off + ci0, x0 + dx, y0 + dy, img, bar);
-            tma_load_2d(sb0 + s * B_BYTES, &tb, tap * a.cin + ci0, n0, bar);
+            uint32_t q = 0;
+            for (int g = blockIdx.x; g < total && !abort_flag; g += gridDim.x) {
+                int img, x0, y0;
+                tile_of(a, g, img, x0, y0);
+                for (int grp = 0; grp < groups; grp++, q++) {
+                    const uint32_t s = q % (uint32_t)ns;
+                    if (q >= (uint32_t)ns && !mbar_wait(smem_addr(&empty[s]), ((q / ns) - 1) & 1, &abort_flag)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    const uint32_t bar = smem_addr(&full[s]), sa = st0 + s * a.stage_bytes;
+                    mbar_expect_tx(bar, 2 * BOX_BYTES + (a.resident ? 0u : grp_bytes));
+                    const int c = a.in_off + 16 * grp;
+                    tma_load_4d(sa, &ta, c, x0 - 1, y0 - 1, img, bar);
+                    tma_load_4d(sa + HALF_BYTES, &ta, c + 8, x0 - 1, y0 - 1, img, bar);
+                    if (!a.resident) bulk_load(sa + A_BYTES, a.wt + (size_t)grp * 9 * BN * 16, grp_bytes, bar);
+                }
+            }
         }
-    } else if (tid == 32) {
-        // the MMA issuer
-        const uint32_t idesc = idesc_bf16<BN>();
-        bool ok = true;
-        for (int kc = 0; kc < kchunks; kc++) {
-            const int s = kc % TC_STAGES;
-            if (!mbar_wait(smem_addr(&full[s]), (kc / TC_STAGES) & 1, &abort_flag)) {
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // the MMA issuer: nine taps per group; tile i accumulates in buffer i % 2
+            const uint32_t idesc = idesc_bf16<BN>();
+            if (a.resident && !mbar_wait(smem_addr(&wbar), 0, &abort_flag)) abort_flag = 1;
+            uint32_t q = 0;
+            int i = 0;
+            for (int g = blockIdx.x; g < total && !abort_flag; g += gridDim.x, i++) {
+                const int buf = i & 1;
+                if (i >= 2 && !mbar_wait(smem_addr(&acc_empty[buf]), ((i >> 1) - 1) & 1, &abort_flag)) {
+                    abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)buf * COLS;
+                for (int grp = 0; grp < groups; grp++, q++) {
+                    const uint32_t s = q % (uint32_t)ns;
+                    if (!mbar_wait(smem_addr(&full[s]), (q / ns) & 1, &abort_flag)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = st0 + s * a.stage_bytes;
+                    const uint32_t sb = a.resident ? w0 + (uint32_t)grp * grp_bytes : sa + A_BYTES;
+#pragma unroll
+                    for (int tap = 0; tap < 9; tap++) {
+                        const int dy = tap / 3, dx = tap % 3;  // (offsets + 1)
+                        const uint64_t ad = desc_plain(sa + (uint32_t)(dy * HALO_W + dx) * 16, HALF_BYTES, HALO_W * 16);
+                        const uint64_t bd = desc_plain(sb + (uint32_t)tap * B_TAP, BN * 16, 128);
+                        const uint32_t acc = (grp | tap) ? 1u : 0u;
+                        asm volatile(
+                            "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+                            "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                            : "memory");
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_addr(&empty[s]))
+                                 : "memory");
+                }
+                if (abort_flag) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_addr(&acc_full[buf]))
+                             : "memory");
+            }
+        }
+    } else {
+        // the epilogue warps 2..5: warp w reads TMEM lanes 32 (w % 4) .. + 31
+        const int quarter = warp & 3, row = quarter * 32 + lane;
+        int i = 0;
+        for (int g = blockIdx.x; g < total; g += gridDim.x, i++) {
+            const int buf = i & 1;
+            bool ready = mbar_wait(smem_addr(&acc_full[buf]), (i >> 1) & 1, &abort_flag);
+            ready = __all_sync(0xffffffffu, ready);
+            if (!ready) {
                 abort_flag = 1;
-                ok = false;
                 break;
             }
             tc_fence_after();
-            const uint64_t ad = desc_sw32(sa0 + s * A_BYTES), bd = desc_sw32(sb0 + s * B_BYTES);
-            const uint32_t acc = kc > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-                "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                : "memory");
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_addr(&empty[s]))
-                         : "memory");
-        }
-        if (ok)
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_addr(&done))
-                         : "memory");
-    }
-    __syncwarp();
-
-    // the epilogue: TMEM -> registers -> bias, ReLU -> bf16 NHWC
-    bool ready = mbar_wait(smem_addr(&done), 0, &abort_flag);
-    if (!ready) abort_flag = 1;
-    ready = __all_sync(0xffffffffu, ready);
-    tc_fence_after();
-    if (ready) {
-        const int row = warp * 32 + lane;
-        const int px = x0 + row % a.bw, py = y0 + row / a.bw;
-        const bool valid = px < a.w && py < a.h;
-        __nv_bfloat16 *o = a.out + ((size_t)(img * a.h + (valid ? py : 0)) * a.w + (valid ? px : 0)) * a.out_c + a.out_off;
+            int img, x0, y0;
+            tile_of(a, g, img, x0, y0);
+            const int px = x0 + row % TILE_W, py = y0 + row / TILE_W;
+            const bool valid = px < a.w && py < a.h;
+            __nv_bfloat16 *o =
+                a.out + ((size_t)(img * a.h + (valid ? py : 0)) * a.w + (valid ? px : 0)) * a.out_c + a.out_off;
 #pragma unroll
-        for (int c = 0; c < BN; c += 16) {
-            uint32_t r[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                : "r"(taddr)
-                : "memory");
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const int nb = n0 + c;
-            if (valid && nb < a.cout) {
-                float v[16];
-#pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    v[k] = __uint_as_float(r[k]);
-                    if (a.bias && nb + k < a.cout) v[k] += a.bias[nb + k];
-                    if (a.relu) v[k] = fmaxf(v[k], 0.0f);
-                }
-                if (nb + 16 <= a.cout) {
-                    __align__(16) __nv_bfloat162 p[8];
-                    uint4 *dst = reinterpret_cast<uint4 *>(o + nb);
-                    if (a.accumulate) {
-                        uint4 old0 = dst[0], old1 = dst[1];
-                        const __nv_bfloat162 *q0 = reinterpret_cast<const __nv_bfloat162 *>(&old0);
-                        const __nv_bfloat162 *q1 = reinterpret_cast<const __nv_bfloat162 *>(&old1);
-#pragma unroll
-                        for (int k = 0; k < 4; k++) {
-                            v[2 * k] += __low2float(q0[k]);
-                            v[2 * k + 1] += __high2float(q0[k]);
-                            v[8 + 2 * k] += __low2float(q1[k]);
-                            v[8 + 2 * k + 1] += __high2float(q1[k]);
-                        }
-                    }
-#pragma unroll
-                    for (int k = 0; k < 8; k++) p[k] = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
-                    dst[0] = *reinterpret_cast<const uint4 *>(&p[0]);
-                    dst[1] = *reinterpret_cast<const uint4 *>(&p[4]);
-                } else {
-                    for (int k = 0; k < 16 && nb + k < a.cout; k++) {
-                        float x = v[k];
-                        if (a.accumulate) x += __bfloat162float(o[nb + k]);
-                        o[nb + k] = __float2bfloat16_rn(x);
-                    }
-                }
+            for (int c = 0; c < BN; c += 16) {
+                uint32_t r[16];
+                const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * COLS + c);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                    : "r"(taddr)
+                    : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (valid && c < a.cout) store16(o, c, r, a);
             }
+            // the accumulator buffer is free for the MMAs of tile i + 2
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&acc_empty[buf])) : "memory");
         }
     }
-    if (tid == 0 && abort_flag) atomicExch(a.err, 1);
     tc_fence_before();
     __syncthreads();
+    if (tid == 0 && abort_flag) atomicExch(a.err, 1);
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(COLS) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * COLS) : "memory");
 }
 
 // cuTensorMapEncodeTiled from the driver, looked up once
@@ -274,41 +349,44 @@ int *err_word() {
     return e;
 }
 
-template <int BN>
-void launch_tc(const CUtensorMap &ta, const CUtensorMap &tb, const ConvTc &c, int tiles, int ntiles, cudaStream_t s) {
-    const size_t smem = 1024 + (size_t)TC_STAGES * (TC_M * 32 + BN * 32);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_conv3x3_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
+int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            n < 1)
+            n = 148;
     }
-    k_conv3x3_tc<BN><<<dim3(tiles, ntiles), 128, smem, s>>>(ta, tb, c);
+    return n;
+}
+
+template <int BN>
+void launch_tc(const CUtensorMap &ta, ConvTc c, int total, cudaStream_t s) {
+    // the weights stay in shared memory where they leave room for 8 stages
+    const uint32_t grp_bytes = 9u * BN * 32u;
+    c.w_bytes = (uint32_t)(c.cin / 16) * grp_bytes;
+    c.resident = c.w_bytes <= RESIDENT_MAX && c.w_bytes + 8 * A_BYTES <= SMEM_BUDGET;
+    c.stage_bytes = c.resident ? A_BYTES : A_BYTES + grp_bytes;
+    const uint32_t room = SMEM_BUDGET - (c.resident ? c.w_bytes : 0u);
+    int st = (int)(room / c.stage_bytes);
+    c.stages = st > MAX_STAGES ? MAX_STAGES : st < 2 ? 2 : st;
+    const size_t smem = 1024 + (c.resident ? c.w_bytes : 0u) + (size_t)c.stages * c.stage_bytes;
+    cudaFuncSetAttribute(k_conv3x3_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int grid = sm_count();
+    if (grid > total) grid = total;
+    k_conv3x3_tc<BN><<<grid, 192, smem, s>>>(ta, c);
 }
 
 }  // namespace
 
-// the picture box of a tile: 128 pixels, as wide as the picture needs (a
-// power of two from 8 to 128)
-static void tile_box(int w, int &bw, int &bh) {
-    bw = 128;
-    while (bw > 8 && bw / 2 >= w) bw /= 2;
-    bh = TC_M / bw;
-}
-
 int dn_conv(const ConvArgs &a, cudaStream_t s) {
-    if (a.cin % 16 || a.cout <= 0 || a.in_c % 8 || a.in_off % 8 || a.out_c % 8 || a.out_off % 8) return -1;
+    if (a.cin % 16 || a.cout % 16 || a.cout > 256 || a.in_c % 8 || a.in_off % 8 || a.out_c % 8 || a.out_off % 8) return -1;
     if (a.n < 1 || a.h < 1 || a.w < 1 || a.in_c < a.in_off + a.cin || a.out_c < a.out_off + a.cout) return -1;
     EncodeTiledFn enc = encode_fn();
     int *err = err_word();
     if (!enc || !err) return -1;
-    const int bn_max = 256;
-    int bn = ((a.cout + 15) / 16) * 16;
-    int ntiles = 1;
-    if (bn > bn_max) {
-        ntiles = (a.cout + bn_max - 1) / bn_max;
-        bn = ((a.cout + ntiles * 16 - 1) / (ntiles * 16)) * 16;
-    }
     ConvTc c;
+    c.wt = a.wt;
     c.bias = a.bias;
     c.out = a.out;
     c.n = a.n;
@@ -321,45 +399,41 @@ int dn_conv(const ConvArgs &a, cudaStream_t s) {
     c.cout = a.cout;
     c.relu = a.relu;
     c.accumulate = a.accumulate;
-    tile_box(a.w, c.bw, c.bh);
-    c.tiles_x = (a.w + c.bw - 1) / c.bw;
-    c.tiles_y = (a.h + c.bh - 1) / c.bh;
+    c.tiles_x = (a.w + TILE_W - 1) / TILE_W;
+    c.tiles_y = (a.h + TILE_H - 1) / TILE_H;
     c.err = err;
-    // the activations: dims (channels, x, y, image), the box 16 channels x bw x bh
-    CUtensorMap ta, tb;
+    c.stages = 2;
+    c.resident = 0;
+    c.w_bytes = 0;
+    c.stage_bytes = 0;
+    // the activations: dims (channels, x, y, image), the box 8 channels x the
+    // tile's 10 x 18 pixels with the halo
+    CUtensorMap ta;
     cuuint64_t da[4] = {(cuuint64_t)a.in_c, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
     cuuint64_t sa[3] = {(cuuint64_t)a.in_c * 2, (cuuint64_t)a.in_c * 2 * a.w, (cuuint64_t)a.in_c * 2 * a.w * a.h};
-    cuuint32_t ba[4] = {16, (cuuint32_t)c.bw, (cuuint32_t)c.bh, 1};
+    cuuint32_t ba[4] = {8, (cuuint32_t)HALO_W, (cuuint32_t)HALO_H, 1};
     cuuint32_t ea[4] = {1, 1, 1, 1};
     if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.in, da, sa, ba, ea, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return -1;
-    // the weights [cout][9 * cin]: the box 16 K-columns x bn rows
-    cuuint64_t dw[2] = {(cuuint64_t)9 * a.cin, (cuuint64_t)a.cout};
-    cuuint64_t sw[1] = {(cuuint64_t)9 * a.cin * 2};
-    cuuint32_t bw_[2] = {16, (cuuint32_t)bn};
-    cuuint32_t ew[2] = {1, 1};
-    if (enc(&tb, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)a.wt, dw, sw, bw_, ew, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return -1;
     const int tiles = a.n * c.tiles_y * c.tiles_x;
-    switch (bn) {
-        case 16: launch_tc<16>(ta, tb, c, tiles, ntiles, s); break;
-        case 32: launch_tc<32>(ta, tb, c, tiles, ntiles, s); break;
-        case 48: launch_tc<48>(ta, tb, c, tiles, ntiles, s); break;
-        case 64: launch_tc<64>(ta, tb, c, tiles, ntiles, s); break;
-        case 80: launch_tc<80>(ta, tb, c, tiles, ntiles, s); break;
-        case 96: launch_tc<96>(ta, tb, c, tiles, ntiles, s); break;
-        case 112: launch_tc<112>(ta, tb, c, tiles, ntiles, s); break;
-        case 128: launch_tc<128>(ta, tb, c, tiles, ntiles, s); break;
-        case 144: launch_tc<144>(ta, tb, c, tiles, ntiles, s); break;
-        case 160: launch_tc<160>(ta, tb, c, tiles, ntiles, s); break;
-        case 176: launch_tc<176>(ta, tb, c, tiles, ntiles, s); break;
-        case 192: launch_tc<192>(ta, tb, c, tiles, ntiles, s); break;
-        case 208: launch_tc<208>(ta, tb, c, tiles, ntiles, s); break;
-        case 224: launch_tc<224>(ta, tb, c, tiles, ntiles, s); break;
-        case 240: launch_tc<240>(ta, tb, c, tiles, ntiles, s); break;
-        default: launch_tc<256>(ta, tb, c, tiles, ntiles, s); break;
+    switch (a.cout) {
+        case 16: launch_tc<16>(ta, c, tiles, s); break;
+        case 32: launch_tc<32>(ta, c, tiles, s); break;
+        case 48: launch_tc<48>(ta, c, tiles, s); break;
+        case 64: launch_tc<64>(ta, c, tiles, s); break;
+        case 80: launch_tc<80>(ta, c, tiles, s); break;
+        case 96: launch_tc<96>(ta, c, tiles, s); break;
+        case 112: launch_tc<112>(ta, c, tiles, s); break;
+        case 128: launch_tc<128>(ta, c, tiles, s); break;
+        case 144: launch_tc<144>(ta, c, tiles, s); break;
+        case 160: launch_tc<160>(ta, c, tiles, s); break;
+        case 176: launch_tc<176>(ta, c, tiles, s); break;
+        case 192: launch_tc<192>(ta, c, tiles, s); break;
+        case 208: launch_tc<208>(ta, c, tiles, s); break;
+        case 224: launch_tc<224>(ta, c, tiles, s); break;
+        case 240: launch_tc<240>(ta, c, tiles, s); break;
+        default: launch_tc<256>(ta, c, tiles, s); break;
     }
     return 0;
 }
