@@ -249,6 +249,14 @@ def mc_figures(card, ref_rays):
     dn = mb3dcu.Denoiser(card)
     dn.set_params(np.fromfile(T.WEIGHTS, "<f4"))
     ref, st_ref = trace(ref_rays, 4096)  # (independent rays, each with its own Halton record)
+    paint_opts = mb3dcu.mc_paint_default()
+    ref8 = card.mc_paint(ref["radiance"], paint_opts).astype(np.float64)
+
+    def psnr8(x):
+        # the reference's displayed picture (paint_recs, 8 bits) against the reference trace's
+        mse = np.mean((card.mc_paint(x, paint_opts).astype(np.float64) - ref8) ** 2)
+        return float(10 * np.log10(255.0 ** 2 / max(mse, 1e-12)))
+
     out = {"workload": "c5: hybrid scene 1920x1080, MCDepth 4, light 1 + sky; rectangle 480x270 at (720, 405)",
            "ref_rays": ref_rays, "ms_ref": st_ref["ms_total"],
            "mpaths_per_s": rect[2] * rect[3] * ref_rays / st_ref["ms_total"] / 1e3,
@@ -271,10 +279,14 @@ def mc_figures(card, ref_rays):
         out["levels"].append({"rays": rays, "ms_trace": st["ms_total"], "ms_denoise": ms_dn,
                               "psnr_noisy": T.psnr(r["radiance"], ref["radiance"]),
                               "psnr_denoised": T.psnr(den, ref["radiance"]),
-                              "psnr_with_fallback": T.psnr(comp, ref["radiance"]), "fallback_rate": fb})
+                              "psnr_with_fallback": T.psnr(comp, ref["radiance"]), "fallback_rate": fb,
+                              "psnr8_noisy": psnr8(r["radiance"]), "psnr8_denoised": psnr8(den),
+                              "psnr8_with_fallback": psnr8(comp)})
     l16 = out["levels"][1]
     out["time_ratio_16_denoised_vs_ref"] = (l16["ms_trace"] + l16["ms_denoise"]) / out["ms_ref"]
-    out["psnr_metric"] = "PSNR of x/(1+x) tone-mapped linear records against the plain trace of ref_rays rays"
+    out["psnr_metric"] = ("psnr_*: PSNR of x/(1+x) tone-mapped linear records against the plain trace of ref_rays "
+                          "rays; psnr8_*: PSNR of the 8-bit pictures paint_recs makes of both (default display "
+                          "settings), on the card")
     dn.close()
     card.set_stream(None)
     return out
@@ -454,7 +466,8 @@ def main():
                    "h2d_bytes_per_step": ctypes.sizeof(mb3dcu.Scene), "d2h_bytes_per_step": npix * 20},
            "gpu_launches": launches, "roofline": roof, "stages_ms": stage,
            "peaks": {"fp32_fma_tflops": peak32, "fp64_fma_tflops": peak64},
-           "counted": {"de_evals": counted["de_evals"], "orbit_its": counted["orbit_its"]},
+           "counted": {"de_evals": counted["de_evals"], "orbit_its": counted["orbit_its"],
+                       "march_de_evals_per_s": counted["de_evals"] / (k_ms / 1000.0)},
            "clocks": clocks}
     if rank == 0:
         # the plain FP64 march (the drop-in) on the same frame, and the mixed

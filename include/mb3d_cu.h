@@ -345,6 +345,28 @@ int mb3d_cu_mc_render(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_c
                       const mb3d_cu_mc_opts *opts, int precision, const mb3d_cu_mc_out *out,
                       const volatile int *cancel);
 
+/* The display settings of the Monte Carlo picture (McSettings::contrast,
+ * saturation, options; Lighting::gamma; src/scene.rs:591-598): */
+typedef struct {
+    uint8_t contrast;   /* MCcontrast, exposure 0..255 (128 = 1) */
+    uint8_t saturation; /* 0..127 (32 = 1) */
+    uint8_t options;    /* bit 0: soft clipping (HDR) */
+    uint8_t pad;
+    float gamma;        /* the lighting's gamma slider (32 = none) */
+} mb3d_cu_mc_paint_opts;
+
+/* mb3d_cu_mc_paint_opts of McSettings::default and Lighting::default. */
+void mb3d_cu_mc_paint_default(mb3d_cu_mc_paint_opts *out);
+
+/* paint_recs (src/mc.rs:3957-4005) on the card: the records' colours (3
+ * floats per pixel, e.g. mb3d_cu_mc_render's radiance or the denoised
+ * picture) to 8-bit RGB: exposure, squared, to Lab, the gamma curve and
+ * the soft clip on L, saturation, back to RGB, square root, rounded.  `rays`
+ * (npix bytes, or NULL: every pixel has rays) marks pixels without rays,
+ * which stay black.  Host or device buffers. */
+int mb3d_cu_mc_paint(mb3d_cu_ctx *ctx, const float *colour, const uint8_t *rays, uint32_t npix,
+                     const mb3d_cu_mc_paint_opts *opts, uint8_t *rgb);
+
 /* ---- the learned denoiser of the Monte Carlo pictures ----
  * A 5-level U-Net of 3x3 convolutions (32/48/64/80/96 channels) that
  * takes the noisy colour and the albedo, normal and depth guides of a

@@ -72,6 +72,8 @@ struct mb3d_cu_ctx {
     size_t mc_cap = 0;
     unsigned char *d_mcs = nullptr;  // the split render's paths, requests, results, list
     size_t mcs_cap = 0;
+    unsigned char *d_paint = nullptr;  // the painter's staging of host buffers
+    size_t paint_cap = 0;
     std::mutex mu;
 };
 
@@ -170,6 +172,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_halton);
     cudaFree(c->d_mc);
     cudaFree(c->d_mcs);
+    cudaFree(c->d_paint);
     for (auto &ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     for (auto &s : c->fscratch) {
@@ -714,6 +717,52 @@ int mb3d_cu_mc_light_default(const mb3d_cu_scene *sc, mb3d_cu_mc_light *out) {
     if (!sc || !out) return fail(MB3D_CU_EINVAL, "NULL argument");
     if (sc->width <= 0 || sc->height <= 0 || !(sc->zoom > 0.0)) return fail(MB3D_CU_EINVAL, "bad picture size or zoom");
     return mc_light_default(*sc, *out);
+}
+
+void mb3d_cu_mc_paint_default(mb3d_cu_mc_paint_opts *o) {
+    if (!o) return;
+    o->contrast = 128;
+    o->saturation = 32;
+    o->options = 2;
+    o->pad = 0;
+    o->gamma = 32.0f;
+}
+
+int mb3d_cu_mc_paint(mb3d_cu_ctx *c, const float *col, const uint8_t *rays, uint32_t npix, const mb3d_cu_mc_paint_opts *o,
+                     uint8_t *rgb) {
+    if (!c || !col || !o || !rgb) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (npix == 0) return 0;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    cudaStream_t s = c->stream;
+    const bool dc = is_device_ptr(col), dr = !rays || is_device_ptr(rays), dg = is_device_ptr(rgb);
+    const size_t bc = (size_t)npix * 12, br = npix, bg = (size_t)npix * 3;
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    size_t need = (dc ? 0 : up16(bc)) + (dr ? 0 : up16(br)) + (dg ? 0 : up16(bg));
+    if (need)
+        if (int r = grow((void **)&c->d_paint, &c->paint_cap, need)) return r;
+    unsigned char *q = c->d_paint;
+    const float *dcol = col;
+    const uint8_t *drays = rays;
+    uint8_t *drgb = rgb;
+    if (!dc) {
+        CU_TRY(cudaMemcpyAsync(q, col, bc, cudaMemcpyHostToDevice, s));
+        dcol = (const float *)q;
+        q += up16(bc);
+    }
+    if (!dr) {
+        CU_TRY(cudaMemcpyAsync(q, rays, br, cudaMemcpyHostToDevice, s));
+        drays = q;
+        q += up16(br);
+    }
+    if (!dg) drgb = q;
+    int blocks = (int)std::min<size_t>(((size_t)npix + 255) / 256, (size_t)c->sms * 8);
+    mc_paint_launch(dcol, drays, npix, *o, drgb, blocks, s);
+    if (int r = check_launch("k_mc_paint")) return r;
+    if (!dg) CU_TRY(cudaMemcpyAsync(rgb, drgb, bg, cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    return 0;
 }
 
 static int mc_halton(mb3d_cu_ctx *c) {

@@ -103,4 +103,8 @@ void launch_mc_logic(const DevParams &p, const McDev &m, const McAcc &acc, void 
                      unsigned int *n_list, int sms, cudaStream_t s);
 void launch_mc_final(const McAcc &acc, uint32_t npix, int rays, float *radiance, uint8_t *hit, cudaStream_t s);
 
+// paint_recs of the Monte Carlo records' colours (mc_paint.cu)
+void mc_paint_launch(const float *col, const uint8_t *rays, uint32_t n, const mb3d_cu_mc_paint_opts &mc, uint8_t *out,
+                     int blocks, cudaStream_t s);
+
 }  // namespace mb3dcu

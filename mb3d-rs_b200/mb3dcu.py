@@ -123,6 +123,19 @@ class McOut(ctypes.Structure):
                 ("depth", ctypes.c_void_p), ("hit", ctypes.c_void_p)]
 
 
+class McPaintOpts(ctypes.Structure):
+    """mb3d_cu_mc_paint_opts: McSettings' contrast, saturation, options and the
+    lighting's gamma."""
+    _fields_ = [("contrast", ctypes.c_uint8), ("saturation", ctypes.c_uint8), ("options", ctypes.c_uint8),
+                ("pad", ctypes.c_uint8), ("gamma", ctypes.c_float)]
+
+
+def mc_paint_default():
+    o = McPaintOpts()
+    lib().mb3d_cu_mc_paint_default(ctypes.byref(o))
+    return o
+
+
 def mc_opts(rays, depth=3, ray0=0, secant=True, soft_shadow_radius=1.0, rect=None):
     """McSettings' defaults (src/scene.rs:607-624): depth 3, options 2 (secant)."""
     x0, y0, w, h = rect if rect is not None else (0, 0, 0, 0)
@@ -194,6 +207,9 @@ def lib():
         L.mb3d_cu_mc_batch.argtypes = [vp, sp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_uint32, vp]
         L.mb3d_cu_mc_render.argtypes = [vp, sp, ctypes.POINTER(McLight), ctypes.POINTER(McOpts), ctypes.c_int,
                                         ctypes.POINTER(McOut), vp]
+        L.mb3d_cu_mc_paint_default.argtypes = [ctypes.POINTER(McPaintOpts)]
+        L.mb3d_cu_mc_paint_default.restype = None
+        L.mb3d_cu_mc_paint.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.POINTER(McPaintOpts), vp]
         _lib = L
     return _lib
 
@@ -202,6 +218,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render",
+            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
             "mb3d_cu_dn_conv_check"]
@@ -343,6 +360,22 @@ class Card:
         self._check(lib().mb3d_cu_mc_batch(self._ctx, ctypes.byref(scene), precision, int(bool(secant)),
                                            ctypes.addressof(reqs), n, ctypes.addressof(res)))
         return res
+
+    def mc_paint(self, colour, opts=None, rays=None, out=None):
+        """paint_recs on the card: colours (..., 3) float32 (numpy, or a torch
+        CUDA tensor) to 8-bit RGB (..., 3); `rays` marks pixels with rays."""
+        opts = mc_paint_default() if opts is None else opts
+        if isinstance(colour, np.ndarray):
+            colour = np.ascontiguousarray(colour, dtype=np.float32)
+        if out is None:
+            out = np.zeros(tuple(colour.shape[:-1]) + (3,), np.uint8)
+        if rays is not None and isinstance(rays, np.ndarray):
+            rays = np.ascontiguousarray(rays, dtype=np.uint8)
+        n = int(np.prod(colour.shape[:-1]))
+        self._order(colour, rays, out)
+        self._check(lib().mb3d_cu_mc_paint(self._ctx, _ptr(colour)[0], None if rays is None else _ptr(rays)[0], n,
+                                           ctypes.byref(opts), _ptr(out)[0]))
+        return out
 
     def mc_render(self, scene, opts, light=None, precision=FP32_FP64, out=None, cancel=None):
         """The Monte Carlo rays of opts on the card: a dict of radiance, albedo,

@@ -882,11 +882,107 @@ struct Tracer {
     }
 };
 
+// SVecRGB2Lab (src/mc.rs:3906-3919), single precision
+static void rgb_to_lab(const float v[3], float o[3]) {
+    const float sftc = 216.0f / (29.0f * 29.0f * 29.0f), s4d29 = 4.0f / 29.0f, smul = 29.0f * 29.0f / 108.0f;
+    float x[3] = {(0.412453f * v[0] + 0.35758f * v[1] + 0.180423f * v[2]) * 1.052111f,
+                  0.212671f * v[0] + 0.71516f * v[1] + 0.072169f * v[2],
+                  (0.019334f * v[0] + 0.119193f * v[1] + 0.950227f * v[2]) * 0.918417f};
+    for (float &c : x) c = c > sftc ? std::cbrt(c) : smul * c + s4d29;
+    o[0] = 1.16f * x[1] - 0.16f;
+    o[1] = x[0] - x[1];
+    o[2] = x[1] - x[2];
+}
+
+// SVecLab2RGB (src/mc.rs:3922-3938)
+static void lab_to_rgb(const float v[3], float o[3]) {
+    const float sftc = 6.0f / 29.0f, s4d29 = 4.0f / 29.0f, smul = 108.0f / 841.0f;
+    float y = (v[0] + 0.16f) / 1.16f;
+    float x[3] = {y + v[1], y, y - v[2]};
+    for (float &c : x) c = c > sftc ? c * c * c : (c - s4d29) * smul;
+    x[0] *= 0.95047f;
+    x[2] *= 1.08883f;
+    o[0] = 3.240479f * x[0] - 1.537150f * x[1] - 0.498535f * x[2];
+    o[1] = -0.969256f * x[0] + 1.875992f * x[1] + 0.041556f * x[2];
+    o[2] = 0.055648f * x[0] - 0.204043f * x[1] + 1.057311f * x[2];
+}
+
+// paint_recs (src/mc.rs:3957-4005): records' colours to 8-bit RGB
+static void paint_recs(const float *col, const uint8_t *rays, size_t n, const mb3d_cu_mc_paint_opts &mc, uint8_t *out) {
+    float contrast = (float)mc.contrast / 256.0f + 0.5f;
+    contrast = contrast * contrast;
+    const bool soft_clip = (mc.options & 1) != 0;
+    const float saturation = (float)(mc.saturation & 0x7F) / 32.0f;
+    // (gamma.round() as i32).clamp(0, 63): the cast saturates, NaN gives 0
+    float gr = std::round(mc.gamma);
+    int ig = std::isnan(gr) ? 0 : gr < 0.0f ? 0 : gr > 63.0f ? 63 : (int)gr;
+    int igamma = (ig << 2) & 0xFC;
+    if (soft_clip) {
+        igamma = std::max(igamma - 20, 0);
+        contrast *= 1.1f;
+    }
+    int gmode;
+    float sgamma;
+    if (igamma > 128) {
+        gmode = 1;
+        sgamma = (float)(igamma - 128) / 127.0f;
+    } else if (igamma < 128) {
+        gmode = -1;
+        sgamma = 1.0f - (float)igamma / 128.0f;
+    } else {
+        gmode = 0;
+        sgamma = 1.0f;
+    }
+    for (size_t i = 0; i < n; i++) {
+        uint8_t *o = out + 3 * i;
+        o[0] = o[1] = o[2] = 0;
+        if (rays && !rays[i]) continue;
+        float v[3];
+        for (int k = 0; k < 3; k++) {
+            float c = std::max(col[3 * i + k] * contrast, 0.0f);
+            v[k] = c * c;
+        }
+        float lab[3];
+        rgb_to_lab(v, lab);
+        float scol = saturation;
+        if (lab[0] > 0.0f) {
+            if (gmode != 0) {
+                float s2 = lab[0];
+                float s = gmode > 0 ? std::sqrt(lab[0]) : lab[0] * lab[0];
+                lab[0] += (s - lab[0]) * sgamma;
+                if (gmode > 0 && s2 > 1.0f) scol *= lab[0] / s2;
+            }
+            if (soft_clip) {
+                float s = lab[0];
+                float x2 = s * s;
+                float q = x2 * 0.9f;
+                lab[0] = std::sqrt(x2 / std::sqrt(q * q + 1.0f));
+                scol *= lab[0] / s;
+            }
+        }
+        lab[1] *= scol;
+        lab[2] *= scol;
+        float rgb[3];
+        lab_to_rgb(lab, rgb);
+        for (int k = 0; k < 3; k++) {
+            float c = std::sqrt(std::max(rgb[k], 0.0f));
+            c = std::min(std::max(c, 0.0f), 1.0f) * 255.0f;
+            o[k] = (uint8_t)std::round(c);
+        }
+    }
+}
+
 }  // namespace oracle
 
 using namespace oracle;
 
 extern "C" {
+
+/* paint_recs of n records' colours (3 floats each); rays (n bytes) may be
+ * NULL. */
+void oracle_mc_paint(const float *col, const uint8_t *rays, size_t n, const mb3d_cu_mc_paint_opts *opts, uint8_t *rgb) {
+    paint_recs(col, rays, n, *opts, rgb);
+}
 
 /* The Monte Carlo tracer's rays (ray0 .. ray0+rays-1) on the pixels of the
  * options' rectangle.  Outputs (w*h*3 doubles: radiance, albedo, normal; w*h:

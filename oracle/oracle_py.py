@@ -42,6 +42,8 @@ def lib():
         L.oracle_mc_halton.restype = None
         L.oracle_mc_seed_of.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
         L.oracle_mc_seed_of.restype = ctypes.c_int32
+        L.oracle_mc_paint.argtypes = [vp, vp, ctypes.c_size_t, vp, vp]
+        L.oracle_mc_paint.restype = None
         _lib = L
     return _lib
 
@@ -153,3 +155,15 @@ def mc_halton(i, x1, y):
 
 def mc_seed_of(x, y, b):
     return lib().oracle_mc_seed_of(x, y, b)
+
+
+def mc_paint(colour, opts, rays=None):
+    """paint_recs (src/mc.rs:3957-4005): float colours (..., 3) -> uint8 RGB;
+    opts is an mb3d_cu_mc_paint_opts (mb3dcu.McPaintOpts)."""
+    col = np.ascontiguousarray(colour, dtype=np.float32)
+    n = col.size // 3
+    out = np.zeros(col.shape[:-1] + (3,), np.uint8)
+    r = None if rays is None else np.ascontiguousarray(rays, dtype=np.uint8)
+    lib().oracle_mc_paint(col.ctypes.data, None if r is None else r.ctypes.data, n, ctypes.addressof(opts),
+                          out.ctypes.data)
+    return out

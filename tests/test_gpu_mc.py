@@ -183,6 +183,36 @@ def test_mc_errors(card):
     assert e.value.status == mb3dcu.ECANCELED
 
 
+def test_mc_paint_matches_oracle(card):
+    """paint_recs on the card against the oracle's: HDR and negative colours,
+    the soft clip, both gamma curves, saturation, pixels without rays, host
+    and device buffers.  The same single precision arithmetic, unfused on
+    both sides; cube roots may differ in the last bit, which moves a byte by
+    at most one."""
+    import torch
+    rng = np.random.default_rng(21)
+    c = np.concatenate([rng.uniform(-0.3, 1.5, (30000, 3)), rng.gamma(0.7, 3.0, (10000, 3))]).astype(np.float32)
+    rays = (rng.uniform(size=len(c)) > 0.05).astype(np.uint8)
+    settings = []
+    for contrast, sat, options, gamma in ((128, 32, 2, 32.0), (200, 40, 3, 32.0), (128, 32, 2, 63.0),
+                                          (90, 32, 2, 0.0), (128, 64, 1, 50.0)):
+        o = mb3dcu.mc_paint_default()
+        o.contrast, o.saturation, o.options, o.gamma = contrast, sat, options, gamma
+        settings.append(o)
+    for o in settings:
+        want = O.mc_paint(c, o, rays).astype(int)
+        got = card.mc_paint(c, o, rays).astype(int)
+        assert np.abs(got - want).max() <= 1, (o.contrast, o.options, o.gamma)
+        assert (got == want).mean() >= 0.999, (o.contrast, o.options, o.gamma)
+    # device buffers (torch), no ray mask
+    o = settings[1]
+    dc = torch.from_numpy(c).cuda()
+    dout = torch.zeros((len(c), 3), dtype=torch.uint8, device="cuda")
+    card.mc_paint(dc, o, None, out=dout)
+    want = O.mc_paint(c, o).astype(int)
+    assert np.abs(dout.cpu().numpy().astype(int) - want).max() <= 1
+
+
 def test_split_render_equals_one_kernel_render(card, monkeypatch):
     """The split render (logic kernel + list-fed march kernel, the default)
     traces the same rays as the one-kernel form: in double precision the

@@ -223,6 +223,42 @@ def test_mc_oracle_is_deterministic_and_sane():
     assert np.all(np.abs(n[a["depth"] > 0] - 1.0) < 1e-9)
 
 
+def test_mc_painter_lab_round_trip():
+    """mc.rs lab_roundtrip (src/mc.rs:4187-4195): RGB -> Lab -> RGB within
+    1e-3 for its three colours, seen through the painter with the default
+    settings (exposure 1, no gamma curve, no soft clip, saturation 1), which
+    squares, converts there and back and takes the square root."""
+    opts = mb3dcu.mc_paint_default()
+    assert (opts.contrast, opts.saturation, opts.options, opts.gamma) == (128, 32, 2, 32.0)
+    for v in ([0.2, 0.5, 0.8], [1.0, 1.0, 1.0], [0.01, 0.0, 0.3]):
+        c = np.sqrt(np.array([v], np.float32))
+        rgb = O.mc_paint(c, opts)[0].astype(np.float64)
+        # |sqrt(v + e) - sqrt(v)| * 255 with |e| <= 1e-3, plus the rounding
+        tol = 255 * np.max(np.sqrt(np.array(v) + 1e-3) - np.sqrt(v)) + 0.5
+        assert np.abs(rgb - 255 * c[0]).max() <= tol, (v, rgb)
+
+
+def test_mc_painter_default_settings_and_rays():
+    """With the default settings the painted picture is the clipped colour in
+    8 bits up to the round trip's last bits; pixels without rays are black;
+    the gamma slider and the exposure move the picture the way they say."""
+    rng = np.random.default_rng(11)
+    c = rng.uniform(-0.2, 2.0, (20000, 3)).astype(np.float32)
+    opts = mb3dcu.mc_paint_default()
+    p = O.mc_paint(c, opts).astype(int)
+    e = np.round(np.clip(c, 0, 1) * 255).astype(int)
+    assert np.abs(p - e).max() <= 1 and (p == e).mean() > 0.99
+    rays = (np.arange(len(c)) % 3 != 0).astype(np.uint8)
+    q = O.mc_paint(c, opts, rays)
+    assert (q[rays == 0] == 0).all() and (q[rays == 1] == p[rays == 1]).all()
+    mid = rng.uniform(0.05, 0.6, (2000, 3)).astype(np.float32)
+    base = O.mc_paint(mid, opts).astype(int).sum()
+    bright, dark, expo = mb3dcu.mc_paint_default(), mb3dcu.mc_paint_default(), mb3dcu.mc_paint_default()
+    bright.gamma, dark.gamma, expo.contrast = 63.0, 0.0, 200
+    assert O.mc_paint(mid, bright).astype(int).sum() > base > O.mc_paint(mid, dark).astype(int).sum()
+    assert O.mc_paint(mid, expo).astype(int).sum() > base
+
+
 def test_unet_oracle_backward_matches_finite_differences():
     """The denoiser oracle's backward pass (oracle/unet.py) against central
     differences of its forward pass, FP64, on a 1 x 16 x 16 input."""
