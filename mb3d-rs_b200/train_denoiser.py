@@ -167,7 +167,10 @@ def fallback_tiles(noisy_a, noisy_b, den, tile=16, k=3.0):
 
 def evaluate(card, dn, rect=(720, 405, 480, 270), ref_rays=1024, log=print):
     """The 1920x1080 workload on a rectangle: the plain trace at ref_rays,
-    the 4..64-ray traces and their denoised pictures; times on the card."""
+    the 4..64-ray traces and their denoised pictures; times on the card.
+    PSNRs of the tone-mapped linear records (psnr_*) and of the 8-bit
+    pictures the reference's painter makes of them (psnr8_*, paint_recs with
+    the default display settings, on the card)."""
     torch = _torch()
     sc = scenes.c5_mc()
     lv = mb3dcu.mc_light_default(sc)
@@ -179,6 +182,13 @@ def evaluate(card, dn, rect=(720, 405, 480, 270), ref_rays=1024, log=print):
 
     ref, ms_ref = trace(ref_rays, ray0=4096)  # (rays of their own, each with its own Halton record (< 65536))
     res = {"rect": list(rect), "ref_rays": ref_rays, "ms_ref": ms_ref, "levels": []}
+    paint_opts = mb3dcu.mc_paint_default()
+    ref8 = card.mc_paint(ref["radiance"], paint_opts).astype(np.float64)
+
+    def psnr8(x):
+        mse = float(np.mean((card.mc_paint(x, paint_opts).astype(np.float64) - ref8) ** 2))
+        return 10.0 * math.log10(255.0 ** 2 / max(mse, 1e-12))
+
     for rays in (4, 8, 16, 32, 64):
         r, ms = trace(rays)
         dmax = float(r["depth"].max()) or 1.0
@@ -200,10 +210,12 @@ def evaluate(card, dn, rect=(720, 405, 480, 270), ref_rays=1024, log=print):
         comp, fb = fallback_tiles(ha["radiance"], hb["radiance"], den)
         lvl = {"rays": rays, "ms_trace": ms, "ms_denoise": ms_dn, "psnr_noisy": psnr(r["radiance"], ref["radiance"]),
                "psnr_denoised": psnr(den, ref["radiance"]), "psnr_with_fallback": psnr(comp, ref["radiance"]),
-               "fallback_rate": fb}
+               "fallback_rate": fb, "psnr8_noisy": psnr8(r["radiance"]), "psnr8_denoised": psnr8(den),
+               "psnr8_with_fallback": psnr8(comp)}
         res["levels"].append(lvl)
         log(f"  {rays} rays: trace {ms:.1f} ms, denoise {ms_dn:.2f} ms, PSNR noisy {lvl['psnr_noisy']:.2f} "
-            f"denoised {lvl['psnr_denoised']:.2f} (fallback {fb:.3f}: {lvl['psnr_with_fallback']:.2f})", flush=True)
+            f"denoised {lvl['psnr_denoised']:.2f} (fallback {fb:.3f}: {lvl['psnr_with_fallback']:.2f}); 8-bit "
+            f"noisy {lvl['psnr8_noisy']:.2f} denoised {lvl['psnr8_denoised']:.2f}", flush=True)
     ok = [lv_ for lv_ in res["levels"] if lv_["psnr_denoised"] >= 35.0]
     if ok:
         best = min(ok, key=lambda l: l["ms_trace"] + l["ms_denoise"])
@@ -213,6 +225,14 @@ def evaluate(card, dn, rect=(720, 405, 480, 270), ref_rays=1024, log=print):
     plain = [lv_ for lv_ in res["levels"] if lv_["psnr_noisy"] >= 35.0]
     if plain:
         res["plain_to_35db_rays"] = min(l["rays"] for l in plain)
+    ok8 = [lv_ for lv_ in res["levels"] if lv_["psnr8_denoised"] >= 35.0]
+    if ok8:
+        best = min(ok8, key=lambda l: l["ms_trace"] + l["ms_denoise"])
+        res["time_to_35db_8bit_ms"] = best["ms_trace"] + best["ms_denoise"]
+        res["time_to_35db_8bit_rays"] = best["rays"]
+    plain8 = [lv_ for lv_ in res["levels"] if lv_["psnr8_noisy"] >= 35.0]
+    if plain8:
+        res["plain_to_35db_8bit_rays"] = min(l["rays"] for l in plain8)
     return res
 
 
