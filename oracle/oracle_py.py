@@ -44,6 +44,7 @@ def lib():
         L.oracle_mc_seed_of.restype = ctypes.c_int32
         L.oracle_mc_paint.argtypes = [vp, vp, ctypes.c_size_t, vp, vp]
         L.oracle_mc_paint.restype = None
+        L.oracle_paint.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp]
         _lib = L
     return _lib
 
@@ -166,4 +167,14 @@ def mc_paint(colour, opts, rays=None):
     r = None if rays is None else np.ascontiguousarray(rays, dtype=np.uint8)
     lib().oracle_mc_paint(col.ctypes.data, None if r is None else r.ctypes.data, n, ctypes.addressof(opts),
                           out.ctypes.data)
+    return out
+
+
+def paint(sc, gbuf, row0=0):
+    """render::paint (src/render.rs:2499): 8-bit RGB (rows, width, 3) of G-buffer
+    records (a structured array of the card's record layout, rows * width)."""
+    g = np.ascontiguousarray(gbuf)
+    rows = g.size // sc.width
+    out = np.zeros((rows, sc.width, 3), np.uint8)
+    _chk(lib().oracle_paint(ctypes.addressof(sc), g.ctypes.data, row0, rows, out.ctypes.data))
     return out

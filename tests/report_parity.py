@@ -1,6 +1,8 @@
 """Prints the parity figures behind the GPU tests' thresholds (a report, not
 a test): the card's FP64 drop-in march and the mixed march against the
-oracle on the workloads, the Monte Carlo render against its oracle.
+oracle on the workloads (and the PSNR of the oracle's painter applied to
+both G-buffers), the whole C2 frame painted, the Monte Carlo render
+against its oracle.
 
     python tests/report_parity.py > parity.json      (on a B200)
 """
@@ -25,6 +27,13 @@ def zc(sc):
     return p[7], p[6]
 
 
+def painted_psnr(sc, a, b):
+    """PSNR of the oracle's painter (render::paint) applied to two G-buffers."""
+    pa, pb = O.paint(sc, a).astype(np.float64), O.paint(sc, b).astype(np.float64)
+    mse = float(np.mean((pa - pb) ** 2))
+    return float(10 * np.log10(255.0 ** 2 / max(mse, 1e-12)))
+
+
 def main():
     card = mb3dcu.Card(0)
     out = {}
@@ -37,10 +46,20 @@ def main():
         ref = O.march(sc, mb3dcu.SILIGHT)
         row = {}
         for prec, pn in ((mb3dcu.FP64, "fp64"), (mb3dcu.FP32_FP64, "mixed")):
-            row[pn] = compare(card.march(sc, prec), ref, *zc(sc))
+            g = card.march(sc, prec)
+            row[pn] = compare(g, ref, *zc(sc))
             row[pn]["fp64_pixels"] = card.stats()["fp64_pixels"]
+            row[pn]["painted_psnr"] = painted_psnr(sc, g, ref)
         out[name] = row
         print(name, json.dumps(row), file=sys.stderr, flush=True)
+    # the whole C2 frame (march, hard shadows, DE AO) painted
+    sc = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    ref = O.deao(sc, O.shadows(sc, O.march(sc, mb3dcu.SILIGHT), per_pixel=True))
+    row = {}
+    for prec, pn in ((mb3dcu.FP64, "fp64"), (mb3dcu.FP32_FP64, "mixed")):
+        row[pn] = {"painted_psnr": painted_psnr(sc, card.render(sc, prec), ref)}
+    out["c2_hybrid_480x270_render"] = row
+    print("c2_hybrid_480x270_render", json.dumps(row), file=sys.stderr, flush=True)
     sc = scenes.scaled(scenes.c2_hybrid(), 160, 90)
     lv = mb3dcu.mc_light_default(sc)
     opts = mb3dcu.mc_opts(8, depth=4)

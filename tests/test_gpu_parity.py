@@ -125,6 +125,32 @@ def test_menger_shadows_iteration_limited_surfaces(card):
             assert (a["shadow"] == b["shadow"])[obj].mean() >= 0.999
 
 
+def _painted_psnr(sc, a, b):
+    pa, pb = O.paint(sc, a).astype(np.float64), O.paint(sc, b).astype(np.float64)
+    return 10 * np.log10(255.0 ** 2 / max(float(np.mean((pa - pb) ** 2)), 1e-12))
+
+
+def test_painted_pictures_match_the_oracle(card):
+    """The parity of the pictures: the oracle's painter (render::paint,
+    default lighting) applied to the card's G-buffer and to the oracle's.
+    The FP64 drop-in paints the oracle's picture (measured 99-168 dB); the
+    mixed mode's surfaces lie a fraction of a step away and its normals
+    follow the rough fractal surface there (measured 30.6-37.2 dB)."""
+    c1 = scenes.c1_plain_bulb()
+    ref = O.march(c1, mb3dcu.SILIGHT)
+    assert _painted_psnr(c1, card.march(c1, mb3dcu.FP64), ref) >= 60.0
+    assert _painted_psnr(c1, card.march(c1, mb3dcu.FP32_FP64), ref) >= 35.0
+    # the whole C2 frame: march, hard shadows, DE AO
+    c2 = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    ref = O.deao(c2, O.shadows(c2, O.march(c2, mb3dcu.SILIGHT), per_pixel=True))
+    assert _painted_psnr(c2, card.render(c2, mb3dcu.FP64), ref) >= 60.0
+    assert _painted_psnr(c2, card.render(c2, mb3dcu.FP32_FP64), ref) >= 29.5
+    c4 = scenes.scaled(scenes.c4_frames(8)[0], 320, 180)
+    ref = O.march(c4, mb3dcu.SILIGHT)
+    assert _painted_psnr(c4, card.march(c4, mb3dcu.FP64), ref) >= 60.0
+    assert _painted_psnr(c4, card.march(c4, mb3dcu.FP32_FP64), ref) >= 33.0
+
+
 def test_render_device_buffer_equals_host_buffer(card):
     import torch
     sc = scenes.scaled(scenes.c2_hybrid(), 240, 136)

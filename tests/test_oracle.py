@@ -259,6 +259,35 @@ def test_mc_painter_default_settings_and_rays():
     assert O.mc_paint(mid, expo).astype(int).sum() > base
 
 
+def test_painter_background_shadows_and_occlusion():
+    """The oracle's Calculate 3D painter (render::paint, default lighting):
+    with the default dynamic fog the background is the depth colour gradient
+    (top depth_col to bottom depth_col2, src/lighting.rs:1791) up to
+    rounding; a hard shadow bit and the ambient occlusion only darken."""
+    sc = scenes.scaled(scenes.c2_hybrid(), 96, 54)
+    g = O.deao(sc, O.shadows(sc, O.march(sc, mb3dcu.SILIGHT), per_pixel=True))
+    img = O.paint(sc, g).astype(int)
+    h, w = sc.height, sc.width
+    bg = ((g["zpos_fine"] >> 16) >= 32768).reshape(h, w)
+    obj = mb3dcu.hit_mask(g).reshape(h, w)
+    assert bg.mean() > 0.2 and obj.mean() > 0.1
+    yp = (np.arange(h, dtype=np.float32) / np.float32(h))[:, None, None]
+    top = np.array([0x1D, 0x49, 0x8B], np.float32)
+    bottom = np.array([0x9F, 0xC4, 0xFF], np.float32)
+    want = np.round(top + yp * (bottom - top)) * np.ones((1, w, 1))
+    assert np.abs(img[bg] - want[bg]).max() <= 1
+    lit = g.copy()
+    lit["shadow"] &= 0x3FF
+    a = O.paint(sc, lit).astype(int).sum(-1)
+    shadowed = ((g["shadow"] & 0x400) != 0).reshape(h, w) & obj
+    assert shadowed.sum() > 20
+    assert (img.sum(-1)[shadowed] <= a[shadowed]).all() and (img.sum(-1)[shadowed] < a[shadowed]).mean() > 0.95
+    open_ = g.copy()
+    open_["amb_shadow"] = 0
+    c = O.paint(sc, open_).astype(int).sum(-1)
+    assert (img.sum(-1)[obj] <= c[obj]).mean() > 0.99
+
+
 def test_unet_oracle_backward_matches_finite_differences():
     """The denoiser oracle's backward pass (oracle/unet.py) against central
     differences of its forward pass, FP64, on a 1 x 16 x 16 input."""
