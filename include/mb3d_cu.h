@@ -367,6 +367,20 @@ void mb3d_cu_mc_paint_default(mb3d_cu_mc_paint_opts *out);
 int mb3d_cu_mc_paint(mb3d_cu_ctx *ctx, const float *colour, const uint8_t *rays, uint32_t npix,
                      const mb3d_cu_mc_paint_opts *opts, uint8_t *rgb);
 
+/* render::paint (src/render.rs:2499-2501, paint_core :2676-2720) on the
+ * card: the 8-bit RGB picture (3 bytes per pixel) of rows row0 ..
+ * row0+rows-1 of the scene from their G-buffer records (rows * width, e.g.
+ * mb3d_cu_render's), with Lighting::default and the scene's lights
+ * (src/lighting.rs:290-391): shade (src/lighting.rs:1802-2162) along its
+ * default path -- directional lights not visible in the picture, the
+ * palette's colours, ambient top/bottom light, the hard shadows the scene's
+ * shadow pass marked, the DE ambient occlusion, the depth and dynamic fog --
+ * and pixel_color_s (:1739-1760) clipped and rounded to 8 bits.  Single
+ * precision, unfused, as the reference's CPU painter.  Host or device
+ * buffers. */
+int mb3d_cu_paint(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_silight *gbuf, uint32_t row0,
+                  uint32_t rows, uint8_t *rgb);
+
 /* ---- the learned denoiser of the Monte Carlo pictures ----
  * A 5-level U-Net of 3x3 convolutions (32/48/64/80/96 channels) that
  * takes the noisy colour and the albedo, normal and depth guides of a

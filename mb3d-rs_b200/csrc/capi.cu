@@ -765,6 +765,42 @@ int mb3d_cu_mc_paint(mb3d_cu_ctx *c, const float *col, const uint8_t *rays, uint
     return 0;
 }
 
+int mb3d_cu_paint(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_silight *gbuf, uint32_t row0, uint32_t rows,
+                  uint8_t *rgb) {
+    if (!c || !sc || !gbuf || !rgb) return fail(MB3D_CU_EINVAL, "NULL argument");
+    DevParams p;
+    std::string err;
+    int r = setup_params(*sc, p, err);
+    if (r < 0) return fail(r, err);
+    if ((uint64_t)row0 + rows > (uint64_t)p.height || rows == 0) return fail(MB3D_CU_EINVAL, "rows outside the picture");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    cudaStream_t s = c->stream;
+    const uint32_t npix = rows * (uint32_t)p.width;
+    const bool dg = is_device_ptr(gbuf), dr = is_device_ptr(rgb);
+    const size_t bg = (size_t)npix * sizeof(mb3d_cu_silight), br = (size_t)npix * 3;
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    size_t need = (dg ? 0 : up16(bg)) + (dr ? 0 : up16(br));
+    if (need)
+        if (int e = grow((void **)&c->d_paint, &c->paint_cap, need)) return e;
+    unsigned char *q = c->d_paint;
+    const mb3d_cu_silight *dgb = gbuf;
+    uint8_t *drgb = rgb;
+    if (!dg) {
+        CU_TRY(cudaMemcpyAsync(q, gbuf, bg, cudaMemcpyHostToDevice, s));
+        dgb = (const mb3d_cu_silight *)q;
+        q += up16(bg);
+    }
+    if (!dr) drgb = q;
+    int blocks = (int)std::min<size_t>(((size_t)npix + 255) / 256, (size_t)c->sms * 8);
+    paint_launch(*sc, p, row0, dgb, npix, drgb, blocks, s);
+    if (int e = check_launch("k_paint")) return e;
+    if (!dr) CU_TRY(cudaMemcpyAsync(rgb, drgb, br, cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    return 0;
+}
+
 static int mc_halton(mb3d_cu_ctx *c) {
     if (c->d_halton) return 0;
     const std::vector<uint32_t> &t = mc_halton_table();

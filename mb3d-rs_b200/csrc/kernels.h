@@ -107,4 +107,8 @@ void launch_mc_final(const McAcc &acc, uint32_t npix, int rays, float *radiance,
 void mc_paint_launch(const float *col, const uint8_t *rays, uint32_t n, const mb3d_cu_mc_paint_opts &mc, uint8_t *out,
                      int blocks, cudaStream_t s);
 
+// render::paint of G-buffer records, default lighting (paint.cu)
+void paint_launch(const mb3d_cu_scene &sc, const DevParams &p, uint32_t row0, const mb3d_cu_silight *gbuf, uint32_t n,
+                  uint8_t *rgb, int blocks, cudaStream_t s);
+
 }  // namespace mb3dcu

@@ -210,6 +210,7 @@ def lib():
         L.mb3d_cu_mc_paint_default.argtypes = [ctypes.POINTER(McPaintOpts)]
         L.mb3d_cu_mc_paint_default.restype = None
         L.mb3d_cu_mc_paint.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.POINTER(McPaintOpts), vp]
+        L.mb3d_cu_paint.argtypes = [vp, sp, vp, ctypes.c_uint32, ctypes.c_uint32, vp]
         _lib = L
     return _lib
 
@@ -218,7 +219,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render",
-            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint",
+            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
             "mb3d_cu_dn_conv_check"]
@@ -375,6 +376,22 @@ class Card:
         self._order(colour, rays, out)
         self._check(lib().mb3d_cu_mc_paint(self._ctx, _ptr(colour)[0], None if rays is None else _ptr(rays)[0], n,
                                            ctypes.byref(opts), _ptr(out)[0]))
+        return out
+
+    def paint(self, scene, gbuf, row0=0, out=None):
+        """render::paint on the card: 8-bit RGB (rows, width, 3) of G-buffer
+        records (numpy SILIGHT array or a torch CUDA byte tensor of rows *
+        width records) with the default lighting; `out` may be a torch CUDA
+        tensor."""
+        if isinstance(gbuf, np.ndarray):
+            gbuf = np.ascontiguousarray(gbuf)
+            rows = gbuf.size // scene.width
+        else:
+            rows = gbuf.numel() * gbuf.element_size() // (SILIGHT.itemsize * scene.width)
+        if out is None:
+            out = np.zeros((rows, scene.width, 3), np.uint8)
+        self._order(gbuf, out)
+        self._check(lib().mb3d_cu_paint(self._ctx, ctypes.byref(scene), _ptr(gbuf)[0], row0, rows, _ptr(out)[0]))
         return out
 
     def mc_render(self, scene, opts, light=None, precision=FP32_FP64, out=None, cancel=None):

@@ -151,6 +151,36 @@ def test_painted_pictures_match_the_oracle(card):
     assert _painted_psnr(c4, card.march(c4, mb3dcu.FP32_FP64), ref) >= 33.0
 
 
+def test_card_painter_matches_the_oracle(card):
+    """mb3d_cu_paint (render::paint on the card) against the oracle's
+    painter on the same records: both single precision and unfused; the
+    card's sinf/cosf of the view vector may move a channel by one step."""
+    import torch
+    cases = []
+    c2 = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    cases.append((c2, card.render(c2, mb3dcu.FP64)))
+    c4 = scenes.scaled(scenes.c4_frames(8)[3], 320, 180)
+    cases.append((c4, card.render(c4, mb3dcu.FP32_FP64)))
+    c1 = scenes.scaled(scenes.c1_plain_bulb(), 320, 240)
+    cases.append((c1, card.march(c1, mb3dcu.FP32_FP64)))
+    for sc, g in cases:
+        want = O.paint(sc, g).astype(np.int64)
+        got = card.paint(sc, g).astype(np.int64)
+        d = np.abs(got - want)
+        assert (d == 0).mean() >= 0.999 and d.max() <= 1, ((d == 0).mean(), d.max())
+        # a band of rows, on device buffers
+        r0, rows = sc.height // 3, sc.height // 4
+        band = g[r0 * sc.width:(r0 + rows) * sc.width]
+        dg = torch.from_numpy(band.view(np.uint8).copy()).cuda()
+        dout = torch.zeros((rows, sc.width, 3), dtype=torch.uint8, device="cuda")
+        card.paint(sc, dg, row0=r0, out=dout)
+        torch.cuda.synchronize()
+        assert np.array_equal(dout.cpu().numpy(), got[r0:r0 + rows])
+    with pytest.raises(mb3dcu.CardError) as e:
+        card.paint(c1, cases[2][1], row0=10)
+    assert e.value.status == mb3dcu.EINVAL
+
+
 def test_render_device_buffer_equals_host_buffer(card):
     import torch
     sc = scenes.scaled(scenes.c2_hybrid(), 240, 136)
