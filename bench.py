@@ -308,6 +308,33 @@ def _timed_render(card, sc, prec, gbuf, flush, stream, reps):
     return statistics.mean(ms)
 
 
+def paint_figures(card, sc, gbuf, g_a, g_b, flush, stream, reps=5):
+    """render::paint on the card (default lighting) of the frame's records
+    resident on the device: its time, and the PSNR of the 8-bit pictures of
+    the two precisions' G-buffers (g_a, g_b: host copies of both)."""
+    import torch
+    rgb = torch.empty((sc.height, sc.width, 3), dtype=torch.uint8, device="cuda")
+    card.paint(sc, gbuf, out=rgb)
+    ms = []
+    for _ in range(reps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        card.paint(sc, gbuf, out=rgb)
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    m = statistics.mean(ms)
+    npix = sc.width * sc.height
+    pa = card.paint(sc, g_a).astype(np.float64)
+    pb = card.paint(sc, g_b).astype(np.float64)
+    mse = float(np.mean((pa - pb) ** 2))
+    return {"ms": m, "mpixels_s": npix / (m / 1000.0) / 1e6, "gbs": npix * 23 / (m / 1000.0) / 1e9,
+            "psnr_8bit_mixed_vs_fp64": 10 * np.log10(255.0 ** 2 / max(mse, 1e-12)),
+            "note": "k_paint: render::paint with the default lighting, 20 bytes in and 3 out per pixel"}
+
+
 def config_figures(card, flush, stream, reps=3):
     """The other workloads, one GPU, device-resident outputs: the plain
     Mandelbulb (640x480) and the deep zoom (1920x1080) in both precisions
@@ -467,7 +494,10 @@ def main():
            "gpu_launches": launches, "roofline": roof, "stages_ms": stage,
            "peaks": {"fp32_fma_tflops": peak32, "fp64_fma_tflops": peak64},
            "counted": {"de_evals": counted["de_evals"], "orbit_its": counted["orbit_its"],
-                       "march_de_evals_per_s": counted["de_evals"] / (k_ms / 1000.0)},
+                       "march_de_evals_per_s": counted["de_evals"] / (k_ms / 1000.0),
+                       "march_iteration_lane_use": counted["march_lane_its"] / max(32 * counted["march_warp_its"], 1),
+                       "march_busy_lane_use": counted["march_busy_lanes"] / max(32 * counted["march_trips"], 1),
+                       "march_warp_trips": counted["march_trips"]},
            "clocks": clocks}
     if rank == 0:
         # the plain FP64 march (the drop-in) on the same frame, and the mixed
@@ -492,6 +522,7 @@ def main():
             out["fp64_march"] = {"value": npix / (om / 1000.0) / 1e6, "unit": "Mrays/s", "ms_per_step": om,
                                  "mixed_over_fp64": om / ms}
             out["parity_vs_fp64"] = parity_vs_fp64(sc, mixed_g, other_g)
+        out["paint"] = paint_figures(card, sc, gbuf, mixed_g, other_g, flush, stream)
         card.set_stream(None)
         if not args.no_configs and args.scale == 1.0:
             out["configs"] = config_figures(card, flush, stream)

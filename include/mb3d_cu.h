@@ -222,6 +222,11 @@ typedef struct mb3d_cu_stats {
     uint64_t orbit_its[6];/* formula iterations per slot, all orbits (counting mode only) */
     uint32_t mc_inside_rays; /* Monte Carlo rays that started inside the set (left dark) */
     uint32_t mc_fp64_rays;   /* Monte Carlo rays whose single precision DE fell back to double */
+    /* the march kernel's use of its warps' lanes (counting mode only): */
+    uint64_t march_lane_its;   /* the DEs' iterations summed over the lanes */
+    uint64_t march_warp_its;   /* per warp and loop trip the most iterations of its lanes, summed */
+    uint64_t march_trips;      /* warp loop trips that evaluated DEs */
+    uint64_t march_busy_lanes; /* the lanes with a ray in those trips, summed */
 } mb3d_cu_stats;
 
 typedef struct mb3d_cu_ctx mb3d_cu_ctx;
@@ -279,7 +284,8 @@ int mb3d_cu_de_probe(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision
 /* Launch settings of the wavefront kernels (picked by mb3d_cu_autotune). */
 typedef struct mb3d_cu_tune {
     int32_t blocks_per_sm; /* resident blocks of 256 threads per SM the persistent kernels start with */
-    int32_t refill_min;    /* idle lanes of a warp that make it take new rays (the compaction interval) */
+    int32_t refill_min;    /* idle lanes of a warp that make the march and finish kernels take new rays
+                            * (32: only a wholly idle warp; the shadow and DE AO ray kernels keep 8) */
     int32_t streams;       /* frames in flight at once in a frame batch */
     int32_t pad;
 } mb3d_cu_tune;

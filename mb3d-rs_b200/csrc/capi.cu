@@ -282,9 +282,10 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
     }
     CU_TRY(cudaEventRecord(c->ev[4], s));
     if (passes & MB3D_CU_POST_DEAO) {
+        launch_ao_prep(p, c->d_ps, dg, cnt, c->sms * 8, s);
         launch_ao_rays(p, mixed, c->d_ps, dg, cnt, c->d_minra, cnt + 2, c->sms * p.blocks_per_sm, s);
         launch_ao_final(p, c->d_ps, cnt, c->d_minra, dg, c->sms * 8, s);
-        c->stats.launches += 2;
+        c->stats.launches += 3;
         if (int r = check_launch("k_ao")) return r;
     }
     CU_TRY(cudaEventRecord(c->ev[5], s));
@@ -301,6 +302,10 @@ static int finish_call(mb3d_cu_ctx *c, bool marched, bool posted) {
         CU_TRY(cudaMemcpy(h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost));
         for (int k = 0; k < 6; k++) c->stats.orbit_its[k] = h[k];
         c->stats.de_evals = h[6];
+        c->stats.march_lane_its = h[7];
+        c->stats.march_warp_its = h[8];
+        c->stats.march_trips = h[9];
+        c->stats.march_busy_lanes = h[10];
     }
     float ms = 0.f;
     if (marched) {
@@ -320,7 +325,7 @@ static int finish_call(mb3d_cu_ctx *c, bool marched, bool posted) {
     return 0;
 }
 
-// launch tuning: MB3D_CU_TUNE="refill=8,blocks=4,margin=4,back=2"
+// launch tuning: MB3D_CU_TUNE="refill=8,refill_sh=8,refill_ao=16,blocks=4,margin=4,back=2"
 static void apply_tuning(DevParams &p) {
     const char *t = getenv("MB3D_CU_TUNE");
     if (!t) return;
@@ -335,6 +340,8 @@ static void apply_tuning(DevParams &p) {
             std::string k = kv.substr(0, e);
             double v = atof(kv.c_str() + e + 1);
             if (k == "refill" && v >= 1 && v <= 32) p.refill_min = (int)v;
+            else if (k == "refill_sh" && v >= 1 && v <= 32) p.refill_shadow = (int)v;
+            else if (k == "refill_ao" && v >= 1 && v <= 32) p.refill_ao = (int)v;
             else if (k == "blocks" && v >= 1 && v <= 16) p.blocks_per_sm = (int)v;
             else if (k == "margin" && v >= 1) p.hand_margin = (float)v;
             else if (k == "back" && v >= 0 && v <= 2) p.hand_back = (int)v;
@@ -529,6 +536,7 @@ static int enqueue_frame(mb3d_cu_ctx *c, mb3d_cu_ctx::Scratch &sc, const DevPara
         launch_post_start(p, mixed, 0, passes, dg, sc.slist, cnt, cnt + 3, sc.ps, c->sms * p.blocks_per_sm, s);
         if (passes & MB3D_CU_POST_SHADOW) launch_shadow_rays(p, mixed, 0, sc.ps, cnt, dg, cnt + 1, c->sms * p.blocks_per_sm, s);
         if (passes & MB3D_CU_POST_DEAO) {
+            launch_ao_prep(p, sc.ps, dg, cnt, c->sms * 8, s);
             launch_ao_rays(p, mixed, sc.ps, dg, cnt, sc.minra, cnt + 2, c->sms * p.blocks_per_sm, s);
             launch_ao_final(p, sc.ps, cnt, sc.minra, dg, c->sms * 8, s);
         }
@@ -611,7 +619,7 @@ static int render_frames_locked(mb3d_cu_ctx *c, const mb3d_cu_scene *frames, uin
         bool mixed = precision != MB3D_CU_FP64 && !P[f].all_fp64;
         int i = (int)(f % (uint32_t)streams);
         rc = enqueue_frame(c, c->fscratch[i], P[f], mixed, passes, dg + (size_t)f * npix, c->fstreams[i]);
-        c->stats.launches += 2 + (passes ? 2 : 0) + ((passes & MB3D_CU_POST_SHADOW) ? 1 : 0) + ((passes & MB3D_CU_POST_DEAO) ? 2 : 0);
+        c->stats.launches += 2 + (passes ? 2 : 0) + ((passes & MB3D_CU_POST_SHADOW) ? 1 : 0) + ((passes & MB3D_CU_POST_DEAO) ? 3 : 0);
     }
     for (int i = 0; i < streams && !rc; i++) {
         if (cudaEventRecord(c->fevents[i], c->fstreams[i]) != cudaSuccess || cudaStreamWaitEvent(s0, c->fevents[i], 0) != cudaSuccess)
@@ -661,9 +669,9 @@ int mb3d_cu_autotune(mb3d_cu_ctx *c, const mb3d_cu_scene *frames, uint32_t n, ui
     mb3d_cu_silight *buf = nullptr;
     if (int e = grow((void **)&c->d_frames, &c->frames_cap, pick.size() * npix * sizeof(mb3d_cu_silight))) return e;
     buf = c->d_frames;
-    const int blocks[3] = {2, 3, 4}, refills[3] = {8, 16, 24}, streams[3] = {1, 2, 4};
+    const int blocks[3] = {2, 3, 4}, refills[3] = {16, 24, 32}, streams[3] = {1, 2, 4};
     float best = 1e30f;
-    mb3d_cu_tune bt = {3, 16, 2, 0};
+    mb3d_cu_tune bt = {3, 32, 2, 0};
     for (int b : blocks)
         for (int r : refills)
             for (int s : streams) {

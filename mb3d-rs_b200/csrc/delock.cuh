@@ -93,17 +93,24 @@ __device__ __forceinline__ void step_orbits(const DevSlot &s, R (&v)[Q][4], R (&
 
 // Counting (bench and roofline only): orbit iterations per slot and DE
 // evaluations, kept per thread and added to global counters at the end.
+// The march kernel adds its warps' lane use: [0] the rays' lock-step
+// iterations, [1] per warp trip the most iterations of its lanes, [2] the
+// warp trips that evaluated DEs, [3] the lanes busy in them.
 struct DECount {
     unsigned long long its[MB3D_MAX_SLOTS];
     unsigned long long evals;
+    unsigned long long lanes[4];
     __device__ void clear() {
         for (int k = 0; k < MB3D_MAX_SLOTS; k++) its[k] = 0;
         evals = 0;
+        for (int k = 0; k < 4; k++) lanes[k] = 0;
     }
     __device__ void flush(unsigned long long *g) {
         for (int k = 0; k < MB3D_MAX_SLOTS; k++)
             if (its[k]) atomicAdd(&g[k], its[k]);
         if (evals) atomicAdd(&g[MB3D_MAX_SLOTS], evals);
+        for (int k = 0; k < 4; k++)
+            if (lanes[k]) atomicAdd(&g[MB3D_MAX_SLOTS + 1 + k], lanes[k]);
     }
 };
 

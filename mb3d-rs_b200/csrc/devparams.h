@@ -41,6 +41,7 @@ struct DevParams {
     float hand_margin;  // the mixed march hands over from where DE >= this x DE stop
     int32_t hand_back;  // ... at most this many steps back
     int32_t refill_min, blocks_per_sm;  // wavefront: idle lanes that trigger a refill; resident blocks
+    int32_t refill_shadow, refill_ao;   // ... of the shadow and DE AO ray kernels
     float d_rstop_f, rstop3d_f, soft_radius, hs_max_len_mul;
     double d_rstop, rstop3d, zcorr, zc_mul;
     double zend, step_width, fov_y, coord_eps;

@@ -13,6 +13,10 @@ void launch_surface(const DevParams &p, int npix, int passes, mb3d_cu_silight *g
                     unsigned int *count, int blocks, cudaStream_t s) {
     k_surface<<<blocks, 256, 0, s>>>(p, npix, passes, gbuf, list, count);
 }
+void launch_ao_prep(const DevParams &p, PostStart *ps, const mb3d_cu_silight *gbuf, const unsigned int *count,
+                    int blocks, cudaStream_t s) {
+    k_ao_prep<<<blocks, 128, 0, s>>>(p, ps, gbuf, count);
+}
 void launch_ao_final(const DevParams &p, const PostStart *ps, const unsigned int *count, const float *min_ra,
                      mb3d_cu_silight *gbuf, int blocks, cudaStream_t s) {
     k_ao_final<<<blocks, 128, 0, s>>>(p, ps, count, min_ra, gbuf);

@@ -35,6 +35,12 @@ struct PostStart {
     uint32_t pix;
     uint32_t flags;  // bit l: the surface faces away from light l
     uint32_t pad;
+    // the DE AO rays' per-pixel set-up (k_ao_prep): the turn of the ray
+    // table to the surface normal, the first step, the rays' length, the
+    // DE stop and the openness offset per unit of length
+    float ao_rot[3][3];
+    uint32_t pad2;
+    double ao_step0, ao_max_dist, ao_msd, ao_md_d10;
 };
 
 // The formula sets the kernels are built for (FKIND_* bits, formulas.cuh):
@@ -78,6 +84,8 @@ void launch_shadow_rays(const DevParams &p, bool mixed, int row0, const PostStar
                         mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s);
 void launch_ao_rays(const DevParams &p, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,
                     const unsigned int *count, float *min_ra, unsigned int *queue, int blocks, cudaStream_t s);
+void launch_ao_prep(const DevParams &p, PostStart *ps, const mb3d_cu_silight *gbuf, const unsigned int *count,
+                    int blocks, cudaStream_t s);
 void launch_ao_final(const DevParams &p, const PostStart *ps, const unsigned int *count, const float *min_ra,
                      mb3d_cu_silight *gbuf, int blocks, cudaStream_t s);
 void launch_de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s);

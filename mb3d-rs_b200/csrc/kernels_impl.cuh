@@ -237,6 +237,16 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_MARCH) k_march(const __gr
             }
             cur_de = dtmp;
         }
+        if (COUNT) {
+            const int itl = cur_it;  // (0: no DE this trip)
+            const int mx = __reduce_max_sync(0xffffffffu, itl);
+            cnt.lanes[0] += (unsigned long long)itl;
+            if ((threadIdx.x & 31) == 0) {
+                cnt.lanes[1] += (unsigned long long)mx;
+                cnt.lanes[2] += 1;
+                cnt.lanes[3] += (unsigned long long)__popc(busy);
+            }
+        }
         Hand h;
         if (hand) {
             h.pix = pix;
@@ -932,7 +942,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_shadow_rays(const __gr
     float ms = 0.f, rsf = 2.f, zr = 1.f, zrs_mul = 0.f;
     bool stepped = false;
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
-        uint32_t item = warp_take(!active, queue, n_items, p.refill_min, open);
+        uint32_t item = warp_take(!active, queue, n_items, p.refill_shadow, open);
         if (item != UINT32_MAX) {
             uint32_t i = item % npx;
             li = (int)(item / npx);
@@ -1087,12 +1097,13 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_c
     const uint32_t n_items = npx * (uint32_t)p.ao_rays;
     bool open = true, active = false, b_end = false;
     uint32_t slot = 0;
-    double ic[3] = {0, 0, 0}, sv[3] = {0, 0, 0}, dt1 = 0, s_tmp = 1, msd = 0, max_dist = 0, md_d10 = 0, de_mul = 1;
+    double ic[3] = {0, 0, 0}, sv[3] = {0, 0, 0}, dt1 = 0, s_tmp = 1, msd = 0, max_dist = 0, md_d10 = 0;
     float ms_s = 0.f;
     int guard = 0;
     const double dsm = (double)p.ao_d_step_mul;
+    const double de_mul = sqrt((double)p.ao_rays * 0.5);
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
-        uint32_t item = warp_take(!active, queue, n_items, p.refill_min, open);
+        uint32_t item = warp_take(!active, queue, n_items, p.refill_ao, open);
         if (item != UINT32_MAX) {
             uint32_t i = item % npx;
             int k = (int)(item / npx);
@@ -1100,30 +1111,16 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_c
             slot = item;
             ic[0] = s.ao_c[0]; ic[1] = s.ao_c[1]; ic[2] = s.ao_c[2];
             ms_s = s.ao_ms;
-            AOc a = ao_consts(p, ms_s);
-            msd = a.msd;
-            max_dist = a.max_dist;
-            md_d10 = a.md_d10;
-            de_mul = a.de_mul;
+            msd = s.ao_msd;
+            max_dist = s.ao_max_dist;
+            md_d10 = s.ao_md_d10;
             // the ray's direction: the table direction turned to the normal,
             // then to world space, one step width long
-            G si;
-            si.load(gbuf[s.pix]);
-            float nrm[3];
-            {
-                float v[3] = {(float)si.n0, (float)si.n1, (float)si.n2};
-                float l = fmaxf(__fsqrt_rn(sdot3(v, v)), 1e-30f);
-                nrm[0] = __fdiv_rn(v[0], l);
-                nrm[1] = __fdiv_rn(v[1], l);
-                nrm[2] = __fdiv_rn(v[2], l);
-            }
-            float rot_w[3][3];
-            normal_matrix_d(nrm, rot_w);
             const float *dk = p.ao_dirs[k];
-            float vv[3] = {sdot3(rot_w[0], dk), sdot3(rot_w[1], dk), sdot3(rot_w[2], dk)};
+            float vv[3] = {sdot3(s.ao_rot[0], dk), sdot3(s.ao_rot[1], dk), sdot3(s.ao_rot[2], dk)};
             double vd[3] = {(double)vv[0], (double)vv[1], (double)vv[2]};
             rot_rev(vd, p.ao_rot, sv);
-            dt1 = a.step_ao * dsm;
+            dt1 = s.ao_step0;
             s_tmp = 1.0;
             b_end = false;
             guard = 0;
@@ -1155,6 +1152,33 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_c
 }
 
 #ifdef MB3D_COMMON_KERNELS
+// per surface pixel, before the DE AO rays: the turn of the ray table to
+// the surface normal (src/deao.rs:301-316) and the per-pixel constants
+// (src/deao.rs:285-300), once for all of the pixel's rays
+__global__ void k_ao_prep(const __grid_constant__ DevParams p, PostStart *ps, const mb3d_cu_silight *gbuf,
+                          const unsigned int *count) {
+    const uint32_t npx = count[0];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < npx; i += gridDim.x * blockDim.x) {
+        PostStart &s = ps[i];
+        G si;
+        si.load(gbuf[s.pix]);
+        float nrm[3];
+        {
+            float v[3] = {(float)si.n0, (float)si.n1, (float)si.n2};
+            float l = fmaxf(__fsqrt_rn(sdot3(v, v)), 1e-30f);
+            nrm[0] = __fdiv_rn(v[0], l);
+            nrm[1] = __fdiv_rn(v[1], l);
+            nrm[2] = __fdiv_rn(v[2], l);
+        }
+        normal_matrix_d(nrm, s.ao_rot);
+        AOc a = ao_consts(p, s.ao_ms);
+        s.ao_step0 = a.step_ao * (double)p.ao_d_step_mul;
+        s.ao_max_dist = a.max_dist;
+        s.ao_msd = a.msd;
+        s.ao_md_d10 = a.md_d10;
+    }
+}
+
 // per surface pixel: the correction of the closed rays by their open
 // neighbours and the mean (src/deao.rs:361-413)
 __global__ void k_ao_final(const __grid_constant__ DevParams p, const PostStart *ps, const unsigned int *count,

@@ -317,7 +317,13 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     p.hand_margin = 4.0f;
     p.hand_back = 2;
     p.finish_slow = (p.sm_normals > 0 || !p.normals_on_de || p.color_on_it != 0) ? 1 : 0;
-    p.refill_min = 16;
+    // (measured on the 1920x1080 hybrid frame: the march and its finish are
+    // fastest when a warp takes new rays only once all of its lanes are idle
+    // -- rays that start together iterate alike -- the shadow and DE AO rays
+    // when a quarter of the lanes are idle)
+    p.refill_min = 32;
+    p.refill_shadow = 8;
+    p.refill_ao = 8;
     p.blocks_per_sm = 3;
 
     // shadow lights (render::shadow_job): HSvecs = RotateVectorReverse(-sw * LN, M)

@@ -72,7 +72,9 @@ class Stats(ctypes.Structure):
     _fields_ = [("ms_march", ctypes.c_float), ("ms_finish", ctypes.c_float), ("ms_shadow", ctypes.c_float),
                 ("ms_deao", ctypes.c_float), ("ms_total", ctypes.c_float), ("launches", ctypes.c_uint32),
                 ("fp64_pixels", ctypes.c_uint32), ("de_evals", ctypes.c_uint64), ("orbit_its", ctypes.c_uint64 * 6),
-                ("mc_inside_rays", ctypes.c_uint32), ("mc_fp64_rays", ctypes.c_uint32)]
+                ("mc_inside_rays", ctypes.c_uint32), ("mc_fp64_rays", ctypes.c_uint32),
+                ("march_lane_its", ctypes.c_uint64), ("march_warp_its", ctypes.c_uint64),
+                ("march_trips", ctypes.c_uint64), ("march_busy_lanes", ctypes.c_uint64)]
 
 
 # ---- the Monte Carlo tracer (src/mc.rs) ----
