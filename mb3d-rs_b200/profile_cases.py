@@ -4,6 +4,7 @@
     python mb3d-rs_b200/profile_cases.py denoise   # the denoiser on one 1920x1080 picture (6 passes)
     python mb3d-rs_b200/profile_cases.py c1        # the plain bulb 640x480: one mixed, one FP64 render
     python mb3d-rs_b200/profile_cases.py c4        # frame 37 of the 240-frame flight: one mixed, one FP64 render
+    python mb3d-rs_b200/profile_cases.py de        # single precision DEs of the C2 scene at 3, 6 and 30 iterations
 
 The Calculate 3D kernels are profiled through bench.py (--scale 0.25).
 """
@@ -65,5 +66,20 @@ def c4():
     _both(scenes.c4_frames(240)[37])
 
 
+def de():
+    """The instruction cost of one DE: 16 M seeded points of the C2 scene
+    probed once in double precision (one launch), then three launches of
+    32768 points in single precision whose double precision iteration
+    count is 3, 6 and 30 (every lane of a warp at the same count)."""
+    card = mb3dcu.Card(0)
+    sc = scenes.c2_hybrid()
+    pts = np.random.default_rng(5).uniform(-2.0, 2.0, size=(16_000_000, 3))
+    _, its = card.de_probe(sc, pts, mb3dcu.FP64)
+    for n in (3, 6, 30):
+        sel = pts[its == n][:32768]
+        _, i = card.de_probe(sc, sel, mb3dcu.FP32_FP64)
+        print("ok", n, len(sel), "mean iterations", float(i.mean()))
+
+
 if __name__ == "__main__":
-    {"mc": mc, "denoise": denoise, "c1": c1, "c4": c4}[sys.argv[1]]()
+    {"mc": mc, "denoise": denoise, "c1": c1, "c4": c4, "de": de}[sys.argv[1]]()
