@@ -430,7 +430,7 @@ int mb3d_cu_dn_gradient(mb3d_cu_dn *dn, int n, int h, int w, const float *radian
                         float *grad);
 
 /* Test hook: one 3x3 convolution (NHWC, cin and cout multiples of 16,
- * cout <= 96, weights [cout][3][3][cin]) and its gradients for the output
+ * cout <= 128, weights [cout][3][3][cin]) and its gradients for the output
  * gradient dy, through the same kernels, on float host arrays (BF16
  * inside). */
 int mb3d_cu_dn_conv_check(mb3d_cu_ctx *ctx, int n, int h, int w, int cin, int cout, const float *x, const float *wt,

@@ -515,7 +515,7 @@ int mb3d_cu_dn_train_step(mb3d_cu_dn *d, int n, int hs, int ws, const float *rad
 int mb3d_cu_dn_conv_check(mb3d_cu_ctx *ctx, int n, int h, int w, int cin, int cout, const float *x, const float *wt,
                           const float *b, const float *dy, float *y, float *dx, float *dw, float *db) {
     if (!ctx || !x || !wt || !b || !dy || !y || !dx || !dw || !db) return dn_fail(MB3D_CU_EINVAL, "NULL argument");
-    if (cin % 16 || cout % 16 || cout > 96 || n < 1 || h < 1 || w < 1) return dn_fail(MB3D_CU_EINVAL, "bad shape");
+    if (cin % 16 || cout % 16 || cout > 128 || n < 1 || h < 1 || w < 1) return dn_fail(MB3D_CU_EINVAL, "bad shape");
     if (cudaSetDevice(dn_device(ctx)) != cudaSuccess) return dn_fail(MB3D_CU_EIO, "cudaSetDevice failed");
     cudaStream_t s = dn_stream(ctx);
     size_t m = (size_t)n * h * w, nw = (size_t)cout * 9 * cin;

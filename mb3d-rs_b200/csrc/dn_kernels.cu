@@ -1,7 +1,6 @@
-// The denoiser's kernels besides the convolution itself (dn_tc.cu): the
-// weight and bias gradients of a 3x3 convolution on the BF16 tensor cores
-// with FP32 accumulation, and the elementwise pieces of the U-Net (pooling,
-// upsampling, ReLU masks, input packing, the loss, Adam).
+// The denoiser's kernels besides the tensor-core convolution and weight
+// gradient (dn_tc.cu): the bias gradient and the elementwise pieces of the
+// U-Net (pooling, upsampling, ReLU masks, input packing, the loss, Adam).
 //
 // Activations are NHWC bf16 tensors whose channel counts are multiples of
 // 16; a convolution reads `cin` channels at offset `in_off` of a tensor of
@@ -15,139 +14,8 @@
 
 namespace mb3dcu {
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void cp_async16(void *dst, const void *src, bool valid) {
-    // zero-fills the 16 bytes when !valid (src-size 0)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
-
-__device__ __forceinline__ void ldsm_x4(uint32_t r[4], const void *p) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
-__device__ __forceinline__ void ldsm_x4_t(uint32_t r[4], const void *p) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
-__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// ---------------------------------------------------------------------------
-// Weight gradient: dW[co][tap][ci] += sum over pixels p of
-// dz[p][co] * x[p + tap][ci] (zero outside the picture).  GEMM with
-// M = cout (CO = cout/16 m16 tiles), N = 16 input channels of one tap
-// (blockIdx.x = tap x cin/16), K = the pixels of the block's chunk
-// (blockIdx.y); each warp takes every 4th 16-pixel step of the chunk with its
-// own double-buffered shared slice, the warps' sums meet in shared memory and
-// go to dW with one FP32 atomicAdd per element.
-constexpr int WG_PIX = 2048;  // pixels per block
-
-template <int CO>
-__global__ void __launch_bounds__(128) k_conv3x3_wgrad(WgradArgs a) {
-    constexpr int COUT = CO * 16;
-    constexpr int LDZ = COUT + 8;  // dz rows (16 B pad: conflict-free ldmatrix)
-    constexpr int LDX = 16 + 8;
-    __shared__ __align__(128) __nv_bfloat16 sz[4][2][16 * LDZ];
-    __shared__ __align__(128) __nv_bfloat16 sx[4][2][16 * LDX];
-    __shared__ float red[4][COUT * 16 / 4];  // (reused per warp pair below)
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int cin16 = a.cin >> 4;
-    const int tap = blockIdx.x / cin16, ci0 = (blockIdx.x - tap * cin16) << 4;
-    const int dy = tap / 3 - 1, dx = tap - (tap / 3) * 3 - 1;
-    const int p_begin = blockIdx.y * WG_PIX, p_end = min(p_begin + WG_PIX, a.m);
-    const int hw = a.h * a.w;
-    float acc[CO][2][4];
-#pragma unroll
-    for (int i = 0; i < CO; i++)
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-#pragma unroll
-            for (int k = 0; k < 4; k++) acc[i][j][k] = 0.0f;
-    // one 16-pixel step: dz rows (COUT*2 B each) and x rows (32 B each)
-    auto load = [&](int p0, int buf) {
-        for (int e = lane; e < 16 * (COUT / 8); e += 32) {
-            int row = e / (COUT / 8), piece = e - row * (COUT / 8);
-            int p = p0 + row;
-            bool v = p < p_end;
-            const __nv_bfloat16 *src = v ? a.dz + (size_t)p * a.dz_c + a.dz_off + piece * 8 : a.dz;
-            cp_async16(&sz[warp][buf][row * LDZ + piece * 8], src, v);
-        }
-        {
-            int row = lane >> 1, half = lane & 1;
-            int p = p0 + row;
-            bool v = p < p_end;
-            if (v) {
-                int n = p / hw, r = p - n * hw, y = r / a.w, x = r - y * a.w;
-                y += dy;
-                x += dx;
-                v = (unsigned)y < (unsigned)a.h && (unsigned)x < (unsigned)a.w;
-                if (v) p = (n * a.h + y) * a.w + x;
-            }
-            const __nv_bfloat16 *src = v ? a.x + (size_t)p * a.x_c + a.x_off + ci0 + half * 8 : a.x;
-            cp_async16(&sx[warp][buf][row * LDX + half * 8], src, v);
-        }
-    };
-    int step = 0;
-    int p0 = p_begin + warp * 16;
-    if (p0 < p_end) load(p0, 0);
-    cp_async_commit();
-    for (; p0 < p_end; p0 += 64, step++) {
-        const int buf = step & 1;
-        if (p0 + 64 < p_end) load(p0 + 64, buf ^ 1);
-        cp_async_commit();
-        cp_async_wait<1>();
-        __syncwarp();
-        // B fragments: x rows = k (pixels), 16 channels = two n8 tiles
-        uint32_t bx[4];
-        {
-            int r = (lane & 7) + (((lane >> 3) & 1) << 3);  // k rows 0..15
-            int c = (lane >> 4) * 8;                          // n block
-            ldsm_x4_t(bx, &sx[warp][buf][r * LDX + c]);
-        }
-#pragma unroll
-        for (int i = 0; i < CO; i++) {
-            // A = dz^T: m = co (16), k = pixels (16)
-            uint32_t af[4];
-            int r = (lane & 7) + ((lane >> 4) << 3);  // pixel rows
-            int c = i * 16 + ((lane >> 3) & 1) * 8;    // co block
-            ldsm_x4_t(af, &sz[warp][buf][r * LDZ + c]);
-            mma16816(acc[i][0], af, bx[0], bx[1]);
-            mma16816(acc[i][1], af, bx[2], bx[3]);
-        }
-        __syncwarp();
-    }
-    cp_async_wait<0>();
-    // the warps' sums: warp 0..3 add into shared memory, then atomics
-    __syncthreads();
-    float *rs = &red[0][0];  // COUT x 16 floats
-    for (int e = tid; e < COUT * 16; e += 128) rs[e] = 0.0f;
-    __syncthreads();
-    const int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int i = 0; i < CO; i++)
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                int co = i * 16 + g + (k >> 1) * 8, ci = j * 8 + 2 * t + (k & 1);
-                atomicAdd(&rs[co * 16 + ci], acc[i][j][k]);
-            }
-    __syncthreads();
-    for (int e = tid; e < COUT * 16; e += 128) {
-        int co = e >> 4, ci = e & 15;
-        if (co < a.cout) atomicAdd(&a.dw[((size_t)co * 9 + tap) * a.cin + ci0 + ci], rs[e]);
-    }
-}
+// pixels per block of the bias gradient
+constexpr int WG_PIX = 2048;
 
 // bias gradient: db[c] += sum over the block's pixels of dz[p][c]
 __global__ void k_bias_grad(const __nv_bfloat16 *dz, int dz_c, int dz_off, int cout, int m, float *db) {
@@ -375,16 +243,7 @@ static int grid_for(size_t n, int per = 256) {
 }
 
 int dn_wgrad(const WgradArgs &a, float *db, cudaStream_t s) {
-    if (a.cin % 16 || a.cout % 16 || a.cout > 96 || a.dz_c % 8 || a.dz_off % 8 || a.x_c % 8 || a.x_off % 8) return -1;
-    dim3 grid(9 * (a.cin / 16), (a.m + WG_PIX - 1) / WG_PIX);
-    switch (a.cout / 16) {
-        case 1: k_conv3x3_wgrad<1><<<grid, 128, 0, s>>>(a); break;
-        case 2: k_conv3x3_wgrad<2><<<grid, 128, 0, s>>>(a); break;
-        case 3: k_conv3x3_wgrad<3><<<grid, 128, 0, s>>>(a); break;
-        case 4: k_conv3x3_wgrad<4><<<grid, 128, 0, s>>>(a); break;
-        case 5: k_conv3x3_wgrad<5><<<grid, 128, 0, s>>>(a); break;
-        default: k_conv3x3_wgrad<6><<<grid, 128, 0, s>>>(a); break;
-    }
+    if (dn_wgrad_tc(a, s)) return -1;
     if (db) k_bias_grad<<<(a.m + WG_PIX - 1) / WG_PIX, 128, 0, s>>>(a.dz, a.dz_c, a.dz_off, a.cout, a.m, db);
     return 0;
 }

@@ -5,6 +5,7 @@
     python mb3d-rs_b200/profile_cases.py c1        # the plain bulb 640x480: one mixed, one FP64 render
     python mb3d-rs_b200/profile_cases.py c4        # frame 37 of the 240-frame flight: one mixed, one FP64 render
     python mb3d-rs_b200/profile_cases.py de        # single precision DEs of the C2 scene at 3, 6 and 30 iterations
+    python mb3d-rs_b200/profile_cases.py train     # 20 denoiser training steps, batch 16 of 128x128 (after 3)
 
 The Calculate 3D kernels are profiled through bench.py (--scale 0.25).
 """
@@ -50,6 +51,30 @@ def denoise():
     print("ok denoise 1920x1080 ms", e0.elapsed_time(e1) / 5)
 
 
+def train():
+    import torch
+    card = mb3dcu.Card(0)
+    dn = mb3dcu.Denoiser(card)
+    n, h, w = 16, 128, 128
+    g = torch.Generator(device="cuda").manual_seed(0)
+    rad = torch.rand((n, h, w, 3), device="cuda", generator=g) * 2.0
+    tgt = rad * 0.9
+    alb = torch.rand((n, h, w, 3), device="cuda", generator=g)
+    nrm = torch.rand((n, h, w, 3), device="cuda", generator=g)
+    dep = torch.rand((n, h, w), device="cuda", generator=g)
+    card.set_stream(torch.cuda.current_stream().cuda_stream)
+    for _ in range(3):
+        dn.train_step(rad, tgt, alb, nrm, dep, depth_scale=1.0, lr=1e-3)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(20):
+        loss = dn.train_step(rad, tgt, alb, nrm, dep, depth_scale=1.0, lr=1e-3)
+    e1.record()
+    torch.cuda.synchronize()
+    print("ok train step (16 x 128 x 128) ms", e0.elapsed_time(e1) / 20, "loss", loss)
+
+
 def _both(sc):
     card = mb3dcu.Card(0)
     for prec in (mb3dcu.FP32_FP64, mb3dcu.FP64):
@@ -82,4 +107,4 @@ def de():
 
 
 if __name__ == "__main__":
-    {"mc": mc, "denoise": denoise, "c1": c1, "c4": c4, "de": de}[sys.argv[1]]()
+    {"mc": mc, "denoise": denoise, "c1": c1, "c4": c4, "de": de, "train": train}[sys.argv[1]]()

@@ -18,16 +18,19 @@ import unet
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("cin,cout", [(16, 32), (32, 32), (48, 64), (80, 48), (32, 96), (112, 16), (176, 80)])
-def test_conv_kernels_match_fp64(card, cin, cout):
-    rng = np.random.default_rng(cin * 1000 + cout)
-    n, h, w = 2, 9, 13  # ragged: partial pixel tiles, every border
+@pytest.mark.parametrize("cin,cout,n,h,w", [(16, 32, 2, 9, 13), (32, 32, 2, 9, 13), (48, 64, 2, 9, 13),
+                                             (80, 48, 2, 9, 13), (32, 96, 2, 9, 13), (112, 16, 2, 9, 13),
+                                             (176, 80, 2, 9, 13), (16, 128, 2, 9, 13),
+                                             # more tiles than blocks: each block's accumulators
+                                             # take several tiles through the stage ring
+                                             (16, 32, 8, 100, 124), (64, 48, 3, 61, 77)])
+def test_conv_kernels_match_fp64(card, cin, cout, n, h, w):
+    rng = np.random.default_rng(cin * 1000 + cout + h)
+    # (9 x 13: ragged, partial pixel tiles, every border)
     x = unet.bf16(rng.standard_normal((n, h, w, cin)))
     wt = unet.bf16(rng.standard_normal((cout, 9, cin)) * np.sqrt(2.0 / (9 * cin)))
     b = rng.standard_normal(cout).astype(np.float32)
     dy = unet.bf16(rng.standard_normal((n, h, w, cout)))
-    if cout > 96:
-        pytest.skip("the weight gradient kernel takes cout <= 96")
     y, dx, dw, db = mb3dcu.conv_check(card, x, wt, b, dy)
     ye = unet.conv(x.astype(np.float64), wt.astype(np.float64), b.astype(np.float64))
     dxe, dwe, dbe = unet.conv_bwd(x.astype(np.float64), wt.astype(np.float64), dy.astype(np.float64))
