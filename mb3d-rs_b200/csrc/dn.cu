@@ -203,9 +203,11 @@ int forward(mb3d_cu_dn *d, cudaStream_t s) {
 }
 
 // the gradients of layer li: dz (a slot of a tensor, already masked by the
-// ReLU) and its input x; dx_out (may be null) receives the input's gradient
+// ReLU) and its input x; dx_out (may be null) receives the input's gradient,
+// masked by dx_mask (may be null: the ReLU output the layer's input is, same
+// layout as dx)
 int layer_bwd(mb3d_cu_dn *d, int li, const bf16 *dz, int dz_c, int dz_off, const bf16 *x, int x_c, int x_off, bf16 *dx,
-              int dx_c, int n, int h, int w, cudaStream_t s) {
+              int dx_c, int n, int h, int w, cudaStream_t s, const bf16 *dx_mask = nullptr) {
     const Layer &L = d->layers[li];
     WgradArgs wa;
     wa.dz = dz;
@@ -240,6 +242,11 @@ int layer_bwd(mb3d_cu_dn *d, int li, const bf16 *dz, int dz_c, int dz_off, const
         a.cout = L.cin;
         a.relu = 0;
         a.accumulate = 0;
+        // (the ReLU's backward of the layer below, when its output is x: dx
+        // stays where x > 0)
+        a.mask = dx_mask;
+        a.mask_c = dx_c;
+        a.mask_off = 0;
         DN_TRY(dn_conv(a, s));
     }
     return 0;
@@ -249,13 +256,15 @@ int backward(mb3d_cu_dn *d, cudaStream_t s) {
     const int n = d->n, h = d->h, w = d->w;
     Acts &A = d->a, &G = d->g;
     // the output layer (no ReLU): g.pred holds the loss gradient
-    if (int e = layer_bwd(d, L_OUT, G.pred, OUT_C, 0, A.db[0], CH[0], 0, G.db[0], CH[0], n, h, w, s)) return e;
+    // (the ReLU masks of the gradients that a convolution's input gradient
+    // writes whole are fused into that convolution's store)
+    if (int e = layer_bwd(d, L_OUT, G.pred, OUT_C, 0, A.db[0], CH[0], 0, G.db[0], CH[0], n, h, w, s, A.db[0])) return e;
     for (int l = 0; l < 4; l++) {
         int hl = h >> l, wl = w >> l, cu = CH[l + 1] + CH[l];
         size_t Ml = (size_t)n * hl * wl;
-        dn_relu_mask(G.db[l], A.db[l], CH[l], 0, CH[l], Ml, s);
-        if (int e = layer_bwd(d, l_dec(l, 1), G.db[l], CH[l], 0, A.da[l], CH[l], 0, G.da[l], CH[l], n, hl, wl, s)) return e;
-        dn_relu_mask(G.da[l], A.da[l], CH[l], 0, CH[l], Ml, s);
+        if (l > 0) dn_relu_mask(G.db[l], A.db[l], CH[l], 0, CH[l], Ml, s);
+        if (int e = layer_bwd(d, l_dec(l, 1), G.db[l], CH[l], 0, A.da[l], CH[l], 0, G.da[l], CH[l], n, hl, wl, s, A.da[l]))
+            return e;
         if (int e = layer_bwd(d, l_dec(l, 0), G.da[l], CH[l], 0, A.cat[l], cu, 0, G.cat[l], cu, n, hl, wl, s)) return e;
         bf16 *glow = l == 3 ? G.bb : G.db[l + 1];
         dn_up2_bwd(G.cat[l], cu, 0, CH[l + 1], n, hl, wl, glow, s);
@@ -263,8 +272,7 @@ int backward(mb3d_cu_dn *d, cudaStream_t s) {
     int h4 = h >> 4, w4 = w >> 4;
     size_t M4 = (size_t)n * h4 * w4;
     dn_relu_mask(G.bb, A.bb, CH[4], 0, CH[4], M4, s);
-    if (int e = layer_bwd(d, L_BOT_B, G.bb, CH[4], 0, A.ba, CH[4], 0, G.ba, CH[4], n, h4, w4, s)) return e;
-    dn_relu_mask(G.ba, A.ba, CH[4], 0, CH[4], M4, s);
+    if (int e = layer_bwd(d, L_BOT_B, G.bb, CH[4], 0, A.ba, CH[4], 0, G.ba, CH[4], n, h4, w4, s, A.ba)) return e;
     if (int e = layer_bwd(d, L_BOT_A, G.ba, CH[4], 0, A.pool[4], CH[3], 0, G.pool[4], CH[3], n, h4, w4, s)) return e;
     for (int l = 3; l >= 0; l--) {
         int hl = h >> l, wl = w >> l, cu = CH[l + 1] + CH[l];
@@ -272,9 +280,9 @@ int backward(mb3d_cu_dn *d, cudaStream_t s) {
         // the skip's gradient: from the decoder (in g.cat) plus the pooling's
         dn_pool2_bwd(A.cat[l], cu, CH[l + 1], CH[l], n, hl, wl, G.pool[l + 1], G.cat[l], s);
         dn_relu_mask(G.cat[l], A.cat[l], cu, CH[l + 1], CH[l], Ml, s);
-        if (int e = layer_bwd(d, l_enc(l, ENC_B), G.cat[l], cu, CH[l + 1], A.ea[l], CH[l], 0, G.ea[l], CH[l], n, hl, wl, s))
+        if (int e = layer_bwd(d, l_enc(l, ENC_B), G.cat[l], cu, CH[l + 1], A.ea[l], CH[l], 0, G.ea[l], CH[l], n, hl, wl, s,
+                              A.ea[l]))
             return e;
-        dn_relu_mask(G.ea[l], A.ea[l], CH[l], 0, CH[l], Ml, s);
         const bf16 *x = l == 0 ? A.x0 : A.pool[l];
         int xc = l == 0 ? IN_C : CH[l - 1];
         if (int e = layer_bwd(d, l_enc(l, ENC_A), G.ea[l], CH[l], 0, x, xc, 0, l == 0 ? nullptr : G.pool[l], xc, n, hl, wl, s))

@@ -16,6 +16,11 @@ struct ConvArgs {
     int in_c, in_off, cin;
     int out_c, out_off, cout;
     int relu, accumulate;
+    // (or null) the ReLU's backward fused into the store: the outputs whose
+    // value in mask (mask_c channels per pixel, cout of them at mask_off) is
+    // not positive are zero
+    const __nv_bfloat16 *mask = nullptr;
+    int mask_c = 0, mask_off = 0;
 };
 
 // its weight gradient: dw[co][tap][ci] += sum_p dz[p][co] x[p + tap][ci]
@@ -35,9 +40,10 @@ int dn_conv(const ConvArgs &a, cudaStream_t s);
 // last call; synchronises s
 int dn_conv_error(cudaStream_t s);
 int dn_wgrad(const WgradArgs &a, float *db, cudaStream_t s);
-// (its tensor-core kernel, dn_tc.cu: cin and cout multiples of 16, cout <=
-// 128, the channel counts and offsets multiples of 8; -1 on bad arguments)
-int dn_wgrad_tc(const WgradArgs &a, cudaStream_t s);
+// (its tensor-core kernel, dn_tc.cu, with the bias gradient db (or null):
+// cin and cout multiples of 16, cout <= 128, the channel counts and offsets
+// multiples of 8; -1 on bad arguments)
+int dn_wgrad_tc(const WgradArgs &a, float *db, cudaStream_t s);
 void dn_relu_mask(__nv_bfloat16 *d, const __nv_bfloat16 *y, int c_tot, int off, int cn, size_t m, cudaStream_t s);
 void dn_pool2(const __nv_bfloat16 *in, int in_c, int in_off, int cn, int n, int h, int w, __nv_bfloat16 *out,
               cudaStream_t s);

@@ -1,6 +1,6 @@
-// The denoiser's kernels besides the tensor-core convolution and weight
-// gradient (dn_tc.cu): the bias gradient and the elementwise pieces of the
-// U-Net (pooling, upsampling, ReLU masks, input packing, the loss, Adam).
+// The denoiser's kernels besides the tensor-core convolution, weight and
+// bias gradients (dn_tc.cu): the elementwise pieces of the U-Net (pooling,
+// upsampling, ReLU masks, input packing, the loss, Adam).
 //
 // Activations are NHWC bf16 tensors whose channel counts are multiples of
 // 16; a convolution reads `cin` channels at offset `in_off` of a tensor of
@@ -13,23 +13,6 @@
 #include "dn.h"
 
 namespace mb3dcu {
-
-// pixels per block of the bias gradient
-constexpr int WG_PIX = 2048;
-
-// bias gradient: db[c] += sum over the block's pixels of dz[p][c]
-__global__ void k_bias_grad(const __nv_bfloat16 *dz, int dz_c, int dz_off, int cout, int m, float *db) {
-    __shared__ float s[128];
-    const int c = threadIdx.x;
-    float acc = 0.0f;
-    if (c < cout) {
-        int p_end = min((int)(blockIdx.x + 1) * WG_PIX, m);
-        for (int p = blockIdx.x * WG_PIX; p < p_end; p++) acc += __bfloat162float(dz[(size_t)p * dz_c + dz_off + c]);
-    }
-    s[c] = acc;
-    __syncthreads();
-    if (c < cout) atomicAdd(&db[c], s[c]);
-}
 
 // ---------------------------------------------------------------------------
 // elementwise pieces (one thread per element or per 2x2 group)
@@ -242,11 +225,7 @@ static int grid_for(size_t n, int per = 256) {
     return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
 }
 
-int dn_wgrad(const WgradArgs &a, float *db, cudaStream_t s) {
-    if (dn_wgrad_tc(a, s)) return -1;
-    if (db) k_bias_grad<<<(a.m + WG_PIX - 1) / WG_PIX, 128, 0, s>>>(a.dz, a.dz_c, a.dz_off, a.cout, a.m, db);
-    return 0;
-}
+int dn_wgrad(const WgradArgs &a, float *db, cudaStream_t s) { return dn_wgrad_tc(a, db, s) ? -1 : 0; }
 
 void dn_relu_mask(__nv_bfloat16 *d, const __nv_bfloat16 *y, int c_tot, int off, int cn, size_t m, cudaStream_t s) {
     k_relu_mask<<<grid_for(m * cn), 256, 0, s>>>(d, y, c_tot, off, cn, m);

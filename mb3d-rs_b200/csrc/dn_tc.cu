@@ -54,6 +54,8 @@ struct ConvTc {
     int in_off, cin;
     int out_c, out_off, cout;
     int relu, accumulate;
+    const __nv_bfloat16 *mask;
+    int mask_c, mask_off;
     int tiles_x, tiles_y;
     int stages, resident;
     uint32_t w_bytes, stage_bytes;
@@ -116,8 +118,10 @@ __device__ __forceinline__ uint32_t idesc_bf16() {
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// 16 accumulator columns of one pixel: bias, ReLU, (the old value), bf16
-__device__ __forceinline__ void store16(__nv_bfloat16 *o, int nb, const uint32_t (&r)[16], const ConvTc &a) {
+// 16 accumulator columns of one pixel: bias, ReLU, (the old value), (the
+// mask), bf16
+__device__ __forceinline__ void store16(__nv_bfloat16 *o, const __nv_bfloat16 *mk, int nb, const uint32_t (&r)[16],
+                                        const ConvTc &a) {
     float v[16];
 #pragma unroll
     for (int k = 0; k < 16; k++) {
@@ -140,6 +144,18 @@ __device__ __forceinline__ void store16(__nv_bfloat16 *o, int nb, const uint32_t
                 v[8 + 2 * k + 1] += __high2float(q1[k]);
             }
         }
+        if (mk) {
+            const uint4 m0 = reinterpret_cast<const uint4 *>(mk + nb)[0], m1 = reinterpret_cast<const uint4 *>(mk + nb)[1];
+            const __nv_bfloat162 *q0 = reinterpret_cast<const __nv_bfloat162 *>(&m0);
+            const __nv_bfloat162 *q1 = reinterpret_cast<const __nv_bfloat162 *>(&m1);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                if (!(__low2float(q0[k]) > 0.0f)) v[2 * k] = 0.0f;
+                if (!(__high2float(q0[k]) > 0.0f)) v[2 * k + 1] = 0.0f;
+                if (!(__low2float(q1[k]) > 0.0f)) v[8 + 2 * k] = 0.0f;
+                if (!(__high2float(q1[k]) > 0.0f)) v[8 + 2 * k + 1] = 0.0f;
+            }
+        }
 #pragma unroll
         for (int k = 0; k < 8; k++) p[k] = __floats2bfloat162_rn(v[2 * k], v[2 * k + 1]);
         dst[0] = *reinterpret_cast<const uint4 *>(&p[0]);
@@ -148,6 +164,7 @@ __device__ __forceinline__ void store16(__nv_bfloat16 *o, int nb, const uint32_t
         for (int k = 0; k < 16 && nb + k < a.cout; k++) {
             float x = v[k];
             if (a.accumulate) x += __bfloat162float(o[nb + k]);
+            if (mk && !(__bfloat162float(mk[nb + k]) > 0.0f)) x = 0.0f;
             o[nb + k] = __float2bfloat16_rn(x);
         }
     }
@@ -294,8 +311,9 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
             tile_of(a, g, img, x0, y0);
             const int px = x0 + row % TILE_W, py = y0 + row / TILE_W;
             const bool valid = px < a.w && py < a.h;
-            __nv_bfloat16 *o =
-                a.out + ((size_t)(img * a.h + (valid ? py : 0)) * a.w + (valid ? px : 0)) * a.out_c + a.out_off;
+            const size_t pix = (size_t)(img * a.h + (valid ? py : 0)) * a.w + (valid ? px : 0);
+            __nv_bfloat16 *o = a.out + pix * a.out_c + a.out_off;
+            const __nv_bfloat16 *mk = a.mask ? a.mask + pix * a.mask_c + a.mask_off : nullptr;
 #pragma unroll
             for (int c = 0; c < BN; c += 16) {
                 uint32_t r[16];
@@ -308,7 +326,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                     : "r"(taddr)
                     : "memory");
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (valid && c < a.cout) store16(o, c, r, a);
+                if (valid && c < a.cout) store16(o, mk, c, r, a);
             }
             // the accumulator buffer is free for the MMAs of tile i + 2
             tc_fence_before();
@@ -341,17 +359,21 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
 // nine taps accumulate in nine 16 G-column TMEM accumulators over all of the
 // block's tiles (72 tcgen05.mma M=128 N=16 G K=16 per tile: nine taps x
 // eight K steps), and at the end the four warps read them (warp w: co
-// 32 w .. 32 w + 31) and add them to dW with 16-byte FP32 atomics.  Roles:
+// 32 w .. 32 w + 31) and add them to dW with 16-byte FP32 atomics.  The
+// blocks of the first channel set also form the bias gradient, db[co] = sum
+// over p of dz[p][co], as one more MMA per K step with a B operand of ones
+// into a tenth accumulator.  Roles:
 // lane 0 of warp 0 issues the TMA loads, lane 0 of warp 1 the MMAs; every
 // wait is bounded as in the forward kernel.
 constexpr uint32_t WG_A_GROUP = TILE_W * TILE_H * 16;  // one 8-co box of a tile (2048 bytes)
 constexpr uint32_t WG_A_BYTES = 16 * WG_A_GROUP;        // M = 128: 16 boxes
 constexpr int WG_G = 3;                                 // channel groups of 16 per block, at most
 constexpr int WG_MAX_STAGES = 6;
-constexpr uint32_t WG_COLS = 512;                       // nine accumulators of up to 48 columns
+constexpr uint32_t WG_COLS = 512;                       // nine accumulators of up to 48 columns, the bias's 16
+constexpr uint32_t WG_ONES = 1024;                      // the ones operand (512 bytes) before the stages
 
 struct WgTc {
-    float *dw;
+    float *dw, *db;
     int n, h, w, cin, cout, dz_off, x_off;
     int tiles_x, tiles_y, groups, sets, stages;
     uint32_t stage_bytes;
@@ -365,9 +387,10 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
     uint8_t *base = dyn + ((1024u - (smem_addr(dyn) & 1023u)) & 1023u);
-    const uint32_t st0 = smem_addr(base);
+    const uint32_t ones = smem_addr(base), st0 = ones + WG_ONES;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int set = (int)blockIdx.x % a.sets;
+    const bool bias = a.db && set == 0;
     const int g0 = set * WG_G, ng = min(WG_G, a.groups - g0);  // this block's channel groups
     const int first = (int)blockIdx.x / a.sets, step = (int)gridDim.x / a.sets;
     const int total = a.n * a.tiles_y * a.tiles_x;
@@ -375,10 +398,11 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
     const int ns = a.stages;
     // the boxes past cout stay zero (the rows of M that no output channel has)
     for (int st = 0; st < ns; st++) {
-        uint4 *z = reinterpret_cast<uint4 *>(base + (size_t)st * a.stage_bytes + (size_t)cog * WG_A_GROUP);
+        uint4 *z = reinterpret_cast<uint4 *>(base + WG_ONES + (size_t)st * a.stage_bytes + (size_t)cog * WG_A_GROUP);
         const int n16 = (16 - cog) * (int)(WG_A_GROUP / 16);
         for (int i = tid; i < n16; i += blockDim.x) z[i] = make_uint4(0u, 0u, 0u, 0u);
     }
+    if (tid < 32) reinterpret_cast<uint4 *>(base)[tid] = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (tid == 0) {
         for (int st = 0; st < ns; st++) {
@@ -438,6 +462,21 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
             const uint32_t sa = st0 + st * a.stage_bytes, sb = sa + WG_A_BYTES;
             const uint64_t ad0 = desc_plain(sa, 128u, WG_A_GROUP);
             const uint64_t bd0 = desc_plain(sb, HALO_W * 16u, HALF_BYTES);
+            if (bias) {
+                // 16 pixels x 16 columns of ones: every column of the tenth
+                // accumulator sums dz over the pixels
+                const uint32_t idesc1 = (idesc & ~(0x3Fu << 17)) | (2u << 17);
+                const uint64_t od = desc_plain(ones, 128u, 256u);
+#pragma unroll
+                for (int k = 0; k < 8; k++) {
+                    const uint32_t acc = (q | (uint32_t)k) ? 1u : 0u;
+                    asm volatile(
+                        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + 9u * tap_cols),
+                        "l"(ad0 + (uint64_t)(k * 16)), "l"(od), "r"(idesc1), "r"(acc)
+                        : "memory");
+                }
+            }
 #pragma unroll
             for (int tap = 0; tap < 9; tap++) {
                 const int dy = tap / 3, dx = tap % 3;  // (offsets + 1)
@@ -468,6 +507,19 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
     if (ok && first < total) {
         tc_fence_after();
         const int co = warp * 32 + lane;
+        if (bias) {
+            uint32_t r[16];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + 9u * tap_cols;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(taddr)
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (co < a.cout) atomicAdd(a.db + co, __uint_as_float(r[0]));
+        }
         for (int tap = 0; tap < 9; tap++) {
             for (int j = 0; j < ng; j++) {
                 uint32_t r[16];
@@ -555,6 +607,7 @@ void launch_tc(const CUtensorMap &ta, ConvTc c, int total, cudaStream_t s) {
 
 int dn_conv(const ConvArgs &a, cudaStream_t s) {
     if (a.cin % 16 || a.cout % 16 || a.cout > 256 || a.in_c % 8 || a.in_off % 8 || a.out_c % 8 || a.out_off % 8) return -1;
+    if (a.mask && (a.mask_c % 8 || a.mask_off % 8 || a.mask_c < a.mask_off + a.cout)) return -1;
     if (a.n < 1 || a.h < 1 || a.w < 1 || a.in_c < a.in_off + a.cin || a.out_c < a.out_off + a.cout) return -1;
     EncodeTiledFn enc = encode_fn();
     int *err = err_word();
@@ -573,6 +626,9 @@ int dn_conv(const ConvArgs &a, cudaStream_t s) {
     c.cout = a.cout;
     c.relu = a.relu;
     c.accumulate = a.accumulate;
+    c.mask = a.mask;
+    c.mask_c = a.mask_c;
+    c.mask_off = a.mask_off;
     c.tiles_x = (a.w + TILE_W - 1) / TILE_W;
     c.tiles_y = (a.h + TILE_H - 1) / TILE_H;
     c.err = err;
@@ -612,7 +668,7 @@ int dn_conv(const ConvArgs &a, cudaStream_t s) {
     return 0;
 }
 
-int dn_wgrad_tc(const WgradArgs &a, cudaStream_t s) {
+int dn_wgrad_tc(const WgradArgs &a, float *db, cudaStream_t s) {
     if (a.cin % 16 || a.cout % 16 || a.cout > 128 || a.dz_c % 8 || a.dz_off % 8 || a.x_c % 8 || a.x_off % 8) return -1;
     if (a.n < 1 || a.h < 1 || a.w < 1 || a.dz_c < a.dz_off + a.cout || a.x_c < a.x_off + a.cin) return -1;
     EncodeTiledFn enc = encode_fn();
@@ -620,6 +676,7 @@ int dn_wgrad_tc(const WgradArgs &a, cudaStream_t s) {
     if (!enc || !err) return -1;
     WgTc c;
     c.dw = a.dw;
+    c.db = db;
     c.n = a.n;
     c.h = a.h;
     c.w = a.w;
@@ -635,7 +692,7 @@ int dn_wgrad_tc(const WgradArgs &a, cudaStream_t s) {
     // the stages: the tile's dz boxes and its input boxes (up to 2 G of them)
     const int g_max = c.groups < WG_G ? c.groups : WG_G;
     c.stage_bytes = WG_A_BYTES + (uint32_t)(2 * g_max) * HALF_BYTES;
-    c.stages = (int)((220u * 1024u) / c.stage_bytes);
+    c.stages = (int)((219u * 1024u) / c.stage_bytes);
     if (c.stages > WG_MAX_STAGES) c.stages = WG_MAX_STAGES;
     // dz: dims (channels, x, y, image), one 8-channel box of a tile's 8 x 16 pixels
     CUtensorMap tz, tx;
@@ -658,7 +715,7 @@ int dn_wgrad_tc(const WgradArgs &a, cudaStream_t s) {
     int chunks = sm_count() / c.sets;
     if (chunks > tiles / 4) chunks = tiles / 4;
     if (chunks < 1) chunks = 1;
-    const size_t smem = 1024 + (size_t)c.stages * c.stage_bytes;
+    const size_t smem = 1024 + WG_ONES + (size_t)c.stages * c.stage_bytes;
     cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_wgrad_tc<<<c.sets * chunks, 128, smem, s>>>(tz, tx, c);
     return 0;
