@@ -346,66 +346,63 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
 // The weight gradient on the same tensor cores:
 //   dW[co][tap][ci] += sum over the pixels p of dz[p][co] x[p + tap][ci]
 // as a GEMM with M = 128 rows of co (cout <= 128; the rows past cout read
-// zeros), N = the 16 G input channels of up to G = 3 groups of 16 for one
-// tap, K = the 128 pixels of a tile (8 x 16).  Both operands are read in the
-// MN-major layout without swizzle.  A = dz transposed: the TMA brings the
-// tile's dz as one box [16 rows][8 pixels][8 co] per 8 output channels, i.e.
-// core matrices of 8 pixels x 8 co, 128 bytes apart along K and one box
-// apart along M.  B = the tile's input box with its one-pixel halo, one box
-// per 8 input channels as the forward convolution loads it: for tap (dy, dx)
-// the operand starts at ((dy + 1) * 10 + dx + 1) * 16, its 8-pixel groups
-// 160 bytes apart along K and its 8-channel boxes one box apart along N.  A
-// block takes a set of G channel groups and every (grid / sets)-th tile; the
-// nine taps accumulate in nine 16 G-column TMEM accumulators over all of the
-// block's tiles (72 tcgen05.mma M=128 N=16 G K=16 per tile: nine taps x
-// eight K steps), and at the end the four warps read them (warp w: co
-// 32 w .. 32 w + 31) and add them to dW with 16-byte FP32 atomics.  The
-// blocks of the first channel set also form the bias gradient, db[co] = sum
-// over p of dz[p][co], as one more MMA per K step with a B operand of ones
-// into a tenth accumulator.  Roles:
-// lane 0 of warp 0 issues the TMA loads, lane 0 of warp 1 the MMAs; every
-// wait is bounded as in the forward kernel.
-constexpr uint32_t WG_A_GROUP = TILE_W * TILE_H * 16;  // one 8-co box of a tile (2048 bytes)
-constexpr uint32_t WG_A_BYTES = 16 * WG_A_GROUP;        // M = 128: 16 boxes
-constexpr int WG_G = 3;                                 // channel groups of 16 per block, at most
-constexpr int WG_MAX_STAGES = 6;
-constexpr uint32_t WG_COLS = 512;                       // nine accumulators of up to 48 columns, the bias's 16
-constexpr uint32_t WG_ONES = 1024;                      // the ones operand (512 bytes) before the stages
+// zeros), N = 144 columns (tap, ci) of one group of 16 input channels,
+// K = the 128 pixels of a tile (8 x 16), in eight K steps of 16 pixels.
+// Both operands are arrays of TMA boxes [16 rows][8 pixels][8 channels]
+// (2048 bytes), read in the MN-major layout without swizzle: core matrices
+// of 8 pixels x 8 channels, 128 bytes apart along K and one box apart along
+// M or N.  A = dz transposed: one box per 8 output channels.  B = the
+// tile's input seen from each tap: for tap (dy, dx) and channel half h the
+// TMA brings the 8 x 16 box of the input shifted by (dx - 1, dy - 1), its
+// zero fill the picture's border, as box 2 tap + h -- so that one MMA of
+// N = 144 takes all nine taps and A is read once per K step.  A block takes
+// one channel group and every (grid / groups)-th tile and accumulates in
+// TMEM over all of its tiles; the blocks of group 0 also form the bias
+// gradient db[co] = sum over p of dz[p][co], as one more MMA per K step with
+// a B operand of ones into 16 more columns.  At the end the four warps read
+// the accumulators (warp w: co 32 w .. 32 w + 31) and add them to dW and db
+// with FP32 atomics.  Roles: lane 0 of warp 0 issues the TMA loads, lane 0 of
+// warp 1 the MMAs; every wait is bounded as in the forward kernel.
+constexpr uint32_t WG_BOX = TILE_W * TILE_H * 16;    // one box of a tile (2048 bytes)
+constexpr uint32_t WG_A_BYTES = 16 * WG_BOX;          // M = 128: 16 boxes of 8 output channels
+constexpr uint32_t WG_B_BYTES = 18 * WG_BOX;          // nine taps x two channel halves
+constexpr uint32_t WG_STAGE = WG_A_BYTES + WG_B_BYTES;
+constexpr int WG_STAGES = 3;
+constexpr uint32_t WG_COLS = 256;                     // 144 columns of (tap, ci), 16 of the bias
+constexpr uint32_t WG_ONES = 1024;                    // the ones operand (512 bytes) before the stages
 
 struct WgTc {
     float *dw, *db;
     int n, h, w, cin, cout, dz_off, x_off;
-    int tiles_x, tiles_y, groups, sets, stages;
-    uint32_t stage_bytes;
+    int tiles_x, tiles_y, groups;
     int *err;
 };
 
 __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUtensorMap tz,
                                                      const __grid_constant__ CUtensorMap tx, const WgTc a) {
     extern __shared__ __align__(1024) uint8_t dyn[];
-    __shared__ __align__(8) uint64_t full[WG_MAX_STAGES], empty[WG_MAX_STAGES], done;
+    __shared__ __align__(8) uint64_t full[WG_STAGES], empty[WG_STAGES], done;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
     uint8_t *base = dyn + ((1024u - (smem_addr(dyn) & 1023u)) & 1023u);
     const uint32_t ones = smem_addr(base), st0 = ones + WG_ONES;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int set = (int)blockIdx.x % a.sets;
-    const bool bias = a.db && set == 0;
-    const int g0 = set * WG_G, ng = min(WG_G, a.groups - g0);  // this block's channel groups
-    const int first = (int)blockIdx.x / a.sets, step = (int)gridDim.x / a.sets;
+    const int grp = (int)blockIdx.x % a.groups;
+    const bool bias = a.db && grp == 0;
+    const int first = (int)blockIdx.x / a.groups, step = (int)gridDim.x / a.groups;
     const int total = a.n * a.tiles_y * a.tiles_x;
-    const int cog = a.cout >> 3;  // the 8-co boxes of a tile
-    const int ns = a.stages;
-    // the boxes past cout stay zero (the rows of M that no output channel has)
-    for (int st = 0; st < ns; st++) {
-        uint4 *z = reinterpret_cast<uint4 *>(base + WG_ONES + (size_t)st * a.stage_bytes + (size_t)cog * WG_A_GROUP);
-        const int n16 = (16 - cog) * (int)(WG_A_GROUP / 16);
+    const int cog = a.cout >> 3;  // the dz boxes of a tile
+    // the A boxes past cout stay zero (the rows of M that no output channel
+    // has); the ones operand
+    for (int st = 0; st < WG_STAGES; st++) {
+        uint4 *z = reinterpret_cast<uint4 *>(base + WG_ONES + (size_t)st * WG_STAGE + (size_t)cog * WG_BOX);
+        const int n16 = (16 - cog) * (int)(WG_BOX / 16);
         for (int i = tid; i < n16; i += blockDim.x) z[i] = make_uint4(0u, 0u, 0u, 0u);
     }
     if (tid < 32) reinterpret_cast<uint4 *>(base)[tid] = make_uint4(0x3F803F80u, 0x3F803F80u, 0x3F803F80u, 0x3F803F80u);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (tid == 0) {
-        for (int st = 0; st < ns; st++) {
+        for (int st = 0; st < WG_STAGES; st++) {
             mbar_init(smem_addr(&full[st]), 1);
             mbar_init(smem_addr(&empty[st]), 1);
         }
@@ -424,73 +421,62 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = tmem_slot;
-    const uint32_t tap_cols = 16u * WG_G;
 
     if (warp == 0 && lane == 0) {
         // the TMA producer: one stage per tile
         uint32_t q = 0;
         for (int g = first; g < total && !abort_flag; g += step, q++) {
-            const uint32_t st = q % (uint32_t)ns;
-            if (q >= (uint32_t)ns && !mbar_wait(smem_addr(&empty[st]), ((q / ns) - 1) & 1, &abort_flag)) {
+            const uint32_t st = q % (uint32_t)WG_STAGES;
+            if (q >= (uint32_t)WG_STAGES &&
+                !mbar_wait(smem_addr(&empty[st]), ((q / WG_STAGES) - 1) & 1, &abort_flag)) {
                 abort_flag = 1;
                 break;
             }
             const int tx_ = g % a.tiles_x, rest = g / a.tiles_x;
             const int x0 = tx_ * TILE_W, y0 = (rest % a.tiles_y) * TILE_H, img = rest / a.tiles_y;
-            const uint32_t bar = smem_addr(&full[st]), sa = st0 + st * a.stage_bytes;
-            mbar_expect_tx(bar, (uint32_t)cog * WG_A_GROUP + (uint32_t)(2 * ng) * BOX_BYTES);
-            for (int j = 0; j < cog; j++) tma_load_4d(sa + (uint32_t)j * WG_A_GROUP, &tz, a.dz_off + 8 * j, x0, y0, img, bar);
-            for (int j = 0; j < 2 * ng; j++)
-                tma_load_4d(sa + WG_A_BYTES + (uint32_t)j * HALF_BYTES, &tx, a.x_off + 16 * g0 + 8 * j, x0 - 1, y0 - 1, img,
-                            bar);
+            const uint32_t bar = smem_addr(&full[st]), sa = st0 + st * WG_STAGE, sb = sa + WG_A_BYTES;
+            mbar_expect_tx(bar, (uint32_t)(cog + 18) * WG_BOX);
+            for (int j = 0; j < cog; j++) tma_load_4d(sa + (uint32_t)j * WG_BOX, &tz, a.dz_off + 8 * j, x0, y0, img, bar);
+            const int c = a.x_off + 16 * grp;
+            for (int tap = 0; tap < 9; tap++) {
+                const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+                tma_load_4d(sb + (uint32_t)(2 * tap) * WG_BOX, &tx, c, x0 + dx, y0 + dy, img, bar);
+                tma_load_4d(sb + (uint32_t)(2 * tap + 1) * WG_BOX, &tx, c + 8, x0 + dx, y0 + dy, img, bar);
+            }
         }
     } else if (warp == 1 && lane == 0) {
-        // the MMA issuer: per tile nine taps x eight K steps of 16 pixels; the
-        // descriptors of a step are the stage's first ones plus the step's
-        // offset in 16-byte units (the address field is their low 14 bits)
-        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
-                               ((uint32_t)(2 * ng) << 17) | ((uint32_t)(TC_M >> 4) << 24);
-        // (FP32 += BF16 x BF16, A and B MN-major, N = 16 ng, M = 128)
+        // the MMA issuer: per tile eight K steps of one N = 144 MMA (and the
+        // bias's N = 16 one); a step's descriptors are the stage's first ones
+        // plus the step's 256 bytes in 16-byte units (the address field is
+        // their low 14 bits)
+        const uint32_t mn = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) | ((uint32_t)(TC_M >> 4) << 24);
+        const uint32_t idesc = mn | ((144u >> 3) << 17), idesc_b = mn | ((16u >> 3) << 17);
+        // (FP32 += BF16 x BF16, A and B MN-major, M = 128)
+        const uint64_t od = desc_plain(ones, 128u, 256u);
         uint32_t q = 0;
         for (int g = first; g < total && !abort_flag; g += step, q++) {
-            const uint32_t st = q % (uint32_t)ns;
-            if (!mbar_wait(smem_addr(&full[st]), (q / ns) & 1, &abort_flag)) {
+            const uint32_t st = q % (uint32_t)WG_STAGES;
+            if (!mbar_wait(smem_addr(&full[st]), (q / WG_STAGES) & 1, &abort_flag)) {
                 abort_flag = 1;
                 break;
             }
             tc_fence_after();
-            const uint32_t sa = st0 + st * a.stage_bytes, sb = sa + WG_A_BYTES;
-            const uint64_t ad0 = desc_plain(sa, 128u, WG_A_GROUP);
-            const uint64_t bd0 = desc_plain(sb, HALO_W * 16u, HALF_BYTES);
-            if (bias) {
-                // 16 pixels x 16 columns of ones: every column of the tenth
-                // accumulator sums dz over the pixels
-                const uint32_t idesc1 = (idesc & ~(0x3Fu << 17)) | (2u << 17);
-                const uint64_t od = desc_plain(ones, 128u, 256u);
+            const uint32_t sa = st0 + st * WG_STAGE;
+            const uint64_t ad0 = desc_plain(sa, 128u, WG_BOX), bd0 = desc_plain(sa + WG_A_BYTES, 128u, WG_BOX);
 #pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const uint32_t acc = (q | (uint32_t)k) ? 1u : 0u;
+            for (int k = 0; k < 8; k++) {
+                const uint32_t acc = (q | (uint32_t)k) ? 1u : 0u;
+                asm volatile(
+                    "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                    " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(ad0 + (uint64_t)(k * 16)), "l"(bd0 + (uint64_t)(k * 16)), "r"(idesc), "r"(acc)
+                    : "memory");
+                if (bias)
                     asm volatile(
                         "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + 9u * tap_cols),
-                        "l"(ad0 + (uint64_t)(k * 16)), "l"(od), "r"(idesc1), "r"(acc)
+                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + 144u),
+                        "l"(ad0 + (uint64_t)(k * 16)), "l"(od), "r"(idesc_b), "r"(acc)
                         : "memory");
-                }
-            }
-#pragma unroll
-            for (int tap = 0; tap < 9; tap++) {
-                const int dy = tap / 3, dx = tap % 3;  // (offsets + 1)
-#pragma unroll
-                for (int k = 0; k < 8; k++) {
-                    const uint64_t ad = ad0 + (uint64_t)(k * 16);                              // + k * 256 bytes
-                    const uint64_t bd = bd0 + (uint64_t)((dy * HALO_W + dx) + k * 2 * HALO_W);  // + k * 2 rows
-                    const uint32_t acc = (q | (uint32_t)k) ? 1u : 0u;
-                    asm volatile(
-                        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-                        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem + (uint32_t)tap * tap_cols),
-                        "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
-                        : "memory");
-                }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_addr(&empty[st]))
@@ -507,9 +493,9 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
     if (ok && first < total) {
         tc_fence_after();
         const int co = warp * 32 + lane;
-        if (bias) {
+        for (int col = 0; col < (bias ? 160 : 144); col += 16) {
             uint32_t r[16];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + 9u * tap_cols;
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)col;
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
                 "[%16];"
@@ -518,23 +504,12 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
                 : "r"(taddr)
                 : "memory");
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (co < a.cout) atomicAdd(a.db + co, __uint_as_float(r[0]));
-        }
-        for (int tap = 0; tap < 9; tap++) {
-            for (int j = 0; j < ng; j++) {
-                uint32_t r[16];
-                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)tap * tap_cols + 16u * j;
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                    "[%16];"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-                      "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
-                      "=r"(r[15])
-                    : "r"(taddr)
-                    : "memory");
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (co < a.cout) {
-                    float4 *d = reinterpret_cast<float4 *>(a.dw + ((size_t)co * 9 + tap) * a.cin + 16 * (g0 + j));
+            if (co < a.cout) {
+                if (col == 144) {
+                    atomicAdd(a.db + co, __uint_as_float(r[0]));
+                } else {
+                    const int tap = col >> 4;
+                    float4 *d = reinterpret_cast<float4 *>(a.dw + ((size_t)co * 9 + tap) * a.cin + 16 * grp);
 #pragma unroll
                     for (int k = 0; k < 4; k++)
                         atomicAdd(d + k, make_float4(__uint_as_float(r[4 * k]), __uint_as_float(r[4 * k + 1]),
@@ -687,37 +662,29 @@ int dn_wgrad_tc(const WgradArgs &a, float *db, cudaStream_t s) {
     c.tiles_x = (a.w + TILE_W - 1) / TILE_W;
     c.tiles_y = (a.h + TILE_H - 1) / TILE_H;
     c.groups = a.cin / 16;
-    c.sets = (c.groups + WG_G - 1) / WG_G;
     c.err = err;
-    // the stages: the tile's dz boxes and its input boxes (up to 2 G of them)
-    const int g_max = c.groups < WG_G ? c.groups : WG_G;
-    c.stage_bytes = WG_A_BYTES + (uint32_t)(2 * g_max) * HALF_BYTES;
-    c.stages = (int)((219u * 1024u) / c.stage_bytes);
-    if (c.stages > WG_MAX_STAGES) c.stages = WG_MAX_STAGES;
-    // dz: dims (channels, x, y, image), one 8-channel box of a tile's 8 x 16 pixels
+    // dz and x: dims (channels, x, y, image), one 8-channel box of 8 x 16 pixels
     CUtensorMap tz, tx;
     cuuint64_t dz[4] = {(cuuint64_t)a.dz_c, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
     cuuint64_t sz[3] = {(cuuint64_t)a.dz_c * 2, (cuuint64_t)a.dz_c * 2 * a.w, (cuuint64_t)a.dz_c * 2 * a.w * a.h};
-    cuuint32_t bz[4] = {8, (cuuint32_t)TILE_W, (cuuint32_t)TILE_H, 1};
-    // x: the forward convolution's input box with the halo
     cuuint64_t dx[4] = {(cuuint64_t)a.x_c, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
     cuuint64_t sx[3] = {(cuuint64_t)a.x_c * 2, (cuuint64_t)a.x_c * 2 * a.w, (cuuint64_t)a.x_c * 2 * a.w * a.h};
-    cuuint32_t bx[4] = {8, (cuuint32_t)HALO_W, (cuuint32_t)HALO_H, 1};
+    cuuint32_t box[4] = {8, (cuuint32_t)TILE_W, (cuuint32_t)TILE_H, 1};
     cuuint32_t e1[4] = {1, 1, 1, 1};
-    if (enc(&tz, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.dz, dz, sz, bz, e1, CU_TENSOR_MAP_INTERLEAVE_NONE,
+    if (enc(&tz, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.dz, dz, sz, box, e1, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
-        enc(&tx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.x, dx, sx, bx, e1, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        enc(&tx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.x, dx, sx, box, e1, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return -1;
     const int tiles = a.n * c.tiles_y * c.tiles_x;
     // blocks: about one per SM, each with at least 4 tiles (every block adds
     // its sums to dW once)
-    int chunks = sm_count() / c.sets;
+    int chunks = sm_count() / c.groups;
     if (chunks > tiles / 4) chunks = tiles / 4;
     if (chunks < 1) chunks = 1;
-    const size_t smem = 1024 + WG_ONES + (size_t)c.stages * c.stage_bytes;
+    const size_t smem = 1024 + WG_ONES + (size_t)WG_STAGES * WG_STAGE;
     cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_wgrad_tc<<<c.sets * chunks, 128, smem, s>>>(tz, tx, c);
+    k_wgrad_tc<<<c.groups * chunks, 128, smem, s>>>(tz, tx, c);
     return 0;
 }
 
