@@ -261,8 +261,7 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
     if (!(passes & MB3D_CU_POST_SHADOW) || p.n_lights == 0) passes &= ~MB3D_CU_POST_SHADOW;
     if (!(passes & MB3D_CU_POST_DEAO) || p.ao_quality < 0 || p.ao_rays == 0) passes &= ~MB3D_CU_POST_DEAO;
     size_t npix = (size_t)rows * p.width;
-    // (the surface list, then the list of the pixels whose start points need double precision)
-    if (int r = grow((void **)&c->d_slist, &c->slist_cap, 2 * npix * sizeof(uint32_t))) return r;
+    if (int r = grow((void **)&c->d_slist, &c->slist_cap, npix * sizeof(uint32_t))) return r;
     if (int r = grow((void **)&c->d_ps, &c->ps_cap, npix * sizeof(PostStart))) return r;
     if (passes & MB3D_CU_POST_DEAO)
         if (int r = grow((void **)&c->d_minra, &c->minra_cap, npix * (size_t)p.ao_rays * sizeof(float))) return r;
@@ -272,8 +271,8 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
     launch_surface(p, (int)npix, passes, dg, c->d_slist, cnt, c->sms * 4, s);
     c->stats.launches += 1;
     if (passes) {
-        launch_post_start(p, mixed, row0, passes, dg, c->d_slist, cnt, c->d_ps, c->d_slist + npix, c->sms * p.blocks_per_sm, s);
-        c->stats.launches += mixed ? 2 : 1;
+        launch_post_start(p, mixed, row0, passes, dg, c->d_slist, cnt, cnt + 3, c->d_ps, c->sms * p.blocks_per_sm, s);
+        c->stats.launches += 1;
         if (int r = check_launch("k_post_start")) return r;
     }
     if (passes & MB3D_CU_POST_SHADOW) {
@@ -534,7 +533,7 @@ static int enqueue_frame(mb3d_cu_ctx *c, mb3d_cu_ctx::Scratch &sc, const DevPara
     if (passes) {
         unsigned int *cnt = sc.counters + 8;
         launch_surface(p, (int)npix, passes, dg, sc.slist, cnt, c->sms * 4, s);
-        launch_post_start(p, mixed, 0, passes, dg, sc.slist, cnt, sc.ps, sc.slist + npix, c->sms * p.blocks_per_sm, s);
+        launch_post_start(p, mixed, 0, passes, dg, sc.slist, cnt, cnt + 3, sc.ps, c->sms * p.blocks_per_sm, s);
         if (passes & MB3D_CU_POST_SHADOW) launch_shadow_rays(p, mixed, 0, sc.ps, cnt, dg, cnt + 1, c->sms * p.blocks_per_sm, s);
         if (passes & MB3D_CU_POST_DEAO) {
             launch_ao_prep(p, sc.ps, dg, cnt, c->sms * 8, s);
@@ -567,7 +566,7 @@ static int ensure_frame_resources(mb3d_cu_ctx *c, int streams, size_t npix, size
             sc = mb3d_cu_ctx::Scratch();
             CU_TRY(cudaMalloc(&sc.hand, npix * sizeof(Hand)));
             CU_TRY(cudaMalloc(&sc.slow, npix * sizeof(Hand)));
-            CU_TRY(cudaMalloc(&sc.slist, 2 * npix * sizeof(uint32_t)));
+            CU_TRY(cudaMalloc(&sc.slist, npix * sizeof(uint32_t)));
             CU_TRY(cudaMalloc(&sc.ps, npix * sizeof(PostStart)));
             CU_TRY(cudaMalloc(&sc.minra, (nray > 0 ? nray : 1) * sizeof(float)));
             CU_TRY(cudaMalloc(&sc.counters, 64 * sizeof(unsigned int)));
@@ -620,8 +619,7 @@ static int render_frames_locked(mb3d_cu_ctx *c, const mb3d_cu_scene *frames, uin
         bool mixed = precision != MB3D_CU_FP64 && !P[f].all_fp64;
         int i = (int)(f % (uint32_t)streams);
         rc = enqueue_frame(c, c->fscratch[i], P[f], mixed, passes, dg + (size_t)f * npix, c->fstreams[i]);
-        c->stats.launches += 2 + (passes ? (mixed ? 3 : 2) : 0) + ((passes & MB3D_CU_POST_SHADOW) ? 1 : 0) +
-                             ((passes & MB3D_CU_POST_DEAO) ? 3 : 0);
+        c->stats.launches += 2 + (passes ? 2 : 0) + ((passes & MB3D_CU_POST_SHADOW) ? 1 : 0) + ((passes & MB3D_CU_POST_DEAO) ? 3 : 0);
     }
     for (int i = 0; i < streams && !rc; i++) {
         if (cudaEventRecord(c->fevents[i], c->fstreams[i]) != cudaSuccess || cudaStreamWaitEvent(s0, c->fevents[i], 0) != cudaSuccess)

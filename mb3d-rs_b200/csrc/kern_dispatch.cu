@@ -32,12 +32,9 @@ void launch_finish(const DevParams &p, bool mixed, int row0, const Hand *list, u
     table(p.fmask).finish(p, mixed, row0, list, counters, slow, out, blocks, s);
 }
 void launch_post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
-                       const uint32_t *list, unsigned int *count, PostStart *ps, uint32_t *defer, int blocks,
+                       const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps, int blocks,
                        cudaStream_t s) {
-    const LaunchTable &t = table(p.fmask);
-    t.post_start(p, mixed, row0, passes, gbuf, list, count, count + 3, ps, nullptr, mixed ? defer : nullptr, count + 4,
-                 blocks, s);
-    if (mixed) t.post_start(p, false, row0, passes, gbuf, list, count + 4, count + 5, ps, defer, nullptr, nullptr, blocks, s);
+    table(p.fmask).post_start(p, mixed, row0, passes, gbuf, list, count, queue, ps, blocks, s);
 }
 void launch_shadow_rays(const DevParams &p, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
                         mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s) {

@@ -59,7 +59,7 @@ struct LaunchTable {
                    mb3d_cu_silight *out, int blocks, cudaStream_t s);
     void (*post_start)(const DevParams &, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
                        const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps,
-                       const uint32_t *remap, uint32_t *defer, unsigned int *defer_count, int blocks, cudaStream_t s);
+                       int blocks, cudaStream_t s);
     void (*shadow_rays)(const DevParams &, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
                         mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s);
     void (*ao_rays)(const DevParams &, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,
@@ -77,12 +77,8 @@ void launch_finish(const DevParams &p, bool mixed, int row0, const Hand *list, u
                    mb3d_cu_silight *out, int blocks, cudaStream_t s);
 void launch_surface(const DevParams &p, int npix, int passes, mb3d_cu_silight *gbuf, uint32_t *list,
                     unsigned int *count, int blocks, cudaStream_t s);
-// the start points of the post passes; in the mixed mode the pixels that
-// need double precision are listed in defer (npix entries) and taken by a
-// second, double precision launch: count[4] is that list's length, count[5]
-// its queue
 void launch_post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
-                       const uint32_t *list, unsigned int *count, PostStart *ps, uint32_t *defer, int blocks,
+                       const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps, int blocks,
                        cudaStream_t s);
 void launch_shadow_rays(const DevParams &p, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
                         mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s);

@@ -701,20 +701,11 @@ __global__ void k_surface(const __grid_constant__ DevParams p, int npix, int pas
 #define Q_BSI1 4  // RMdoBinSearchIt: the DE at the stepped position
 #define Q_BSI2 5  // ... and 0.001 behind it
 
-// In the mixed mode a pixel whose single precision DE cannot decide is not
-// started over in place: it is listed in `defer`, and a second launch in
-// double precision (remap = that list) takes those pixels with warps of
-// their own.  There the shadow start and the DE AO start of a pixel are two
-// work items on two lanes (they are independent searches from the same
-// stored depth): the few pixels of that launch are sequences of double
-// precision DEs, and its length is the longest sequence.
 template <int FM, bool MIXED>
 __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __grid_constant__ DevParams p, int row0, int passes,
                                                     const mb3d_cu_silight *gbuf, const uint32_t *list,
-                                                    const unsigned int *count, unsigned int *queue, PostStart *ps,
-                                                    const uint32_t *remap, uint32_t *defer, unsigned int *defer_count) {
-    const bool split = remap != nullptr;
-    const uint32_t n_items = split ? 2u * count[0] : count[0];
+                                                    const unsigned int *count, unsigned int *queue, PostStart *ps) {
+    const uint32_t n_items = count[0];
     const bool do_sh = (passes & MB3D_CU_POST_SHADOW) && p.n_lights > 0;
     const bool do_ao = (passes & MB3D_CU_POST_DEAO) && p.ao_rays > 0;
     const float bsi_yp = (float)p.max_it - 0.99f, bsi_top = (float)(p.max_it + 1) - 0.1f;
@@ -730,8 +721,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
         uint32_t item = warp_take(phase == Q_IDLE, queue, n_items, p.refill_min, open);
         bool begin = false;
         if (item != UINT32_MAX) {
-            idx = split ? remap[item >> 1] : item;
-            uint32_t pix = list[idx];
+            idx = item;
+            uint32_t pix = list[item];
             int x = (int)(pix % (uint32_t)p.width), y = row0 + (int)(pix / (uint32_t)p.width);
             G si;
             si.load(gbuf[pix]);
@@ -750,9 +741,9 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
             ps[idx].pix = pix;
             ps[idx].flags = flags;
             ps[idx].pad = 0;
-            ao = split ? (item & 1u) != 0 : !do_sh;
+            ao = !do_sh;
             p64 = !MIXED;
-            begin = split ? (ao ? do_ao : do_sh) : (do_sh || do_ao);
+            begin = do_sh || do_ao;
         }
         // ---- a task starts (or starts over in double precision) at the stored depth
 #define POST_BEGIN()                                   \
@@ -770,18 +761,6 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
             continue;
         }
         // ---- one DE for the lanes whose phase asks for one
-        bool deferred = false;
-        // (the pixel goes to the double precision launch)
-#define POST_DEFER()            \
-    do {                        \
-        if (MIXED && defer) {   \
-            deferred = true;    \
-            phase = Q_IDLE;     \
-        } else {                \
-            p64 = true;         \
-            POST_BEGIN();       \
-        }                       \
-    } while (0)
         DEr r;
         r.de = 0.0;
         r.it = 0;
@@ -804,7 +783,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                 if (!ao) {
                     const bool limited = r.it < p.max_it || r.de < (double)ms;
                     if (!p64 && (r.need64 || !limited)) {
-                        POST_DEFER();
+                        p64 = true;
+                        POST_BEGIN();
                     } else if (limited) {
                         dcur = r.de;
                         itmp = 8;
@@ -817,7 +797,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                     dcur = fmin(r.de, (double)ms * 2.0);
                     const bool limited = r.it < p.max_it || dcur < (double)ms;
                     if (!p64 && (r.need64 || !limited)) {
-                        POST_DEFER();
+                        p64 = true;
+                        POST_BEGIN();
                     } else if (limited) {
                         itmp = 5;
                         dt1 = digit;
@@ -836,7 +817,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                 }
             } else if (phase == Q_BIS || phase == Q_LIM) {
                 if (MIXED && !p64 && r.need64) {
-                    POST_DEFER();
+                    p64 = true;
+                    POST_BEGIN();
                 } else {
                     dcur = r.de;
                     if (phase == Q_BIS) {
@@ -917,7 +899,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                     add_w(c, vf, -0.1);
                     ps[idx].sh_c[0] = c[0]; ps[idx].sh_c[1] = c[1]; ps[idx].sh_c[2] = c[2];
                     ps[idx].sh_mzz = mzz;
-                    if (do_ao && !split) {
+                    if (do_ao) {
                         ao = true;
                         p64 = !MIXED;
                         POST_BEGIN();
@@ -931,8 +913,6 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                 }
             }
         }
-        if (MIXED && defer) warp_append(deferred, defer_count, idx, defer);
-#undef POST_DEFER
 #undef POST_BEGIN
     }
 }
@@ -1265,14 +1245,9 @@ struct Launch {
     }
     static void post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
                            const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps,
-                           const uint32_t *remap, uint32_t *defer, unsigned int *defer_count, int blocks,
-                           cudaStream_t s) {
-        if (mixed)
-            k_post_start<FM, true><<<blocks, 256, 0, s>>>(p, row0, passes, gbuf, list, count, queue, ps, remap, defer,
-                                                          defer_count);
-        else
-            k_post_start<FM, false><<<blocks, 256, 0, s>>>(p, row0, passes, gbuf, list, count, queue, ps, remap, nullptr,
-                                                           nullptr);
+                           int blocks, cudaStream_t s) {
+        if (mixed) k_post_start<FM, true><<<blocks, 256, 0, s>>>(p, row0, passes, gbuf, list, count, queue, ps);
+        else k_post_start<FM, false><<<blocks, 256, 0, s>>>(p, row0, passes, gbuf, list, count, queue, ps);
     }
     static void shadow_rays(const DevParams &p, bool mixed, int row0, const PostStart *ps, const unsigned int *count,
                             mb3d_cu_silight *gbuf, unsigned int *queue, int blocks, cudaStream_t s) {
