@@ -717,6 +717,12 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
     float ms = 0.f, b_last_si = 0.f, b_last_dif = 0.f;
     int itmp = 0;
     bool ao = false, p64 = !MIXED, b_first = false;
+    // (snap: the shadow task's iteration count search is the one the DE AO
+    // task would run -- both from the same DE at the same stored depth, in
+    // the same precision -- and the DE AO search is its first six rounds:
+    // the shadow search leaves the DE AO start at its sixth round and the
+    // DE AO task is not run again)
+    bool snap = !MIXED, ao_done = false;
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
         uint32_t item = warp_take(phase == Q_IDLE, queue, n_items, p.refill_min, open);
         bool begin = false;
@@ -743,6 +749,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
             ps[idx].pad = 0;
             ao = !do_sh;
             p64 = !MIXED;
+            snap = !MIXED;
+            ao_done = false;
             begin = do_sh || do_ao;
         }
         // ---- a task starts (or starts over in double precision) at the stored depth
@@ -784,6 +792,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                     const bool limited = r.it < p.max_it || r.de < (double)ms;
                     if (!p64 && (r.need64 || !limited)) {
                         p64 = true;
+                        snap = true;
                         POST_BEGIN();
                     } else if (limited) {
                         dcur = r.de;
@@ -818,6 +827,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
             } else if (phase == Q_BIS || phase == Q_LIM) {
                 if (MIXED && !p64 && r.need64) {
                     p64 = true;
+                    snap = false;
                     POST_BEGIN();
                 } else {
                     dcur = r.de;
@@ -882,6 +892,13 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                 }
             } else if (go == 3) {
                 b_first = false;
+                if (!ao && snap && do_ao && itmp == 8 - 5) {
+                    // (the sixth round of the shadow search, before its step:
+                    // where the DE AO search, 5 steps, ends)
+                    ps[idx].ao_c[0] = c[0]; ps[idx].ao_c[1] = c[1]; ps[idx].ao_c[2] = c[2];
+                    ps[idx].ao_ms = (float)((double)p.de_stop * (1.0 + fabs(mzz) * (double)p.de_stop_factor));
+                    ao_done = true;
+                }
                 if (--itmp < 0) {
                     // surface_point's DE stop after the iteration count search
                     if (ao) ms = (float)((double)p.de_stop * (1.0 + fabs(mzz) * (double)p.de_stop_factor));
@@ -899,7 +916,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                     add_w(c, vf, -0.1);
                     ps[idx].sh_c[0] = c[0]; ps[idx].sh_c[1] = c[1]; ps[idx].sh_c[2] = c[2];
                     ps[idx].sh_mzz = mzz;
-                    if (do_ao) {
+                    if (do_ao && !ao_done) {
                         ao = true;
                         p64 = !MIXED;
                         POST_BEGIN();
