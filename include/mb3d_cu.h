@@ -211,8 +211,8 @@ typedef struct mb3d_cu_mc_out {
 typedef struct mb3d_cu_stats {
     float ms_march;       /* primary march (+ finish) kernels, CUDA events */
     float ms_finish;      /* the FP64 finish kernel alone */
-    float ms_shadow;
-    float ms_deao;
+    float ms_shadow;      /* the post passes' surface list, start points and shadow rays */
+    float ms_deao;        /* the DE AO kernels (with both passes they run beside the shadow rays) */
     float ms_total;       /* first launch to last, device time */
     uint32_t launches;    /* this library's kernel launches in the call */
     uint32_t fp64_pixels; /* mixed mode: the pixels marched in double precision from the start plane or finished

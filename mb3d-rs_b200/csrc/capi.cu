@@ -47,7 +47,10 @@ struct mb3d_cu_ctx {
     bool read_slow = false;
     double *d_probe = nullptr;
     size_t probe_cap = 0;
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[9] = {};
+    // the post passes: the shadow rays run on `aux` beside the DE AO rays
+    cudaStream_t aux = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     // the frame batches: extra streams, their scratch sets, the output staging
     struct Scratch {
         Hand *hand = nullptr, *slow = nullptr;
@@ -145,6 +148,12 @@ int mb3d_cu_init(int device, mb3d_cu_ctx **out) {
     }
     c->stream = c->own;
     for (auto &ev : c->ev) cudaEventCreate(&ev);
+    if (cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) != cudaSuccess) {
+        mb3d_cu_free(c);
+        return fail(MB3D_CU_EIO, "stream create failed");
+    }
     if (cudaMalloc(&c->d_counters, 64 * sizeof(unsigned int)) != cudaSuccess ||
         cudaMallocHost(&c->h_counters, 16 * sizeof(unsigned int)) != cudaSuccess) {
         mb3d_cu_free(c);
@@ -159,6 +168,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaSetDevice(c->device);
     if (c->own) cudaStreamSynchronize(c->own);
     if (c->stream && c->stream != c->own) cudaStreamSynchronize(c->stream);
+    if (c->aux) cudaStreamSynchronize(c->aux);
     cudaFree(c->d_gbuf);
     cudaFree(c->d_hand);
     cudaFree(c->d_slow);
@@ -175,6 +185,8 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_paint);
     for (auto &ev : c->ev)
         if (ev) cudaEventDestroy(ev);
+    if (c->fork) cudaEventDestroy(c->fork);
+    if (c->join) cudaEventDestroy(c->join);
     for (auto &s : c->fscratch) {
         cudaFree(s.hand);
         cudaFree(s.slow);
@@ -187,6 +199,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     for (auto e : c->fevents) cudaEventDestroy(e);
     cudaFree(c->d_frames);
     if (c->own) cudaStreamDestroy(c->own);
+    if (c->aux) cudaStreamDestroy(c->aux);
     delete c;
 }
 
@@ -275,15 +288,31 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
         c->stats.launches += 1;
         if (int r = check_launch("k_post_start")) return r;
     }
+    // with both passes the shadow rays run on the second stream beside the DE
+    // AO rays (they share only the start points, read-only; the shadow bits
+    // are atomic updates of a word the DE AO rays do not use), and the DE AO
+    // pass's last kernel, which writes that word, waits for them
+    const bool both = (passes & MB3D_CU_POST_SHADOW) && (passes & MB3D_CU_POST_DEAO);
     if (passes & MB3D_CU_POST_SHADOW) {
-        launch_shadow_rays(p, mixed, row0, c->d_ps, cnt, dg, cnt + 1, c->sms * p.blocks_per_sm, s);
+        cudaStream_t ss = s;
+        if (both) {
+            CU_TRY(cudaEventRecord(c->fork, s));
+            CU_TRY(cudaStreamWaitEvent(c->aux, c->fork, 0));
+            ss = c->aux;
+        }
+        launch_shadow_rays(p, mixed, row0, c->d_ps, cnt, dg, cnt + 1, c->sms * p.blocks_per_sm, ss);
         c->stats.launches += 1;
         if (int r = check_launch("k_shadow_rays")) return r;
+        CU_TRY(cudaEventRecord(c->ev[8], ss));
+        if (both) CU_TRY(cudaEventRecord(c->join, ss));
+    } else {
+        CU_TRY(cudaEventRecord(c->ev[8], s));
     }
     CU_TRY(cudaEventRecord(c->ev[4], s));
     if (passes & MB3D_CU_POST_DEAO) {
         launch_ao_prep(p, c->d_ps, dg, cnt, c->sms * 8, s);
         launch_ao_rays(p, mixed, c->d_ps, dg, cnt, c->d_minra, cnt + 2, c->sms * p.blocks_per_sm, s);
+        if (both) CU_TRY(cudaStreamWaitEvent(s, c->join, 0));
         launch_ao_final(p, c->d_ps, cnt, c->d_minra, dg, c->sms * 8, s);
         c->stats.launches += 3;
         if (int r = check_launch("k_ao")) return r;
@@ -315,7 +344,7 @@ static int finish_call(mb3d_cu_ctx *c, bool marched, bool posted) {
         c->stats.ms_finish = ms;
     }
     if (posted) {
-        cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]);
+        cudaEventElapsedTime(&ms, c->ev[3], c->ev[8]);
         c->stats.ms_shadow = ms;
         cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
         c->stats.ms_deao = ms;
