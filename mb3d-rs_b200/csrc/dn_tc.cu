@@ -352,21 +352,25 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
 // (2048 bytes), read in the MN-major layout without swizzle: core matrices
 // of 8 pixels x 8 channels, 128 bytes apart along K and one box apart along
 // M or N.  A = dz transposed: one box per 8 output channels.  B = the
-// tile's input seen from each tap: for tap (dy, dx) and channel half h the
-// TMA brings the 8 x 16 box of the input shifted by (dx - 1, dy - 1), its
-// zero fill the picture's border, as box 2 tap + h -- so that one MMA of
-// N = 144 takes all nine taps and A is read once per K step.  A block takes
+// tile's input seen from each tap: the TMA brings the tile's input box with
+// its one-pixel halo (10 x 18 pixels, zero fill at the picture's border, two
+// channel halves), and two warps copy out of it, for tap (dy, dx) and half
+// h, the 8 x 16 box shifted by (dx - 1, dy - 1) as box 2 tap + h -- so that
+// one MMA of N = 144 takes all nine taps and A is read once per K step,
+// while the input crosses L2 once per tile.  A block takes
 // one channel group and every (grid / groups)-th tile and accumulates in
 // TMEM over all of its tiles; the blocks of group 0 also form the bias
 // gradient db[co] = sum over p of dz[p][co], as one more MMA per K step with
 // a B operand of ones into 16 more columns.  At the end the four warps read
 // the accumulators (warp w: co 32 w .. 32 w + 31) and add them to dW and db
 // with FP32 atomics.  Roles: lane 0 of warp 0 issues the TMA loads, lane 0 of
-// warp 1 the MMAs; every wait is bounded as in the forward kernel.
+// warp 1 the MMAs, warps 2 and 3 make the shifted boxes; every wait is
+// bounded as in the forward kernel.
 constexpr uint32_t WG_BOX = TILE_W * TILE_H * 16;    // one box of a tile (2048 bytes)
 constexpr uint32_t WG_A_BYTES = 16 * WG_BOX;          // M = 128: 16 boxes of 8 output channels
+constexpr uint32_t WG_HALO = 2 * HALF_BYTES;          // the input box with its halo, two channel halves
 constexpr uint32_t WG_B_BYTES = 18 * WG_BOX;          // nine taps x two channel halves
-constexpr uint32_t WG_STAGE = WG_A_BYTES + WG_B_BYTES;
+constexpr uint32_t WG_STAGE = WG_A_BYTES + WG_HALO + WG_B_BYTES;
 constexpr int WG_STAGES = 3;
 constexpr uint32_t WG_COLS = 256;                     // 144 columns of (tap, ci), 16 of the bias
 constexpr uint32_t WG_ONES = 1024;                    // the ones operand (512 bytes) before the stages
@@ -381,7 +385,7 @@ struct WgTc {
 __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUtensorMap tz,
                                                      const __grid_constant__ CUtensorMap tx, const WgTc a) {
     extern __shared__ __align__(1024) uint8_t dyn[];
-    __shared__ __align__(8) uint64_t full[WG_STAGES], empty[WG_STAGES], done;
+    __shared__ __align__(8) uint64_t full[WG_STAGES], copied[WG_STAGES], empty[WG_STAGES], done;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
     uint8_t *base = dyn + ((1024u - (smem_addr(dyn) & 1023u)) & 1023u);
@@ -404,6 +408,7 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
     if (tid == 0) {
         for (int st = 0; st < WG_STAGES; st++) {
             mbar_init(smem_addr(&full[st]), 1);
+            mbar_init(smem_addr(&copied[st]), 2);
             mbar_init(smem_addr(&empty[st]), 1);
         }
         mbar_init(smem_addr(&done), 1);
@@ -434,15 +439,38 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
             }
             const int tx_ = g % a.tiles_x, rest = g / a.tiles_x;
             const int x0 = tx_ * TILE_W, y0 = (rest % a.tiles_y) * TILE_H, img = rest / a.tiles_y;
-            const uint32_t bar = smem_addr(&full[st]), sa = st0 + st * WG_STAGE, sb = sa + WG_A_BYTES;
-            mbar_expect_tx(bar, (uint32_t)(cog + 18) * WG_BOX);
+            const uint32_t bar = smem_addr(&full[st]), sa = st0 + st * WG_STAGE, sh = sa + WG_A_BYTES;
+            mbar_expect_tx(bar, (uint32_t)cog * WG_BOX + 2 * BOX_BYTES);
             for (int j = 0; j < cog; j++) tma_load_4d(sa + (uint32_t)j * WG_BOX, &tz, a.dz_off + 8 * j, x0, y0, img, bar);
             const int c = a.x_off + 16 * grp;
-            for (int tap = 0; tap < 9; tap++) {
-                const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-                tma_load_4d(sb + (uint32_t)(2 * tap) * WG_BOX, &tx, c, x0 + dx, y0 + dy, img, bar);
-                tma_load_4d(sb + (uint32_t)(2 * tap + 1) * WG_BOX, &tx, c + 8, x0 + dx, y0 + dy, img, bar);
+            tma_load_4d(sh, &tx, c, x0 - 1, y0 - 1, img, bar);
+            tma_load_4d(sh + HALF_BYTES, &tx, c + 8, x0 - 1, y0 - 1, img, bar);
+        }
+    } else if (warp >= 2) {
+        // warps 2 and 3: each tap's shifted 8 x 16 box, two channel halves,
+        // copied out of the halo box (16 bytes a pixel) for the B operand
+        const int t = tid - 64;
+        uint32_t q = 0;
+        for (int g = first; g < total && !abort_flag; g += step, q++) {
+            const uint32_t st = q % (uint32_t)WG_STAGES;
+            bool ready = mbar_wait(smem_addr(&full[st]), (q / WG_STAGES) & 1, &abort_flag);
+            ready = __all_sync(0xffffffffu, ready);
+            if (!ready) {
+                abort_flag = 1;
+                break;
             }
+            const uint8_t *halo = base + WG_ONES + (size_t)st * WG_STAGE + WG_A_BYTES;
+            uint8_t *bbox = base + WG_ONES + (size_t)st * WG_STAGE + WG_A_BYTES + WG_HALO;
+            for (int i = t; i < 18 * 128; i += 64) {
+                const int box = i >> 7, within = i & 127, r = within >> 3, x = within & 7;
+                const int tap = box >> 1, h = box & 1, dy = tap / 3, dx = tap % 3;
+                *reinterpret_cast<uint4 *>(bbox + (size_t)box * WG_BOX + (size_t)within * 16) =
+                    *reinterpret_cast<const uint4 *>(halo + (size_t)h * HALF_BYTES + (size_t)((r + dy) * HALO_W + x + dx) * 16);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&copied[st])) : "memory");
         }
     } else if (warp == 1 && lane == 0) {
         // the MMA issuer: per tile eight K steps of one N = 144 MMA (and the
@@ -456,13 +484,13 @@ __global__ void __launch_bounds__(128, 1) k_wgrad_tc(const __grid_constant__ CUt
         uint32_t q = 0;
         for (int g = first; g < total && !abort_flag; g += step, q++) {
             const uint32_t st = q % (uint32_t)WG_STAGES;
-            if (!mbar_wait(smem_addr(&full[st]), (q / WG_STAGES) & 1, &abort_flag)) {
+            if (!mbar_wait(smem_addr(&copied[st]), (q / WG_STAGES) & 1, &abort_flag)) {
                 abort_flag = 1;
                 break;
             }
             tc_fence_after();
             const uint32_t sa = st0 + st * WG_STAGE;
-            const uint64_t ad0 = desc_plain(sa, 128u, WG_BOX), bd0 = desc_plain(sa + WG_A_BYTES, 128u, WG_BOX);
+            const uint64_t ad0 = desc_plain(sa, 128u, WG_BOX), bd0 = desc_plain(sa + WG_A_BYTES + WG_HALO, 128u, WG_BOX);
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 const uint32_t acc = (q | (uint32_t)k) ? 1u : 0u;
@@ -670,10 +698,11 @@ int dn_wgrad_tc(const WgradArgs &a, float *db, cudaStream_t s) {
     cuuint64_t dx[4] = {(cuuint64_t)a.x_c, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
     cuuint64_t sx[3] = {(cuuint64_t)a.x_c * 2, (cuuint64_t)a.x_c * 2 * a.w, (cuuint64_t)a.x_c * 2 * a.w * a.h};
     cuuint32_t box[4] = {8, (cuuint32_t)TILE_W, (cuuint32_t)TILE_H, 1};
+    cuuint32_t hbox[4] = {8, (cuuint32_t)HALO_W, (cuuint32_t)HALO_H, 1};
     cuuint32_t e1[4] = {1, 1, 1, 1};
     if (enc(&tz, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.dz, dz, sz, box, e1, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS ||
-        enc(&tx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.x, dx, sx, box, e1, CU_TENSOR_MAP_INTERLEAVE_NONE,
+        enc(&tx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.x, dx, sx, hbox, e1, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return -1;
     const int tiles = a.n * c.tiles_y * c.tiles_x;
