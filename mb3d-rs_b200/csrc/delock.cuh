@@ -257,6 +257,80 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
         R rold0 = 0, rold3 = 0, otrap3 = rout[3];
         int n = 0, btmp = p.slots[0].iterations, it = 0;
         unsigned int unc = 0;
+        // single precision with Integer Power 8 and the Amazing Box only: the
+        // orbits in two packed pairs (formulas.cuh), the same loop
+        constexpr bool PACKED = sizeof(R) == 4 && !FULL && (FM == FKIND_IP8 || FM == (FKIND_IP8 | FKIND_BOX));
+        if constexpr (PACKED) {
+            float2 V[2][3], J[2][3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                V[0][k] = make_float2((float)v[0][k], (float)v[1][k]);
+                V[1][k] = make_float2((float)v[2][k], (float)v[3][k]);
+                J[0][k] = make_float2((float)j[0][k], (float)j[1][k]);
+                J[1][k] = make_float2((float)j[2][k], (float)j[3][k]);
+            }
+            for (;;) {
+                int guard = 0;
+                while (btmp <= 0) {
+                    n += 1;
+                    if (n > p.end_to) n = p.repeat_from;
+                    btmp = p.slots[n].iterations;
+                    if (++guard > 64) goto done_x2;
+                }
+                {
+                    const DevSlot &s = p.slots[n];
+                    if (FM == FKIND_IP8 || s.kind == FKIND_IP8) {
+                        const float zmul = s.of[1];
+                        f_int_pow8_x2(zmul, V[0], J[0]);
+                        f_int_pow8_x2(zmul, V[1], J[1]);
+                    } else if (s.kind == FKIND_BOX) {
+                        const float scale = s.of[0], min_r = s.of[1], fold = s.of[2];
+                        f_amazing_box_x2(scale, min_r, fold, V[0], J[0]);
+                        f_amazing_box_x2(scale, min_r, fold, V[1], J[1]);
+                    }
+                    if (s.julia_add) {
+#pragma unroll
+                        for (int k = 0; k < 3; k++) {
+                            V[0][k] = padd(V[0][k], J[0][k]);
+                            V[1][k] = padd(V[1][k], J[1][k]);
+                        }
+                    }
+                    if (COUNT) cnt->its[n] += 4;
+                    btmp -= 1;
+                    if (s.uncounted) {
+                        if (++unc > 100000u) goto done_x2;
+                        continue;
+                    }
+                }
+                it += 1;
+                const float2 r01 = psq3(V[0]), r23 = psq3(V[1]);
+                rout[0] = r01.x;
+                const float rn[4] = {0.0f, r01.y, r23.x, r23.y};
+#pragma unroll
+                for (int q = 1; q < 4; q++) {
+                    const bool stop = live[q] && rn[q] > (float)rstop3d;
+                    rout[q] = live[q] ? rn[q] : rout[q];
+                    if (stop) {
+                        const int pq = q >> 1;
+                        float vf[4];
+#pragma unroll
+                        for (int k = 0; k < 3; k++) vf[k] = (q & 1) ? V[pq][k].y : V[pq][k].x;
+                        vf[3] = 0.f;
+                        lr_frozen[q] = log_len2_f(vf);
+                    }
+                    live[q] = live[q] && !stop;
+                }
+                if (it >= max_it || rout[0] > rstop) break;
+            }
+        done_x2:
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                v[0][k] = V[0][k].x;
+                v[1][k] = V[0][k].y;
+                v[2][k] = V[1][k].x;
+                v[3][k] = V[1][k].y;
+            }
+        } else
         for (;;) {
             if (FULL) {
                 rold0 = rout[0];

@@ -286,4 +286,70 @@ __device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], const 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Pairs of single precision orbits in the packed FP32 instructions of sm_100
+// (FFMA2 / FMUL2 / FADD2: two lanes of arithmetic per instruction).  The
+// numeric DE iterates its four orbits in lock-step, so orbits (0, 1) and
+// (2, 3) go through the formulas as two float2; the multiply-adds are
+// packed, the reciprocals, square roots, absolute values and choices stay
+// per orbit.  Each lane is an IEEE single precision operation, as in the
+// scalar single precision formulas above (whose contraction the compiler
+// chooses).
+__device__ __forceinline__ float2 p2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b (b times -1 is exact: one rounding, as a scalar subtraction)
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a); }
+__device__ __forceinline__ float2 pabs(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+__device__ __forceinline__ float2 psq3(const float2 v[3]) { return pfma(v[0], v[0], pfma(v[1], v[1], pmul(v[2], v[2]))); }
+
+// the integer power 8 of f_int_pow (HybridIntP8) on a pair of orbits
+__device__ __forceinline__ void f_int_pow8_x2(float zmul, float2 v[3], const float2 j[3]) {
+    const float2 x = v[0], y = v[1], z = v[2];
+    const float2 xx = pmul(x, x), yy = pmul(y, y), zz = pmul(z, z);
+    const float2 r = padd(xx, yy);
+    const float2 rr = pmul(r, r);
+    const float2 zzzz = pmul(zz, zz);
+    float2 sr;  // sqrt(r): r * rsqrt(r), 0 where r is not positive
+    sr.x = r.x > 0.0f ? rsqrtf(r.x) : 0.0f;
+    sr.y = r.y > 0.0f ? rsqrtf(r.y) : 0.0f;
+    sr = pmul(r, sr);
+    // t = (zzzz - 6 r zz + rr) (zz - r) sqrt(r)
+    const float2 t = pmul(pmul(padd(pfma(pmul(p2(-6.0f), r), zz, zzzz), rr), psub(zz, r)), sr);
+    v[2] = pfma(pmul(pmul(t, z), p2(-8.0f)), p2(zmul), j[2]);
+    // a = ((rr 70 + zzzz) zzzz - 28 zz r (zzzz + rr)) / (rr rr + eps) + 1
+    const float2 num = pfma(pmul(pmul(p2(-28.0f), zz), r), padd(zzzz, rr), pmul(pfma(rr, p2(70.0f), zzzz), zzzz));
+    const float2 den = pfma(rr, rr, p2(1.2e-38f));
+    const float2 a = pfma(num, make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y)), p2(1.0f));
+    const float2 xxxx = pmul(xx, xx), yyyy = pmul(yy, yy);
+    // v1 = (yyyy (7 xx - yy) + xxxx (xx - 7 yy)) 8 x y a + j1
+    const float2 s1 = pfma(yyyy, psub(pmul(p2(7.0f), xx), yy), pmul(xxxx, pfma(p2(-7.0f), yy, xx)));
+    v[1] = pfma(pmul(pmul(pmul(s1, p2(8.0f)), x), y), a, j[1]);
+    // v0 = a (xxxx xxxx + yyyy (70 xxxx + yyyy) - 28 xx yy (yyyy + xxxx)) + j0
+    const float2 s0 = pfma(xxxx, xxxx, pmul(yyyy, pfma(p2(70.0f), xxxx, yyyy)));
+    v[0] = pfma(a, pfma(p2(-28.0f), pmul(pmul(xx, yy), padd(yyyy, xxxx)), s0), j[0]);
+}
+
+// |x + f| - (|x - f| + x), box_fold on a pair
+__device__ __forceinline__ float2 box_fold_x2(float2 x, float2 f) {
+    return psub(pabs(padd(x, f)), padd(pabs(psub(x, f)), x));
+}
+
+// the Amazing Box (HybridCube) on a pair of orbits; the numeric DE does not
+// use the derivative w, which is left out
+__device__ __forceinline__ void f_amazing_box_x2(float scale, float min_r, float fold, float2 v[3], const float2 j[3]) {
+    const float2 F = p2(fold);
+    const float2 x = box_fold_x2(v[0], F), y = box_fold_x2(v[1], F), z = box_fold_x2(v[2], F);
+    const float2 r = pfma(x, x, pfma(y, y, pmul(z, z)));
+    const float m = fmaxf(min_r, 1.2e-38f), sqr_min_r = m * m;
+    const bool bx = r.x < sqr_min_r, by = r.y < sqr_min_r;
+    float2 mul;
+    mul.x = (!bx && 1.0f < r.x) ? scale : __fdividef(scale, bx ? sqr_min_r : r.x);
+    mul.y = (!by && 1.0f < r.y) ? scale : __fdividef(scale, by ? sqr_min_r : r.y);
+    v[2] = pfma(z, mul, j[2]);
+    v[1] = pfma(y, mul, j[1]);
+    v[0] = pfma(x, mul, j[0]);
+}
+
 }  // namespace mb3dcu
