@@ -259,7 +259,7 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
         unsigned int unc = 0;
         // single precision with Integer Power 8 and the Amazing Box only: the
         // orbits in two packed pairs (formulas.cuh), the same loop
-        constexpr bool PACKED = sizeof(R) == 4 && !FULL && (FM == FKIND_IP8 || FM == (FKIND_IP8 | FKIND_BOX));
+        constexpr bool PACKED = sizeof(R) == 4 && (FM == FKIND_IP8 || FM == (FKIND_IP8 | FKIND_BOX));
         if constexpr (PACKED) {
             float2 V[2][3], J[2][3];
 #pragma unroll
@@ -270,6 +270,10 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
                 J[1][k] = make_float2((float)j[2][k], (float)j[3][k]);
             }
             for (;;) {
+                if (FULL) {
+                    rold0 = rout[0];
+                    rold3 = live[3] ? rout[3] : rold3;
+                }
                 int guard = 0;
                 while (btmp <= 0) {
                     n += 1;
@@ -309,6 +313,7 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
 #pragma unroll
                 for (int q = 1; q < 4; q++) {
                     const bool stop = live[q] && rn[q] > (float)rstop3d;
+                    if (FULL && q == 3) otrap3 = (live[3] && rn[3] < otrap3) ? rn[3] : otrap3;
                     rout[q] = live[q] ? rn[q] : rout[q];
                     if (stop) {
                         const int pq = q >> 1;
