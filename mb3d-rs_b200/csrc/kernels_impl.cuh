@@ -786,7 +786,9 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
             // DE AO search's test, 3 the iteration count search's next step,
             // 4 the task is done
             int go = 0;
-            const int bsi_steps = ao ? 5 : 8;
+            // (RMdoBinSearchIt's steps: 8 for the shadow start, 5 for the DE AO start)
+            constexpr int BSI_SH = 8, BSI_AO = 5;
+            const int bsi_steps = ao ? BSI_AO : BSI_SH;
             if (phase == Q_D0) {
                 if (!ao) {
                     const bool limited = r.it < p.max_it || r.de < (double)ms;
@@ -892,7 +894,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
                 }
             } else if (go == 3) {
                 b_first = false;
-                if (!ao && snap && do_ao && itmp == 8 - 5) {
+                if (!ao && snap && do_ao && itmp == BSI_SH - BSI_AO) {
                     // (the sixth round of the shadow search, before its step:
                     // where the DE AO search, 5 steps, ends)
                     ps[idx].ao_c[0] = c[0]; ps[idx].ao_c[1] = c[1]; ps[idx].ao_c[2] = c[2];
