@@ -246,7 +246,7 @@ static int march_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int r
         CU_TRY(cudaMemsetAsync(c->d_count, 0, 16 * sizeof(unsigned long long), s));
     }
     int items = ((p.width + 7) / 8) * ((rows + 3) / 4);  // warps' worth of work
-    int blocks = c->sms * p.blocks_per_sm;
+    int blocks = c->sms * (mixed ? p.blocks_march32 : p.blocks_per_sm);
     int need = (items + 7) / 8;
     if (blocks > need) blocks = need > 0 ? need : 1;
     CU_TRY(cudaEventRecord(c->ev[0], s));
@@ -371,6 +371,7 @@ static void apply_tuning(DevParams &p) {
             if (k == "refill" && v >= 1 && v <= 32) p.refill_min = (int)v;
             else if (k == "refill_sh" && v >= 1 && v <= 32) p.refill_shadow = (int)v;
             else if (k == "refill_ao" && v >= 1 && v <= 32) p.refill_ao = (int)v;
+            else if (k == "blocks32" && v >= 1 && v <= 8) p.blocks_march32 = (int)v;
             else if (k == "blocks" && v >= 1 && v <= 16) p.blocks_per_sm = (int)v;
             else if (k == "margin" && v >= 1) p.hand_margin = (float)v;
             else if (k == "back" && v >= 0 && v <= 2) p.hand_back = (int)v;
@@ -533,7 +534,7 @@ int mb3d_cu_march_noalloc(const mb3d_cu_scene *sc, int precision, uint32_t row0,
     CU_TRY(cudaMemsetAsync(counters, 0, NOALLOC_COUNTER_BYTES, s));
     bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
     int items = ((p.width + 7) / 8) * (((int)rows + 3) / 4);
-    int blocks = d.sms * p.blocks_per_sm;
+    int blocks = d.sms * (mixed ? p.blocks_march32 : p.blocks_per_sm);
     int need = (items + 7) / 8;
     if (blocks > need) blocks = need > 0 ? need : 1;
     launch_march(p, mixed, (int)row0, (int)rows, gbuf, list, counters, nullptr, blocks, s);
@@ -554,7 +555,7 @@ static int enqueue_frame(mb3d_cu_ctx *c, mb3d_cu_ctx::Scratch &sc, const DevPara
     size_t npix = (size_t)rows * p.width;
     CU_TRY(cudaMemsetAsync(sc.counters, 0, 64 * sizeof(unsigned int), s));
     int items = ((p.width + 7) / 8) * ((rows + 3) / 4);
-    int blocks = c->sms * p.blocks_per_sm;
+    int blocks = c->sms * (mixed ? p.blocks_march32 : p.blocks_per_sm);
     int need = (items + 7) / 8;
     if (blocks > need) blocks = need > 0 ? need : 1;
     launch_march(p, mixed, 0, rows, dg, sc.hand, sc.counters, nullptr, blocks, s);

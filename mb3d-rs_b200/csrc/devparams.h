@@ -42,6 +42,7 @@ struct DevParams {
     int32_t hand_back;  // ... at most this many steps back
     int32_t refill_min, blocks_per_sm;  // wavefront: idle lanes that trigger a refill; resident blocks
     int32_t refill_shadow, refill_ao;   // ... of the shadow and DE AO ray kernels
+    int32_t blocks_march32, pad_b;      // resident blocks of the single precision march
     float d_rstop_f, rstop3d_f, soft_radius, hs_max_len_mul;
     double d_rstop, rstop3d, zcorr, zc_mul;
     double zend, step_width, fov_y, coord_eps;

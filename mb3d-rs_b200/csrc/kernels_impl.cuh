@@ -33,6 +33,11 @@
 #ifndef MB3D_MIN_BLOCKS_MARCH
 #define MB3D_MIN_BLOCKS_MARCH MB3D_MIN_BLOCKS
 #endif
+// (the single precision march: 4 blocks of 64 registers, its spills cost
+// less than the warps it gains)
+#ifndef MB3D_MIN_BLOCKS_MARCH32
+#define MB3D_MIN_BLOCKS_MARCH32 4
+#endif
 
 namespace mb3dcu {
 
@@ -116,7 +121,7 @@ __device__ __forceinline__ float de_stop_at(const DevParams &p, double zz) {
 #define PH_HALF 3
 
 template <typename R, int FM, bool COUNT>
-__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_MARCH) k_march(const __grid_constant__ DevParams p, int row0, int rows,
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 : MB3D_MIN_BLOCKS_MARCH) k_march(const __grid_constant__ DevParams p, int row0, int rows,
                                                mb3d_cu_silight *out, Hand *list, unsigned int *counters,
                                                unsigned long long *gcount) {
     const bool MIXED = sizeof(R) == 4;
