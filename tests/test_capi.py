@@ -58,3 +58,44 @@ def test_init_without_device_fails_loudly():
         assert False
     except mb3dcu.CardError as e:
         assert e.status in (mb3dcu.ENODEV, mb3dcu.EIO)
+
+
+def test_stats_layout():
+    # mb3d_cu_stats: 5 floats and 2 uint32 (padded to 32 bytes), de_evals,
+    # orbit_its[6], 2 uint32, the march's 4 lane counters
+    assert ctypes.sizeof(mb3dcu.Stats) == 32 + 8 + 48 + 8 + 32
+    assert mb3dcu.Stats.march_lane_its.offset == 96
+
+
+def test_null_arguments_fail_on_the_host():
+    """Every entry point answers a missing context or buffer with EINVAL and
+    a reason, before it touches a device (the reference's Err(String))."""
+    L = mb3dcu.lib()
+    sc = scenes.preset("Integer Power", 64, 48)
+    buf = np.zeros(64 * 48, dtype=mb3dcu.SILIGHT)
+    rgb = np.zeros((48, 64, 3), np.uint8)
+    col = np.zeros((48, 64, 3), np.float32)
+    calls = [
+        lambda: L.mb3d_cu_march(None, ctypes.byref(sc), mb3dcu.FP64, 0, 48, buf.ctypes.data, None),
+        lambda: L.mb3d_cu_post(None, ctypes.byref(sc), mb3dcu.FP64, mb3dcu.POST_SHADOW, 0, 48, buf.ctypes.data, None),
+        lambda: L.mb3d_cu_paint(None, ctypes.byref(sc), buf.ctypes.data, 0, 48, rgb.ctypes.data),
+        lambda: L.mb3d_cu_mc_paint(None, col.ctypes.data, None, 64 * 48, ctypes.byref(mb3dcu.mc_paint_default()),
+                                   rgb.ctypes.data),
+    ]
+    for call in calls:
+        assert call() == mb3dcu.EINVAL
+        assert L.mb3d_cu_last_error()
+
+
+def test_display_and_light_defaults_on_the_host():
+    o = mb3dcu.mc_paint_default()
+    assert (o.contrast, o.saturation, o.options, o.gamma) == (128, 32, 2, 32.0)
+    lv = mb3dcu.mc_light_default(scenes.c5_mc())
+    assert lv is not None
+    bad = scenes.preset("Integer Power", 64, 48)
+    bad.width = 0
+    try:
+        mb3dcu.mc_light_default(bad)
+        assert False, "a picture without pixels must raise"
+    except mb3dcu.CardError as e:
+        assert e.status == mb3dcu.EINVAL
