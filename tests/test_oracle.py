@@ -322,3 +322,72 @@ def test_unet_oracle_backward_matches_finite_differences():
         e[i] = 1e-6
         num = (loss(p + e) - loss(p - e)) / 2e-6
         assert abs(num - g[i]) <= 1e-4 * max(1.0, abs(num)), (i, num, g[i])
+
+
+# ---- the screen space ambient occlusion (ssao::ssao24), the reference's own
+# tests restated (src/ssao.rs:338-417)
+
+def test_ssao_rne_matches_round_ties_even():
+    vals = [0.0, -0.0, 0.5, -0.5, 1.5, 2.5, -2.5, 8388607.5, 4194304.5, -4194303.5, 1e10, -1e10, math.inf, -math.inf]
+    rng = np.random.default_rng(12345)
+    bits = rng.integers(0, 2 ** 32, 20000, dtype=np.uint64).astype(np.uint32)
+    f = bits.view(np.float32)
+    f = np.fmod(f[np.isfinite(f)], np.float32(1e8))
+    vals += [float(x) for x in f]
+    for x in vals:
+        want = np.rint(np.float32(x))
+        got = np.float32(O.ssao_rne(x))
+        assert got.tobytes() == want.tobytes(), x
+    assert math.isnan(O.ssao_rne(math.nan))
+
+
+def test_ssao_levels():
+    assert O.ssao_levels(100, 100) == 5
+    assert O.ssao_levels(6000, 6000) <= 15
+
+
+def _depth_gbuf(w, h, depth):
+    g = np.zeros(w * h, dtype=mb3dcu.SILIGHT)
+    g["zpos_fine"] = (np.asarray(depth, np.int64).reshape(-1).astype(np.uint32) << 8)
+    return g
+
+
+def test_ssao_flat_plane_has_no_occlusion_and_a_pit_has():
+    w = h = 64
+    y, x = np.mgrid[0:h, 0:w] - 32
+    pit = np.where(x * x + y * y < 36, 20000, 0)
+    g = O.ssao24(_depth_gbuf(w, h, 4_000_000 - pit), w, h, 300.0, 0.001)
+    center, far = int(g["amb_shadow"][32 * w + 32]), int(g["amb_shadow"][5 * w + 5])
+    assert center > far + 1000, (center, far)
+
+
+def test_ssao_wrapped_occlusion_turns_with_the_picture():
+    """A panorama has no left or right border: the occlusion of the picture
+    turned sideways by an even number of columns is the turned occlusion."""
+    w, h = 96, 48
+
+    def scene(shift):
+        yy, xx = np.mgrid[0:h, 0:w]
+        xs = (xx + shift) % w
+        pit = ((xs - 3) ** 2 + (yy - 24) ** 2 < 30) | ((xs - 60) ** 2 + (yy - 10) ** 2 < 20)
+        depth = np.where(pit, 20000, (xs * 37 % 11) * 300)
+        return _depth_gbuf(w, h, 4_000_000 - depth)
+
+    a = O.ssao24(scene(0), w, h, 300.0, 0.001, wrap_x=True)["amb_shadow"].reshape(h, w)
+    k = 38
+    b = O.ssao24(scene(k), w, h, 300.0, 0.001, wrap_x=True)["amb_shadow"].reshape(h, w)
+    assert np.array_equal(b, np.roll(a, -k, axis=1))
+
+
+def test_ssao_leaves_the_background_and_stays_in_range():
+    w, h = 80, 60
+    yy, xx = np.mgrid[0:h, 0:w]
+    depth = 4_000_000 - ((xx * 7919 + yy * 104729) % 5000)
+    g = _depth_gbuf(w, h, depth)
+    g["zpos_fine"][:w * 5] = np.uint32(0xFFFFFF00)  # background rows (zpos >= 32768)
+    g["amb_shadow"] = 777
+    for t0 in (False, True):
+        for mirror in (0.0, 0.3):
+            o = O.ssao24(g, w, h, 300.0, 0.001, threshold=1.5, border_mirror=mirror, t0=t0)
+            assert (o["amb_shadow"][:w * 5] == 777).all()
+            assert (o["amb_shadow"][w * 5:] <= 16383).all()
