@@ -387,6 +387,29 @@ int mb3d_cu_mc_paint(mb3d_cu_ctx *ctx, const float *colour, const uint8_t *rays,
 int mb3d_cu_paint(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_silight *gbuf, uint32_t row0,
                   uint32_t rows, uint8_t *rgb);
 
+/* The 24-bit screen space ambient occlusion (SsaoParams, src/ssao.rs:14-33),
+ * regular sampling: */
+typedef struct {
+    float threshold;     /* sAmbShadowThreshold (z/r); 2 by default */
+    float border_mirror; /* bSSAO24BorderMirrorSize * 0.01, 0..0.9 */
+    uint8_t t0;          /* the "threshold down to 0" variant (TAmbHiQCalcT0) */
+    uint8_t wrap_x;      /* a panorama: the left and right edges are neighbours */
+    uint8_t pad[2];
+} mb3d_cu_ssao_opts;
+
+/* SsaoParams::default (threshold 2, no mirrored border, no wrap). */
+void mb3d_cu_ssao_default(mb3d_cu_ssao_opts *out);
+
+/* Replaces gpu::ssao24 (src/gpu.rs:3503; ssao::ssao24, src/ssao.rs:129-335):
+ * the scene's whole G-buffer (width * height records, host or device) gets
+ * the ambient shadow (amb_shadow, 0..16383) of its object pixels from the
+ * depth buffer alone: per pixel the largest elevation angle in 32 directions
+ * on ever smoother levels of the depth buffer, their arctangents summed.
+ * The random sampling (SsaoParams::random) and the 15-bit variant are not on
+ * the card (EINVAL for an opts outside the documented ranges). */
+int mb3d_cu_ssao24(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_ssao_opts *opts,
+                   mb3d_cu_silight *gbuf);
+
 /* ---- the learned denoiser of the Monte Carlo pictures ----
  * A 5-level U-Net of 3x3 convolutions (32/48/64/80/96 channels) that
  * takes the noisy colour and the albedo, normal and depth guides of a

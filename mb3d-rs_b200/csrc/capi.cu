@@ -77,6 +77,8 @@ struct mb3d_cu_ctx {
     size_t mcs_cap = 0;
     unsigned char *d_paint = nullptr;  // the painter's staging of host buffers
     size_t paint_cap = 0;
+    unsigned char *d_ssao = nullptr;   // the SSAO's levels and angles (and a host G-buffer's staging)
+    size_t ssao_cap = 0;
     std::mutex mu;
 };
 
@@ -183,6 +185,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_mc);
     cudaFree(c->d_mcs);
     cudaFree(c->d_paint);
+    cudaFree(c->d_ssao);
     for (auto &ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     if (c->fork) cudaEventDestroy(c->fork);
@@ -836,6 +839,47 @@ int mb3d_cu_paint(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_silight
     if (!dr) CU_TRY(cudaMemcpyAsync(rgb, drgb, br, cudaMemcpyDeviceToHost, s));
     cudaError_t e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+void mb3d_cu_ssao_default(mb3d_cu_ssao_opts *o) {
+    if (!o) return;
+    o->threshold = 2.0f;
+    o->border_mirror = 0.0f;
+    o->t0 = 0;
+    o->wrap_x = 0;
+    o->pad[0] = o->pad[1] = 0;
+}
+
+int mb3d_cu_ssao24(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_ssao_opts *o, mb3d_cu_silight *gbuf) {
+    if (!c || !sc || !o || !gbuf) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (!(o->border_mirror >= 0.0f && o->border_mirror <= 0.9f) || !(o->threshold == o->threshold))
+        return fail(MB3D_CU_EINVAL, "border_mirror outside 0..0.9 or threshold not a number");
+    DevParams p;
+    std::string err;
+    int r = setup_params(*sc, p, err);
+    if (r < 0) return fail(r, err);
+    const int w = p.width, h = p.height;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    cudaStream_t s = c->stream;
+    const size_t npix = (size_t)w * h, gb = npix * sizeof(mb3d_cu_silight);
+    const bool dev = is_device_ptr(gbuf);
+    const size_t scratch = (ssao_scratch_bytes(w, h) + 255) & ~(size_t)255;
+    if (int e = grow((void **)&c->d_ssao, &c->ssao_cap, scratch + (dev ? 0 : gb))) return e;
+    mb3d_cu_silight *dg = dev ? gbuf : reinterpret_cast<mb3d_cu_silight *>(c->d_ssao + scratch);
+    if (!dev) CU_TRY(cudaMemcpyAsync(dg, gbuf, gb, cudaMemcpyHostToDevice, s));
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    ssao24_launch(dg, w, h, p.zc_mul, p.zcorr, *o, c->d_ssao, c->sms, s);
+    if (int e = check_launch("k_ssao")) return e;
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    if (!dev) CU_TRY(cudaMemcpyAsync(gbuf, dg, gb, cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
     return 0;
 }
 

@@ -115,6 +115,12 @@ void launch_mc_final(const McAcc &acc, uint32_t npix, int rays, float *radiance,
 void mc_paint_launch(const float *col, const uint8_t *rays, uint32_t n, const mb3d_cu_mc_paint_opts &mc, uint8_t *out,
                      int blocks, cudaStream_t s);
 
+// the 24-bit screen space ambient occlusion of a w x h G-buffer (ssao.cu);
+// scratch holds ssao_scratch_bytes(w, h)
+size_t ssao_scratch_bytes(int w, int h);
+void ssao24_launch(mb3d_cu_silight *gbuf, int w, int h, double zc_mul, double zcorr, const mb3d_cu_ssao_opts &o,
+                   void *scratch, int sms, cudaStream_t s);
+
 // render::paint of G-buffer records, default lighting (paint.cu)
 void paint_launch(const mb3d_cu_scene &sc, const DevParams &p, uint32_t row0, const mb3d_cu_silight *gbuf, uint32_t n,
                   uint8_t *rgb, int blocks, cudaStream_t s);

@@ -132,6 +132,19 @@ class McPaintOpts(ctypes.Structure):
                 ("pad", ctypes.c_uint8), ("gamma", ctypes.c_float)]
 
 
+class SsaoOpts(ctypes.Structure):
+    """mb3d_cu_ssao_opts: SsaoParams (src/ssao.rs:14-33) with regular sampling."""
+    _fields_ = [("threshold", ctypes.c_float), ("border_mirror", ctypes.c_float), ("t0", ctypes.c_uint8),
+                ("wrap_x", ctypes.c_uint8), ("pad", ctypes.c_uint8 * 2)]
+
+
+def ssao_default():
+    """SsaoParams::default."""
+    o = SsaoOpts()
+    lib().mb3d_cu_ssao_default(ctypes.byref(o))
+    return o
+
+
 def mc_paint_default():
     o = McPaintOpts()
     lib().mb3d_cu_mc_paint_default(ctypes.byref(o))
@@ -213,6 +226,9 @@ def lib():
         L.mb3d_cu_mc_paint_default.restype = None
         L.mb3d_cu_mc_paint.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.POINTER(McPaintOpts), vp]
         L.mb3d_cu_paint.argtypes = [vp, sp, vp, ctypes.c_uint32, ctypes.c_uint32, vp]
+        L.mb3d_cu_ssao_default.argtypes = [ctypes.POINTER(SsaoOpts)]
+        L.mb3d_cu_ssao_default.restype = None
+        L.mb3d_cu_ssao24.argtypes = [vp, sp, ctypes.POINTER(SsaoOpts), vp]
         _lib = L
     return _lib
 
@@ -221,7 +237,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render",
-            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint",
+            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
             "mb3d_cu_dn_conv_check"]
@@ -395,6 +411,17 @@ class Card:
         self._order(gbuf, out)
         self._check(lib().mb3d_cu_paint(self._ctx, ctypes.byref(scene), _ptr(gbuf)[0], row0, rows, _ptr(out)[0]))
         return out
+
+    def ssao24(self, scene, gbuf, opts=None):
+        """gpu::ssao24 on the card: the G-buffer's amb_shadow from its depth
+        buffer.  A numpy G-buffer is returned as a new array; a torch CUDA
+        byte tensor is changed in place (and returned)."""
+        opts = ssao_default() if opts is None else opts
+        if isinstance(gbuf, np.ndarray):
+            gbuf = np.ascontiguousarray(gbuf).copy()
+        self._order(gbuf)
+        self._check(lib().mb3d_cu_ssao24(self._ctx, ctypes.byref(scene), ctypes.byref(opts), _ptr(gbuf)[0]))
+        return gbuf
 
     def mc_render(self, scene, opts, light=None, precision=FP32_FP64, out=None, cancel=None):
         """The Monte Carlo rays of opts on the card: a dict of radiance, albedo,

@@ -6,6 +6,7 @@
     python mb3d-rs_b200/profile_cases.py c4        # frame 37 of the 240-frame flight: one mixed, one FP64 render
     python mb3d-rs_b200/profile_cases.py de        # single precision DEs of the C2 scene at 3, 6 and 30 iterations
     python mb3d-rs_b200/profile_cases.py train     # 20 denoiser training steps, batch 16 of 128x128 (after 3)
+    python mb3d-rs_b200/profile_cases.py ssao      # the 24-bit SSAO of the 1920x1080 hybrid frame's G-buffer
 
 The Calculate 3D kernels are profiled through bench.py (--scale 0.25).
 """
@@ -75,6 +76,22 @@ def train():
     print("ok train step (16 x 128 x 128) ms", e0.elapsed_time(e1) / 20, "loss", loss)
 
 
+def ssao():
+    import torch
+    card = mb3dcu.Card(0)
+    sc = scenes.c2_hybrid()
+    npix = sc.width * sc.height
+    g = torch.empty(npix * 20, dtype=torch.uint8, device="cuda")
+    card.render(sc, mb3dcu.FP32_FP64, out=g)
+    for _ in range(3):
+        card.ssao24(sc, g)
+    ms = []
+    for _ in range(5):
+        card.ssao24(sc, g)
+        ms.append(card.stats()["ms_total"])
+    print("ok ssao24 1920x1080 ms", sum(ms) / len(ms), "Mpixels/s", npix / (sum(ms) / len(ms)) / 1e3)
+
+
 def _both(sc):
     card = mb3dcu.Card(0)
     for prec in (mb3dcu.FP32_FP64, mb3dcu.FP64):
@@ -107,4 +124,4 @@ def de():
 
 
 if __name__ == "__main__":
-    {"mc": mc, "denoise": denoise, "c1": c1, "c4": c4, "de": de, "train": train}[sys.argv[1]]()
+    {"mc": mc, "denoise": denoise, "c1": c1, "c4": c4, "de": de, "train": train, "ssao": ssao}[sys.argv[1]]()

@@ -81,6 +81,7 @@ def test_null_arguments_fail_on_the_host():
         lambda: L.mb3d_cu_paint(None, ctypes.byref(sc), buf.ctypes.data, 0, 48, rgb.ctypes.data),
         lambda: L.mb3d_cu_mc_paint(None, col.ctypes.data, None, 64 * 48, ctypes.byref(mb3dcu.mc_paint_default()),
                                    rgb.ctypes.data),
+        lambda: L.mb3d_cu_ssao24(None, ctypes.byref(sc), ctypes.byref(mb3dcu.ssao_default()), buf.ctypes.data),
     ]
     for call in calls:
         assert call() == mb3dcu.EINVAL
@@ -90,6 +91,8 @@ def test_null_arguments_fail_on_the_host():
 def test_display_and_light_defaults_on_the_host():
     o = mb3dcu.mc_paint_default()
     assert (o.contrast, o.saturation, o.options, o.gamma) == (128, 32, 2, 32.0)
+    a = mb3dcu.ssao_default()
+    assert (a.threshold, a.border_mirror, a.t0, a.wrap_x) == (2.0, 0.0, 0, 0)
     lv = mb3dcu.mc_light_default(scenes.c5_mc())
     assert lv is not None
     bad = scenes.preset("Integer Power", 64, 48)

@@ -181,6 +181,37 @@ def test_card_painter_matches_the_oracle(card):
     assert e.value.status == mb3dcu.EINVAL
 
 
+def test_ssao_matches_the_oracle(card):
+    """gpu::ssao24 (the 24-bit SSAO, regular sampling) against the oracle's
+    ssao::ssao24 on the same G-buffer: the angles are the reference's bit
+    for bit (single precision, unfused); the sum of their arctangents uses
+    the card's atanf, so a pixel may land one step away from the oracle's
+    where the sum sits at a rounding boundary."""
+    import torch
+    c2 = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    g = O.march(c2, mb3dcu.SILIGHT)
+    zm, zr = zc(c2)
+    obj = ~mb3dcu.is_background(g)
+    assert obj.mean() > 0.2
+    cases = [dict(), dict(threshold=1.5, t0=True), dict(border_mirror=0.3), dict(wrap_x=True, threshold=3.0)]
+    for kw in cases:
+        o = mb3dcu.ssao_default()
+        for k, v in kw.items():
+            setattr(o, k, v)
+        want = O.ssao24(g, c2.width, c2.height, zm, zr, **kw)
+        got = card.ssao24(c2, g, o)
+        d = np.abs(got["amb_shadow"].astype(np.int64) - want["amb_shadow"].astype(np.int64))[obj]
+        assert (d == 0).mean() >= 0.99 and d.max() <= 1, (kw, (d == 0).mean(), d.max())
+        assert np.array_equal(got["amb_shadow"][~obj], g["amb_shadow"][~obj])
+        assert np.array_equal(got["zpos_fine"], g["zpos_fine"])
+    # a device G-buffer, changed in place, equals the host one
+    dev = torch.from_numpy(g.view(np.uint8).copy()).cuda()
+    card.ssao24(c2, dev)
+    torch.cuda.synchronize()
+    host = card.ssao24(c2, g)
+    assert dev.cpu().numpy().tobytes() == host.tobytes()
+
+
 def test_render_device_buffer_equals_host_buffer(card):
     import torch
     sc = scenes.scaled(scenes.c2_hybrid(), 240, 136)
