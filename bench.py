@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--no-mc", action="store_true", help="skip the Monte Carlo / denoiser figures")
     ap.add_argument("--mc-ref-rays", type=int, default=1024)
     ap.add_argument("--no-configs", action="store_true", help="skip the plain bulb, deep zoom and flight figures")
+    ap.add_argument("--case", default=None, choices=sorted(CASES),
+                    help="run one small fixed workload for a profiler instead of the benchmark")
     return ap.parse_args()
 
 
@@ -393,8 +395,117 @@ def load_traffic():
         return {}
 
 
+# ---------------------------------------------------------------------------
+# small fixed workloads for profiler runs (ncu), one per hot kernel family;
+# `python bench.py --case NAME` runs one and prints a line of its timings
+
+def case_mc():
+    """Monte Carlo: the hybrid scene at 480x270, 4 rays, MCDepth 4, mixed."""
+    card = mb3dcu.Card(0)
+    sc = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    lv = mb3dcu.mc_light_default(sc)
+    card.mc_render(sc, mb3dcu.mc_opts(4, depth=4), lv, mb3dcu.FP32_FP64)
+    st = card.stats()
+    print("ok mc", st["ms_total"], st["de_evals"])
+
+
+def case_denoise():
+    """The denoiser on one 1920x1080 picture (6 passes)."""
+    import torch
+    card = mb3dcu.Card(0)
+    dn = mb3dcu.Denoiser(card)
+    h, w = 1080, 1920
+    rng = np.random.default_rng(0)
+    rad = torch.from_numpy(rng.gamma(1.0, 0.4, (1, h, w, 3)).astype(np.float32)).cuda()
+    alb = torch.rand((1, h, w, 3), device="cuda")
+    nrm = torch.rand((1, h, w, 3), device="cuda")
+    dep = torch.rand((1, h, w), device="cuda")
+    out = dn.denoise(rad, alb, nrm, dep, depth_scale=1.0)
+    torch.cuda.synchronize()
+    card.set_stream(torch.cuda.current_stream().cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        dn.denoise(rad, alb, nrm, dep, depth_scale=1.0, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    print("ok denoise 1920x1080 ms", e0.elapsed_time(e1) / 5)
+
+
+def case_train():
+    """20 denoiser training steps of batch 16 of 128x128 (after 3)."""
+    import torch
+    card = mb3dcu.Card(0)
+    dn = mb3dcu.Denoiser(card)
+    n, h, w = 16, 128, 128
+    g = torch.Generator(device="cuda").manual_seed(0)
+    rad = torch.rand((n, h, w, 3), device="cuda", generator=g) * 2.0
+    tgt = rad * 0.9
+    alb = torch.rand((n, h, w, 3), device="cuda", generator=g)
+    nrm = torch.rand((n, h, w, 3), device="cuda", generator=g)
+    dep = torch.rand((n, h, w), device="cuda", generator=g)
+    card.set_stream(torch.cuda.current_stream().cuda_stream)
+    for _ in range(3):
+        dn.train_step(rad, tgt, alb, nrm, dep, depth_scale=1.0, lr=1e-3)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(20):
+        loss = dn.train_step(rad, tgt, alb, nrm, dep, depth_scale=1.0, lr=1e-3)
+    e1.record()
+    torch.cuda.synchronize()
+    print("ok train step (16 x 128 x 128) ms", e0.elapsed_time(e1) / 20, "loss", loss)
+
+
+def case_ssao():
+    """The 24-bit SSAO of the 1920x1080 hybrid frame's G-buffer."""
+    import torch
+    card = mb3dcu.Card(0)
+    sc = scenes.c2_hybrid()
+    npix = sc.width * sc.height
+    g = torch.empty(npix * 20, dtype=torch.uint8, device="cuda")
+    card.render(sc, mb3dcu.FP32_FP64, out=g)
+    for _ in range(3):
+        card.ssao24(sc, g)
+    ms = []
+    for _ in range(5):
+        card.ssao24(sc, g)
+        ms.append(card.stats()["ms_total"])
+    print("ok ssao24 1920x1080 ms", sum(ms) / len(ms), "Mpixels/s", npix / (sum(ms) / len(ms)) / 1e3)
+
+
+def _case_both(sc):
+    card = mb3dcu.Card(0)
+    for prec in (mb3dcu.FP32_FP64, mb3dcu.FP64):
+        card.render(sc, prec)
+        st = card.stats()
+        print("ok", prec, "ms", st["ms_total"], "finish", st["ms_finish"], "fp64 pixels", st["fp64_pixels"])
+
+
+def case_c1():
+    """The plain bulb 640x480: one mixed, one FP64 render."""
+    _case_both(scenes.c1_plain_bulb())
+
+
+def case_c2small():
+    """The hybrid frame at 480x270 (march, shadows, DE AO): one mixed, one FP64 render."""
+    _case_both(scenes.scaled(scenes.c2_hybrid(), 480, 270))
+
+
+def case_c4():
+    """Frame 37 of the 240-frame flight: one mixed, one FP64 render."""
+    _case_both(scenes.c4_frames(240)[37])
+
+
+CASES = {"mc": case_mc, "denoise": case_denoise, "train": case_train, "ssao": case_ssao, "c1": case_c1,
+         "c2small": case_c2small, "c4": case_c4}
+
+
 def main():
     args = parse()
+    if args.case:
+        CASES[args.case]()
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

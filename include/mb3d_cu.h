@@ -468,8 +468,10 @@ int mb3d_cu_dn_conv_check(mb3d_cu_ctx *ctx, int n, int h, int w, int cin, int co
  * backend allocates its wgpu buffers per render).
  *
  * It marches rows row0 .. row0+rows of the picture into `gbuf`, which must
- * be device memory (rows * width records), on `stream` (a cudaStream_t, NULL
- * for the default stream), and returns when the work is queued.  Its
+ * be device memory (rows * width records), on `stream` (a cudaStream_t of
+ * gbuf's device, NULL for that device's default stream), and returns when the
+ * work is queued; the calling thread's current device is the same after the
+ * call as before it.  Its
  * scratch (the lists the march hands its surfaces over in) is a static
  * device array of this library, MB3D_CU_NOALLOC_MAX_PIXELS pixels' worth
  * (10.5 MB, held by every GPU that loads the library until the process

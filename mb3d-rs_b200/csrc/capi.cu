@@ -510,6 +510,7 @@ int mb3d_cu_march_noalloc(const mb3d_cu_scene *sc, int precision, uint32_t row0,
     std::string err;
     int r = setup_params(*sc, p, err);
     if (r < 0) return fail(r, err);
+    apply_tuning(p);  // (the launch settings mb3d_cu_march takes, so that the records are its records)
     if (rows == 0 || (uint64_t)row0 + rows > (uint64_t)p.height) return fail(MB3D_CU_EINVAL, "rows outside the picture");
     uint64_t npix = (uint64_t)rows * (uint64_t)p.width;
     if (npix > MB3D_CU_NOALLOC_MAX_PIXELS)
@@ -523,9 +524,13 @@ int mb3d_cu_march_noalloc(const mb3d_cu_scene *sc, int precision, uint32_t row0,
     }
     int dev = a.device;
     int cur = -1;
-    if (cudaGetDevice(&cur) != cudaSuccess || cur != dev) {
-        if (cudaSetDevice(dev) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
-    }
+    if (cudaGetDevice(&cur) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaGetDevice failed");
+    if (cur != dev && cudaSetDevice(dev) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    // the caller's current device is put back on every return
+    struct Restore {
+        int dev;
+        ~Restore() { cudaSetDevice(dev); }
+    } restore{cur};
     NoallocDevice d;
     if (int e = noalloc_setup(dev, d)) return e;
     cudaStream_t s = (cudaStream_t)stream;
