@@ -8,8 +8,9 @@ and DE ambient occlusion with 17 rays: the primary march (single precision
 bulk, double precision origin, ray parameter and finish), the shadow pass
 and the DE AO pass, into a device-resident G-buffer.  The metric is primary
 rays per second (Mrays/s) of the whole frame.  With N GPUs every rank
-renders its own frame (its own camera seed): weak scaling, no collective on
-the data path; the time is the max over ranks.
+renders its own frame (its own camera seed) and the frames' G-buffers are
+all-gathered over NCCL inside the step: weak scaling; the time is the max
+over ranks.
 
   value   device-resident G-buffer, kernels timed with CUDA events
   e2e     the same through the C ABI with a pinned host G-buffer (the copy
@@ -548,12 +549,16 @@ def main():
     clk.start()
     step_ms, kern = [], []
     launches = 0
+    import cards
     for _ in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         card.render(sc, prec, out=gbuf)
+        if world > 1:
+            # the frames of all ranks on every rank: one NCCL all_gather (NVLink)
+            cards.gather(gbuf, [npix] * world, 20)
         e1.record(stream)
         e1.synchronize()
         step_ms.append(e0.elapsed_time(e1))
@@ -598,7 +603,8 @@ def main():
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32+f64" if prec == mb3dcu.FP32_FP64 else "f64", "data": "synthetic",
            "config": {"workload": WORKLOAD, "width": sc.width, "height": sc.height, "seed": scenes.C2_SEED,
-                      "precision": args.precision, "parallelism": f"frame per rank x{world}",
+                      "precision": args.precision,
+                      "parallelism": f"frame per rank x{world}" + (", G-buffers all-gathered in the step" if world > 1 else ""),
                       "l2": "512 MiB buffer written between timed steps (outside the step events)"},
            "e2e": {"value": world * npix / (e2e / 1000.0) / 1e6, "unit": "Mrays/s",
                    "h2d_bytes_per_step": ctypes.sizeof(mb3dcu.Scene), "d2h_bytes_per_step": npix * 20},

@@ -227,6 +227,9 @@ typedef struct mb3d_cu_stats {
     uint64_t march_warp_its;   /* per warp and loop trip the most iterations of its lanes, summed */
     uint64_t march_trips;      /* warp loop trips that evaluated DEs */
     uint64_t march_busy_lanes; /* the lanes with a ray in those trips, summed */
+    uint32_t fp32_overflow_pixels; /* mixed mode: pixels whose single precision DE overflowed (marched on in
+                                    * double precision) */
+    uint32_t pad_stats;
 } mb3d_cu_stats;
 
 typedef struct mb3d_cu_ctx mb3d_cu_ctx;
@@ -263,6 +266,41 @@ int mb3d_cu_unsupported(const mb3d_cu_scene *scene, char *reason, size_t cap);
  * polled between launches. */
 int mb3d_cu_march(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, uint32_t row0, uint32_t rows,
                   mb3d_cu_silight *gbuf, const volatile int *cancel);
+
+/* Called after each band of mb3d_cu_march_ex (gpu::march's `progress`,
+ * src/gpu.rs:2296-2302): rows_done of the call's rows_total rows are in the
+ * G-buffer (a host buffer has them copied back).  It runs on the calling
+ * thread; a non-zero return cancels the call, which then returns
+ * MB3D_CU_ECANCELED (the convention of mb3d_progress, capi/include/mb3d.h). */
+typedef int (*mb3d_cu_progress_fn)(uint32_t rows_done, uint32_t rows_total, void *user);
+
+/* What gpu::march (src/gpu.rs:2296) takes beyond mb3d_cu_march's arguments,
+ * and the card's two limits.  All zero: mb3d_cu_march's behaviour. */
+typedef struct mb3d_cu_march_opts {
+    const volatile int *cancel;   /* polled between bands (NULL: never cancelled) */
+    mb3d_cu_progress_fn progress; /* called after each band (NULL: none) */
+    void *user;                   /* progress's last argument */
+    uint32_t band_rows;           /* rows per band (0: the whole range is one band) */
+    int32_t overflow_fail;        /* 1: return MB3D_CU_EOVERFLOW when the single precision DE overflowed in more
+                                   * than 1/500 of the pixels, as the reference's card gives such a picture up
+                                   * (src/gpu.rs:2361-2370); 0: those pixels are marched in double precision */
+    double budget_ms;             /* device time budget of the call in ms (0: none): once it is spent the
+                                   * kernels take no new rays, finish the ones they hold, and the call returns
+                                   * MB3D_CU_ETIMEDOUT */
+} mb3d_cu_march_opts;
+
+/* Replaces gpu::march with its progress, cancel and sink (src/gpu.rs:2296,
+ * march_card :2308-2400): the rows row0 .. row0+rows marched into `gbuf`
+ * band by band (each band whole before the next; a host G-buffer gets each
+ * band's rows as soon as it is done, as the reference's sink does).
+ * MB3D_CU_ETIMEDOUT leaves the work done so far on the context: calling
+ * again with the same arguments (scene bytes, precision, rows, gbuf,
+ * band_rows) goes on where the budget stopped it, and the G-buffer it
+ * finally returns equals one marched without a budget.  Any other call on
+ * the context in between drops that state (the next call starts over).
+ * `opts` may be NULL. */
+int mb3d_cu_march_ex(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, uint32_t row0, uint32_t rows,
+                     mb3d_cu_silight *gbuf, const mb3d_cu_march_opts *opts);
 
 /* Replaces gpu::post_on_card (src/gpu.rs:1649) / post_bands (:1715): the
  * hard (or soft) shadows and/or the DE ambient occlusion computed in place

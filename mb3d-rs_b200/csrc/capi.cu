@@ -79,6 +79,19 @@ struct mb3d_cu_ctx {
     size_t paint_cap = 0;
     unsigned char *d_ssao = nullptr;   // the SSAO's levels and angles (and a host G-buffer's staging)
     size_t ssao_cap = 0;
+    // a budgeted march (mb3d_cu_march_ex) that ran out of time: where it
+    // stopped; the device keeps its G-buffer rows, lists and queue counters
+    // until the same call comes again (any other call drops it)
+    struct Resume {
+        bool active = false;
+        mb3d_cu_scene scene;
+        int precision = 0;
+        uint32_t row0 = 0, rows = 0, band_rows = 0;
+        mb3d_cu_silight *gbuf = nullptr;
+        uint32_t band = 0;   // the band in progress
+        int stage = 0;       // 0 its counters to clear, 1 the march, 2 the finish, 3 the slow finish
+        uint64_t overflow = 0, fp64_pixels = 0;  // summed over the finished bands
+    } resume;
     std::mutex mu;
 };
 
@@ -157,7 +170,7 @@ int mb3d_cu_init(int device, mb3d_cu_ctx **out) {
         return fail(MB3D_CU_EIO, "stream create failed");
     }
     if (cudaMalloc(&c->d_counters, 64 * sizeof(unsigned int)) != cudaSuccess ||
-        cudaMallocHost(&c->h_counters, 16 * sizeof(unsigned int)) != cudaSuccess) {
+        cudaMallocHost(&c->h_counters, 64 * sizeof(unsigned int)) != cudaSuccess) {
         mb3d_cu_free(c);
         return fail(MB3D_CU_ENOMEM, "device memory");
     }
@@ -264,7 +277,8 @@ static int march_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int r
     // the slow list's length: the mixed mode's pixels finished by the
     // per-thread double precision marcher
     c->read_slow = mixed;
-    if (mixed) CU_TRY(cudaMemcpyAsync(c->h_counters, c->d_counters, 4 * sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    if (mixed) CU_TRY(cudaMemcpyAsync(c->h_counters, c->d_counters, (CNT_OVERFLOW + 1) * sizeof(unsigned int),
+                                      cudaMemcpyDeviceToHost, s));
     return 0;
 }
 
@@ -327,7 +341,10 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
 static int finish_call(mb3d_cu_ctx *c, bool marched, bool posted) {
     cudaError_t e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
-    if (marched && c->read_slow) c->stats.fp64_pixels = c->h_counters[2];
+    if (marched && c->read_slow) {
+        c->stats.fp64_pixels = c->h_counters[CNT_SLOW];
+        c->stats.fp32_overflow_pixels = c->h_counters[CNT_OVERFLOW];
+    }
     c->read_slow = false;
     if (marched && c->counting && c->d_count) {
         unsigned long long h[16];
@@ -378,6 +395,7 @@ static void apply_tuning(DevParams &p) {
             else if (k == "blocks" && v >= 1 && v <= 16) p.blocks_per_sm = (int)v;
             else if (k == "margin" && v >= 1) p.hand_margin = (float)v;
             else if (k == "back" && v >= 0 && v <= 2) p.hand_back = (int)v;
+            else if (k == "near" && (v == 0 || v == 1)) p.hand_near = (int)v;
         }
         i = j + 1;
     }
@@ -388,6 +406,7 @@ static int run(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, int passe
     if (!c || !sc || !gbuf) return fail(MB3D_CU_EINVAL, "NULL argument");
     if (precision != MB3D_CU_FP64 && precision != MB3D_CU_FP32_FP64) return fail(MB3D_CU_EINVAL, "unknown precision");
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     DevParams p;
     std::string err;
@@ -437,11 +456,142 @@ int mb3d_cu_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, mb3d_
     return run(c, sc, precision, passes, true, 0, (uint32_t)sc->height, gbuf, cancel);
 }
 
+// ---------------------------------------------------------------------------
+// the march with gpu::march's progress and cancel per band, the device time
+// budget (resumable) and the reference card's overflow rule
+
+static bool same_scene(const mb3d_cu_scene &a, const mb3d_cu_scene &b) { return std::memcmp(&a, &b, sizeof a) == 0; }
+
+// one stage of a band on the context's stream; with a budget it waits for
+// the launch and tells whether the budget stopped it (*stopped)
+static int band_stage(mb3d_cu_ctx *c, const DevParams &p, bool mixed, int stage, int r0, int nr, mb3d_cu_silight *dg,
+                      bool *stopped) {
+    cudaStream_t s = c->stream;
+    *stopped = false;
+    int blocks = c->sms * p.blocks_per_sm;
+    if (stage == 1) {
+        int items = ((p.width + 7) / 8) * ((nr + 3) / 4);
+        int mb = c->sms * (mixed ? p.blocks_march32 : p.blocks_per_sm);
+        int need = (items + 7) / 8;
+        if (mb > need) mb = need > 0 ? need : 1;
+        launch_march(p, mixed, r0, nr, dg, c->d_hand, c->d_counters, nullptr, mb, s);
+    } else if (stage == 2) {
+        launch_finish_fast(p, mixed, r0, c->d_hand, c->d_counters, c->d_slow, dg, blocks, s);
+    } else {
+        launch_finish_slow(p, mixed, r0, c->d_hand, c->d_counters, c->d_slow, dg, blocks, s);
+    }
+    if (int e = check_launch(stage == 1 ? "k_march" : stage == 2 ? "k_finish" : "k_finish_slow")) return e;
+    c->stats.launches += 1;
+    if (p.budget_ns != 0) {
+        CU_TRY(cudaMemcpyAsync(c->h_counters, c->d_counters, (CNT_OVERFLOW + 1) * sizeof(unsigned int),
+                               cudaMemcpyDeviceToHost, s));
+        CU_TRY(cudaStreamSynchronize(s));
+        const unsigned int bit = stage == 1 ? 1u : stage == 2 ? 2u : 4u;
+        *stopped = (c->h_counters[CNT_STATUS] & bit) != 0;
+    }
+    return 0;
+}
+
+int mb3d_cu_march_ex(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, uint32_t row0, uint32_t rows,
+                     mb3d_cu_silight *gbuf, const mb3d_cu_march_opts *opts) {
+    if (!c || !sc || !gbuf) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (precision != MB3D_CU_FP64 && precision != MB3D_CU_FP32_FP64) return fail(MB3D_CU_EINVAL, "unknown precision");
+    mb3d_cu_march_opts o = {};
+    if (opts) o = *opts;
+    if (!(o.budget_ms >= 0.0) || o.budget_ms > 3.6e6) return fail(MB3D_CU_EINVAL, "budget_ms outside 0 .. 3.6e6");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    DevParams p;
+    std::string err;
+    int r = setup_params(*sc, p, err);
+    if (r < 0) {
+        c->resume.active = false;
+        return fail(r, err);
+    }
+    apply_tuning(p);
+    if ((uint64_t)row0 + rows > (uint64_t)p.height || rows == 0) {
+        c->resume.active = false;
+        return fail(MB3D_CU_EINVAL, "rows outside the picture");
+    }
+    const uint32_t band_rows = o.band_rows == 0 || o.band_rows > rows ? rows : o.band_rows;
+    mb3d_cu_ctx::Resume &rs = c->resume;
+    const bool resuming = rs.active && same_scene(rs.scene, *sc) && rs.precision == precision && rs.row0 == row0 &&
+                          rs.rows == rows && rs.gbuf == gbuf && rs.band_rows == band_rows;
+    if (!resuming) {
+        rs = mb3d_cu_ctx::Resume();
+        rs.scene = *sc;
+        rs.precision = precision;
+        rs.row0 = row0;
+        rs.rows = rows;
+        rs.band_rows = band_rows;
+        rs.gbuf = gbuf;
+    }
+    rs.active = false;  // (set again only where the budget stops the call)
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    p.budget_ns = (unsigned long long)(o.budget_ms * 1e6);
+    if (o.budget_ms > 0.0 && p.budget_ns == 0) p.budget_ns = 1;
+    const bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
+    const size_t npix = (size_t)rows * p.width, band_pix = (size_t)band_rows * p.width;
+    const bool dev = is_device_ptr(gbuf);
+    mb3d_cu_silight *dg = gbuf;
+    if (!dev) {
+        if (int e = grow((void **)&c->d_gbuf, &c->gbuf_cap, npix * sizeof(mb3d_cu_silight))) return e;
+        dg = c->d_gbuf;
+    }
+    if (int e = grow((void **)&c->d_hand, &c->hand_cap, band_pix * sizeof(Hand))) return e;
+    if (int e = grow((void **)&c->d_slow, &c->slow_cap, band_pix * sizeof(Hand))) return e;
+    cudaStream_t s = c->stream;
+    const uint32_t n_bands = (rows + band_rows - 1) / band_rows;
+    for (; rs.band < n_bands; rs.band++, rs.stage = 0) {
+        const uint32_t r0 = rs.band * band_rows, nr = std::min(band_rows, rows - r0);
+        mb3d_cu_silight *bg = dg + (size_t)r0 * p.width;
+        if (rs.stage == 0) {
+            CU_TRY(cudaMemsetAsync(c->d_counters, 0, 64 * sizeof(unsigned int), s));
+            rs.stage = 1;
+        } else {
+            // a new call: the budget's clock and status start again
+            CU_TRY(cudaMemsetAsync(c->d_counters + CNT_T0, 0, 3 * sizeof(unsigned int), s));
+        }
+        for (; rs.stage <= 3; rs.stage++) {
+            bool stopped = false;
+            if (int e = band_stage(c, p, mixed, rs.stage, (int)(row0 + r0), (int)nr, bg, &stopped)) return e;
+            if (stopped) {
+                rs.active = true;
+                c->stats.fp64_pixels = (uint32_t)rs.fp64_pixels;
+                return fail(MB3D_CU_ETIMEDOUT, "the device time budget ran out in band " + std::to_string(rs.band) +
+                                                   " (call again with the same arguments to go on)");
+            }
+        }
+        // the band is done: its counts, its rows to the host, progress, cancel
+        CU_TRY(cudaMemcpyAsync(c->h_counters, c->d_counters, (CNT_OVERFLOW + 1) * sizeof(unsigned int),
+                               cudaMemcpyDeviceToHost, s));
+        if (!dev)
+            CU_TRY(cudaMemcpyAsync(gbuf + (size_t)r0 * p.width, bg, (size_t)nr * p.width * sizeof(mb3d_cu_silight),
+                                   cudaMemcpyDeviceToHost, s));
+        CU_TRY(cudaStreamSynchronize(s));
+        rs.overflow += c->h_counters[CNT_OVERFLOW];
+        if (mixed) rs.fp64_pixels += c->h_counters[CNT_SLOW];
+        if (o.progress && o.progress(r0 + nr, rows, o.user) != 0) return fail(MB3D_CU_ECANCELED, "cancelled");
+        if (o.cancel && *o.cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
+    }
+    c->stats.fp64_pixels = (uint32_t)(mixed ? rs.fp64_pixels : (precision != MB3D_CU_FP64 ? npix : 0));
+    c->stats.fp32_overflow_pixels = (uint32_t)rs.overflow;
+    // src/gpu.rs:2361-2370: many pixels whose single precision DE overflowed
+    // make the reference's card give the picture up (the host then renders
+    // it on the CPU); here they were marched in double precision, and the
+    // rule applies only where the caller asks for it
+    if (o.overflow_fail && mixed && rs.overflow * 500 > npix)
+        return fail(MB3D_CU_EOVERFLOW, "single precision overflows in " + std::to_string(rs.overflow) + " of " +
+                                           std::to_string(npix) + " pixels");
+    return 0;
+}
+
 int mb3d_cu_de_probe(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, const double *pos, uint32_t n, double *de,
                      int32_t *its) {
     if (!c || !sc || !pos || !de || !its) return fail(MB3D_CU_EINVAL, "NULL argument");
     if (n == 0) return 0;
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     DevParams p;
     std::string err;
@@ -690,6 +840,7 @@ int mb3d_cu_render_frames(mb3d_cu_ctx *c, const mb3d_cu_scene *frames, uint32_t 
                           const mb3d_cu_tune *tune, mb3d_cu_silight *out) {
     if (!c) return fail(MB3D_CU_EINVAL, "ctx is NULL");
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     std::memset(&c->stats, 0, sizeof(c->stats));
     return render_frames_locked(c, frames, n, precision, tune, out, nullptr);
@@ -699,6 +850,7 @@ int mb3d_cu_autotune(mb3d_cu_ctx *c, const mb3d_cu_scene *frames, uint32_t n, ui
                      mb3d_cu_tune *out) {
     if (!c || !frames || n == 0 || !out) return fail(MB3D_CU_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     if (sample == 0 || sample > n) sample = n < 8 ? n : 8;
     std::vector<mb3d_cu_scene> pick;
@@ -736,6 +888,7 @@ int mb3d_cu_set_counting(mb3d_cu_ctx *c, int on) {
 int mb3d_cu_fma_peak(mb3d_cu_ctx *c, int fp64, double *tflops) {
     if (!c || !tflops) return fail(MB3D_CU_EINVAL, "NULL argument");
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     if (int e = grow((void **)&c->d_probe, &c->probe_cap, 64)) return e;
     int blocks = c->sms * 8, iters = fp64 ? 512 : 2048;
@@ -779,6 +932,7 @@ int mb3d_cu_mc_paint(mb3d_cu_ctx *c, const float *col, const uint8_t *rays, uint
     if (!c || !col || !o || !rgb) return fail(MB3D_CU_EINVAL, "NULL argument");
     if (npix == 0) return 0;
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     cudaStream_t s = c->stream;
     const bool dc = is_device_ptr(col), dr = !rays || is_device_ptr(rays), dg = is_device_ptr(rgb);
@@ -820,6 +974,7 @@ int mb3d_cu_paint(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_silight
     if (r < 0) return fail(r, err);
     if ((uint64_t)row0 + rows > (uint64_t)p.height || rows == 0) return fail(MB3D_CU_EINVAL, "rows outside the picture");
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     cudaStream_t s = c->stream;
     const uint32_t npix = rows * (uint32_t)p.width;
@@ -866,6 +1021,7 @@ int mb3d_cu_ssao24(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_ssao_o
     if (r < 0) return fail(r, err);
     const int w = p.width, h = p.height;
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     cudaStream_t s = c->stream;
     const size_t npix = (size_t)w * h, gb = npix * sizeof(mb3d_cu_silight);
@@ -910,6 +1066,7 @@ int mb3d_cu_mc_batch(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, int
             if (reqs[i].inside) return fail(MB3D_CU_ENOTSUP, "inside rendering is not on the card");
         }
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     DevParams p;
     McDev m;
@@ -971,6 +1128,7 @@ int mb3d_cu_mc_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_
     if (w <= 0 || h <= 0 || x0 < 0 || y0 < 0 || (int64_t)x0 + w > sc->width || (int64_t)y0 + h > sc->height)
         return fail(MB3D_CU_EINVAL, "rectangle outside the picture");
     std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
     if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
     DevParams p;
     McDev m;

@@ -28,7 +28,8 @@ namespace mb3dcu {
 struct DEr {
     double de;
     int it;
-    bool need64;  // single precision cannot resolve the offset here
+    bool need64;    // single precision cannot resolve the offset here
+    bool overflow;  // ... because its DE overflowed (not finite)
 };
 
 // The iteration state a full DE leaves for the colouring (the record's
@@ -150,6 +151,7 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
     if (COUNT) cnt->evals++;
     DEr out;
     out.need64 = false;
+    out.overflow = false;
     const int max_it = p.max_it + max_add;  // (max_add: doBinSearchIt's one more iteration)
     const R rstop = param_f<R>(p, p.d_rstop, p.d_rstop_f);
     if (p.is_custom_de) {
@@ -429,7 +431,7 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
     }
     // (single precision that overflowed, e.g. a vanishing gradient sum with
     // exp(-ln R) underflowing: the double precision DE decides)
-    if (sizeof(R) == 4 && !isfinite(out.de)) out.need64 = true;
+    if (sizeof(R) == 4 && !isfinite(out.de)) out.need64 = out.overflow = true;
     double mn = (double)ms_de_stop * 0.25;
     if (out.de < mn || isnan(out.de)) out.de = mn;
     return out;

@@ -42,7 +42,8 @@ struct DevParams {
     int32_t hand_back;  // ... at most this many steps back
     int32_t refill_min, blocks_per_sm;  // wavefront: idle lanes that trigger a refill; resident blocks
     int32_t refill_shadow, refill_ao;   // ... of the shadow and DE AO ray kernels
-    int32_t blocks_march32, pad_b;      // resident blocks of the single precision march
+    int32_t blocks_march32;             // resident blocks of the single precision march
+    int32_t hand_near;                  // the mixed march hands over at the first DE < hand_margin x DE stop
     float d_rstop_f, rstop3d_f, soft_radius, hs_max_len_mul;
     double d_rstop, rstop3d, zcorr, zc_mul;
     double zend, step_width, fov_y, coord_eps;
@@ -58,4 +59,18 @@ struct DevParams {
     float ao_d_step_mul, ao_d_min_a_dif, ao_corr_weight, ao_max_len;
     float ao_dirs[MB3D_MAX_AO_RAYS][3];
     double ao_rot[3][3];  // camera rows, step width long (normalise_matrix_to(sw, vgrads))
+    // the call's device time budget (0: none): the march and finish kernels
+    // take no new rays once this many nanoseconds have passed since the
+    // first warp of the call asked (their queue counters stay resumable)
+    unsigned long long budget_ns;
 };
+
+// the counters' slots (unsigned int) the march kernels share with the host
+#define CNT_HAND 0        // hand-over list length
+#define CNT_MARCH_Q 1     // the march's queue
+#define CNT_SLOW 2        // slow list length
+#define CNT_FINISH_Q 3    // the finish's queue
+#define CNT_SLOW_Q 4      // the slow finish's queue
+#define CNT_T0 32         // (two slots) %globaltimer of the call's first take
+#define CNT_STATUS 34     // bits: 1 the march, 2 the finish, 4 the slow finish stopped on the budget
+#define CNT_OVERFLOW 35   // pixels whose single precision DE overflowed

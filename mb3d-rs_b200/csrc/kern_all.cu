@@ -5,7 +5,8 @@
 namespace mb3dcu {
 LaunchTable table_all() {
     typedef Launch<KSET_ALL> L;
-    return LaunchTable{&L::march, &L::finish, &L::post_start, &L::shadow_rays, &L::ao_rays, &L::de_probe};
+    return LaunchTable{&L::march, &L::finish, &L::post_start, &L::shadow_rays, &L::ao_rays, &L::de_probe,
+                       &L::finish_fast, &L::finish_slow};
 }
 
 // the kernels every formula set shares

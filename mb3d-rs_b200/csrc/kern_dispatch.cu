@@ -31,6 +31,14 @@ void launch_finish(const DevParams &p, bool mixed, int row0, const Hand *list, u
                    mb3d_cu_silight *out, int blocks, cudaStream_t s) {
     table(p.fmask).finish(p, mixed, row0, list, counters, slow, out, blocks, s);
 }
+void launch_finish_fast(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                        mb3d_cu_silight *out, int blocks, cudaStream_t s) {
+    table(p.fmask).finish_fast(p, mixed, row0, list, counters, slow, out, blocks, s);
+}
+void launch_finish_slow(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                        mb3d_cu_silight *out, int blocks, cudaStream_t s) {
+    table(p.fmask).finish_slow(p, mixed, row0, list, counters, slow, out, blocks, s);
+}
 void launch_post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
                        const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps, int blocks,
                        cudaStream_t s) {

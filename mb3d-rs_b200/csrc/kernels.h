@@ -65,6 +65,12 @@ struct LaunchTable {
     void (*ao_rays)(const DevParams &, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,
                     const unsigned int *count, float *min_ra, unsigned int *queue, int blocks, cudaStream_t s);
     void (*de_probe)(const DevParams &, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s);
+    // the finish's two kernels one at a time (a budgeted call checks its
+    // status between them): the wavefront, then the per-thread rare cases
+    void (*finish_fast)(const DevParams &, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                        mb3d_cu_silight *out, int blocks, cudaStream_t s);
+    void (*finish_slow)(const DevParams &, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                        mb3d_cu_silight *out, int blocks, cudaStream_t s);
 };
 LaunchTable table_ip8();
 LaunchTable table_ip8box();
@@ -75,6 +81,10 @@ void launch_march(const DevParams &p, bool mixed, int row0, int rows, mb3d_cu_si
                   unsigned int *counters, unsigned long long *gcount, int blocks, cudaStream_t s);
 void launch_finish(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
                    mb3d_cu_silight *out, int blocks, cudaStream_t s);
+void launch_finish_fast(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                        mb3d_cu_silight *out, int blocks, cudaStream_t s);
+void launch_finish_slow(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
+                        mb3d_cu_silight *out, int blocks, cudaStream_t s);
 void launch_surface(const DevParams &p, int npix, int passes, mb3d_cu_silight *gbuf, uint32_t *list,
                     unsigned int *count, int blocks, cudaStream_t s);
 void launch_post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,

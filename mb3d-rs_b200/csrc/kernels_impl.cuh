@@ -89,6 +89,37 @@ __device__ __forceinline__ uint32_t warp_take(bool idle_lane, unsigned int *queu
     return item < n_items ? item : UINT32_MAX;
 }
 
+// The call's device time budget: true once p.budget_ns nanoseconds have
+// passed since the call's first take (the first warp to ask stamps it);
+// sets `bit` in the status word.  Asked by one lane before a take, so a
+// warp that stops has finished every ray it took.
+__device__ __forceinline__ bool budget_spent(const DevParams &p, unsigned int *counters, unsigned int bit) {
+    if (p.budget_ns == 0) return false;
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    unsigned long long *t0p = reinterpret_cast<unsigned long long *>(counters + CNT_T0);
+    unsigned long long t0 = atomicCAS(t0p, 0ull, now);
+    if (t0 == 0ull) t0 = now;
+    if (now - t0 <= p.budget_ns) return false;
+    atomicOr(counters + CNT_STATUS, bit);
+    return true;
+}
+
+// warp_take under the budget: no new items once it is spent (the queue's
+// counter then says how far the call got; a later launch goes on from there)
+__device__ __forceinline__ uint32_t warp_take_b(const DevParams &p, bool idle_lane, unsigned int *counters, int queue,
+                                                uint32_t n_items, int min_idle, bool &open, unsigned int bit) {
+    if (p.budget_ns != 0 && open) {
+        unsigned int idle = __ballot_sync(0xffffffffu, idle_lane);
+        if (__popc(idle) >= min_idle || idle == 0xffffffffu) {
+            int spent = 0;
+            if ((threadIdx.x & 31) == 0) spent = budget_spent(p, counters, bit) ? 1 : 0;
+            if (__shfl_sync(0xffffffffu, spent, 0)) open = false;
+        }
+    }
+    return warp_take(idle_lane, &counters[queue], n_items, min_idle, open);
+}
+
 __device__ __forceinline__ void item_pixel(uint32_t item, int tiles_x, int &x, int &ly) {
     uint32_t t = item >> 5, l = item & 31u;
     x = (int)(t % (uint32_t)tiles_x) * 8 + (int)(l & 7u);
@@ -142,7 +173,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
     float b0_cnt = 0, b1_cnt = 0;
     int nb = 0;
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
-        uint32_t item = warp_take(phase == PH_IDLE, &counters[1], n_items, p.refill_min, open);
+        uint32_t item = warp_take_b(p, phase == PH_IDLE, counters, CNT_MARCH_Q, n_items, p.refill_min, open, 1u);
         if (item != UINT32_MAX) {
             item_pixel(item, tiles_x, x, ly);
             if (x < p.width && ly < rows) {
@@ -158,7 +189,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             if (!open) break;
             continue;
         }
-        bool hand = false, full = false, done_bg = false, resume = false;
+        bool hand = false, full = false, done_bg = false, resume = false, overflowed = false;
         double cur_de = 0.0;
         int cur_it = 0;
         if (phase != PH_IDLE) {
@@ -168,13 +199,15 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             int it = r.it;
             bool skip_half = false, decide = true;
             if (MIXED && r.need64) {
+                overflowed = r.overflow;
                 hand = true;
                 full = phase == PH_START;
                 resume = !full;
                 decide = false;
             } else if (phase == PH_START) {
-                if (it >= p.max_it || dtmp < (double)ms) {
-                    hand = true;  // inside the set at the start plane
+                if (it >= p.max_it || dtmp < (double)ms ||
+                    (MIXED && p.hand_near && (it >= p.max_it - 1 || dtmp < (double)p.hand_margin * (double)ms))) {
+                    hand = true;  // inside the set at the start plane (or too near it for single precision)
                     full = true;
                     decide = false;
                 } else {
@@ -192,6 +225,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                     rsf = t < 1.0 ? (float)fmax(0.5, t) : 1.0f;
                 } else {
                     rsf = 1.0f;
+                }
+                if (MIXED && p.hand_near && (it >= p.max_it - 1 || dtmp < (double)p.hand_margin * (double)ms)) {
+                    // near the surface (or the iteration limit): from here on
+                    // every decision is the double precision march's own
+                    hand = true;
+                    resume = true;
+                    decide = false;
                 }
             } else {  // PH_HALF: the DE after the half step back
                 skip_half = true;
@@ -293,7 +333,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             si.store(out + pix);
             phase = PH_IDLE;
         }
-        warp_append(hand, &counters[0], h, list);
+        warp_append(hand, &counters[CNT_HAND], h, list);
+        if (MIXED) {
+            // (a ray hands over once: this counts pixels)
+            const unsigned int ov = __ballot_sync(0xffffffffu, overflowed);
+            if (ov && (threadIdx.x & 31) == __ffs(ov) - 1) atomicAdd(&counters[CNT_OVERFLOW], (unsigned int)__popc(ov));
+        }
     }
     if (COUNT) cnt.flush(gcount);
 }
@@ -302,11 +347,17 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
 // a pixel inside the set at the start plane, a surface whose binary search
 // is on the iteration count (RMdoBinSearchIt), the smoothed normals, normals
 // on the smooth iterations, colour on an iteration.
+// Its items are taken one per thread from a queue (CNT_SLOW_Q), so that a
+// launch stopped by the budget has finished exactly the items before the
+// queue's counter.
 template <int FM>
 __global__ void __launch_bounds__(128) k_finish_slow(const __grid_constant__ DevParams p, int row0, const Hand *list,
-                                                     const unsigned int *count, mb3d_cu_silight *out) {
-    unsigned int n = count[0];
-    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+                                                     unsigned int *counters, mb3d_cu_silight *out) {
+    const unsigned int n = counters[CNT_SLOW];
+    for (int guard = 0; guard < (1 << 30); guard++) {
+        if (p.budget_ns != 0 && budget_spent(p, counters, 4u)) break;
+        const unsigned int i = atomicAdd(&counters[CNT_SLOW_Q], 1u);
+        if (i >= n) break;
         Hand h = list[i];
         int x = (int)(h.pix % (uint32_t)p.width);
         int y = row0 + (int)(h.pix / (uint32_t)p.width);
@@ -384,7 +435,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
     bool it_limited = false, b_first = false;
     unsigned int guard = 0;
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
-        uint32_t item = warp_take(phase == F_IDLE, &counters[3], n_items, p.refill_min, open);
+        uint32_t item = warp_take_b(p, phase == F_IDLE, counters, CNT_FINISH_Q, n_items, p.refill_min, open, 2u);
         bool to_slow = false;
         Hand hs;
         int entry = 0;  // 2: a surface already evaluated (the plain march)
@@ -1265,7 +1316,15 @@ struct Launch {
     static void finish(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters,
                        Hand *slow, mb3d_cu_silight *out, int blocks, cudaStream_t s) {
         k_finish<FM><<<blocks, 256, 0, s>>>(p, row0, list, counters, slow, out);
-        k_finish_slow<FM><<<blocks, 128, 0, s>>>(p, row0, slow, counters + 2, out);
+        k_finish_slow<FM><<<blocks, 128, 0, s>>>(p, row0, slow, counters, out);
+    }
+    static void finish_fast(const DevParams &p, bool, int row0, const Hand *list, unsigned int *counters,
+                            Hand *slow, mb3d_cu_silight *out, int blocks, cudaStream_t s) {
+        k_finish<FM><<<blocks, 256, 0, s>>>(p, row0, list, counters, slow, out);
+    }
+    static void finish_slow(const DevParams &p, bool, int row0, const Hand *, unsigned int *counters,
+                            Hand *slow, mb3d_cu_silight *out, int blocks, cudaStream_t s) {
+        k_finish_slow<FM><<<blocks, 128, 0, s>>>(p, row0, slow, counters, out);
     }
     static void post_start(const DevParams &p, bool mixed, int row0, int passes, const mb3d_cu_silight *gbuf,
                            const uint32_t *list, const unsigned int *count, unsigned int *queue, PostStart *ps,

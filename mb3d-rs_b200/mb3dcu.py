@@ -74,7 +74,18 @@ class Stats(ctypes.Structure):
                 ("fp64_pixels", ctypes.c_uint32), ("de_evals", ctypes.c_uint64), ("orbit_its", ctypes.c_uint64 * 6),
                 ("mc_inside_rays", ctypes.c_uint32), ("mc_fp64_rays", ctypes.c_uint32),
                 ("march_lane_its", ctypes.c_uint64), ("march_warp_its", ctypes.c_uint64),
-                ("march_trips", ctypes.c_uint64), ("march_busy_lanes", ctypes.c_uint64)]
+                ("march_trips", ctypes.c_uint64), ("march_busy_lanes", ctypes.c_uint64),
+                ("fp32_overflow_pixels", ctypes.c_uint32), ("pad_stats", ctypes.c_uint32)]
+
+
+PROGRESS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p)
+
+
+class MarchOpts(ctypes.Structure):
+    """mb3d_cu_march_opts: gpu::march's progress and cancel, bands, the
+    device time budget and the overflow rule."""
+    _fields_ = [("cancel", ctypes.c_void_p), ("progress", PROGRESS_FN), ("user", ctypes.c_void_p),
+                ("band_rows", ctypes.c_uint32), ("overflow_fail", ctypes.c_int32), ("budget_ms", ctypes.c_double)]
 
 
 # ---- the Monte Carlo tracer (src/mc.rs) ----
@@ -198,6 +209,8 @@ def lib():
         L.mb3d_cu_set_stream.argtypes = [vp, vp]
         L.mb3d_cu_unsupported.argtypes = [sp, ctypes.c_char_p, ctypes.c_size_t]
         L.mb3d_cu_march.argtypes = [vp, sp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
+        L.mb3d_cu_march_ex.argtypes = [vp, sp, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp,
+                                       ctypes.POINTER(MarchOpts)]
         L.mb3d_cu_post.argtypes = [vp, sp, ctypes.c_int, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32, vp, vp]
         L.mb3d_cu_render.argtypes = [vp, sp, ctypes.c_int, vp, vp]
         L.mb3d_cu_de_probe.argtypes = [vp, sp, ctypes.c_int, vp, ctypes.c_uint32, vp, vp]
@@ -234,7 +247,7 @@ def lib():
 
 
 EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_free", "mb3d_cu_set_stream",
-            "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
+            "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_march_ex", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render",
             "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24",
@@ -321,6 +334,28 @@ class Card:
         self._order(out)
         cp = ctypes.cast(ctypes.byref(cancel), ctypes.c_void_p) if cancel is not None else None
         self._check(lib().mb3d_cu_march(self._ctx, ctypes.byref(scene), precision, row0, rows, p, cp))
+        return out
+
+    def march_ex(self, scene, precision=FP32_FP64, row0=0, rows=None, out=None, band_rows=0, budget_ms=0.0,
+                 overflow_fail=False, progress=None, cancel=None):
+        """gpu::march with progress (a callable (rows_done, rows_total) -> bool,
+        True cancels), bands, the device time budget (CardError with status
+        ETIMEDOUT when it runs out: the same call again goes on) and the
+        reference card's overflow rule."""
+        rows = scene.height - row0 if rows is None else rows
+        if out is None:
+            out = np.zeros(rows * scene.width, dtype=SILIGHT)
+        p, _ = _ptr(out)
+        self._order(out)
+        o = MarchOpts()
+        o.band_rows, o.overflow_fail, o.budget_ms = band_rows, int(bool(overflow_fail)), budget_ms
+        if cancel is not None:
+            o.cancel = ctypes.cast(ctypes.byref(cancel), ctypes.c_void_p)
+        cb = None
+        if progress is not None:
+            cb = PROGRESS_FN(lambda done, total, user: 1 if progress(done, total) else 0)
+            o.progress = cb
+        self._check(lib().mb3d_cu_march_ex(self._ctx, ctypes.byref(scene), precision, row0, rows, p, ctypes.byref(o)))
         return out
 
     def post_on_card(self, scene, gbuf, passes=POST_SHADOW | POST_DEAO, precision=FP32_FP64, row0=0, rows=None):

@@ -60,11 +60,40 @@ def test_init_without_device_fails_loudly():
         assert e.status in (mb3dcu.ENODEV, mb3dcu.EIO)
 
 
-def test_stats_layout():
-    # mb3d_cu_stats: 5 floats and 2 uint32 (padded to 32 bytes), de_evals,
-    # orbit_its[6], 2 uint32, the march's 4 lane counters
-    assert ctypes.sizeof(mb3dcu.Stats) == 32 + 8 + 48 + 8 + 32
-    assert mb3dcu.Stats.march_lane_its.offset == 96
+# the ctypes mirrors of the header's structs (C name, ctypes class)
+MIRRORS = [("mb3d_cu_slot", "Slot"), ("mb3d_cu_light", "Light"), ("mb3d_cu_scene", "Scene"),
+           ("mb3d_cu_stats", "Stats"), ("mb3d_cu_tune", "Tune"), ("mb3d_cu_mc_req", "McReq"),
+           ("mb3d_cu_mc_res", "McRes"), ("mb3d_cu_mc_light", "McLight"), ("mb3d_cu_mc_opts", "McOpts"),
+           ("mb3d_cu_mc_out", "McOut"), ("mb3d_cu_mc_paint_opts", "McPaintOpts"), ("mb3d_cu_ssao_opts", "SsaoOpts"),
+           ("mb3d_cu_march_opts", "MarchOpts")]
+
+
+def test_every_struct_mirror_matches_the_header(tmp_path):
+    """Size and every field offset of each ctypes mirror against the C
+    compiler's layout of include/mb3d_cu.h (gcc, the host ABI)."""
+    import subprocess
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mb3d_cu.h"', "int main(void) {"]
+    for cname, pyname in MIRRORS:
+        cls = getattr(mb3dcu, pyname)
+        lines.append(f'printf("{pyname} size %zu\\n", sizeof({cname}));')
+        for f in cls._fields_:
+            lines.append(f'printf("{pyname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    checked = 0
+    for line in out:
+        if not line:
+            continue
+        pyname, field, value = line.split()
+        cls = getattr(mb3dcu, pyname)
+        want = ctypes.sizeof(cls) if field == "size" else getattr(cls, field).offset
+        assert want == int(value), (pyname, field, want, value)
+        checked += 1
+    assert checked > 100
 
 
 def test_null_arguments_fail_on_the_host():

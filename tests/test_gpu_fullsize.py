@@ -1,0 +1,138 @@
+"""Parity at the workloads' own sizes, pixel by pixel, against the oracle.
+
+The other parity tests run reduced pictures; these run the configurations'
+full sizes through the C ABI and compare every pixel (or a seeded sample of
+rows where the oracle would take minutes) with the oracle, the C++ FP64
+restatement of the reference CPU renderer:
+
+  - the hybrid frame, 1920x1080, whole (march, hard shadows, 17-ray DE AO);
+  - two frames of the 1280x720 Menger IFS + Amazing Box flight;
+  - the deep zoom at 1920x1080 (view width 1e-6) on 48 seeded rows;
+  - the Monte Carlo tracer's FP64 rays on two 1920x16 row strips of the
+    1920x1080 hybrid frame.
+
+Per-pixel figures: the share of the pixels both hit whose relative depth
+error |t - t_oracle| / t_oracle (t in step widths) is within 1e-6 (the FP64
+drop-in) or 1e-4 (the mixed march), and the hit/miss agreement.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import mb3dcu
+import oracle_py as O
+import scenes
+from gbcompare import compare, depth
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# the mixed march's share of both-hit pixels within 1e-4 relative depth of
+# the oracle on the full frames
+MIXED_WITHIN_1E4 = 0.995
+
+
+def zc(sc):
+    p = O.params(sc)
+    return p[7], p[6]
+
+
+def rel_depth(a, b, sc):
+    """Relative depth error of the pixels both hit (t from zpos, step widths)."""
+    both = mb3dcu.hit_mask(a) & mb3dcu.hit_mask(b)
+    da, db = depth(a[both], *zc(sc)), depth(b[both], *zc(sc))
+    return np.abs(da - db) / np.maximum(np.abs(db), 1e-30)
+
+
+def post_agreement(a, b):
+    """Hard shadow bit of light 1 and DE AO of the pixels both hit."""
+    both = mb3dcu.hit_mask(a) & mb3dcu.hit_mask(b)
+    sh = ((a["shadow"] & 0x400) == (b["shadow"] & 0x400))[both].mean()
+    dao = np.abs(a["amb_shadow"].astype(np.int64) - b["amb_shadow"].astype(np.int64))[both] / 16383.0
+    return float(sh), float(dao.mean()), float((dao > 0.1).mean())
+
+
+@pytest.fixture(scope="module")
+def c2_full():
+    sc = scenes.c2_hybrid()
+    ref = O.deao(sc, O.shadows(sc, O.march(sc, mb3dcu.SILIGHT), per_pixel=True))
+    return sc, ref
+
+
+def test_c2_full_frame_fp64(card, c2_full):
+    sc, ref = c2_full
+    g = card.render(sc, mb3dcu.FP64)
+    r = compare(g, ref, *zc(sc))
+    assert r["hit_agree"] >= 0.9999, r
+    assert r["exact"] >= 0.95, r
+    rel = rel_depth(g, ref, sc)
+    assert (rel <= 1e-6).mean() >= 0.999, np.quantile(rel, [0.5, 0.99, 0.999])
+    sh, dao, dao_far = post_agreement(g, ref)
+    assert sh >= 0.999 and dao < 0.002 and dao_far < 0.002, (sh, dao, dao_far)
+
+
+def test_c2_full_frame_mixed(card, c2_full):
+    sc, ref = c2_full
+    g = card.render(sc, mb3dcu.FP32_FP64)
+    r = compare(g, ref, *zc(sc))
+    assert r["hit_agree"] >= 0.999, r
+    rel = rel_depth(g, ref, sc)
+    assert np.median(rel) <= 1e-5, np.quantile(rel, [0.5, 0.99])
+    assert (rel <= 1e-4).mean() >= MIXED_WITHIN_1E4, np.quantile(rel, [0.5, 0.99, 0.999])
+    assert r["normal_cos_mean"] > 0.99, r
+    sh, dao, dao_far = post_agreement(g, ref)
+    assert sh >= 0.995 and dao < 0.005 and dao_far < 0.01, (sh, dao, dao_far)
+
+
+@pytest.mark.parametrize("k", [37, 150])
+def test_c4_frames_full_size(card, k):
+    sc = scenes.c4_frames(240)[k]
+    assert (sc.width, sc.height) == (1280, 720)
+    ref = O.shadows(sc, O.march(sc, mb3dcu.SILIGHT), per_pixel=True)
+    g64 = card.render(sc, mb3dcu.FP64)
+    r = compare(g64, ref, *zc(sc))
+    assert r["hit_agree"] >= 0.9999 and r["exact"] >= 0.95, r
+    assert (rel_depth(g64, ref, sc) <= 1e-6).mean() >= 0.999
+    assert post_agreement(g64, ref)[0] >= 0.999
+    gm = card.render(sc, mb3dcu.FP32_FP64)
+    rm = compare(gm, ref, *zc(sc))
+    assert rm["hit_agree"] >= 0.999, rm
+    rel = rel_depth(gm, ref, sc)
+    assert (rel <= 1e-4).mean() >= MIXED_WITHIN_1E4, np.quantile(rel, [0.5, 0.99, 0.999])
+    assert post_agreement(gm, ref)[0] >= 0.995
+
+
+def c3_scene(w, h):
+    f = json.load(open(os.path.join(HERE, "golden", "c3_point.json")))
+    return scenes.c3_deep_zoom(f["point"], f["view_dir"], w, h)
+
+
+def test_c3_full_size_row_sample(card):
+    sc = c3_scene(1920, 1080)
+    rows = np.sort(np.random.default_rng(3).choice(1080, 48, replace=False))
+    want = np.concatenate([O.march(sc, mb3dcu.SILIGHT, int(y), 1) for y in rows])
+    assert mb3dcu.hit_mask(want).mean() > 0.5
+    for prec in (mb3dcu.FP64, mb3dcu.FP32_FP64):
+        got = card.march(sc, prec).reshape(1080, 1920)[rows].reshape(-1)
+        r = compare(got, want, *zc(sc))
+        assert r["hit_agree"] >= 0.999, (prec, r)
+        rel = rel_depth(got, want, sc)
+        assert (rel <= 1e-4).mean() >= 0.999, (prec, np.quantile(rel, [0.5, 0.99, 0.999]))
+        if prec == mb3dcu.FP64:
+            assert (rel <= 1e-6).mean() >= 0.99, np.quantile(rel, [0.5, 0.99])
+
+
+def test_mc_c5_fp64_row_strips(card):
+    sc = scenes.c5_mc()
+    lv = mb3dcu.mc_light_default(sc)
+    for y0 in (300, 700):
+        opts = mb3dcu.mc_opts(4, depth=scenes.C5_DEPTH, rect=(0, y0, 1920, 16))
+        got = card.mc_render(sc, opts, lv, mb3dcu.FP64)
+        want = O.mc_render(sc, lv, opts)
+        assert (got["hit"] == want["hit"]).mean() >= 0.999
+        scale = want["radiance"].max()
+        close = np.all(np.abs(got["radiance"] - want["radiance"]) <= 1e-5 * scale, axis=2)
+        assert close.mean() >= 0.97, (y0, close.mean())
+        assert abs(got["radiance"].mean() - want["radiance"].mean()) <= 0.01 * abs(want["radiance"].mean())

@@ -243,3 +243,49 @@ def test_errors_and_cancel(card):
     assert e.value.status == mb3dcu.ECANCELED
     # the context still works after the failures
     assert mb3dcu.hit_mask(card.march(sc, mb3dcu.FP64)).mean() > 0.05
+
+
+def _six_lights(sc):
+    """All six lights on, spread around the object; every light casts shadows."""
+    import math
+    for i in range(6):
+        sc.lights[i] = mb3dcu.Light(1, 0, (i * 60.0 - 150.0) * math.pi / 180.0, (35.0 - 12.0 * i) * math.pi / 180.0)
+    sc.shadow_lights = 0x3F
+    return sc
+
+
+def test_six_light_hard_shadows(card):
+    """The hard shadow pass with six lights (one shadow bit each,
+    0x400 << light) on the oracle's G-buffer, against hard_shadow_row of
+    the oracle (src/calc.rs:2777-2898) per light."""
+    sc = _six_lights(scenes.scaled(scenes.c2_hybrid(), 240, 135))
+    ref = O.march(sc, mb3dcu.SILIGHT)
+    obj = mb3dcu.hit_mask(ref)
+    b = O.shadows(sc, ref.copy(), per_pixel=True)
+    assert all(0.05 < ((b["shadow"] & (0x400 << k)) != 0)[obj].mean() < 0.999 for k in range(6))
+    for prec, agree in ((mb3dcu.FP64, 0.999), (mb3dcu.FP32_FP64, 0.99)):
+        a = card.post_on_card(sc, ref.copy(), mb3dcu.POST_SHADOW, prec)
+        for light in range(6):
+            bit = 0x400 << light
+            same = ((a["shadow"] & bit) == (b["shadow"] & bit))[obj].mean()
+            assert same >= agree, (prec, light, same)
+        assert ((a["shadow"] & 0x3FF) == (ref["shadow"] & 0x3FF)).all()  # the step count is kept
+
+
+@pytest.mark.parametrize("radius", [1.0, 3.0])
+def test_soft_shadow(card, radius):
+    """The soft shadow (calcHSsoft, src/calc.rs:2901-2979): a 6-bit light
+    value in bits 10..15 for the last selected light, against the oracle."""
+    sc = scenes.scaled(scenes.c2_hybrid(), 240, 135)
+    sc.shadow_soft, sc.soft_radius = 1, radius
+    ref = O.march(sc, mb3dcu.SILIGHT)
+    obj = mb3dcu.hit_mask(ref)
+    b = O.shadows(sc, ref.copy(), per_pixel=True)
+    vb = (b["shadow"] >> 10).astype(np.int64)
+    assert (vb[obj] < 63).mean() > 0.05  # some pixels are in (part) shadow
+    for prec, tol, share in ((mb3dcu.FP64, 1, 0.999), (mb3dcu.FP32_FP64, 2, 0.98)):
+        a = card.post_on_card(sc, ref.copy(), mb3dcu.POST_SHADOW, prec)
+        va = (a["shadow"] >> 10).astype(np.int64)
+        d = np.abs(va - vb)[obj]
+        assert (d <= tol).mean() >= share, (prec, radius, (d <= tol).mean(), d.max())
+        assert d.mean() < 0.5, (prec, radius, d.mean())
