@@ -497,6 +497,15 @@ int mb3d_cu_dn_gradient(mb3d_cu_dn *dn, int n, int h, int w, const float *radian
 int mb3d_cu_dn_conv_check(mb3d_cu_ctx *ctx, int n, int h, int w, int cin, int cout, const float *x, const float *wt,
                           const float *b, const float *dy, float *y, float *dx, float *dw, float *db);
 
+/* Test hook of the tensor-core pipeline's bounded waits: one 16 -> 16
+ * channel convolution of a 16 x 16 picture whose waits give up after
+ * wait_us microseconds (1 .. 2e6).  With no_issue the TMA and MMA lanes
+ * issue nothing, so the epilogue's first accumulator wait runs out with no
+ * copy or MMA in flight: the kernel frees its tensor memory and returns,
+ * and the call answers MB3D_CU_EIO ("a pipeline wait ran out"); the context
+ * stays usable.  No counterpart in the reference (it has no network). */
+int mb3d_cu_dn_wait_check(mb3d_cu_ctx *ctx, double wait_us, int no_issue);
+
 /* The march without any device allocation, for callers that cannot
  * allocate GPU memory: a renderer whose device memory belongs to another
  * allocator (an engine's fixed pool, PyTorch's caching allocator), which may

@@ -145,9 +145,13 @@ __device__ __forceinline__ float smooth_of(const DevParams &p, R rout, R rold, c
     }
 }
 
-template <typename R, int FM, bool COUNT = false, bool FULL = false>
-__device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], float ms_de_stop, DECount *cnt = nullptr,
+// The position c is double (the FP64 march, and the single precision DE of
+// a double precision position) or, for the single precision DE only, float
+// (P = float: the bulk march keeps its position in single precision).
+template <typename R, int FM, bool COUNT = false, bool FULL = false, typename P = double>
+__device__ __forceinline__ DEr de_lock(const DevParams &p, const P c[3], float ms_de_stop, DECount *cnt = nullptr,
                                        DEstate *st = nullptr, bool calc_sit = false, int max_add = 0) {
+    static_assert(sizeof(P) == 8 || sizeof(R) == 4, "a single precision position needs the single precision DE");
     if (COUNT) cnt->evals++;
     DEr out;
     out.need64 = false;
@@ -227,22 +231,31 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
         R v[4][4], j[4][3], rout[4];
         float corr[3] = {1.f, 1.f, 1.f};
         const double off = (double)p.de_offset;
+        R cr[3], orr[3];  // the centre and the offset coordinates
         if (sizeof(R) == 4) {
             // (o - cf is exact in single precision where the two are within a
             // factor of 2 of each other, i.e. wherever |c| >= the offset)
 #pragma unroll
             for (int k = 0; k < 3; k++) {
                 float cf = (float)c[k];
-                float o = (float)(c[k] + off);
+                float o = sizeof(P) == 4 ? cf + p.de_offset : (float)((double)c[k] + off);
                 float h = o - cf;
                 if (!(h > 0.0f)) out.need64 = true;
                 corr[k] = __fdividef(p.de_offset, fmaxf(h, 1e-30f));
+                cr[k] = (R)cf;
+                orr[k] = (R)o;
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                cr[k] = (R)c[k];
+                orr[k] = (R)((double)c[k] + off);
             }
         }
 #pragma unroll
         for (int q = 0; q < 4; q++) {
 #pragma unroll
-            for (int k = 0; k < 3; k++) v[q][k] = (R)((q == k + 1) ? c[k] + off : c[k]);
+            for (int k = 0; k < 3; k++) v[q][k] = (q == k + 1) ? orr[k] : cr[k];
             v[q][3] = R(0);
             if (p.do_julia) {
                 j[q][0] = param_f<R>(p, p.ju[0], p.ju_f[0]);
@@ -271,11 +284,76 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
                 J[0][k] = make_float2((float)j[0][k], (float)j[1][k]);
                 J[1][k] = make_float2((float)j[2][k], (float)j[3][k]);
             }
-            for (;;) {
+            // after a counted iteration: the lengths, the offset orbits' own
+            // bailouts, and whether the centre stops
+            auto counted = [&]() -> bool {
+                it += 1;
+                const float2 r01 = psq3(V[0]), r23 = psq3(V[1]);
+                rout[0] = r01.x;
+                const float rn[4] = {0.0f, r01.y, r23.x, r23.y};
+#pragma unroll
+                for (int q = 1; q < 4; q++) {
+                    const bool stop = live[q] && rn[q] > (float)rstop3d;
+                    if (FULL && q == 3) otrap3 = (live[3] && rn[3] < otrap3) ? rn[3] : otrap3;
+                    rout[q] = live[q] ? rn[q] : rout[q];
+                    if (stop) {
+                        const int pq = q >> 1;
+                        float vf[4];
+#pragma unroll
+                        for (int k = 0; k < 3; k++) vf[k] = (q & 1) ? V[pq][k].y : V[pq][k].x;
+                        vf[3] = 0.f;
+                        lr_frozen[q] = log_len2_f(vf);
+                    }
+                    live[q] = live[q] && !stop;
+                }
+                return it >= max_it || rout[0] > rstop;
+            };
+            auto before = [&]() {
                 if (FULL) {
                     rold0 = rout[0];
                     rold3 = live[3] ? rout[3] : rold3;
                 }
+            };
+            if ((FM & FKIND_BOX) && p.sched == SCHED_BOX2_IP8) {
+                // Amazing Box, Amazing Box, Integer Power 8, repeating from the
+                // first iteration, all counted: the slots' order unrolled
+                const float scale = p.slots[0].of[0], min_r = p.slots[0].of[1], fold = p.slots[0].of[2];
+                const float zmul = p.slots[1].of[1];
+                for (int g = 0; g < (1 << 20); g++) {
+                    before();
+                    f_amazing_box_x2(scale, min_r, fold, V[0], J[0]);
+                    f_amazing_box_x2(scale, min_r, fold, V[1], J[1]);
+                    if (COUNT) cnt->its[0] += 4;
+                    n = 0;
+                    if (counted()) break;
+                    before();
+                    f_amazing_box_x2(scale, min_r, fold, V[0], J[0]);
+                    f_amazing_box_x2(scale, min_r, fold, V[1], J[1]);
+                    if (COUNT) cnt->its[0] += 4;
+                    if (counted()) break;
+                    before();
+                    f_int_pow8_x2(zmul, V[0], J[0]);
+                    f_int_pow8_x2(zmul, V[1], J[1]);
+                    if (COUNT) cnt->its[1] += 4;
+                    n = 1;
+                    if (counted()) break;
+                }
+                goto done_x2;
+            }
+            if (p.sched == SCHED_IP8) {
+                // one Integer Power 8 slot, all iterations counted
+                const float zmul = p.slots[0].of[1];
+                for (int g = 0; g < (1 << 20); g++) {
+                    before();
+                    f_int_pow8_x2(zmul, V[0], J[0]);
+                    f_int_pow8_x2(zmul, V[1], J[1]);
+                    if (COUNT) cnt->its[0] += 4;
+                    if (counted()) break;
+                }
+                goto done_x2;
+            }
+            for (;;) {
+                before();
                 int guard = 0;
                 while (btmp <= 0) {
                     n += 1;
@@ -308,26 +386,7 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const double c[3], fl
                         continue;
                     }
                 }
-                it += 1;
-                const float2 r01 = psq3(V[0]), r23 = psq3(V[1]);
-                rout[0] = r01.x;
-                const float rn[4] = {0.0f, r01.y, r23.x, r23.y};
-#pragma unroll
-                for (int q = 1; q < 4; q++) {
-                    const bool stop = live[q] && rn[q] > (float)rstop3d;
-                    if (FULL && q == 3) otrap3 = (live[3] && rn[3] < otrap3) ? rn[3] : otrap3;
-                    rout[q] = live[q] ? rn[q] : rout[q];
-                    if (stop) {
-                        const int pq = q >> 1;
-                        float vf[4];
-#pragma unroll
-                        for (int k = 0; k < 3; k++) vf[k] = (q & 1) ? V[pq][k].y : V[pq][k].x;
-                        vf[3] = 0.f;
-                        lr_frozen[q] = log_len2_f(vf);
-                    }
-                    live[q] = live[q] && !stop;
-                }
-                if (it >= max_it || rout[0] > rstop) break;
+                if (counted()) break;
             }
         done_x2:
 #pragma unroll

@@ -44,6 +44,8 @@ struct DevParams {
     int32_t refill_shadow, refill_ao;   // ... of the shadow and DE AO ray kernels
     int32_t blocks_march32;             // resident blocks of the single precision march
     int32_t hand_near;                  // the mixed march hands over at the first DE < hand_margin x DE stop
+    int32_t sched;                      // SCHED_*: the slots' order when it is one the DE loop has unrolled
+    int32_t pad_s;
     float d_rstop_f, rstop3d_f, soft_radius, hs_max_len_mul;
     double d_rstop, rstop3d, zcorr, zc_mul;
     double zend, step_width, fov_y, coord_eps;
@@ -64,6 +66,11 @@ struct DevParams {
     // first warp of the call asked (their queue counters stay resumable)
     unsigned long long budget_ns;
 };
+
+// slot orders the single precision DE loop knows at compile time
+#define SCHED_GENERIC 0
+#define SCHED_BOX2_IP8 1  // Amazing Box x2, Integer Power 8 x1, repeating from slot 0
+#define SCHED_IP8 2       // one Integer Power 8 slot
 
 // the counters' slots (unsigned int) the march kernels share with the host
 #define CNT_HAND 0        // hand-over list length

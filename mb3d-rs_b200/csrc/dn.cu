@@ -578,4 +578,44 @@ int mb3d_cu_dn_conv_check(mb3d_cu_ctx *ctx, int n, int h, int w, int cin, int co
     return 0;
 }
 
+int mb3d_cu_dn_wait_check(mb3d_cu_ctx *ctx, double wait_us, int no_issue) {
+    if (!ctx) return dn_fail(MB3D_CU_EINVAL, "NULL argument");
+    if (!(wait_us >= 1.0 && wait_us <= 2e6)) return dn_fail(MB3D_CU_EINVAL, "wait_us outside 1 .. 2e6");
+    if (cudaSetDevice(dn_device(ctx)) != cudaSuccess) return dn_fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    int khz = 0;
+    if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, dn_device(ctx)) != cudaSuccess || khz <= 0) khz = 2000000;
+    cudaStream_t s = dn_stream(ctx);
+    const int n = 1, h = 16, w = 16, c = 16;
+    const size_t m = (size_t)n * h * w, nw = (size_t)c * 9 * c;
+    bf16 *din = nullptr, *dout = nullptr, *dwf = nullptr, *dwb = nullptr;
+    float *dwt = nullptr;
+    bool ok = cudaMalloc((void **)&din, m * c * 2) == cudaSuccess && cudaMalloc((void **)&dout, m * c * 2) == cudaSuccess &&
+              cudaMalloc((void **)&dwf, nw * 2) == cudaSuccess && cudaMalloc((void **)&dwb, nw * 2) == cudaSuccess &&
+              cudaMalloc((void **)&dwt, nw * 4) == cudaSuccess;
+    if (ok) {
+        cudaMemsetAsync(din, 0, m * c * 2, s);
+        cudaMemsetAsync(dwt, 0, nw * 4, s);
+        dn_cast_weights(dwt, c, c, dwf, dwb, s);
+    }
+    int r = -1;
+    if (ok) {
+        ConvArgs a;
+        a.in = din; a.wt = dwf; a.bias = nullptr; a.out = dout;
+        a.n = n; a.h = h; a.w = w; a.m = (int)m;
+        a.in_c = c; a.in_off = 0; a.cin = c;
+        a.out_c = c; a.out_off = 0; a.cout = c;
+        a.relu = 0; a.accumulate = 0;
+        a.wait_cycles = (long long)(wait_us * (double)khz * 1e-3);
+        a.no_issue = no_issue ? 1 : 0;
+        r = dn_conv(a, s);
+    }
+    cudaError_t e = cudaStreamSynchronize(s);
+    cudaFree(din); cudaFree(dout); cudaFree(dwf); cudaFree(dwb); cudaFree(dwt);
+    if (!ok) return dn_fail(MB3D_CU_ENOMEM, "device memory");
+    if (r) return dn_fail(MB3D_CU_EINVAL, "convolution launch arguments");
+    if (e != cudaSuccess) return dn_fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    if (dn_conv_error(s)) return dn_fail(MB3D_CU_EIO, "convolution: a pipeline wait ran out");
+    return 0;
+}
+
 }  // extern "C"

@@ -21,6 +21,12 @@ struct ConvArgs {
     // not positive are zero
     const __nv_bfloat16 *mask = nullptr;
     int mask_c = 0, mask_off = 0;
+    // the limit of every wait in the tensor-core pipeline, clock cycles (0:
+    // about one second); no_issue (a test of the limit): the TMA and MMA
+    // lanes issue nothing, so the epilogue's first wait runs out with no copy
+    // or MMA in flight
+    long long wait_cycles = 0;
+    int no_issue = 0;
 };
 
 // its weight gradient: dw[co][tap][ci] += sum_p dz[p][co] x[p + tap][ci]

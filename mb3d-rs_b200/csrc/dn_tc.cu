@@ -60,6 +60,8 @@ struct ConvTc {
     int stages, resident;
     uint32_t w_bytes, stage_bytes;
     int *err;
+    long long wait_cycles;  // the limit of every wait
+    int no_issue;           // (a test of the limit: the TMA and MMA lanes issue nothing)
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -72,7 +74,8 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
 }
 // bounded wait for the phase with parity `parity` to complete (the thread
 // sleeps in the barrier up to 20 us per try, woken by the phase's completion)
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int *abort) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const volatile int *abort,
+                                          long long limit = TC_WAIT_CYCLES) {
     long long t0 = clock64();
     for (;;) {
         uint32_t ok;
@@ -82,7 +85,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, const v
             : "r"(bar), "r"(parity), "r"(20000)
             : "memory");
         if (ok) return true;
-        if (*abort || clock64() - t0 > TC_WAIT_CYCLES) return false;
+        if (*abort || clock64() - t0 > limit) return false;
     }
 }
 
@@ -223,7 +226,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
     const uint32_t tmem = tmem_slot;
 
     if (warp == 0) {
-        if (lane == 0) {
+        if (lane == 0 && !a.no_issue) {
             // the TMA producer
             if (a.resident) {
                 mbar_expect_tx(smem_addr(&wbar), a.w_bytes);
@@ -235,7 +238,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                 tile_of(a, g, img, x0, y0);
                 for (int grp = 0; grp < groups; grp++, q++) {
                     const uint32_t s = q % (uint32_t)ns;
-                    if (q >= (uint32_t)ns && !mbar_wait(smem_addr(&empty[s]), ((q / ns) - 1) & 1, &abort_flag)) {
+                    if (q >= (uint32_t)ns && !mbar_wait(smem_addr(&empty[s]), ((q / ns) - 1) & 1, &abort_flag, a.wait_cycles)) {
                         abort_flag = 1;
                         break;
                     }
@@ -249,15 +252,15 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
             }
         }
     } else if (warp == 1) {
-        if (lane == 0) {
+        if (lane == 0 && !a.no_issue) {
             // the MMA issuer: nine taps per group; tile i accumulates in buffer i % 2
             const uint32_t idesc = idesc_bf16<BN>();
-            if (a.resident && !mbar_wait(smem_addr(&wbar), 0, &abort_flag)) abort_flag = 1;
+            if (a.resident && !mbar_wait(smem_addr(&wbar), 0, &abort_flag, a.wait_cycles)) abort_flag = 1;
             uint32_t q = 0;
             int i = 0;
             for (int g = blockIdx.x; g < total && !abort_flag; g += gridDim.x, i++) {
                 const int buf = i & 1;
-                if (i >= 2 && !mbar_wait(smem_addr(&acc_empty[buf]), ((i >> 1) - 1) & 1, &abort_flag)) {
+                if (i >= 2 && !mbar_wait(smem_addr(&acc_empty[buf]), ((i >> 1) - 1) & 1, &abort_flag, a.wait_cycles)) {
                     abort_flag = 1;
                     break;
                 }
@@ -265,7 +268,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                 const uint32_t d = tmem + (uint32_t)buf * COLS;
                 for (int grp = 0; grp < groups; grp++, q++) {
                     const uint32_t s = q % (uint32_t)ns;
-                    if (!mbar_wait(smem_addr(&full[s]), (q / ns) & 1, &abort_flag)) {
+                    if (!mbar_wait(smem_addr(&full[s]), (q / ns) & 1, &abort_flag, a.wait_cycles)) {
                         abort_flag = 1;
                         break;
                     }
@@ -300,7 +303,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
         int i = 0;
         for (int g = blockIdx.x; g < total; g += gridDim.x, i++) {
             const int buf = i & 1;
-            bool ready = mbar_wait(smem_addr(&acc_full[buf]), (i >> 1) & 1, &abort_flag);
+            bool ready = mbar_wait(smem_addr(&acc_full[buf]), (i >> 1) & 1, &abort_flag, a.wait_cycles);
             ready = __all_sync(0xffffffffu, ready);
             if (!ready) {
                 abort_flag = 1;
@@ -635,6 +638,8 @@ int dn_conv(const ConvArgs &a, cudaStream_t s) {
     c.tiles_x = (a.w + TILE_W - 1) / TILE_W;
     c.tiles_y = (a.h + TILE_H - 1) / TILE_H;
     c.err = err;
+    c.wait_cycles = a.wait_cycles > 0 ? a.wait_cycles : TC_WAIT_CYCLES;
+    c.no_issue = a.no_issue;
     c.stages = 2;
     c.resident = 0;
     c.w_bytes = 0;

@@ -155,7 +155,7 @@ template <typename R, int FM, bool COUNT>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 : MB3D_MIN_BLOCKS_MARCH) k_march(const __grid_constant__ DevParams p, int row0, int rows,
                                                mb3d_cu_silight *out, Hand *list, unsigned int *counters,
                                                unsigned long long *gcount) {
-    const bool MIXED = sizeof(R) == 4;
+    constexpr bool MIXED = sizeof(R) == 4;
     DECount cnt;
     if (COUNT) cnt.clear();
     const int tiles_x = (p.width + 7) / 8;
@@ -165,6 +165,9 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
     uint32_t pix = 0;
     int x = 0, ly = 0;
     double c[3] = {0, 0, 0}, vf[3] = {0, 0, 0};
+    // (the single precision march keeps its start point and direction in
+    // single precision and its position as start + direction x mzz)
+    float cf0[3] = {0.f, 0.f, 0.f}, vff[3] = {0.f, 0.f, 0.f};
     double mzz = 0.0, last_step = 0.0, last_de = 0.0;
     float ms = 0.f, rsf = 1.f, step_count = 0.f;
     int32_t seed = 0;
@@ -179,6 +182,13 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             if (x < p.width && ly < rows) {
                 pix = (uint32_t)ly * (uint32_t)p.width + (uint32_t)x;
                 pixel_ray(p, x, row0 + ly, c, vf);
+                if constexpr (MIXED) {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        cf0[k] = (float)c[k];
+                        vff[k] = (float)vf[k];
+                    }
+                }
                 mzz = 0.0;
                 ms = p.de_stop;
                 phase = PH_START;
@@ -193,7 +203,14 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
         double cur_de = 0.0;
         int cur_it = 0;
         if (phase != PH_IDLE) {
-            DEr r = de_lock<R, FM, COUNT>(p, c, ms, &cnt);
+            DEr r;
+            if constexpr (MIXED) {
+                const float t = (float)mzz;
+                const float cp[3] = {fmaf(vff[0], t, cf0[0]), fmaf(vff[1], t, cf0[1]), fmaf(vff[2], t, cf0[2])};
+                r = de_lock<R, FM, COUNT, false, float>(p, cp, ms, &cnt);
+            } else {
+                r = de_lock<R, FM, COUNT>(p, c, ms, &cnt);
+            }
             cur_it = r.it;
             double dtmp = r.de;
             int it = r.it;

@@ -231,6 +231,7 @@ def lib():
         L.mb3d_cu_dn_train_step.argtypes = [vp] + [ctypes.c_int] * 3 + [vp] * 4 + [ctypes.c_float, vp, ctypes.c_float, fp]
         L.mb3d_cu_dn_gradient.argtypes = [vp] + [ctypes.c_int] * 3 + [vp] * 4 + [ctypes.c_float, vp, fp, vp]
         L.mb3d_cu_dn_conv_check.argtypes = [vp] + [ctypes.c_int] * 5 + [vp] * 8
+        L.mb3d_cu_dn_wait_check.argtypes = [vp, ctypes.c_double, ctypes.c_int]
         L.mb3d_cu_mc_light_default.argtypes = [sp, ctypes.POINTER(McLight)]
         L.mb3d_cu_mc_batch.argtypes = [vp, sp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_uint32, vp]
         L.mb3d_cu_mc_render.argtypes = [vp, sp, ctypes.POINTER(McLight), ctypes.POINTER(McOpts), ctypes.c_int,
@@ -253,7 +254,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
-            "mb3d_cu_dn_conv_check"]
+            "mb3d_cu_dn_conv_check", "mb3d_cu_dn_wait_check"]
 
 NOALLOC_MAX_PIXELS = 65536
 

@@ -40,6 +40,26 @@ def test_conv_kernels_match_fp64(card, cin, cout, n, h, w):
     assert np.abs(db - dbe).max() <= 1e-3 * np.abs(dbe).max(), (cin, cout)
 
 
+def test_tensor_core_wait_runs_out_and_the_context_stays_usable(card):
+    """The convolution's pipeline waits are bounded by a launch parameter:
+    with its TMA and MMA lanes told to issue nothing, the epilogue's first
+    accumulator wait runs out after 2 ms (nothing in flight), the kernel
+    frees its tensor memory and the host reads an error status; the next
+    convolutions on the same context work."""
+    L = mb3dcu.lib()
+    assert L.mb3d_cu_dn_wait_check(card._ctx, 2000.0, 1) == mb3dcu.EIO
+    assert "wait ran out" in L.mb3d_cu_last_error().decode()
+    assert L.mb3d_cu_dn_wait_check(card._ctx, 2000.0, 0) == 0
+    rng = np.random.default_rng(11)
+    x = unet.bf16(rng.standard_normal((1, 9, 13, 16)))
+    wt = unet.bf16(rng.standard_normal((32, 9, 16)) * 0.1)
+    b = rng.standard_normal(32).astype(np.float32)
+    dy = unet.bf16(rng.standard_normal((1, 9, 13, 32)))
+    y = mb3dcu.conv_check(card, x, wt, b, dy)[0]
+    ye = unet.conv(x.astype(np.float64), wt.astype(np.float64), b.astype(np.float64))
+    assert np.abs(y - ye).max() <= np.abs(ye).max() / 128
+
+
 def _batch(rng, n, h, w):
     rad = rng.gamma(1.0, 0.4, (n, h, w, 3)).astype(np.float32)
     alb = rng.uniform(0, 1, (n, h, w, 3)).astype(np.float32)
