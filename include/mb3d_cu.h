@@ -207,6 +207,17 @@ typedef struct mb3d_cu_mc_out {
     uint8_t *hit;     /* w*h: a ray of the pixel met the object (McRecord.hit) */
 } mb3d_cu_mc_out;
 
+/* One pixel of a Monte Carlo picture (McRecord, src/mc.rs:194-217; 24
+ * bytes): the average colour of its rays (square roots with internal gamma
+ * 2), their average luminance and squared luminance, how many rays it has
+ * had, and whether one of them met the object. */
+typedef struct mb3d_cu_mc_record {
+    float col[3];
+    float ysum, ysqr;
+    uint16_t ray_count;
+    uint8_t hit, pad;
+} mb3d_cu_mc_record;
+
 /* Per-render counters the last call measured on the device. */
 typedef struct mb3d_cu_stats {
     float ms_march;       /* primary march (+ finish) kernels, CUDA events */

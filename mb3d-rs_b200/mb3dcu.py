@@ -183,6 +183,12 @@ SILIGHT = np.dtype([("normal", "<i2", (3,)), ("pad", "<u2"), ("zpos_fine", "<u4"
 assert SILIGHT.itemsize == 20
 
 
+# the Monte Carlo record (mb3d_cu_mc_record, McRecord: 24 bytes)
+MC_RECORD = np.dtype([("col", "<f4", (3,)), ("ysum", "<f4"), ("ysqr", "<f4"), ("ray_count", "<u2"), ("hit", "u1"),
+                      ("pad", "u1")])
+assert MC_RECORD.itemsize == 24
+
+
 class CardError(RuntimeError):
     def __init__(self, status, text):
         super().__init__(f"{text} (status {status})")

@@ -972,6 +972,183 @@ static void paint_recs(const float *col, const uint8_t *rays, size_t n, const mb
     }
 }
 
+// ---------------------------------------------------------------------------
+// the adaptive pass (src/mc.rs:2657-2834 calc_n and pixel, :3110-3300
+// pass_inner's set-up, :329-358 stats and avg_sqr_noise)
+
+static const double MC_MAX = 1096.6331584284585 - 2.718281828459045 + 2.0;  // src/mc.rs:37
+static inline double clamp_mc(double d) { return rclamp(d, -1.0, MC_MAX); }
+// YofSVec (src/svec.rs:38-40)
+static inline float luma_s(const float v[3]) { return rmaxf(v[0] * 0.3f + v[1] * 0.59f + v[2] * 0.11f, 0.0f); }
+static inline double rec_y(const mb3d_cu_mc_record &r) { return (double)r.ysum; }
+static inline double rec_noise(const mb3d_cu_mc_record &r) { return (double)r.ysqr - rec_y(r) * rec_y(r); }
+
+struct PassArgs {
+    const mb3d_cu_mc_record *snap;
+    int w, h;
+    bool skip_nonzero;
+    double avrg_vari;
+    float avrg_rcount;
+    int max_new;
+    uint32_t pass_nr;
+};
+
+// CalcN: how many more rays the pixel gets in this pass (x1, y1 1-based)
+static int calc_n(Tracer &t, const PassArgs &a, int x1, int y1, const mb3d_cu_mc_record &rec) {
+    const int w = a.w, h = a.h;
+    auto at = [&](int x, int y) -> const mb3d_cu_mc_record & { return a.snap[(size_t)(y - 1) * w + (x - 1)]; };
+    double maxyd = 0, maxyd2 = 0, maxnoise = 0;
+    int n = 0, n2 = 0, avg_rc = 0;
+    const double dt2 = rec_y(rec);
+    if (y1 > 1) {
+        const auto &r = at(x1, y1 - 1);
+        double dt = rec_y(r);
+        maxyd = (dt - dt2) * (dt - dt2);
+        maxnoise = rec_noise(r);
+        avg_rc = r.ray_count;
+        n += 1;
+        if (x1 > 1) {
+            const auto &r3 = at(x1 - 1, y1 - 1);
+            double dt3 = rec_y(r3);
+            maxyd += (dt2 - dt3) * (dt2 - dt3);
+            maxyd2 = (dt - dt3) * (dt - dt3);
+            maxnoise = rmax(maxnoise, rec_noise(r3));
+            avg_rc += r3.ray_count;
+            n += 1;
+            n2 += 1;
+        }
+        if (x1 < w) {
+            const auto &r3 = at(x1 + 1, y1 - 1);
+            double dt3 = rec_y(r3);
+            maxyd += (dt2 - dt3) * (dt2 - dt3);
+            maxyd2 += (dt - dt3) * (dt - dt3);
+            maxnoise = rmax(maxnoise, rec_noise(r3));
+            avg_rc += r3.ray_count;
+            n += 1;
+            n2 += 1;
+        }
+    }
+    double dt = 0;
+    if (x1 > 1) {
+        const auto &r = at(x1 - 1, y1);
+        dt = rec_y(r);
+        maxyd += (dt - dt2) * (dt - dt2);
+        maxnoise = rmax(maxnoise, rec_noise(r));
+        avg_rc += r.ray_count;
+        n += 1;
+    }
+    if (x1 < w) {
+        const auto &r = at(x1 + 1, y1);
+        double dt3 = rec_y(r);
+        maxyd += (dt3 - dt2) * (dt3 - dt2);
+        if (x1 > 1) {
+            maxyd2 += (dt - dt3) * (dt - dt3);
+            n2 += 1;
+        }
+        maxnoise = rmax(maxnoise, rec_noise(r));
+        avg_rc += r.ray_count;
+        n += 1;
+    }
+    if (y1 < h) {
+        const auto &r = at(x1, y1 + 1);
+        double dty = rec_y(r);
+        maxyd += (dty - dt2) * (dty - dt2);
+        maxnoise = rmax(maxnoise, rec_noise(r));
+        avg_rc += r.ray_count;
+        n += 1;
+        if (x1 > 1) {
+            const auto &r3 = at(x1 - 1, y1 + 1);
+            double dt3 = rec_y(r3);
+            maxyd += (dt2 - dt3) * (dt2 - dt3);
+            maxyd2 += (dty - dt3) * (dty - dt3);
+            maxnoise = rmax(maxnoise, rec_noise(r3));
+            avg_rc += r3.ray_count;
+            n += 1;
+            n2 += 1;
+        }
+        if (x1 < w) {
+            const auto &r3 = at(x1 + 1, y1 + 1);
+            double dt3 = rec_y(r3);
+            maxyd += (dt2 - dt3) * (dt2 - dt3);
+            maxyd2 += (dty - dt3) * (dty - dt3);
+            maxnoise = rmax(maxnoise, rec_noise(r3));
+            avg_rc += r3.ray_count;
+            n += 1;
+            n2 += 1;
+        }
+    }
+    const double nf = (double)(n > 1 ? n : 1), n2f = (double)(n2 > 1 ? n2 : 1);
+    maxyd /= nf;
+    maxyd2 /= n2f;
+    const double dt3 = ((double)rec.ysqr - dt2 * dt2) / (rmax(dt2, 0.0) + 0.01);
+    const double dm = !rec.hit ? 0.0
+                               : rmax(rmax(maxyd, maxyd2) - 20.0 * a.avrg_vari, 0.0) *
+                                     rclamp((double)rec.ray_count - (double)avg_rc / nf, -4.0, 4.0);
+    const double q = dt2 / std::sqrt(1.0 + (dt2 * 0.9) * (dt2 * 0.9));
+    const double d = rmax(rmax(dt3, maxnoise) / rmax(q * (double)rec.ray_count, 0.3) - dm, 0.0);
+    const double d2 = d * 4.0 / a.avrg_vari;
+    if (d2 >= 1.0) return (int)rte(rmin((double)a.avrg_rcount * 0.5 + 8.0, d2));
+    if (t.rand() * 1.1 - 0.1 > rmax(d2, 0.0)) return 0;
+    return 1;
+}
+
+// one pixel of TMCCalcThread.Execute: rays in rounds until its noise is low
+static void mc_pixel(Tracer &t, const PassArgs &a, bool sqr, int x1, int y, mb3d_cu_mc_record &rec) {
+    t.seed = mc_seed_of(x1, y, 0x80000000u | a.pass_nr);
+    int total;
+    if (rec.ray_count == 0) total = 4;
+    else if (a.skip_nonzero) return;
+    else total = calc_n(t, a, x1, y + 1, rec);
+    bool hit = rec.hit != 0;
+    for (int round = 0; round < 100000; round++) {
+        if (total + (int)rec.ray_count > 65535) total = 65535 - (int)rec.ray_count;
+        float at[3] = {0.f, 0.f, 0.f};
+        double sum = 0.0, sqr_sum = 0.0;
+        int itcount = 0;
+        const uint32_t rc = rec.ray_count;
+        for (int i = 0; i < total; i++) {
+            float L[3];
+            t.aov = false;
+            t.ray(x1, y, rc + (uint32_t)i, L);
+            hit = hit || t.hit;
+            float sv[3];
+            for (int k = 0; k < 3; k++) sv[k] = rclampf(L[k], 0.0f, 400.0f);
+            double yv = (double)luma_s(sv);
+            sqr_sum += yv * yv;
+            sum += yv;
+            for (int k = 0; k < 3; k++) at[k] = at[k] + sv[k];
+            itcount += 1;
+        }
+        rec.hit = hit ? 1 : 0;
+        if (itcount == 0) return;
+        const double dtmp = (double)rec.ysum, zz = (double)rec.ysqr;
+        const int itmp = rec.ray_count;
+        const double yy = itmp != 0 ? rmax((zz - dtmp * dtmp) * 10.0, 0.03) : 0.0;
+        float light[3];
+        if (sqr) {
+            const float inv = 1.0f / (float)itcount;
+            for (int k = 0; k < 3; k++) {
+                float v = at[k] * inv;
+                light[k] = (v > 0.0f ? std::sqrt(v) : v) * (float)itcount;
+            }
+        } else {
+            for (int k = 0; k < 3; k++) light[k] = at[k];
+        }
+        const double xx = 1.0 / (double)(itmp + itcount);
+        for (int k = 0; k < 3; k++) rec.col[k] = (float)clamp_mc(((double)rec.col[k] * itmp + (double)light[k]) * xx);
+        rec.ysum = (float)clamp_mc((dtmp * itmp + sum) * xx);
+        rec.ysqr = (float)clamp_mc((zz * itmp + sqr_sum) * xx);
+        rec.ray_count = (uint16_t)(itmp + itcount);
+        const double mean = sum / (double)itcount;
+        if (itmp != 0 && (int)rec.ray_count < a.max_new && (mean - dtmp) * (mean - dtmp) > yy) {
+            const int m = std::max(std::min(itmp, itcount), 4);
+            total = (int)rte(std::sqrt((mean - dtmp) * (mean - dtmp) / yy) * (double)m);
+            continue;
+        }
+        return;
+    }
+}
+
 }  // namespace oracle
 
 using namespace oracle;
@@ -1042,6 +1219,57 @@ int oracle_mc_render(const mb3d_cu_scene *sc, const mb3d_cu_mc_light *lv, const 
         });
     for (auto &t : ts) t.join();
     if (inside) *inside = n_inside.load();
+    return 0;
+}
+
+/* One pass of the adaptive Monte Carlo renderer over the whole picture
+ * (mc::pass, src/mc.rs:3110-3300 with the CPU's per-pixel loop): recs holds
+ * width*height records, updated in place.  The options' rays, ray0 and
+ * rectangle are not used. */
+int oracle_mc_pass(const mb3d_cu_scene *sc, const mb3d_cu_mc_light *lv, const mb3d_cu_mc_opts *o, uint32_t pass_nr,
+                   mb3d_cu_mc_record *recs, int threads) {
+    McCtx c;
+    std::string err;
+    if (!make_ctx(*sc, *lv, o->depth, o->secant, o->soft_shadow_radius, c, err)) return -22;
+    const int w = sc->width, h = sc->height;
+    const size_t n = (size_t)w * h;
+    // StartCalc / CalcAvrgNoise (src/mc.rs:3226-3235, stats :329-358)
+    bool fresh = true, zero_counts = false;
+    double rsum = 0.0, noise_sum = 0.0;
+    for (size_t i = 0; i < n; i++) {
+        if (recs[i].ray_count != 0) fresh = false;
+        if (recs[i].ray_count == 0) {
+            zero_counts = true;
+            continue;
+        }
+        rsum += (double)recs[i].ray_count;
+        noise_sum += rmax(rec_noise(recs[i]) / (double)recs[i].ray_count, 0.0);
+    }
+    const double l = (double)(n > 0 ? n : 1);
+    const double avrg_sqr_noise = fresh ? 1.0 : rmax(noise_sum / l + 0.002, 0.002);
+    const float avrg_rcount = fresh ? 0.0f : (float)(rsum / l);
+    PassArgs a;
+    std::vector<mb3d_cu_mc_record> snap(recs, recs + n);
+    a.snap = snap.data();
+    a.w = w;
+    a.h = h;
+    a.skip_nonzero = fresh ? true : zero_counts;
+    a.avrg_vari = rmax(avrg_sqr_noise, 0.001);
+    a.avrg_rcount = avrg_rcount;
+    a.max_new = (int)std::round((avrg_rcount + avrg_rcount * avrg_rcount * 0.2f) * 10.0f);  // (f32, as the reference)
+    a.pass_nr = pass_nr;
+    if (threads < 1) threads = (int)std::thread::hardware_concurrency();
+    if (threads < 1) threads = 1;
+    halton_seq();
+    const bool sqr = lv->sqr != 0;
+    std::vector<std::thread> ts;
+    for (int t = 0; t < threads; t++)
+        ts.emplace_back([&, t]() {
+            Tracer tr(&c);
+            for (int y = t; y < h; y += threads)
+                for (int x = 0; x < w; x++) mc_pixel(tr, a, sqr, x + 1, y, recs[(size_t)y * w + x]);
+        });
+    for (auto &t : ts) t.join();
     return 0;
 }
 

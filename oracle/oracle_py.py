@@ -38,6 +38,7 @@ def lib():
         L.oracle_render_rows.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int]
         L.oracle_mc_render.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int]
         L.oracle_mc_batch.argtypes = [vp, ctypes.c_int, vp, ctypes.c_uint32, vp, ctypes.c_int]
+        L.oracle_mc_pass.argtypes = [vp, vp, vp, ctypes.c_uint32, vp, ctypes.c_int]
         L.oracle_mc_halton.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
         L.oracle_mc_halton.restype = None
         L.oracle_mc_seed_of.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
@@ -141,6 +142,16 @@ def mc_render(scene, light, opts, threads=0):
                                 rad.ctypes.data, alb.ctypes.data, nrm.ctypes.data, dep.ctypes.data, hit.ctypes.data,
                                 ctypes.byref(inside), threads))
     return dict(radiance=rad, albedo=alb, normal=nrm, depth=dep, hit=hit, inside=inside.value)
+
+
+def mc_pass(scene, light, opts, pass_nr, recs, threads=0):
+    """One adaptive Monte Carlo pass (mc::pass, src/mc.rs:3110-3300) over
+    the whole picture: recs (a numpy array of mb3dcu.MC_RECORD, width*height)
+    is updated in place and returned."""
+    assert recs.flags["C_CONTIGUOUS"] and recs.size == scene.width * scene.height
+    _chk(lib().oracle_mc_pass(ctypes.addressof(scene), ctypes.addressof(light), ctypes.addressof(opts), pass_nr,
+                              recs.ctypes.data, threads))
+    return recs
 
 
 def mc_batch(scene, reqs, secant=True, threads=0):

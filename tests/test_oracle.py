@@ -391,3 +391,32 @@ def test_ssao_leaves_the_background_and_stays_in_range():
             o = O.ssao24(g, w, h, 300.0, 0.001, threshold=1.5, border_mirror=mirror, t0=t0)
             assert (o["amb_shadow"][:w * 5] == 777).all()
             assert (o["amb_shadow"][w * 5:] <= 16383).all()
+
+
+def test_mc_passes_converge():
+    """mc.rs's passes_converge (src/mc.rs:4197-4221) on the oracle's pass:
+    the bulb at 48x36, the first pass gives every pixel 4 rays, later passes
+    add rays where the picture is noisy, the painted picture is lit, and the
+    thread count does not change the records."""
+    import mb3dcu
+    sc = scenes.preset("Integer Power", 48, 36)
+    lv = mb3dcu.mc_light_default(sc)
+    opts = mb3dcu.mc_opts(1, depth=3)
+    recs = np.zeros(48 * 36, mb3dcu.MC_RECORD)
+    O.mc_pass(sc, lv, opts, 0, recs, threads=2)
+    assert (recs["ray_count"] == 4).all()
+    hits = int(recs["hit"].sum())
+    assert 200 < hits < 48 * 36, hits
+    avg1 = recs["ray_count"].mean()
+    O.mc_pass(sc, lv, opts, 1, recs, threads=2)
+    O.mc_pass(sc, lv, opts, 2, recs, threads=2)
+    assert recs["ray_count"].mean() > avg1
+    rgb = O.mc_paint(recs["col"].copy(), mb3dcu.mc_paint_default(), (recs["ray_count"] > 0).astype(np.uint8))
+    lit = int((rgb.reshape(-1, 3) > 20).any(axis=1).sum())
+    assert lit > 500, lit
+    a = np.zeros(48 * 36, mb3dcu.MC_RECORD)
+    b = np.zeros(48 * 36, mb3dcu.MC_RECORD)
+    for k in range(2):
+        O.mc_pass(sc, lv, opts, k, a, threads=1)
+        O.mc_pass(sc, lv, opts, k, b, threads=3)
+    assert a.tobytes() == b.tobytes()
