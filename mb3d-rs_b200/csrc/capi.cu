@@ -395,7 +395,6 @@ static void apply_tuning(DevParams &p) {
             else if (k == "blocks" && v >= 1 && v <= 16) p.blocks_per_sm = (int)v;
             else if (k == "margin" && v >= 1) p.hand_margin = (float)v;
             else if (k == "back" && v >= 0 && v <= 2) p.hand_back = (int)v;
-            else if (k == "near" && (v == 0 || v == 1)) p.hand_near = (int)v;
             else if (k == "sched" && v == 0) p.sched = SCHED_GENERIC;
         }
         i = j + 1;

@@ -43,9 +43,7 @@ struct DevParams {
     int32_t refill_min, blocks_per_sm;  // wavefront: idle lanes that trigger a refill; resident blocks
     int32_t refill_shadow, refill_ao;   // ... of the shadow and DE AO ray kernels
     int32_t blocks_march32;             // resident blocks of the single precision march
-    int32_t hand_near;                  // the mixed march hands over at the first DE < hand_margin x DE stop
     int32_t sched;                      // SCHED_*: the slots' order when it is one the DE loop has unrolled
-    int32_t pad_s;
     float d_rstop_f, rstop3d_f, soft_radius, hs_max_len_mul;
     double d_rstop, rstop3d, zcorr, zc_mul;
     double zend, step_width, fov_y, coord_eps;

@@ -222,9 +222,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                 resume = !full;
                 decide = false;
             } else if (phase == PH_START) {
-                if (it >= p.max_it || dtmp < (double)ms ||
-                    (MIXED && p.hand_near && (it >= p.max_it - 1 || dtmp < (double)p.hand_margin * (double)ms))) {
-                    hand = true;  // inside the set at the start plane (or too near it for single precision)
+                if (it >= p.max_it || dtmp < (double)ms) {
+                    hand = true;  // inside the set at the start plane
                     full = true;
                     decide = false;
                 } else {
@@ -242,13 +241,6 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                     rsf = t < 1.0 ? (float)fmax(0.5, t) : 1.0f;
                 } else {
                     rsf = 1.0f;
-                }
-                if (MIXED && p.hand_near && (it >= p.max_it - 1 || dtmp < (double)p.hand_margin * (double)ms)) {
-                    // near the surface (or the iteration limit): from here on
-                    // every decision is the double precision march's own
-                    hand = true;
-                    resume = true;
-                    decide = false;
                 }
             } else {  // PH_HALF: the DE after the half step back
                 skip_half = true;

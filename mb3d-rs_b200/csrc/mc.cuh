@@ -894,10 +894,23 @@ struct McRun {
             case L_RAY_END:
                 if (!BATCH) {  // (render logic: not in the march kernels)
                     // the ray's light into its pixel's sum
+                    float svs[3];
                     for (int k = 0; k < 3; k++) {
                         float sv = fminf(fmaxf(L.tl[k], 0.0f), 400.0f);
+                        svs[k] = sv;
                         unsigned long long q = (unsigned long long)rint((double)sv * 4294967296.0);
                         if (q) atomicAdd(&acc.sum[3 * L.pix + k], q);
+                    }
+                    if (acc.ysum) {
+                        // YofSVec (src/svec.rs:38-40), unfused single precision
+                        const float yl = fmaxf(__fadd_rn(__fadd_rn(__fmul_rn(svs[0], 0.3f), __fmul_rn(svs[1], 0.59f)),
+                                                         __fmul_rn(svs[2], 0.11f)),
+                                               0.0f);
+                        const double yv = (double)yl;
+                        const unsigned long long q1 = (unsigned long long)rint(yv * 4294967296.0);
+                        const unsigned long long q2 = (unsigned long long)rint(yv * yv * 16777216.0);
+                        if (q1) atomicAdd(&acc.ysum[2 * L.pix], q1);
+                        if (q2) atomicAdd(&acc.ysum[2 * L.pix + 1], q2);
                     }
                     if (L.hit) atomicOr(&acc.hit[L.pix], 1u);
                 }
@@ -972,16 +985,26 @@ __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_con
                     L.phase = W_S0;
                 }
             } else {
-                uint32_t within = item % m.npad;
-                int x, ly;
-                item_pixel(within, (int)m.tiles_x, x, ly);
-                if (x < m.w && ly < m.h) {
-                    L.pix = (uint32_t)ly * (uint32_t)m.w + (uint32_t)x;
-                    L.x1 = m.x0 + x + 1;
-                    L.y = m.y0 + ly;
-                    L.b = m.ray0 + (int)(item / m.npad);
-                    L.aov = L.b == m.ray0;
-                    L.phase = L_RAY;  // (its logic runs below, its first DE on the next trip)
+                if (m.items) {
+                    const uint2 it = m.items[item];
+                    L.pix = it.x;
+                    L.x1 = m.x0 + (int)(it.x % (uint32_t)m.w) + 1;
+                    L.y = m.y0 + (int)(it.x / (uint32_t)m.w);
+                    L.b = (int)it.y;
+                    L.aov = false;
+                    L.phase = L_RAY;
+                } else {
+                    uint32_t within = item % m.npad;
+                    int x, ly;
+                    item_pixel(within, (int)m.tiles_x, x, ly);
+                    if (x < m.w && ly < m.h) {
+                        L.pix = (uint32_t)ly * (uint32_t)m.w + (uint32_t)x;
+                        L.x1 = m.x0 + x + 1;
+                        L.y = m.y0 + ly;
+                        L.b = m.ray0 + (int)(item / m.npad);
+                        L.aov = L.b == m.ray0;
+                        L.phase = L_RAY;  // (its logic runs below, its first DE on the next trip)
+                    }
                 }
             }
         }
@@ -1082,17 +1105,28 @@ __global__ void __launch_bounds__(128) k_mc_logic(const __grid_constant__ DevPar
                 if (want_item) {
                     uint32_t item = b0 + (uint32_t)__popc(ask & ((1u << lane) - 1u));
                     if (item < n_items) {
-                        uint32_t within = item % m.npad;
-                        int x, ly;
-                        item_pixel(within, (int)m.tiles_x, x, ly);
-                        if (x < m.w && ly < m.h) {
-                            L.pix = (uint32_t)ly * (uint32_t)m.w + (uint32_t)x;
-                            L.x1 = m.x0 + x + 1;
-                            L.y = m.y0 + ly;
-                            L.b = m.ray0 + (int)(item / m.npad);
-                            L.aov = L.b == m.ray0;
+                        if (m.items) {
+                            const uint2 it = m.items[item];
+                            L.pix = it.x;
+                            L.x1 = m.x0 + (int)(it.x % (uint32_t)m.w) + 1;
+                            L.y = m.y0 + (int)(it.x / (uint32_t)m.w);
+                            L.b = (int)it.y;
+                            L.aov = false;
                             L.item = item;
                             L.phase = L_RAY;
+                        } else {
+                            uint32_t within = item % m.npad;
+                            int x, ly;
+                            item_pixel(within, (int)m.tiles_x, x, ly);
+                            if (x < m.w && ly < m.h) {
+                                L.pix = (uint32_t)ly * (uint32_t)m.w + (uint32_t)x;
+                                L.x1 = m.x0 + x + 1;
+                                L.y = m.y0 + ly;
+                                L.b = m.ray0 + (int)(item / m.npad);
+                                L.aov = L.b == m.ray0;
+                                L.item = item;
+                                L.phase = L_RAY;
+                            }
                         }
                         // (a padding item outside the rectangle: the slot asks again)
                     } else {

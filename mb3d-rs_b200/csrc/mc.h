@@ -17,6 +17,9 @@ struct McDev {
     int32_t x0, y0, w, h;
     uint32_t npad, tiles_x;  // the rectangle's pixels in 8x4 tiles (npad = tiles x 32)
     const uint2 *halton;     // halton_seq (src/mc.rs:117-128): (hrx | hry << 16, hdx | hdy << 16)
+    // (or null) the items of an adaptive pass: item i is ray items[i].y of
+    // pixel items[i].x of the rectangle (no first-surface outputs)
+    const uint2 *items;
 };
 
 // per pixel accumulators of a render
@@ -25,6 +28,9 @@ struct McAcc {
     unsigned int *hit;        // 1 per pixel
     float *albedo, *normal, *depth;  // the first surface of ray ray0 (device, may be null)
     unsigned long long *counters;    // [0] DE evaluations, [1] centre iterations, [2] inside starts, [3] FP64 fallbacks
+    // (or null) 2 per pixel: the rays' luminance (YofSVec of the clamped
+    // light) in 32.32 fixed point and its square in 40.24 fixed point
+    unsigned long long *ysum = nullptr;
 };
 
 }  // namespace mb3dcu

@@ -332,7 +332,6 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     p.refill_shadow = 8;
     p.refill_ao = 8;
     p.blocks_march32 = 4;
-    p.hand_near = 0;
     p.blocks_per_sm = 3;
 
     // shadow lights (render::shadow_job): HSvecs = RotateVectorReverse(-sw * LN, M)
