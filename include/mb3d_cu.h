@@ -385,6 +385,23 @@ int mb3d_cu_mc_light_default(const mb3d_cu_scene *scene, mb3d_cu_mc_light *out);
 int mb3d_cu_mc_batch(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, int precision, int secant,
                      const mb3d_cu_mc_req *reqs, uint32_t n, mb3d_cu_mc_res *res);
 
+/* Replaces mc::pass (src/mc.rs:2857, pass_inner :3110-3300 with
+ * Tracer::pixel :2766-2834 and calc_n :2657-2762): one pass of the adaptive
+ * Monte Carlo renderer over the whole picture.  recs (width * height
+ * records, host or device) is the picture so far, all zero before the first
+ * pass; every pixel takes its rays in rounds: 4 in a pixel without rays,
+ * else as many as calc_n finds from its noise and its neighbours in the
+ * records at the start of the pass, and more rounds while a round's mean
+ * luminance leaves the record's by more than its noise.  A ray's number
+ * (its seed and Halton place) follows the pixel's count, so a pass gives
+ * the reference's rays.  `opts` gives depth, secant and the soft shadow
+ * radius (its rays, ray0 and rectangle are not used); pass_nr is the
+ * picture's count of passes so far (McImage::passes).  stats.orbit_its[0]
+ * receives the number of rays traced. */
+int mb3d_cu_mc_pass(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_mc_light *light,
+                    const mb3d_cu_mc_opts *opts, int precision, uint32_t pass_nr, mb3d_cu_mc_record *recs,
+                    const volatile int *cancel);
+
 /* The Monte Carlo tracer's rays traced whole on the card: Tracer::ray
  * (src/mc.rs:2467-2627) with CalcRay (src/mc.rs:1904-2348), the direct
  * light of CalcPhongLight and CalcHSMC (src/mc.rs:1513-1768), the ambient

@@ -75,6 +75,8 @@ struct mb3d_cu_ctx {
     size_t mc_cap = 0;
     unsigned char *d_mcs = nullptr;  // the split render's paths, requests, results, list
     size_t mcs_cap = 0;
+    unsigned char *d_mcitems = nullptr;  // the adaptive pass's items (pixel, ray number)
+    size_t mcitems_cap = 0;
     unsigned char *d_paint = nullptr;  // the painter's staging of host buffers
     size_t paint_cap = 0;
     unsigned char *d_ssao = nullptr;   // the SSAO's levels and angles (and a host G-buffer's staging)
@@ -197,6 +199,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_halton);
     cudaFree(c->d_mc);
     cudaFree(c->d_mcs);
+    cudaFree(c->d_mcitems);
     cudaFree(c->d_paint);
     cudaFree(c->d_ssao);
     for (auto &ev : c->ev)
@@ -1112,6 +1115,205 @@ int mb3d_cu_mc_batch(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, int precision, int
     return 0;
 }
 
+// the split render of n_items items: the paths' logic (k_mc_logic) and their
+// marches (k_mc in batch mode on the list of waiting paths) in turns; ctrl:
+// 3 words of device scratch (next item, list length, march queue)
+static int mc_split(mb3d_cu_ctx *c, const DevParams &p, const McDev &mb, const McAcc &ab, uint32_t n_items, bool mixed,
+                    unsigned int *ctrl, const volatile int *cancel, uint32_t &launches) {
+    cudaStream_t s = c->stream;
+    const uint32_t slots = std::min<uint32_t>(n_items, 1u << 21);
+    const size_t lb = mc_lane_bytes();
+    size_t s_req = align256((size_t)slots * lb), s_res = s_req + align256((size_t)slots * sizeof(mb3d_cu_mc_req));
+    size_t s_list = s_res + align256((size_t)slots * sizeof(mb3d_cu_mc_res));
+    size_t s_need = s_list + align256((size_t)slots * 4);
+    if (int e = grow((void **)&c->d_mcs, &c->mcs_cap, s_need)) return e;
+    unsigned char *S = c->d_mcs;
+    mb3d_cu_mc_req *reqs = (mb3d_cu_mc_req *)(S + s_req);
+    mb3d_cu_mc_res *res = (mb3d_cu_mc_res *)(S + s_res);
+    uint32_t *list = (uint32_t *)(S + s_list);
+    CU_TRY(cudaMemsetAsync(S, 0, (size_t)slots * lb, s));  // (every path idle)
+    CU_TRY(cudaMemsetAsync(ctrl, 0, 12, s));
+    for (int turn = 0;; turn++) {
+        if (turn > 4000000) return fail(MB3D_CU_EIO, "Monte Carlo turns did not end");
+        CU_TRY(cudaMemsetAsync(ctrl + 1, 0, 8, s));
+        launch_mc_logic(p, mb, ab, S, reqs, res, slots, ctrl, n_items, list, ctrl + 1, c->sms, s);
+        if (int e = check_launch("k_mc_logic")) return e;
+        unsigned int h[2];
+        CU_TRY(cudaMemcpyAsync(h, ctrl, 8, cudaMemcpyDeviceToHost, s));
+        CU_TRY(cudaStreamSynchronize(s));
+        launches++;
+        if (h[1] == 0) {
+            if (h[0] >= n_items) break;
+            continue;  // (only padding items were taken this turn)
+        }
+        launch_mc(p, mb, mixed, true, ab, reqs, res, ctrl + 2, h[1], list, c->sms, s);
+        launches++;
+        if (int e = check_launch("k_mc (split)")) return e;
+        if (cancel && (turn & 15) == 15 && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
+    }
+    return 0;
+}
+
+int mb3d_cu_mc_pass(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_light *lv, const mb3d_cu_mc_opts *o,
+                    int precision, uint32_t pass_nr, mb3d_cu_mc_record *recs, const volatile int *cancel) {
+    if (!c || !sc || !lv || !o || !recs) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (precision != MB3D_CU_FP64 && precision != MB3D_CU_FP32_FP64) return fail(MB3D_CU_EINVAL, "unknown precision");
+    if (o->depth < 0 || o->depth > 64) return fail(MB3D_CU_EINVAL, "depth must be 0..64");
+    if (sc->width < 1 || sc->height < 1) return fail(MB3D_CU_EINVAL, "empty picture");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    DevParams p;
+    McDev m;
+    std::string err;
+    int r = mc_setup(*sc, *lv, o->depth, o->secant, o->soft_shadow_radius, p, m, err);
+    if (r < 0) return fail(r, err);
+    apply_tuning(p);
+    if (int e = mc_halton(c)) return e;
+    if (cancel && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    const int w = sc->width, h = sc->height;
+    const size_t npix = (size_t)w * (size_t)h;
+    cudaStream_t s = c->stream;
+    // StartCalc / CalcAvrgNoise (src/mc.rs:3226-3235; McImage::stats and
+    // avg_sqr_noise :329-358) on the host's copy of the records
+    const bool dev = is_device_ptr(recs);
+    std::vector<mb3d_cu_mc_record> hrec;
+    const mb3d_cu_mc_record *hr = recs;
+    if (dev) {
+        hrec.resize(npix);
+        CU_TRY(cudaMemcpyAsync(hrec.data(), recs, npix * sizeof(mb3d_cu_mc_record), cudaMemcpyDeviceToHost, s));
+        CU_TRY(cudaStreamSynchronize(s));
+        hr = hrec.data();
+    }
+    bool fresh = true, zero_counts = false;
+    double rsum = 0.0, noise_sum = 0.0;
+    for (size_t i = 0; i < npix; i++) {
+        const mb3d_cu_mc_record &q = hr[i];
+        if (q.ray_count == 0) {
+            zero_counts = true;
+            continue;
+        }
+        fresh = false;
+        rsum += (double)q.ray_count;
+        const double y = (double)q.ysum;
+        noise_sum += std::fmax(((double)q.ysqr - y * y) / (double)q.ray_count, 0.0);
+    }
+    const double l = (double)npix;
+    const double avrg_sqr_noise = fresh ? 1.0 : std::fmax(noise_sum / l + 0.002, 0.002);
+    McPassArgs a;
+    a.w = w;
+    a.h = h;
+    a.avrg_rcount = fresh ? 0.0f : (float)(rsum / l);
+    a.avrg_vari = std::fmax(avrg_sqr_noise, 0.001);
+    {
+        const volatile float ar = a.avrg_rcount;  // (single precision, as the reference forms it)
+        const volatile float mv = (ar + ar * ar * 0.2f) * 10.0f;
+        a.max_new = (int)std::round((float)mv);
+    }
+    a.skip_nonzero = fresh ? 1 : (zero_counts ? 1 : 0);
+    a.sqr = lv->sqr != 0;
+    a.pass_nr = pass_nr;
+    // device memory: the records (a host array's copy), their snapshot, the
+    // rays per pixel, the round's sums, the blocks' ray counts and the items
+    const int nblk = (int)((npix + 1023) / 1024);
+    size_t o_cnt = 0, o_rec = 256, o_snap = o_rec + align256(npix * sizeof(mb3d_cu_mc_record));
+    size_t o_tot = o_snap + align256(npix * sizeof(mb3d_cu_mc_record)), o_sum = o_tot + align256(npix * 4);
+    size_t o_ys = o_sum + align256(npix * 24), o_hit = o_ys + align256(npix * 16), o_bs = o_hit + align256(npix * 4);
+    size_t o_off = o_bs + align256((size_t)nblk * 4), o_fill = o_off + align256((size_t)nblk * 4);
+    size_t need = o_fill + align256((size_t)nblk * 4);
+    if (int e = grow((void **)&c->d_mc, &c->mc_cap, need)) return e;
+    unsigned char *B = c->d_mc;
+    mb3d_cu_mc_record *drec = dev ? recs : (mb3d_cu_mc_record *)(B + o_rec);
+    a.recs = drec;
+    a.snap = (const mb3d_cu_mc_record *)(B + o_snap);
+    a.total = (int *)(B + o_tot);
+    McAcc acc;
+    acc.counters = (unsigned long long *)(B + o_cnt);
+    acc.sum = (unsigned long long *)(B + o_sum);
+    acc.ysum = (unsigned long long *)(B + o_ys);
+    acc.hit = (unsigned int *)(B + o_hit);
+    acc.albedo = acc.normal = acc.depth = nullptr;
+    unsigned int *bsum = (unsigned int *)(B + o_bs), *boff = (unsigned int *)(B + o_off), *bfill = (unsigned int *)(B + o_fill);
+    unsigned int *more = (unsigned int *)(B + 64), *ctrl = (unsigned int *)(B + 128);
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    CU_TRY(cudaMemsetAsync(B, 0, 256, s));
+    if (!dev) CU_TRY(cudaMemcpyAsync(drec, recs, npix * sizeof(mb3d_cu_mc_record), cudaMemcpyHostToDevice, s));
+    CU_TRY(cudaMemcpyAsync((void *)a.snap, drec, npix * sizeof(mb3d_cu_mc_record), cudaMemcpyDeviceToDevice, s));
+    launch_mcp_start(a, c->sms, s);
+    if (int e = check_launch("k_mcp_start")) return e;
+    const bool mixed = precision != MB3D_CU_FP64 && !p.all_fp64;
+    m.x0 = 0;
+    m.y0 = 0;
+    m.w = w;
+    m.h = h;
+    m.rays = 1;
+    m.ray0 = 0;
+    m.tiles_x = (uint32_t)((w + 7) / 8);
+    m.npad = m.tiles_x * (uint32_t)((h + 3) / 4) * 32u;
+    m.halton = c->d_halton;
+    uint32_t launches = 1;
+    std::vector<unsigned int> hb(nblk), ho(nblk);
+    uint64_t rays_total = 0;
+    for (int round = 0;; round++) {
+        if (round > 100000) return fail(MB3D_CU_EIO, "Monte Carlo rounds did not end");
+        launch_mcp_count(a, bsum, s);
+        CU_TRY(cudaMemcpyAsync(hb.data(), bsum, (size_t)nblk * 4, cudaMemcpyDeviceToHost, s));
+        CU_TRY(cudaStreamSynchronize(s));
+        uint64_t all = 0, most = 0;
+        for (int b = 0; b < nblk; b++) {
+            all += hb[b];
+            most = std::max<uint64_t>(most, hb[b]);
+        }
+        if (all == 0) break;
+        rays_total += all;
+        // the blocks in chunks of at most `cap` items (a block's rays stay together)
+        const uint64_t cap = std::max<uint64_t>((uint64_t)1 << 25, most);
+        size_t items_need = (size_t)std::min<uint64_t>(all, cap) * sizeof(uint2);
+        if (int e = grow((void **)&c->d_mcitems, &c->mcitems_cap, items_need)) return e;
+        for (int b0 = 0; b0 < nblk;) {
+            uint64_t n = 0;
+            int b1 = b0;
+            while (b1 < nblk && n + hb[b1] <= cap) {
+                ho[b1 - b0] = (unsigned int)n;
+                n += hb[b1];
+                b1++;
+            }
+            if (n > 0) {
+                CU_TRY(cudaMemcpyAsync(boff, ho.data(), (size_t)(b1 - b0) * 4, cudaMemcpyHostToDevice, s));
+                CU_TRY(cudaMemsetAsync(bfill, 0, (size_t)(b1 - b0) * 4, s));
+                launch_mcp_items(a, b0, b1, boff, bfill, (uint2 *)c->d_mcitems, acc, s);
+                if (int e = check_launch("k_mcp_items")) return e;
+                McDev mi = m;
+                mi.items = (const uint2 *)c->d_mcitems;
+                if (int e = mc_split(c, p, mi, acc, (uint32_t)n, mixed, ctrl, cancel, launches)) return e;
+                launches += 1;
+            }
+            b0 = b1;
+        }
+        launch_mcp_update(a, acc, more, c->sms, s);
+        if (int e = check_launch("k_mcp_update")) return e;
+        launches += 2;
+        if (cancel && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
+    }
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    if (!dev) CU_TRY(cudaMemcpyAsync(recs, drec, npix * sizeof(mb3d_cu_mc_record), cudaMemcpyDeviceToHost, s));
+    unsigned long long hc[4];
+    CU_TRY(cudaMemcpyAsync(hc, acc.counters, sizeof(hc), cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    c->stats.ms_march = ms;
+    c->stats.launches = launches;
+    c->stats.de_evals = hc[0];
+    c->stats.mc_inside_rays = (uint32_t)hc[2];
+    c->stats.mc_fp64_rays = (uint32_t)hc[3];
+    c->stats.orbit_its[0] = rays_total;  // (the pass's rays)
+    return 0;
+}
+
 int mb3d_cu_mc_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_light *lv, const mb3d_cu_mc_opts *o,
                       int precision, const mb3d_cu_mc_out *out, const volatile int *cancel) {
     if (!c || !sc || !lv || !o || !out || !out->radiance) return fail(MB3D_CU_EINVAL, "NULL argument");
@@ -1199,37 +1401,7 @@ int mb3d_cu_mc_render(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_
         } else {
             // the split render: the paths' logic (k_mc_logic) and their marches
             // (k_mc in batch mode on the list of waiting paths) in turns
-            const uint32_t slots = std::min<uint32_t>(n_items, 1u << 21);
-            const size_t lb = mc_lane_bytes();
-            size_t s_req = align256((size_t)slots * lb), s_res = s_req + align256((size_t)slots * sizeof(mb3d_cu_mc_req));
-            size_t s_list = s_res + align256((size_t)slots * sizeof(mb3d_cu_mc_res));
-            size_t s_need = s_list + align256((size_t)slots * 4);
-            if (int e = grow((void **)&c->d_mcs, &c->mcs_cap, s_need)) return e;
-            unsigned char *S = c->d_mcs;
-            mb3d_cu_mc_req *reqs = (mb3d_cu_mc_req *)(S + s_req);
-            mb3d_cu_mc_res *res = (mb3d_cu_mc_res *)(S + s_res);
-            uint32_t *list = (uint32_t *)(S + s_list);
-            unsigned int *ctrl = (unsigned int *)(B + 128);  // next item, list length, march queue
-            CU_TRY(cudaMemsetAsync(S, 0, (size_t)slots * lb, s));  // (every path idle)
-            CU_TRY(cudaMemsetAsync(ctrl, 0, 12, s));
-            for (int turn = 0;; turn++) {
-                if (turn > 4000000) return fail(MB3D_CU_EIO, "Monte Carlo turns did not end");
-                CU_TRY(cudaMemsetAsync(ctrl + 1, 0, 8, s));
-                launch_mc_logic(p, mb, ab, S, reqs, res, slots, ctrl, n_items, list, ctrl + 1, c->sms, s);
-                if (int e = check_launch("k_mc_logic")) return e;
-                unsigned int h[2];
-                CU_TRY(cudaMemcpyAsync(h, ctrl, 8, cudaMemcpyDeviceToHost, s));
-                CU_TRY(cudaStreamSynchronize(s));
-                launches++;
-                if (h[1] == 0) {
-                    if (h[0] >= n_items) break;
-                    continue;  // (only padding items were taken this turn)
-                }
-                launch_mc(p, mb, mixed, true, ab, reqs, res, ctrl + 2, h[1], list, c->sms, s);
-                launches++;
-                if (int e = check_launch("k_mc (split)")) return e;
-                if (cancel && (turn & 15) == 15 && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
-            }
+            if (int e = mc_split(c, p, mb, ab, n_items, mixed, (unsigned int *)(B + 128), cancel, launches)) return e;
         }
         if (cancel && b0 + (int)per < o->rays) {
             CU_TRY(cudaStreamSynchronize(s));

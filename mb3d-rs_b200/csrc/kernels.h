@@ -121,6 +121,13 @@ void launch_mc_logic(const DevParams &p, const McDev &m, const McAcc &acc, void 
                      unsigned int *n_list, int sms, cudaStream_t s);
 void launch_mc_final(const McAcc &acc, uint32_t npix, int rays, float *radiance, uint8_t *hit, cudaStream_t s);
 
+// the adaptive pass's steps (mc_pass.cu)
+void launch_mcp_start(const McPassArgs &a, int sms, cudaStream_t s);
+void launch_mcp_count(const McPassArgs &a, unsigned int *block_sum, cudaStream_t s);
+void launch_mcp_items(const McPassArgs &a, int b0, int b1, const unsigned int *offset, unsigned int *fill, uint2 *items,
+                      const McAcc &acc, cudaStream_t s);
+void launch_mcp_update(const McPassArgs &a, const McAcc &acc, unsigned int *more, int sms, cudaStream_t s);
+
 // paint_recs of the Monte Carlo records' colours (mc_paint.cu)
 void mc_paint_launch(const float *col, const uint8_t *rays, uint32_t n, const mb3d_cu_mc_paint_opts &mc, uint8_t *out,
                      int blocks, cudaStream_t s);

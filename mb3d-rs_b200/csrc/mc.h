@@ -33,4 +33,16 @@ struct McAcc {
     unsigned long long *ysum = nullptr;
 };
 
+// an adaptive Monte Carlo pass over the whole picture (mc_pass.cu)
+struct McPassArgs {
+    mb3d_cu_mc_record *recs;          // width * height, updated
+    const mb3d_cu_mc_record *snap;    // the records at the start of the pass
+    int *total;                       // per pixel: the rays of its coming round (0: none)
+    int w, h;
+    int skip_nonzero, max_new, sqr;
+    uint32_t pass_nr;
+    double avrg_vari;
+    float avrg_rcount;
+};
+
 }  // namespace mb3dcu

@@ -242,6 +242,8 @@ def lib():
         L.mb3d_cu_mc_batch.argtypes = [vp, sp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_uint32, vp]
         L.mb3d_cu_mc_render.argtypes = [vp, sp, ctypes.POINTER(McLight), ctypes.POINTER(McOpts), ctypes.c_int,
                                         ctypes.POINTER(McOut), vp]
+        L.mb3d_cu_mc_pass.argtypes = [vp, sp, ctypes.POINTER(McLight), ctypes.POINTER(McOpts), ctypes.c_int,
+                                      ctypes.c_uint32, vp, vp]
         L.mb3d_cu_mc_paint_default.argtypes = [ctypes.POINTER(McPaintOpts)]
         L.mb3d_cu_mc_paint_default.restype = None
         L.mb3d_cu_mc_paint.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.POINTER(McPaintOpts), vp]
@@ -256,7 +258,7 @@ def lib():
 EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_free", "mb3d_cu_set_stream",
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_march_ex", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
-            "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render",
+            "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render", "mb3d_cu_mc_pass",
             "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
@@ -484,6 +486,18 @@ class Card:
         self._check(lib().mb3d_cu_mc_render(self._ctx, ctypes.byref(scene), ctypes.byref(light), ctypes.byref(opts),
                                             precision, ctypes.byref(ptrs), cp))
         return res
+
+    def mc_pass(self, scene, opts, recs, pass_nr, light=None, precision=FP32_FP64, cancel=None):
+        """mc::pass: one adaptive pass over the picture; recs (width * height
+        MC_RECORD, numpy or a torch CUDA byte tensor) is updated in place."""
+        light = mc_light_default(scene) if light is None else light
+        if isinstance(recs, np.ndarray):
+            assert recs.dtype == MC_RECORD and recs.flags["C_CONTIGUOUS"] and recs.size == scene.width * scene.height
+        self._order(recs)
+        cp = ctypes.cast(ctypes.byref(cancel), ctypes.c_void_p) if cancel is not None else None
+        self._check(lib().mb3d_cu_mc_pass(self._ctx, ctypes.byref(scene), ctypes.byref(light), ctypes.byref(opts),
+                                          precision, pass_nr, _ptr(recs)[0], cp))
+        return recs
 
     def set_counting(self, on):
         self._check(lib().mb3d_cu_set_counting(self._ctx, int(on)))

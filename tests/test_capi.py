@@ -68,6 +68,10 @@ MIRRORS = [("mb3d_cu_slot", "Slot"), ("mb3d_cu_light", "Light"), ("mb3d_cu_scene
            ("mb3d_cu_march_opts", "MarchOpts")]
 
 
+# the numpy record types of the header's records (C name, dtype name)
+DTYPES = [("mb3d_cu_silight", "SILIGHT"), ("mb3d_cu_mc_record", "MC_RECORD")]
+
+
 def test_every_struct_mirror_matches_the_header(tmp_path):
     """Size and every field offset of each ctypes mirror against the C
     compiler's layout of include/mb3d_cu.h (gcc, the host ABI)."""
@@ -78,6 +82,11 @@ def test_every_struct_mirror_matches_the_header(tmp_path):
         lines.append(f'printf("{pyname} size %zu\\n", sizeof({cname}));')
         for f in cls._fields_:
             lines.append(f'printf("{pyname} {f[0]} %zu\\n", offsetof({cname}, {f[0]}));')
+    for cname, dname in DTYPES:
+        dt = getattr(mb3dcu, dname)
+        lines.append(f'printf("{dname} size %zu\\n", sizeof({cname}));')
+        for f in dt.names:
+            lines.append(f'printf("{dname} {f} %zu\\n", offsetof({cname}, {f}));')
     lines.append("return 0; }")
     src = tmp_path / "layout.c"
     src.write_text("\n".join(lines))
@@ -90,7 +99,10 @@ def test_every_struct_mirror_matches_the_header(tmp_path):
             continue
         pyname, field, value = line.split()
         cls = getattr(mb3dcu, pyname)
-        want = ctypes.sizeof(cls) if field == "size" else getattr(cls, field).offset
+        if isinstance(cls, np.dtype):
+            want = cls.itemsize if field == "size" else cls.fields[field][1]
+        else:
+            want = ctypes.sizeof(cls) if field == "size" else getattr(cls, field).offset
         assert want == int(value), (pyname, field, want, value)
         checked += 1
     assert checked > 100

@@ -239,3 +239,54 @@ def test_split_render_equals_one_kernel_render(card, monkeypatch):
             assert abs(a.mean() - b.mean()) <= 0.01 * a.mean()
             psnr = 10 * np.log10(a.max() ** 2 / max(float(np.mean((a - b) ** 2)), 1e-30))
             assert psnr > 30.0, psnr
+
+
+def test_adaptive_pass_fp64_matches_oracle(card):
+    """mb3d_cu_mc_pass (mc::pass with calc_n and the per-pixel rounds)
+    against the oracle's pass on the same records: the first pass gives every
+    pixel 4 rays; the second, from the same records on both sides, the same
+    ray counts (calc_n and the rounds' noise test decide alike) and the same
+    records up to the rays that part on a grazing step."""
+    sc = scenes.scaled(scenes.c2_hybrid(), 96, 54)
+    lv = mb3dcu.mc_light_default(sc)
+    opts = mb3dcu.mc_opts(1, depth=3)
+    n = sc.width * sc.height
+    a = card.mc_pass(sc, opts, np.zeros(n, mb3dcu.MC_RECORD), 0, lv, mb3dcu.FP64)
+    b = O.mc_pass(sc, lv, opts, 0, np.zeros(n, mb3dcu.MC_RECORD))
+    assert (a["ray_count"] == 4).all() and (b["ray_count"] == 4).all()
+    assert (a["hit"] == b["hit"]).mean() >= 0.99
+    scale = float(np.abs(b["col"]).max())
+    close = np.all(np.abs(a["col"] - b["col"]) <= 1e-5 * scale, axis=1)
+    assert close.mean() >= 0.97, close.mean()
+    # the second pass from the oracle's records on both sides
+    a2 = card.mc_pass(sc, opts, b.copy(), 1, lv, mb3dcu.FP64)
+    b2 = O.mc_pass(sc, lv, opts, 1, b.copy())
+    assert b2["ray_count"].mean() > 4.5
+    same = (a2["ray_count"] == b2["ray_count"]).mean()
+    assert same >= 0.97, same
+    close = np.all(np.abs(a2["col"] - b2["col"]) <= 1e-4 * scale, axis=1)
+    assert close.mean() >= 0.95, close.mean()
+    assert abs(float(a2["ray_count"].sum()) - float(b2["ray_count"].sum())) <= 0.01 * float(b2["ray_count"].sum())
+
+
+def test_adaptive_passes_converge_on_the_card(card):
+    """The reference's passes_converge (src/mc.rs:4197-4221) on the card in
+    the mixed mode, with the records in device memory for the later passes."""
+    import torch
+    sc = scenes.preset("Integer Power", 48, 36)
+    lv = mb3dcu.mc_light_default(sc)
+    opts = mb3dcu.mc_opts(1, depth=3)
+    recs = card.mc_pass(sc, opts, np.zeros(48 * 36, mb3dcu.MC_RECORD), 0, lv)
+    assert (recs["ray_count"] == 4).all()
+    assert 200 < int(recs["hit"].sum()) < 48 * 36
+    avg1 = recs["ray_count"].mean()
+    dev = torch.from_numpy(recs.view(np.uint8).copy()).cuda()
+    for k in (1, 2):
+        card.mc_pass(sc, opts, dev, k, lv)
+    torch.cuda.synchronize()
+    out = np.frombuffer(dev.cpu().numpy().tobytes(), dtype=mb3dcu.MC_RECORD)
+    assert out["ray_count"].mean() > avg1
+    host = recs.copy()
+    for k in (1, 2):
+        card.mc_pass(sc, opts, host, k, lv)
+    assert host.tobytes() == out.tobytes()  # (device and host records: the same passes)
