@@ -534,6 +534,32 @@ int mb3d_cu_dn_conv_check(mb3d_cu_ctx *ctx, int n, int h, int w, int cin, int co
  * stays usable.  No counterpart in the reference (it has no network). */
 int mb3d_cu_dn_wait_check(mb3d_cu_ctx *ctx, double wait_us, int no_issue);
 
+/* Depth of field (DofParams, src/dof.rs:13-31): every pixel of the painted
+ * picture spread over a disk whose radius grows with its distance from the
+ * focus. */
+typedef struct mb3d_cu_dof_opts {
+    float z_sharp, z_sharp2; /* the focus distances as a fraction of the picture's width; between them all is sharp */
+    float aperture;          /* 0.0001 .. 2 */
+    float clip_r;            /* the largest blur radius, pixels */
+    uint8_t passes;          /* 1 .. 4, each with a larger radius */
+    uint8_t forward;         /* 1: the forward variant (all pixels spread at once); 0: the default sorted one (the
+                              * pixels back to front, near blurred objects covering the sharp ones behind them) */
+    uint8_t pad[2];
+} mb3d_cu_dof_opts;
+
+/* DofParams::default (src/dof.rs:33-37).  Host code only. */
+void mb3d_cu_dof_default(mb3d_cu_dof_opts *out);
+
+/* Replaces dof::apply (src/dof.rs:81-122) with its card path
+ * (src/dof.rs:425-723, gpu_dof.wgsl): all passes of the depth of field on
+ * the 8-bit picture `rgb` (width * height * 3, in place) of the G-buffer
+ * `gbuf` (width * height records) of `scene`; both host or device.  Each
+ * output pixel takes its sources in the reference's order (the sorted
+ * variant: back to front by fine depth, ties in pixel order; the forward
+ * one: pixel order), so its sums are the reference's. */
+int mb3d_cu_dof(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_dof_opts *opts,
+                const mb3d_cu_silight *gbuf, uint8_t *rgb);
+
 /* The march without any device allocation, for callers that cannot
  * allocate GPU memory: a renderer whose device memory belongs to another
  * allocator (an engine's fixed pool, PyTorch's caching allocator), which may

@@ -149,6 +149,20 @@ class SsaoOpts(ctypes.Structure):
                 ("wrap_x", ctypes.c_uint8), ("pad", ctypes.c_uint8 * 2)]
 
 
+class DofOpts(ctypes.Structure):
+    """mb3d_cu_dof_opts: DofParams (src/dof.rs:13-31)."""
+    _fields_ = [("z_sharp", ctypes.c_float), ("z_sharp2", ctypes.c_float), ("aperture", ctypes.c_float),
+                ("clip_r", ctypes.c_float), ("passes", ctypes.c_uint8), ("forward", ctypes.c_uint8),
+                ("pad", ctypes.c_uint8 * 2)]
+
+
+def dof_default():
+    """DofParams::default."""
+    o = DofOpts()
+    lib().mb3d_cu_dof_default(ctypes.byref(o))
+    return o
+
+
 def ssao_default():
     """SsaoParams::default."""
     o = SsaoOpts()

@@ -39,6 +39,8 @@ def lib():
         L.oracle_mc_render.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int]
         L.oracle_mc_batch.argtypes = [vp, ctypes.c_int, vp, ctypes.c_uint32, vp, ctypes.c_int]
         L.oracle_mc_pass.argtypes = [vp, vp, vp, ctypes.c_uint32, vp, ctypes.c_int]
+        L.oracle_dof.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, vp, ctypes.c_int]
         L.oracle_mc_halton.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
         L.oracle_mc_halton.restype = None
         L.oracle_mc_seed_of.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32]
@@ -152,6 +154,22 @@ def mc_pass(scene, light, opts, pass_nr, recs, threads=0):
     _chk(lib().oracle_mc_pass(ctypes.addressof(scene), ctypes.addressof(light), ctypes.addressof(opts), pass_nr,
                               recs.ctypes.data, threads))
     return recs
+
+
+def dof_raw(gbuf, rgb, width, height, zc_mul, zcorr, fov_y, opts, threads=0):
+    """dof::apply (src/dof.rs:81-122) on an 8-bit picture (h, w, 3) with the
+    depth constants given: a new picture; opts is an mb3dcu.DofOpts."""
+    out = np.ascontiguousarray(rgb, dtype=np.uint8).copy()
+    g = np.ascontiguousarray(gbuf)
+    _chk(lib().oracle_dof(out.ctypes.data, g.ctypes.data, width, height, zc_mul, zcorr, fov_y,
+                          ctypes.addressof(opts), threads))
+    return out
+
+
+def dof(scene, gbuf, rgb, opts, threads=0):
+    """dof::apply with the scene's depth constants (CalcPPZvals)."""
+    p = params(scene)
+    return dof_raw(gbuf, rgb, scene.width, scene.height, p[7], p[6], scene.fov_y, opts, threads)
 
 
 def mc_batch(scene, reqs, secant=True, threads=0):

@@ -420,3 +420,40 @@ def test_mc_passes_converge():
         O.mc_pass(sc, lv, opts, k, a, threads=1)
         O.mc_pass(sc, lv, opts, k, b, threads=3)
     assert a.tobytes() == b.tobytes()
+
+
+def _dof_checker(w, h):
+    """dof.rs's test scene (src/dof.rs:671-685): left half near, right half
+    far, a 2-pixel checker pattern."""
+    import mb3dcu
+    rgb = np.zeros((h, w, 3), np.uint8)
+    g = np.zeros(w * h, mb3dcu.SILIGHT)
+    for y in range(h):
+        for x in range(w):
+            v = 255 if (x // 2 + y // 2) % 2 == 0 else 0
+            rgb[y, x] = v
+            g[y * w + x]["zpos_fine"] = (8_000_000 if x < w // 2 else 6_000_000) << 8
+    return rgb, g
+
+
+def _contrast(rgb, x0, x1):
+    a = rgb[1:-1, x0 + 1:x1 - 1, 0].astype(np.float64)
+    b = rgb[1:-1, x0 + 2:x1, 0].astype(np.float64)
+    return float(np.abs(a - b).sum())
+
+
+def test_dof_focus_keeps_one_depth_sharp():
+    """dof.rs's focus_keeps_one_depth_sharp (src/dof.rs:700-722) on the
+    oracle's depth of field, both variants."""
+    import mb3dcu
+    w, h = 64, 32
+    for forward in (0, 1):
+        rgb, g = _dof_checker(w, h)
+        before_far = _contrast(rgb, w // 2, w)
+        a = (8388352 - 8_000_000) / 300.0 + 1.0
+        near_z = np.float32((a * a - 1.0) / 0.001)
+        o = mb3dcu.DofOpts(near_z / w, near_z / w, 0.5, 20.0, 1, forward)
+        out = O.dof_raw(g, rgb, w, h, 300.0, 0.001, 30.0, o)
+        near, far = _contrast(out, 4, w // 2 - 4), _contrast(out, w // 2 + 4, w)
+        assert far < before_far * 0.5, (forward, far, before_far)
+        assert near > far * 2.0, (forward, near, far)
