@@ -77,6 +77,8 @@ struct mb3d_cu_ctx {
     size_t mcs_cap = 0;
     unsigned char *d_mcitems = nullptr;  // the adaptive pass's items (pixel, ray number)
     size_t mcitems_cap = 0;
+    unsigned char *d_dof = nullptr;    // the depth of field's pictures, sources and keys
+    size_t dof_cap = 0;
     unsigned char *d_paint = nullptr;  // the painter's staging of host buffers
     size_t paint_cap = 0;
     unsigned char *d_ssao = nullptr;   // the SSAO's levels and angles (and a host G-buffer's staging)
@@ -200,6 +202,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_mc);
     cudaFree(c->d_mcs);
     cudaFree(c->d_mcitems);
+    cudaFree(c->d_dof);
     cudaFree(c->d_paint);
     cudaFree(c->d_ssao);
     for (auto &ev : c->ev)
@@ -1151,6 +1154,153 @@ static int mc_split(mb3d_cu_ctx *c, const DevParams &p, const McDev &mb, const M
         if (int e = check_launch("k_mc (split)")) return e;
         if (cancel && (turn & 15) == 15 && *cancel) return fail(MB3D_CU_ECANCELED, "cancelled");
     }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// depth of field (dof.cu)
+
+void mb3d_cu_dof_default(mb3d_cu_dof_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->z_sharp = 1.0f;
+    o->z_sharp2 = 1.0f;
+    o->aperture = 0.1f;
+    o->clip_r = 30.0f;
+    o->passes = 1;
+    o->forward = 0;
+}
+
+static inline float clampf_(float x, float lo, float hi) { return x < lo ? lo : (x > hi ? hi : x); }
+
+static float zsteps_h(double z, double zc_mul_inv, double zcorr_inv) {
+    const double a = z * zc_mul_inv + 1.0;
+    return (float)((a * a - 1.0) * zcorr_inv);
+}
+
+// focus (src/dof.rs:49-78) in the reference's single precision order
+static void dof_focus(const mb3d_cu_dof_opts &p, uint32_t pass, bool sorted, int width, int height, double fov_y_deg,
+                      DofPass &d) {
+    const float ap0 = clampf_(p.aperture, 0.0001f, 2.0f);
+    const int lp = (int)(p.passes < 1 ? 1 : p.passes > 4 ? 4 : p.passes) - 1;
+    volatile float ap;
+    if (lp == 0) {
+        ap = ap0 * 0.5f;
+    } else if (lp == 1) {
+        ap = sorted ? ap0 * (0.25f + (float)pass * 0.58f) * 0.5f : ap0 * (0.3f + (float)pass * 0.55f) * 0.5f;
+    } else {
+        float p3 = 1.0f;
+        for (uint32_t k = 0; k < pass; k++) p3 *= 3.0f;
+        ap = sorted ? ap0 / 22.0f * p3 : ap0 / 12.0f * (float)(1u << pass);
+    }
+    const float dsf = (float)(std::fmax(fov_y_deg * (3.14159265358979323846 / 180.0), 0.0) / (double)height);
+    const float dw = std::fmin(p.z_sharp, p.z_sharp2) * (float)width;
+    const float st = std::fmax(p.z_sharp, p.z_sharp2) * (float)width;
+    const float w = (1.0f + dw * dsf) / (1.0f + st * dsf);
+    const float z_sharp = (w * st + dw) / (1.0f + w);
+    d.ap = ap;
+    d.dsf = dsf;
+    d.z_sharp = z_sharp;
+    d.r_sub = std::fabs((dw - z_sharp) / (1.0f + dw * dsf) * ap);
+}
+
+int mb3d_cu_dof(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_dof_opts *o, const mb3d_cu_silight *gbuf,
+                uint8_t *rgb) {
+    if (!c || !sc || !o || !gbuf || !rgb) return fail(MB3D_CU_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    DevParams p;
+    std::string err;
+    int r = setup_params(*sc, p, err);
+    if (r < 0) return fail(r, err);
+    const int w = p.width, h = p.height;
+    const size_t n = (size_t)w * h;
+    const bool dg = is_device_ptr(gbuf), dr = is_device_ptr(rgb);
+    size_t o_misc = 0, o_g = 256, o_a = o_g + align256(n * sizeof(mb3d_cu_silight)), o_b = o_a + align256(n * 3);
+    size_t o_src = o_b + align256(n * 3), o_key = o_src + align256(n * sizeof(DofSrc)), need = o_key + align256(n * 8);
+    if (int e = grow((void **)&c->d_dof, &c->dof_cap, need)) return e;
+    unsigned char *B = c->d_dof;
+    unsigned int *misc = (unsigned int *)(B + o_misc);  // [0,1] z range, [2] largest radius bits, [3] overflow
+    const mb3d_cu_silight *g = dg ? gbuf : (const mb3d_cu_silight *)(B + o_g);
+    uint8_t *pa = (uint8_t *)(B + o_a), *pb = (uint8_t *)(B + o_b);
+    DofSrc *src = (DofSrc *)(B + o_src);
+    unsigned long long *key = (unsigned long long *)(B + o_key);
+    cudaStream_t s = c->stream;
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    if (!dg) CU_TRY(cudaMemcpyAsync((void *)g, gbuf, n * sizeof(mb3d_cu_silight), cudaMemcpyHostToDevice, s));
+    CU_TRY(cudaMemcpyAsync(pa, rgb, n * 3, dr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    const double zc_mul_inv = 1.0 / p.zc_mul, zcorr_inv = 1.0 / p.zcorr;
+    const uint32_t passes = o->passes < 1 ? 1 : o->passes > 4 ? 4 : o->passes;
+    const bool forward = o->forward != 0;
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
+    // (the list's room in shared memory: a power of two, as the sort pads to one)
+    int cap_max = 1024;
+    while (cap_max * 2 * 8 + 1024 <= max_smem) cap_max *= 2;
+    uint32_t launches = 0;
+    for (uint32_t pass = 0; pass < passes; pass++) {
+        DofPass d;
+        std::memset(&d, 0, sizeof(d));
+        d.w = w;
+        d.h = h;
+        d.forward = forward ? 1 : 0;
+        d.zc_mul_inv = zc_mul_inv;
+        d.zcorr_inv = zcorr_inv;
+        dof_focus(*o, pass, !forward, w, h, sc->fov_y, d);
+        d.clip_r = clampf_(o->clip_r, 0.1f, 1000.0f);
+        CU_TRY(cudaMemsetAsync(misc, 0, 16, s));
+        unsigned int hm[4] = {32768u, 0u, 0u, 0u};
+        if (!forward) {
+            // the nearest and farthest object depths (src/dof.rs:274-287)
+            CU_TRY(cudaMemcpyAsync(misc, hm, 8, cudaMemcpyHostToDevice, s));
+            dof_zrange(g, n, misc, c->sms, s);
+            CU_TRY(cudaMemcpyAsync(hm, misc, 8, cudaMemcpyDeviceToHost, s));
+            CU_TRY(cudaStreamSynchronize(s));
+            const int64_t zmin = hm[0], zmax = hm[1];
+            float zw = zsteps_h((double)((32768 - zmin) * 256), zc_mul_inv, zcorr_inv);
+            const float r0 = std::fabs((zw - d.z_sharp) * d.ap / (1.0f + zw * d.dsf));
+            zw = zsteps_h((double)((32768 - zmax) * 256), zc_mul_inv, zcorr_inv);
+            d.max_r = std::fmin(d.clip_r, std::fmax(r0, std::fabs((zw - d.z_sharp) / (1.0f + zw * d.dsf) * d.ap)) * 1.5f);
+            d.rmax = (int)std::nearbyint(std::fabs(d.max_r) + 0.5f);
+        } else {
+            d.bg = zsteps_h(8388353.0, zc_mul_inv, zcorr_inv);
+        }
+        dof_src(d, g, pa, src, key, misc + 2, c->sms, s);
+        launches++;
+        if (int e = check_launch("k_dof_src")) return e;
+        if (forward) {
+            unsigned int bits = 0;
+            CU_TRY(cudaMemcpyAsync(&bits, misc + 2, 4, cudaMemcpyDeviceToHost, s));
+            CU_TRY(cudaStreamSynchronize(s));
+            float mr;
+            std::memcpy(&mr, &bits, 4);
+            d.max_r = mr;
+            d.sm = 1.0f / (1.0f + mr);
+            d.rmax = (int)std::nearbyint(mr + 0.5f);
+        }
+        const int64_t win = 16 + 2 * (int64_t)d.rmax;
+        int cap = 1024;
+        while (cap < cap_max && (int64_t)cap < win * win) cap *= 2;
+        if (dof_tiles(d, src, key, pb, cap, misc + 3, s) != 0) return fail(MB3D_CU_EIO, "k_dof_tiles: shared memory");
+        launches++;
+        if (int e = check_launch("k_dof_tiles")) return e;
+        std::swap(pa, pb);
+    }
+    unsigned int ovf = 0;
+    CU_TRY(cudaMemcpyAsync(&ovf, misc + 3, 4, cudaMemcpyDeviceToHost, s));
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    CU_TRY(cudaStreamSynchronize(s));
+    if (ovf)
+        return fail(MB3D_CU_ENOTSUP, "depth of field: the blur radius is beyond the card's tile lists (the CPU does it)");
+    CU_TRY(cudaMemcpyAsync(rgb, pa, n * 3, dr ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    c->stats.launches = launches;
     return 0;
 }
 

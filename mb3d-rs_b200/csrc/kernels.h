@@ -128,6 +128,26 @@ void launch_mcp_items(const McPassArgs &a, int b0, int b1, const unsigned int *o
                       const McAcc &acc, cudaStream_t s);
 void launch_mcp_update(const McPassArgs &a, const McAcc &acc, unsigned int *more, int sms, cudaStream_t s);
 
+// depth of field (dof.cu): one pass's constants (focus, src/dof.rs:49-78)
+struct DofPass {
+    int w, h, forward, rmax;
+    float ap, dsf, z_sharp, r_sub, clip_r, max_r, bg, sm;
+    double zc_mul_inv, zcorr_inv;
+};
+// a source pixel of a pass: its colour, disk and weights
+struct DofSrc {
+    float c[3];
+    float s_ms, sw, rr;
+    int ims, r;
+    uint32_t flags;  // 1: descale (in front of the focus), 2: background
+    uint32_t pad;
+};
+void dof_zrange(const mb3d_cu_silight *g, size_t n, unsigned int *zr, int sms, cudaStream_t s);
+void dof_src(const DofPass &d, const mb3d_cu_silight *g, const uint8_t *rgb, DofSrc *src, unsigned long long *key,
+             unsigned int *max_r_bits, int sms, cudaStream_t s);
+int dof_tiles(const DofPass &d, const DofSrc *src, const unsigned long long *key, uint8_t *out, int cap,
+              unsigned int *overflow, cudaStream_t s);
+
 // paint_recs of the Monte Carlo records' colours (mc_paint.cu)
 void mc_paint_launch(const float *col, const uint8_t *rays, uint32_t n, const mb3d_cu_mc_paint_opts &mc, uint8_t *out,
                      int blocks, cudaStream_t s);

@@ -262,6 +262,9 @@ def lib():
         L.mb3d_cu_mc_paint_default.restype = None
         L.mb3d_cu_mc_paint.argtypes = [vp, vp, vp, ctypes.c_uint32, ctypes.POINTER(McPaintOpts), vp]
         L.mb3d_cu_paint.argtypes = [vp, sp, vp, ctypes.c_uint32, ctypes.c_uint32, vp]
+        L.mb3d_cu_dof_default.argtypes = [ctypes.POINTER(DofOpts)]
+        L.mb3d_cu_dof_default.restype = None
+        L.mb3d_cu_dof.argtypes = [vp, sp, ctypes.POINTER(DofOpts), vp, vp]
         L.mb3d_cu_ssao_default.argtypes = [ctypes.POINTER(SsaoOpts)]
         L.mb3d_cu_ssao_default.restype = None
         L.mb3d_cu_ssao24.argtypes = [vp, sp, ctypes.POINTER(SsaoOpts), vp]
@@ -273,7 +276,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_march_ex", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render", "mb3d_cu_mc_pass",
-            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24",
+            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24", "mb3d_cu_dof_default", "mb3d_cu_dof",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
             "mb3d_cu_dn_conv_check", "mb3d_cu_dn_wait_check"]
@@ -469,6 +472,19 @@ class Card:
         self._order(gbuf, out)
         self._check(lib().mb3d_cu_paint(self._ctx, ctypes.byref(scene), _ptr(gbuf)[0], row0, rows, _ptr(out)[0]))
         return out
+
+    def dof(self, scene, gbuf, rgb, opts=None):
+        """dof::apply on the card: the depth of field of an 8-bit picture
+        (h, w, 3) of the G-buffer gbuf.  A numpy picture is returned as a new
+        array; a torch CUDA tensor is changed in place (and returned)."""
+        opts = dof_default() if opts is None else opts
+        if isinstance(rgb, np.ndarray):
+            rgb = np.ascontiguousarray(rgb, dtype=np.uint8).copy()
+        if isinstance(gbuf, np.ndarray):
+            gbuf = np.ascontiguousarray(gbuf)
+        self._order(gbuf, rgb)
+        self._check(lib().mb3d_cu_dof(self._ctx, ctypes.byref(scene), ctypes.byref(opts), _ptr(gbuf)[0], _ptr(rgb)[0]))
+        return rgb
 
     def ssao24(self, scene, gbuf, opts=None):
         """gpu::ssao24 on the card: the G-buffer's amb_shadow from its depth

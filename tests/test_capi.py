@@ -65,7 +65,7 @@ MIRRORS = [("mb3d_cu_slot", "Slot"), ("mb3d_cu_light", "Light"), ("mb3d_cu_scene
            ("mb3d_cu_stats", "Stats"), ("mb3d_cu_tune", "Tune"), ("mb3d_cu_mc_req", "McReq"),
            ("mb3d_cu_mc_res", "McRes"), ("mb3d_cu_mc_light", "McLight"), ("mb3d_cu_mc_opts", "McOpts"),
            ("mb3d_cu_mc_out", "McOut"), ("mb3d_cu_mc_paint_opts", "McPaintOpts"), ("mb3d_cu_ssao_opts", "SsaoOpts"),
-           ("mb3d_cu_march_opts", "MarchOpts")]
+           ("mb3d_cu_march_opts", "MarchOpts"), ("mb3d_cu_dof_opts", "DofOpts")]
 
 
 # the numpy record types of the header's records (C name, dtype name)
