@@ -453,14 +453,14 @@ int mb3d_cu_mc_paint(mb3d_cu_ctx *ctx, const float *colour, const uint8_t *rays,
 int mb3d_cu_paint(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_silight *gbuf, uint32_t row0,
                   uint32_t rows, uint8_t *rgb);
 
-/* The 24-bit screen space ambient occlusion (SsaoParams, src/ssao.rs:14-33),
- * regular sampling: */
+/* The 24-bit screen space ambient occlusion (SsaoParams, src/ssao.rs:14-33): */
 typedef struct {
     float threshold;     /* sAmbShadowThreshold (z/r); 2 by default */
     float border_mirror; /* bSSAO24BorderMirrorSize * 0.01, 0..0.9 */
     uint8_t t0;          /* the "threshold down to 0" variant (TAmbHiQCalcT0) */
     uint8_t wrap_x;      /* a panorama: the left and right edges are neighbours */
-    uint8_t pad[2];
+    uint8_t random;      /* random sampling with this many passes (TAmbHiQCalcR, SSAORcount); 0: regular */
+    uint8_t pad;
 } mb3d_cu_ssao_opts;
 
 /* SsaoParams::default (threshold 2, no mirrored border, no wrap). */
@@ -471,8 +471,8 @@ void mb3d_cu_ssao_default(mb3d_cu_ssao_opts *out);
  * the ambient shadow (amb_shadow, 0..16383) of its object pixels from the
  * depth buffer alone: per pixel the largest elevation angle in 32 directions
  * on ever smoother levels of the depth buffer, their arctangents summed.
- * The random sampling (SsaoParams::random) and the 15-bit variant are not on
- * the card (EINVAL for an opts outside the documented ranges). */
+ * Regular or random sampling (EINVAL for an opts outside the documented
+ * ranges); the older 15-bit variant is not on the card. */
 int mb3d_cu_ssao24(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_ssao_opts *opts,
                    mb3d_cu_silight *gbuf);
 

@@ -1014,7 +1014,8 @@ void mb3d_cu_ssao_default(mb3d_cu_ssao_opts *o) {
     o->border_mirror = 0.0f;
     o->t0 = 0;
     o->wrap_x = 0;
-    o->pad[0] = o->pad[1] = 0;
+    o->random = 0;
+    o->pad = 0;
 }
 
 int mb3d_cu_ssao24(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_ssao_opts *o, mb3d_cu_silight *gbuf) {
@@ -1032,7 +1033,7 @@ int mb3d_cu_ssao24(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_ssao_o
     cudaStream_t s = c->stream;
     const size_t npix = (size_t)w * h, gb = npix * sizeof(mb3d_cu_silight);
     const bool dev = is_device_ptr(gbuf);
-    const size_t scratch = (ssao_scratch_bytes(w, h) + 255) & ~(size_t)255;
+    const size_t scratch = (ssao_scratch_bytes(w, h, o->random) + 255) & ~(size_t)255;
     if (int e = grow((void **)&c->d_ssao, &c->ssao_cap, scratch + (dev ? 0 : gb))) return e;
     mb3d_cu_silight *dg = dev ? gbuf : reinterpret_cast<mb3d_cu_silight *>(c->d_ssao + scratch);
     if (!dev) CU_TRY(cudaMemcpyAsync(dg, gbuf, gb, cudaMemcpyHostToDevice, s));

@@ -153,8 +153,8 @@ void mc_paint_launch(const float *col, const uint8_t *rays, uint32_t n, const mb
                      int blocks, cudaStream_t s);
 
 // the 24-bit screen space ambient occlusion of a w x h G-buffer (ssao.cu);
-// scratch holds ssao_scratch_bytes(w, h)
-size_t ssao_scratch_bytes(int w, int h);
+// scratch holds ssao_scratch_bytes(w, h, random)
+size_t ssao_scratch_bytes(int w, int h, int random);
 void ssao24_launch(mb3d_cu_silight *gbuf, int w, int h, double zc_mul, double zcorr, const mb3d_cu_ssao_opts &o,
                    void *scratch, int sms, cudaStream_t s);
 

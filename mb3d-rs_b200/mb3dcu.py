@@ -144,9 +144,9 @@ class McPaintOpts(ctypes.Structure):
 
 
 class SsaoOpts(ctypes.Structure):
-    """mb3d_cu_ssao_opts: SsaoParams (src/ssao.rs:14-33) with regular sampling."""
+    """mb3d_cu_ssao_opts: SsaoParams (src/ssao.rs:14-33), regular or random sampling."""
     _fields_ = [("threshold", ctypes.c_float), ("border_mirror", ctypes.c_float), ("t0", ctypes.c_uint8),
-                ("wrap_x", ctypes.c_uint8), ("pad", ctypes.c_uint8 * 2)]
+                ("wrap_x", ctypes.c_uint8), ("random", ctypes.c_uint8), ("pad", ctypes.c_uint8)]
 
 
 class DofOpts(ctypes.Structure):

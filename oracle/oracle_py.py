@@ -49,7 +49,7 @@ def lib():
         L.oracle_mc_paint.restype = None
         L.oracle_paint.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp]
         L.oracle_ssao24.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_float,
-                                    ctypes.c_float, ctypes.c_int, ctypes.c_int]
+                                    ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_ssao_levels.argtypes = [ctypes.c_int, ctypes.c_int]
         L.oracle_ssao_rne.argtypes = [ctypes.c_float]
         L.oracle_ssao_rne.restype = ctypes.c_float
@@ -214,12 +214,14 @@ def paint(sc, gbuf, row0=0):
     return out
 
 
-def ssao24(gbuf, w, h, zc_mul, zcorr, threshold=2.0, border_mirror=0.0, t0=False, wrap_x=False):
-    """ssao::ssao24 (src/ssao.rs:129-335), regular sampling: a copy of the w x h
-    G-buffer records with amb_shadow of the object pixels set."""
+def ssao24(gbuf, w, h, zc_mul, zcorr, threshold=2.0, border_mirror=0.0, t0=False, wrap_x=False, random=0):
+    """ssao::ssao24 (src/ssao.rs:129-335), regular sampling or `random`
+    passes of random sampling: a copy of the w x h G-buffer records with
+    amb_shadow of the object pixels set."""
     g = np.ascontiguousarray(gbuf).copy()
     assert g.size == w * h
-    _chk(lib().oracle_ssao24(g.ctypes.data, w, h, zc_mul, zcorr, threshold, border_mirror, int(t0), int(wrap_x)))
+    _chk(lib().oracle_ssao24(g.ctypes.data, w, h, zc_mul, zcorr, threshold, border_mirror, int(t0), int(wrap_x),
+                             int(random)))
     return g
 
 

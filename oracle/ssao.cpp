@@ -4,8 +4,10 @@
 // angle of the depth buffer in 32 directions, on levels of an ever smoother
 // depth buffer (NextATlevelHiQ, src/ssao.rs:86-110) with the sampling radius
 // doubling per level, the angles' arctangents summed on the last level into
-// amb_shadow.  Regular sampling (SsaoParams::random = 0) only; the threshold,
-// the "down to 0" variant (t0), the mirrored border and the panorama's wrap.
+// amb_shadow.  Regular sampling and random sampling (SsaoParams::random
+// passes, TAmbHiQCalcR: each sample jittered inside its step cell by a
+// per-row LCG chain), the threshold, the "down to 0" variant (t0), the
+// mirrored border and the panorama's wrap.
 // Single precision, unfused, as the reference.
 #include <cmath>
 #include <cstdint>
@@ -83,7 +85,7 @@ float oracle_ssao_rne(float x) { return rne(x); }
 /* ssao24 on the w x h G-buffer gbuf (in place: amb_shadow of the object
  * pixels); zc_mul, zcorr are the scene's z-buffer constants. */
 int oracle_ssao24(mb3d_cu_silight *gbuf, int w_, int h_, double zc_mul, double zcorr, float threshold,
-                  float border_mirror, int t0, int wrap_x) {
+                  float border_mirror, int t0, int wrap_x, int random) {
     if (w_ <= 0 || h_ <= 0) return 0;
     const size_t w = (size_t)w_, h = (size_t)h_, npix = w * h;
     const int levels = oracle_ssao_levels(w_, h_);
@@ -100,28 +102,46 @@ int oracle_ssao24(mb3d_cu_silight *gbuf, int w_, int h_, double zc_mul, double z
     }
     std::vector<uint8_t> object(npix);
     std::vector<uint32_t> pia(npix);
-    for (size_t i = 0; i < npix; i++) {
-        object[i] = (gbuf[i].zpos_fine >> 16) < 32768;
-        pia[i] = object[i] ? (gbuf[i].zpos_fine & 0xFFFFFF00u) >> 1 : 0u;
-    }
     std::vector<uint32_t> zfine(npix);
     for (size_t i = 0; i < npix; i++) zfine[i] = (gbuf[i].zpos_fine & 0xFFFFFF00u) >> 1;
-    std::vector<int16_t> ang(npix * 32, (int16_t)-32768);
+    for (size_t i = 0; i < npix; i++) object[i] = (gbuf[i].zpos_fine >> 16) < 32768;
+    std::vector<int16_t> ang(npix * 32);
+    const int passes = random > 0 ? random : 1;
+    const bool rnd = random > 0;
+    std::vector<uint32_t> acc(npix, 0u);
+    for (int pass = 0; pass < passes; pass++) {
+    for (size_t i = 0; i < npix; i++) pia[i] = object[i] ? zfine[i] : 0u;
+    std::fill(ang.begin(), ang.end(), (int16_t)-32768);
     for (int level = 1; level <= levels; level++) {
         const bool sum_up = level == levels;
         float sit = (float)(z_scale / 22000.0 * 4096.0);
         float szrt = thr * (t0 ? 1.0f : 0.7f) * 4096.0f / sit * std::sqrt(std::sqrt((float)levels / (float)level));
         if (t0) szrt *= szrt;
-        const float at = std::atan(thr * 0.6f * std::sqrt(std::sqrt((float)levels)));
-        const float smul = 1.5f * 32767.0f / ((float)M_PI * 32.0f * (t0 ? at : std::pow(at, 0.9f))) / 1.0f;
-        const int imin = 16383;
+        const float at = rnd ? std::atan(thr * (t0 ? 0.64f : 0.65f) * std::sqrt(std::sqrt((float)levels)))
+                             : std::atan(thr * 0.6f * std::sqrt(std::sqrt((float)levels)));
+        const float smul = 1.5f * 32767.0f / ((float)M_PI * 32.0f * (t0 ? at : std::pow(at, 0.9f))) / (float)passes;
+        const int imin = 16383 / passes;
+        const int64_t iand = ((int64_t)1 << (level - 1)) - 1;
+        const float ssub = (float)iand * 0.5f;
         const int64_t istep = (int64_t)1 << (level - 1);
         const float smin_rad = istep < 2 ? 1.0f : 3.25f * (float)istep;
         const int step_count = istep < 2 ? 5 : 3;
         float rma[5];
         for (int k = 0; k < step_count; k++) rma[k] = 1.0f / (smin_rad + (float)((int64_t)k * istep) + 0.1f);
+        // the random mode's cell corners (src/ssao.rs:188-203)
+        int64_t cells[32][5][2];
+        for (int d = 0; d < 32; d++) {
+            float ox = dx[d] * smin_rad - ssub, oy = dy[d] * smin_rad - ssub;
+            for (int k = 0; k < step_count; k++) {
+                cells[d][k][0] = (int64_t)rne(ox);
+                cells[d][k][1] = (int64_t)rne(oy);
+                ox += dx[d] * (float)istep;
+                oy += dy[d] * (float)istep;
+            }
+        }
         sit *= szrt;
-        for (size_t y = 0; y < h; y++)
+        for (size_t y = 0; y < h; y++) {
+            int32_t seed = (int32_t)(0x24563487LL + ((int64_t)y + 1) * 0x324594A1LL + (int64_t)pass * 0x5851F42DLL);
             for (size_t x = 0; x < w; x++) {
                 const size_t i = y * w + x;
                 if (!object[i]) continue;
@@ -131,8 +151,26 @@ int oracle_ssao24(mb3d_cu_silight *gbuf, int w_, int h_, double zc_mul, double z
                     float sx = (float)x + dx[d] * smin_rad;
                     float sy = (float)y + dy[d] * smin_rad;
                     for (int k = 0; k < step_count; k++) {
-                        const float r = rma[k];
-                        int64_t x2 = (int64_t)rne(sx), y2 = (int64_t)rne(sy);
+                        float r = rma[k];
+                        int64_t x2, y2;
+                        if (rnd) {
+                            // TAmbHiQCalcR: a jittered sample inside the step's cell
+                            seed = (int32_t)((uint32_t)seed * 214013u + 2531011u);
+                            const int64_t jx = cells[d][k][0] + ((int64_t)((uint32_t)seed >> 16) & iand);
+                            const int64_t jy = cells[d][k][1] + ((int64_t)((uint32_t)seed >> 10) & iand);
+                            const float dd = (float)(jx * jx + jy * jy);
+                            if (dd == 0.0f) {
+                                sx += dx[d] * (float)istep;
+                                sy += dy[d] * (float)istep;
+                                continue;
+                            }
+                            r = 1.0f / std::sqrt(dd);
+                            x2 = (int64_t)x + jx;
+                            y2 = (int64_t)y + jy;
+                        } else {
+                            x2 = (int64_t)rne(sx);
+                            y2 = (int64_t)rne(sy);
+                        }
                         if (wrap_x) {
                             x2 = ((x2 % (int64_t)w) + (int64_t)w) % (int64_t)w;
                         } else if (x2 < 0) {
@@ -165,11 +203,15 @@ int oracle_ssao24(mb3d_cu_silight *gbuf, int w_, int h_, double zc_mul, double z
                     const float q = rne(s * smul);
                     int v = q >= 2147483647.0f ? 2147483647 : q <= -2147483648.0f ? (-2147483647 - 1) : (int)q;
                     v = v < 0 ? 0 : v > imin ? imin : v;
-                    gbuf[i].amb_shadow = (uint16_t)(v > 16383 ? 16383 : v);
+                    acc[i] += (uint32_t)v;
                 }
             }
+        }
         if (level < levels) next_level(pia, w, h, (size_t)1 << level, wrap_x != 0);
     }
+    }
+    for (size_t i = 0; i < npix; i++)
+        if (object[i]) gbuf[i].amb_shadow = (uint16_t)(acc[i] > 16383u ? 16383u : acc[i]);
     return 0;
 }
 }

@@ -289,3 +289,31 @@ def test_soft_shadow(card, radius):
         d = np.abs(va - vb)[obj]
         assert (d <= tol).mean() >= share, (prec, radius, (d <= tol).mean(), d.max())
         assert d.mean() < 0.5, (prec, radius, d.mean())
+
+
+def test_random_ssao_matches_the_oracle(card):
+    """The 24-bit SSAO with random sampling (SsaoParams::random passes,
+    TAmbHiQCalcR, src/ssao.rs:207-247): the card keeps each row's number
+    chain exactly (a warp per row), so its samples are the oracle's; each
+    pass's sum may land one step away (the card's atanf)."""
+    c2 = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    g = O.march(c2, mb3dcu.SILIGHT)
+    zm, zr = zc(c2)
+    obj = ~mb3dcu.is_background(g)
+    cases = [dict(random=1), dict(random=3, border_mirror=0.3), dict(random=2, t0=True, threshold=1.5),
+             dict(random=2, wrap_x=True)]
+    for kw in cases:
+        o = mb3dcu.ssao_default()
+        for k, v in kw.items():
+            setattr(o, k, v)
+        want = O.ssao24(g, c2.width, c2.height, zm, zr, **kw)
+        got = card.ssao24(c2, g, o)
+        d = np.abs(got["amb_shadow"].astype(np.int64) - want["amb_shadow"].astype(np.int64))[obj]
+        assert (d == 0).mean() >= 0.99 and d.max() <= kw["random"], (kw, (d == 0).mean(), d.max())
+        assert np.array_equal(got["amb_shadow"][~obj], g["amb_shadow"][~obj])
+    # random sampling differs from regular sampling, but not by much on average
+    reg = card.ssao24(c2, g)["amb_shadow"][obj].astype(np.float64)
+    o = mb3dcu.ssao_default()
+    o.random = 4
+    rnd = card.ssao24(c2, g, o)["amb_shadow"][obj].astype(np.float64)
+    assert (reg != rnd).mean() > 0.3 and abs(rnd.mean() - reg.mean()) < 0.1 * reg.mean()

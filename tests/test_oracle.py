@@ -457,3 +457,23 @@ def test_dof_focus_keeps_one_depth_sharp():
         near, far = _contrast(out, 4, w // 2 - 4), _contrast(out, w // 2 + 4, w)
         assert far < before_far * 0.5, (forward, far, before_far)
         assert near > far * 2.0, (forward, near, far)
+
+
+def test_ssao_random_sampling_sees_the_pit_too():
+    """Random sampling (SsaoParams::random, TAmbHiQCalcR) on the pit of the
+    reference's flat_plane_has_no_occlusion_and_a_pit_has: the pit is
+    occluded, the plane is not, and the passes' mean stays near the regular
+    sampling's occlusion."""
+    w = h = 64
+    y, x = np.mgrid[0:h, 0:w] - 32
+    pit = np.where(x * x + y * y < 36, 20000, 0)
+    gb = _depth_gbuf(w, h, 4_000_000 - pit)
+    reg = O.ssao24(gb, w, h, 300.0, 0.001)["amb_shadow"].astype(np.int64)
+    for passes in (1, 4):
+        g = O.ssao24(gb, w, h, 300.0, 0.001, random=passes)["amb_shadow"].astype(np.int64)
+        center, far = int(g[32 * w + 32]), int(g[5 * w + 5])
+        assert center > far + 1000, (passes, center, far)
+        assert abs(center - int(reg[32 * w + 32])) < 0.25 * int(reg[32 * w + 32]), (passes, center)
+    a = O.ssao24(gb, w, h, 300.0, 0.001, random=2)
+    b = O.ssao24(gb, w, h, 300.0, 0.001, random=2)
+    assert a.tobytes() == b.tobytes()
