@@ -316,26 +316,25 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const P c[3], float m
             };
             if ((FM & FKIND_BOX) && p.sched == SCHED_BOX2_IP8) {
                 // Amazing Box, Amazing Box, Integer Power 8, repeating from the
-                // first iteration, all counted: the slots' order unrolled
+                // first iteration, all counted: the slots' order as a phase
+                // counter (one body of each formula, so the loop stays small)
                 const float scale = p.slots[0].of[0], min_r = p.slots[0].of[1], fold = p.slots[0].of[2];
                 const float zmul = p.slots[1].of[1];
+                int ph = 0;
                 for (int g = 0; g < (1 << 20); g++) {
                     before();
-                    f_amazing_box_x2(scale, min_r, fold, V[0], J[0]);
-                    f_amazing_box_x2(scale, min_r, fold, V[1], J[1]);
-                    if (COUNT) cnt->its[0] += 4;
-                    n = 0;
-                    if (counted()) break;
-                    before();
-                    f_amazing_box_x2(scale, min_r, fold, V[0], J[0]);
-                    f_amazing_box_x2(scale, min_r, fold, V[1], J[1]);
-                    if (COUNT) cnt->its[0] += 4;
-                    if (counted()) break;
-                    before();
-                    f_int_pow8_x2(zmul, V[0], J[0]);
-                    f_int_pow8_x2(zmul, V[1], J[1]);
-                    if (COUNT) cnt->its[1] += 4;
-                    n = 1;
+                    if (ph < 2) {
+                        f_amazing_box_x2(scale, min_r, fold, V[0], J[0]);
+                        f_amazing_box_x2(scale, min_r, fold, V[1], J[1]);
+                        if (COUNT) cnt->its[0] += 4;
+                        n = 0;
+                    } else {
+                        f_int_pow8_x2(zmul, V[0], J[0]);
+                        f_int_pow8_x2(zmul, V[1], J[1]);
+                        if (COUNT) cnt->its[1] += 4;
+                        n = 1;
+                    }
+                    ph = ph == 2 ? 0 : ph + 1;
                     if (counted()) break;
                 }
                 goto done_x2;

@@ -129,6 +129,10 @@ __device__ __forceinline__ void item_pixel(uint32_t item, int tiles_x, int &x, i
 __device__ __forceinline__ float de_stop_at(const DevParams &p, double zz) {
     return (float)((double)p.de_stop * (1.0 + zz * (double)p.de_stop_factor));
 }
+// (the same in single precision, for the mixed march's predicting steps)
+__device__ __forceinline__ float de_stop_at_f(const DevParams &p, double zz) {
+    return p.de_stop * fmaf((float)zz, p.de_stop_factor, 1.0f);
+}
 
 // ---------------------------------------------------------------------------
 // The march as a persistent wavefront: every lane of a warp holds one ray;
@@ -156,6 +160,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                                                mb3d_cu_silight *out, Hand *list, unsigned int *counters,
                                                unsigned long long *gcount) {
     constexpr bool MIXED = sizeof(R) == 4;
+    // the step logic's type: single precision in the mixed march (its
+    // steps only predict; the FP64 finish decides), double in the plain
+    // march (the reference's arithmetic); mzz is double in both
+    typedef R T;
     DECount cnt;
     if (COUNT) cnt.clear();
     const int tiles_x = (p.width + 7) / 8;
@@ -168,12 +176,18 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
     // (the single precision march keeps its start point and direction in
     // single precision and its position as start + direction x mzz)
     float cf0[3] = {0.f, 0.f, 0.f}, vff[3] = {0.f, 0.f, 0.f};
-    double mzz = 0.0, last_step = 0.0, last_de = 0.0;
+    double mzz = 0.0;
+    T last_step = 0, last_de = 0;
     float ms = 0.f, rsf = 1.f, step_count = 0.f;
     int32_t seed = 0;
     bool first = false;
-    double b0_mzz = 0, b0_ls = 0, b0_ld = 0, b1_mzz = 0, b1_ls = 0, b1_ld = 0;
-    float b0_cnt = 0, b1_cnt = 0;
+    // the mixed march's last two states before a step (where a surface is
+    // handed over from), a ring of two slots per thread in shared memory
+    // (hs: the slot of the newest); registers stay free for the DE
+    __shared__ double h_mzz[2][256];
+    __shared__ float h_ls[2][256], h_ld[2][256], h_cnt[2][256];
+    const int tid = (int)threadIdx.x;
+    int hs = 0;
     int nb = 0;
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
         uint32_t item = warp_take_b(p, phase == PH_IDLE, counters, CNT_MARCH_Q, n_items, p.refill_min, open, 1u);
@@ -182,6 +196,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             if (x < p.width && ly < rows) {
                 pix = (uint32_t)ly * (uint32_t)p.width + (uint32_t)x;
                 pixel_ray(p, x, row0 + ly, c, vf);
+                seed = pixel_seed_d(row0 + ly, x);
                 if constexpr (MIXED) {
 #pragma unroll
                     for (int k = 0; k < 3; k++) {
@@ -200,7 +215,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             continue;
         }
         bool hand = false, full = false, done_bg = false, resume = false, overflowed = false;
-        double cur_de = 0.0;
+        T cur_de = 0;
         int cur_it = 0;
         if (phase != PH_IDLE) {
             DEr r;
@@ -212,7 +227,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                 r = de_lock<R, FM, COUNT>(p, c, ms, &cnt);
             }
             cur_it = r.it;
-            double dtmp = r.de;
+            T dtmp = (T)r.de;
             int it = r.it;
             bool skip_half = false, decide = true;
             if (MIXED && r.need64) {
@@ -222,23 +237,27 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                 resume = !full;
                 decide = false;
             } else if (phase == PH_START) {
-                if (it >= p.max_it || dtmp < (double)ms) {
+                if (it >= p.max_it || dtmp < (T)ms) {
                     hand = true;  // inside the set at the start plane
                     full = true;
                     decide = false;
                 } else {
-                    last_step = dtmp * (double)p.z_step_div;
+                    last_step = dtmp * (T)p.z_step_div;
                     rsf = 1.0f;
                     first = p.first_step_random != 0;
                     step_count = 0.f;
-                    seed = pixel_seed_d(row0 + ly, x);
                     nb = -1;
                 }
             } else if (phase == PH_STEP) {
                 if (dtmp > last_de + last_step) dtmp = last_de + last_step;
-                if (last_de > dtmp + 1e-30) {
-                    double t = MIXED ? (double)__fdividef((float)last_step, (float)(last_de - dtmp)) : last_step / (last_de - dtmp);
-                    rsf = t < 1.0 ? (float)fmax(0.5, t) : 1.0f;
+                if (last_de > dtmp + (T)1e-30) {
+                    if constexpr (MIXED) {
+                        const float t = __fdividef(last_step, last_de - dtmp);
+                        rsf = t < 1.0f ? fmaxf(0.5f, t) : 1.0f;
+                    } else {
+                        const double t = last_step / (last_de - dtmp);
+                        rsf = t < 1.0 ? (float)fmax(0.5, t) : 1.0f;
+                    }
                 } else {
                     rsf = 1.0f;
                 }
@@ -248,22 +267,25 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             if (decide) {
                 if (!skip_half && it >= p.max_it) {
                     // src/calc.rs:2544-2551: half a step back
-                    double dt1 = -0.5 * last_step;
-                    mzz += dt1;
-                    add_w(c, vf, dt1);
-                    ms = de_stop_at(p, mzz);
+                    const T dt1 = (T)-0.5 * last_step;
+                    mzz += (double)dt1;
+                    if (!MIXED) add_w(c, vf, (double)dt1);
+                    ms = MIXED ? de_stop_at_f(p, mzz) : de_stop_at(p, mzz);
                     last_step = -dt1;
                     phase = PH_HALF;
-                } else if (it < p.min_it || (it < p.max_it && dtmp >= (double)ms)) {
+                } else if (it < p.min_it || (it < p.max_it && dtmp >= (T)ms)) {
                     if (MIXED) {
-                        if (dtmp >= (double)p.hand_margin * (double)ms && !first) nb = 0;
+                        if (dtmp >= (T)p.hand_margin * (T)ms && !first) nb = 0;
                         else if (nb >= 0 && nb < p.hand_back) nb++;
-                        b1_mzz = b0_mzz; b1_ls = b0_ls; b1_ld = b0_ld; b1_cnt = b0_cnt;
-                        b0_mzz = mzz; b0_ls = last_step; b0_ld = last_de; b0_cnt = step_count;
+                        hs ^= 1;
+                        h_mzz[hs][tid] = mzz;
+                        h_ls[hs][tid] = (float)last_step;
+                        h_ld[hs][tid] = (float)last_de;
+                        h_cnt[hs][tid] = step_count;
                     }
                     last_de = dtmp;
-                    double d = fmax(0.11, (dtmp - (double)p.ms_de_sub * (double)ms) * (double)p.z_step_div * (double)rsf);
-                    double s1 = (double)(fmaxf(ms, 0.4f) * p.mh04zsd);
+                    T d = fmax((T)0.11, (dtmp - (T)p.ms_de_sub * (T)ms) * (T)p.z_step_div * (T)rsf);
+                    const T s1 = (T)(fmaxf(ms, 0.4f) * p.mh04zsd);
                     bool count = p.dfog_on_it == 0 || it == p.dfog_on_it;
                     if (s1 < d) {
                         if (count) step_count += MIXED ? __fdividef((float)s1, (float)d) : (float)(s1 / d);
@@ -274,15 +296,15 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                     if (first) {
                         first = false;
                         seed = (int32_t)((uint32_t)seed * 214013u + 2531011u);
-                        d *= (double)(seed & 0x7FFFFFFF) * (1.0 / 2147483647.0);
+                        d *= (T)((double)(seed & 0x7FFFFFFF) * (1.0 / 2147483647.0));
                     }
-                    mzz += d;
+                    mzz += (double)d;
                     if (mzz > p.zend) {
                         done_bg = true;  // background
                     } else {
                         last_step = d;
-                        add_w(c, vf, d);
-                        ms = de_stop_at(p, mzz);
+                        if (!MIXED) add_w(c, vf, (double)d);
+                        ms = MIXED ? de_stop_at_f(p, mzz) : de_stop_at(p, mzz);
                         phase = PH_STEP;
                     }
                 } else {
@@ -325,12 +347,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                 } else if (nb < 0) {
                     h.flags = HAND_FULL;  // no state to go back to: all in double
                 } else {
-                    bool two = nb >= 1;
+                    const int slot = nb >= 1 ? hs ^ 1 : hs;
                     h.flags = HAND_REMARCH;
-                    h.mzz = two ? b1_mzz : b0_mzz;
-                    h.last_step = two ? b1_ls : b0_ls;
-                    h.last_de = two ? b1_ld : b0_ld;
-                    h.step_count = two ? b1_cnt : b0_cnt;
+                    h.mzz = h_mzz[slot][tid];
+                    h.last_step = h_ls[slot][tid];
+                    h.last_de = h_ld[slot][tid];
+                    h.step_count = h_cnt[slot][tid];
                 }
             }
             phase = PH_IDLE;
@@ -1009,6 +1031,16 @@ __device__ __forceinline__ DEr ray_de(const DevParams &p, const double c[3], flo
     if (sizeof(R) == 4 && r.need64) r = de_lock<double, FM>(p, c, ms);
     return r;
 }
+// (a single precision position: the mixed mode's secondary rays)
+template <typename R, int FM>
+__device__ __forceinline__ DEr ray_de(const DevParams &p, const float c[3], float ms) {
+    DEr r = de_lock<float, FM, false, false, float>(p, c, ms);
+    if (r.need64) {
+        const double cd[3] = {(double)c[0], (double)c[1], (double)c[2]};
+        r = de_lock<double, FM>(p, cd, ms);
+    }
+    return r;
+}
 
 // One lane per shadow ray (surface pixel, light): the march toward the
 // light of hard_shadow_row / soft_shadow_row (src/calc.rs:2836-2893,
@@ -1023,6 +1055,9 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_shadow_rays(const __gr
     uint32_t pix = 0;
     int li = 0, guard = 0;
     double c[3] = {0, 0, 0}, dt1 = 0, dmax = 0, zz2 = 0, zz2mul = 0, d = 0, last_de = 0, st = 0, max_lhs = 1;
+    // (the mixed mode's DE position in single precision: the start point
+    // and the light's direction, and the length marched so far)
+    float cs[3] = {0.f, 0.f, 0.f}, lv[3] = {0.f, 0.f, 0.f};
     float ms = 0.f, rsf = 2.f, zr = 1.f, zrs_mul = 0.f;
     bool stepped = false;
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
@@ -1046,6 +1081,12 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_shadow_rays(const __gr
                 double c0[3], vf[3];
                 pixel_ray(p, x, y, c0, vf);
                 c[0] = s.sh_c[0]; c[1] = s.sh_c[1]; c[2] = s.sh_c[2];
+                if (sizeof(R) == 4) {
+                    for (int k = 0; k < 3; k++) {
+                        cs[k] = (float)s.sh_c[k];
+                        lv[k] = (float)p.light_vec[li][k];
+                    }
+                }
                 zz2 = s.sh_mzz;
                 zz2mul = -dot_normalize_d(p.light_vec[li], vf);
                 dt1 = max_lhs;
@@ -1067,7 +1108,14 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_shadow_rays(const __gr
             continue;
         }
         if (active) {
-            DEr r = ray_de<R, FM>(p, c, ms);
+            DEr r;
+            if constexpr (sizeof(R) == 4) {
+                const float t = -(float)(dmax - dt1);
+                const float cp[3] = {fmaf(lv[0], t, cs[0]), fmaf(lv[1], t, cs[1]), fmaf(lv[2], t, cs[2])};
+                r = ray_de<R, FM>(p, cp, ms);
+            } else {
+                r = ray_de<R, FM>(p, c, ms);
+            }
             bool end = false, shadowed = false;
             if (!stepped) {
                 d = r.de;  // the DE at the ray's start
@@ -1103,7 +1151,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_shadow_rays(const __gr
                     fmaxf(0.11f, (float)((d - (double)p.ms_de_sub * (double)ms) * (double)p.z_step_div * (double)rsf)),
                     fmaxf(ms, 0.4f) * p.mh04zsd);
                 dt1 -= st;
-                add_w(c, p.light_vec[li], -st);
+                if (sizeof(R) == 8) add_w(c, p.light_vec[li], -st);
                 zz2 += st * zz2mul;
                 ms = de_stop_at(p, fabs(zz2));
                 stepped = true;
@@ -1177,14 +1225,17 @@ template <typename R, int FM>
 __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_constant__ DevParams p, const PostStart *ps,
                                                  const mb3d_cu_silight *gbuf, const unsigned int *count,
                                                  float *min_ra, unsigned int *queue) {
+    // the ray's type: single precision in the mixed mode (the DE AO's
+    // openness is a smooth minimum), double in the plain mode
+    typedef R T;
     const uint32_t npx = count[0];
     const uint32_t n_items = npx * (uint32_t)p.ao_rays;
     bool open = true, active = false, b_end = false;
     uint32_t slot = 0;
-    double ic[3] = {0, 0, 0}, sv[3] = {0, 0, 0}, dt1 = 0, s_tmp = 1, msd = 0, max_dist = 0, md_d10 = 0;
+    T ic[3] = {0, 0, 0}, sv[3] = {0, 0, 0}, dt1 = 0, s_tmp = 1, msd = 0, max_dist = 0, md_d10 = 0;
     float ms_s = 0.f;
     int guard = 0;
-    const double dsm = (double)p.ao_d_step_mul;
+    const T dsm = (T)p.ao_d_step_mul;
     const double de_mul = sqrt((double)p.ao_rays * 0.5);
     for (unsigned int trip = 0; trip < 400000000u; trip++) {
         uint32_t item = warp_take(!active, queue, n_items, p.refill_ao, open);
@@ -1193,19 +1244,20 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_c
             int k = (int)(item / npx);
             const PostStart &s = ps[i];
             slot = item;
-            ic[0] = s.ao_c[0]; ic[1] = s.ao_c[1]; ic[2] = s.ao_c[2];
+            ic[0] = (T)s.ao_c[0]; ic[1] = (T)s.ao_c[1]; ic[2] = (T)s.ao_c[2];
             ms_s = s.ao_ms;
-            msd = s.ao_msd;
-            max_dist = s.ao_max_dist;
-            md_d10 = s.ao_md_d10;
+            msd = (T)s.ao_msd;
+            max_dist = (T)s.ao_max_dist;
+            md_d10 = (T)s.ao_md_d10;
             // the ray's direction: the table direction turned to the normal,
             // then to world space, one step width long
             const float *dk = p.ao_dirs[k];
             float vv[3] = {sdot3(s.ao_rot[0], dk), sdot3(s.ao_rot[1], dk), sdot3(s.ao_rot[2], dk)};
-            double vd[3] = {(double)vv[0], (double)vv[1], (double)vv[2]};
-            rot_rev(vd, p.ao_rot, sv);
-            dt1 = s.ao_step0;
-            s_tmp = 1.0;
+            double vd[3] = {(double)vv[0], (double)vv[1], (double)vv[2]}, svd[3];
+            rot_rev(vd, p.ao_rot, svd);
+            sv[0] = (T)svd[0]; sv[1] = (T)svd[1]; sv[2] = (T)svd[2];
+            dt1 = (T)s.ao_step0;
+            s_tmp = (T)1;
             b_end = false;
             guard = 0;
             active = true;
@@ -1220,15 +1272,15 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_c
                 dt1 = max_dist;
                 b_end = true;
             }
-            double c[3] = {ic[0] + sv[0] * dt1, ic[1] + sv[1] * dt1, ic[2] + sv[2] * dt1};
+            T c[3] = {ic[0] + sv[0] * dt1, ic[1] + sv[1] * dt1, ic[2] + sv[2] * dt1};
             DEr r = ray_de<R, FM>(p, c, ms_s);
-            double dt2 = r.de;
-            s_tmp = fmin(s_tmp, sizeof(R) == 4 ? (double)__fdividef((float)(dt2 - msd + dt1 * md_d10), (float)dt1)
-                                               : (dt2 - msd + dt1 * md_d10) / dt1);
-            bool end = s_tmp < 0.02 || b_end || ++guard > 100000;
+            const T dt2 = (T)r.de;
+            if constexpr (sizeof(R) == 4) s_tmp = fminf(s_tmp, __fdividef(dt2 - msd + dt1 * md_d10, dt1));
+            else s_tmp = fmin(s_tmp, (dt2 - msd + dt1 * md_d10) / dt1);
+            bool end = s_tmp < (T)0.02 || b_end || ++guard > 100000;
             if (!end) dt1 += fmax(dt2, dt1 * dsm);
             if (end) {
-                min_ra[slot] = (float)(fmax(s_tmp, 0.0) * de_mul);
+                min_ra[slot] = (float)(fmax((double)s_tmp, 0.0) * de_mul);
                 active = false;
             }
         }
