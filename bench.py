@@ -233,63 +233,23 @@ def parity_vs_fp64(sc, mixed, fp64):
 
 def mc_figures(card, ref_rays):
     """The Monte Carlo workload (the hybrid scene at 1920x1080, 4 ambient
-    bounces) on its middle 480x270 rectangle: the 16-ray trace and its
-    denoised picture against an independent plain trace of ref_rays rays."""
+    bounces), the whole frame: the 4- and 16-ray method (two half traces,
+    denoised, the plain trace kept where the denoised picture leaves it)
+    against an independent plain trace of ref_rays rays."""
     import torch
     import train_denoiser as T
     if not os.path.exists(T.WEIGHTS):
         return {"unavailable": "no trained weights (mb3d-rs_b200/weights/denoiser.f32)"}
-    sc = scenes.c5_mc()
-    lv = mb3dcu.mc_light_default(sc)
-    rect = (720, 405, 480, 270)
-
-    def trace(rays, ray0=0):
-        r = card.mc_render(sc, mb3dcu.mc_opts(rays, depth=scenes.C5_DEPTH, ray0=ray0, rect=rect), lv,
-                           mb3dcu.FP32_FP64)
-        return r, card.stats()
-
     card.set_stream(torch.cuda.current_stream().cuda_stream)  # (the denoiser between the timing events)
     dn = mb3dcu.Denoiser(card)
     dn.set_params(np.fromfile(T.WEIGHTS, "<f4"))
-    ref, st_ref = trace(ref_rays, 4096)  # (independent rays, each with its own Halton record)
-    paint_opts = mb3dcu.mc_paint_default()
-    ref8 = card.mc_paint(ref["radiance"], paint_opts).astype(np.float64)
-
-    def psnr8(x):
-        # the reference's displayed picture (paint_recs, 8 bits) against the reference trace's
-        mse = np.mean((card.mc_paint(x, paint_opts).astype(np.float64) - ref8) ** 2)
-        return float(10 * np.log10(255.0 ** 2 / max(mse, 1e-12)))
-
-    out = {"workload": "c5: hybrid scene 1920x1080, MCDepth 4, light 1 + sky; rectangle 480x270 at (720, 405)",
-           "ref_rays": ref_rays, "ms_ref": st_ref["ms_total"],
-           "mpaths_per_s": rect[2] * rect[3] * ref_rays / st_ref["ms_total"] / 1e3,
-           "de_evals_per_s": st_ref["de_evals"] / st_ref["ms_total"] * 1e3, "levels": []}
-    for rays in (4, 16):
-        r, st = trace(rays)
-        dmax = float(r["depth"].max()) or 1.0
-        ins = [torch.from_numpy(r[k]).cuda()[None] for k in ("radiance", "albedo", "normal", "depth")]
-        dn.denoise(*ins, depth_scale=1.0 / dmax)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        den = dn.denoise(*ins, depth_scale=1.0 / dmax)
-        e1.record()
-        torch.cuda.synchronize()
-        ms_dn = e0.elapsed_time(e1)
-        den = den[0].cpu().numpy()
-        ha, _ = trace(rays // 2, 0)
-        hb, _ = trace(rays // 2, rays // 2)
-        comp, fb = T.fallback_tiles(ha["radiance"], hb["radiance"], den)
-        out["levels"].append({"rays": rays, "ms_trace": st["ms_total"], "ms_denoise": ms_dn,
-                              "psnr_noisy": T.psnr(r["radiance"], ref["radiance"]),
-                              "psnr_denoised": T.psnr(den, ref["radiance"]),
-                              "psnr_with_fallback": T.psnr(comp, ref["radiance"]), "fallback_rate": fb,
-                              "psnr8_noisy": psnr8(r["radiance"]), "psnr8_denoised": psnr8(den),
-                              "psnr8_with_fallback": psnr8(comp)})
+    out = T.evaluate(card, dn, rect=None, ref_rays=ref_rays, levels=(4, 16), log=lambda *a, **k: None)
+    out["workload"] = "c5: hybrid scene 1920x1080, MCDepth 4, light 1 + sky; the whole frame"
     l16 = out["levels"][1]
-    out["time_ratio_16_denoised_vs_ref"] = (l16["ms_trace"] + l16["ms_denoise"]) / out["ms_ref"]
+    out["time_ratio_16_denoised_vs_ref"] = l16["time_ratio_vs_ref"]
     out["psnr_metric"] = ("psnr_*: PSNR of x/(1+x) tone-mapped linear records against the plain trace of ref_rays "
                           "rays; psnr8_*: PSNR of the 8-bit pictures paint_recs makes of both (default display "
-                          "settings), on the card")
+                          "settings), on the card; ms_method: both half traces + denoiser + fallback")
     dn.close()
     card.set_stream(None)
     return out

@@ -505,12 +505,38 @@ int mb3d_cu_dn_set_params(mb3d_cu_dn *dn, const float *params);
 int mb3d_cu_dn_denoise(mb3d_cu_dn *dn, int n, int h, int w, const float *radiance, const float *albedo,
                        const float *normal, const float *depth, float depth_scale, float *out);
 
-/* One Adam step (learning rate lr) on the L1 loss in log space against
- * target (n * h * w * 3 floats); *loss (may be NULL) receives the loss
- * before the step. */
+/* The training loss of the denoiser: the L1 loss of log(1 + x) (the
+ * default); the mean squared error of the tone-mapped colour x / (1 + x)
+ * (its optimum for noisy targets is their mean, where the L1 loss's is a
+ * median); or that plus the mean squared error of the colour clamped to
+ * 0..1, which is what paint_recs makes of a record with its default display
+ * settings (src/mc.rs:3957-4005: contrast 1, gamma and saturation neutral,
+ * so the Lab round trip is the identity). */
+#define MB3D_CU_DN_LOSS_L1_LOG 0
+#define MB3D_CU_DN_LOSS_TONE_MSE 1
+#define MB3D_CU_DN_LOSS_TONE_DISPLAY 2
+int mb3d_cu_dn_set_loss(mb3d_cu_dn *dn, int kind);
+
+/* One Adam step (learning rate lr) on the loss (mb3d_cu_dn_set_loss)
+ * against target (n * h * w * 3 floats); *loss (may be NULL) receives the
+ * loss before the step. */
 int mb3d_cu_dn_train_step(mb3d_cu_dn *dn, int n, int h, int w, const float *radiance, const float *albedo,
                           const float *normal, const float *depth, float depth_scale, const float *target, float lr,
                           float *loss);
+
+/* The plain trace as the denoiser's fallback and the judge of its error:
+ * half_a and half_b are two traces of the same h x w picture from disjoint
+ * halves of the rays (h * w * 3 floats each), den the denoised picture of
+ * the whole trace.  Per tile x tile piece (the last row and column ragged),
+ * in the tone x / (1 + x) of max(x, 0): where the mean of the denoised
+ * piece leaves the mean of (half_a + half_b) / 2 by more than k times that
+ * mean's noise (the halves' mean squared difference / 4 / the piece's
+ * samples, square root, +0.001), out keeps (half_a + half_b) / 2, elsewhere
+ * den; *plain_share (may be NULL) receives the share of such pieces.  out
+ * may be den; every buffer host or device memory.  No counterpart in the
+ * reference (its denoiser, src/oidn.rs:262-277, has no fallback). */
+int mb3d_cu_dn_fallback(mb3d_cu_dn *dn, int h, int w, const float *half_a, const float *half_b, const float *den,
+                        int tile, float k, float *out, float *plain_share);
 
 /* The loss and its gradient with respect to every parameter (grad:
  * mb3d_cu_dn_param_count floats, host or device), without a step. */

@@ -1277,6 +1277,8 @@ int mb3d_cu_dof(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_dof_opts 
             CU_TRY(cudaStreamSynchronize(s));
             float mr;
             std::memcpy(&mr, &bits, 4);
+            // (every radius is clamped to clip_r <= 1000: a larger value is a fault of the reduction)
+            if (!(mr >= 0.0f && mr <= d.clip_r)) return fail(MB3D_CU_EIO, "depth of field: largest radius out of range");
             d.max_r = mr;
             d.sm = 1.0f / (1.0f + mr);
             d.rmax = (int)std::nearbyint(mr + 0.5f);

@@ -92,6 +92,7 @@ struct mb3d_cu_dn {
     float *param = nullptr, *grad = nullptr, *m1 = nullptr, *m2 = nullptr;
     bf16 *wbuf = nullptr;
     int step = 0;
+    int loss_kind = MB3D_CU_DN_LOSS_L1_LOG;
     // activations (and gradients) for n x h x w
     int n = 0, h = 0, w = 0;
     bool train = false;
@@ -99,6 +100,8 @@ struct mb3d_cu_dn {
     std::vector<void *> allocs;
     float *stage = nullptr;  // host inputs and outputs, loss
     size_t stage_cap = 0;
+    unsigned char *fb = nullptr;  // the fallback's host inputs and output, its count
+    size_t fb_cap = 0;
     std::mutex mu;
 };
 
@@ -353,7 +356,10 @@ int grad_pass(mb3d_cu_dn *d, int n, int hs, int ws, const float *rad, const floa
     dn_pack_input(in.rad, in.alb, in.nrm, in.dep, depth_scale, n, hs, ws, h, w, d->a.x0, s);
     if (int e = forward(d, s)) return e;
     cudaMemsetAsync(d->stage, 0, 16 * sizeof(float), s);
-    dn_l1_loss(d->a.pred, in.tgt, n, h, w, hs, ws, d->g.pred, d->stage, s);
+    if (d->loss_kind == MB3D_CU_DN_LOSS_L1_LOG) dn_l1_loss(d->a.pred, in.tgt, n, h, w, hs, ws, d->g.pred, d->stage, s);
+    else
+        dn_tone_loss(d->a.pred, in.tgt, n, h, w, hs, ws, d->loss_kind == MB3D_CU_DN_LOSS_TONE_DISPLAY, d->g.pred,
+                     d->stage, s);
     cudaMemsetAsync(d->grad, 0, d->nparam * sizeof(float), s);
     if (int e = backward(d, s)) return e;
     if (int e = check("denoiser backward")) return e;
@@ -437,6 +443,7 @@ void mb3d_cu_dn_free(mb3d_cu_dn *d) {
     cudaFree(d->m2);
     cudaFree(d->wbuf);
     cudaFree(d->stage);
+    cudaFree(d->fb);
     delete d;
 }
 
@@ -490,6 +497,54 @@ int mb3d_cu_dn_denoise(mb3d_cu_dn *d, int n, int hs, int ws, const float *rad, c
     return 0;
 }
 
+int mb3d_cu_dn_fallback(mb3d_cu_dn *d, int h, int w, const float *half_a, const float *half_b, const float *den,
+                        int tile, float k, float *out, float *plain_share) {
+    if (!d || !half_a || !half_b || !den || !out) return dn_fail(MB3D_CU_EINVAL, "NULL argument");
+    if (h < 1 || w < 1 || h > 16384 || w > 16384) return dn_fail(MB3D_CU_EINVAL, "bad picture size");
+    if (tile < 1 || tile > 1024 || !(k >= 0.0f) || !std::isfinite(k)) return dn_fail(MB3D_CU_EINVAL, "bad tile or k");
+    std::lock_guard<std::mutex> lk(d->mu);
+    if (cudaSetDevice(dn_device(d->ctx)) != cudaSuccess) return dn_fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    cudaStream_t s = dn_stream(d->ctx);
+    const size_t bytes = (size_t)h * w * 3 * sizeof(float);
+    const float *src[3] = {half_a, half_b, den};
+    bool dev[3], dev_out = dn_is_device_ptr(out);
+    size_t need = 256;  // (the count of pieces that keep the plain trace)
+    for (int i = 0; i < 3; i++) {
+        dev[i] = dn_is_device_ptr(src[i]);
+        if (!dev[i]) need += bytes;
+    }
+    if (!dev_out) need += bytes;
+    if (need > d->fb_cap) {
+        cudaFree(d->fb);
+        d->fb = nullptr;
+        d->fb_cap = 0;
+        if (cudaMalloc((void **)&d->fb, need) != cudaSuccess) return dn_fail(MB3D_CU_ENOMEM, "device memory (denoiser)");
+        d->fb_cap = need;
+    }
+    unsigned int *bad = (unsigned int *)d->fb;
+    unsigned char *q = d->fb + 256;
+    const float *dsrc[3];
+    for (int i = 0; i < 3; i++) {
+        dsrc[i] = src[i];
+        if (!dev[i]) {
+            cudaMemcpyAsync(q, src[i], bytes, cudaMemcpyHostToDevice, s);
+            dsrc[i] = (const float *)q;
+            q += bytes;
+        }
+    }
+    float *dout = dev_out ? out : (float *)q;
+    cudaMemsetAsync(bad, 0, sizeof(unsigned int), s);
+    dn_fallback(dsrc[0], dsrc[1], dsrc[2], h, w, tile, k, dout, bad, s);
+    if (!dev_out) cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, s);
+    unsigned int nbad = 0;
+    cudaMemcpyAsync(&nbad, bad, sizeof(nbad), cudaMemcpyDeviceToHost, s);
+    if (int e = check("denoiser fallback")) return e;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return check("denoiser fallback");
+    const double pieces = (double)((w + tile - 1) / tile) * ((h + tile - 1) / tile);
+    if (plain_share) *plain_share = (float)(nbad / pieces);
+    return 0;
+}
+
 int mb3d_cu_dn_gradient(mb3d_cu_dn *d, int n, int hs, int ws, const float *rad, const float *alb, const float *nrm,
                         const float *dep, float depth_scale, const float *target, float *loss, float *grad) {
     if (!d || !rad || !target || !grad) return dn_fail(MB3D_CU_EINVAL, "NULL argument");
@@ -500,6 +555,14 @@ int mb3d_cu_dn_gradient(mb3d_cu_dn *d, int n, int hs, int ws, const float *rad, 
     cudaMemcpyAsync(grad, d->grad, d->nparam * 4, cudaMemcpyDefault, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return check("denoiser gradient");
     if (dn_conv_error(s)) return dn_fail(MB3D_CU_EIO, "denoiser gradient: a convolution's pipeline wait ran out");
+    return 0;
+}
+
+int mb3d_cu_dn_set_loss(mb3d_cu_dn *d, int kind) {
+    if (!d) return dn_fail(MB3D_CU_EINVAL, "NULL argument");
+    if (kind < MB3D_CU_DN_LOSS_L1_LOG || kind > MB3D_CU_DN_LOSS_TONE_DISPLAY) return dn_fail(MB3D_CU_EINVAL, "unknown loss");
+    std::lock_guard<std::mutex> lk(d->mu);
+    d->loss_kind = kind;
     return 0;
 }
 

@@ -63,6 +63,10 @@ void dn_pack_input(const float *rad, const float *alb, const float *nrm, const f
 void dn_unpack_output(const __nv_bfloat16 *pred, int n, int h, int w, int h_src, int w_src, float *out, cudaStream_t s);
 void dn_l1_loss(const __nv_bfloat16 *pred, const float *target, int n, int h, int w, int h_src, int w_src,
                 __nv_bfloat16 *dpred, float *loss, cudaStream_t s);
+void dn_tone_loss(const __nv_bfloat16 *pred, const float *target, int n, int h, int w, int h_src, int w_src,
+                  int display, __nv_bfloat16 *dpred, float *loss, cudaStream_t s);
+void dn_fallback(const float *a, const float *b, const float *den, int h, int w, int tile, float k, float *out,
+                 unsigned int *bad, cudaStream_t s);
 void dn_adam(float *param, const float *grad, float *m1, float *m2, size_t n, float lr, int t, cudaStream_t s);
 void dn_cast_weights(const float *w, int cout, int cin, __nv_bfloat16 *wf, __nv_bfloat16 *wb, cudaStream_t s);
 

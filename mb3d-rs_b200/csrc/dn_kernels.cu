@@ -188,6 +188,100 @@ __global__ void k_l1_loss(const __nv_bfloat16 *pred, const float *target, int n,
     if (threadIdx.x == 0) atomicAdd(loss, s[0] * inv_count);
 }
 
+// the squared error of the tone-mapped colour x / (1 + x) (the space the
+// pictures' PSNR is measured in) on channels 0..2 of the valid pixels: the
+// prediction p is log(1 + x), so its tone is 1 - exp(-p) (taken for every p,
+// a smooth continuation where the output clamps x at 0); with display set,
+// plus the squared error of the colour clamped to 0..1 (what the painter
+// makes of a record with its default settings), whose gradient passes the
+// clamp wherever the two clamped colours differ (so that a prediction above
+// 1 for a target below it is still pulled down); the loss's sum into *loss
+// and its gradient into dpred
+__global__ void k_tone_loss(const __nv_bfloat16 *pred, const float *target, int n, int h, int w, int h_src, int w_src,
+                            float inv_count, int display, __nv_bfloat16 *dpred, float *loss) {
+    __shared__ float s[256];
+    size_t total = (size_t)n * h * w;
+    float acc = 0.0f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        int x = (int)(i % w), y = (int)((i / w) % h), b = (int)(i / ((size_t)w * h));
+        __nv_bfloat16 *d = dpred + i * 16;
+        for (int c = 0; c < 16; c++) d[c] = __float2bfloat16(0.0f);
+        if (y < h_src && x < w_src) {
+            size_t t = ((size_t)b * h_src + y) * w_src + x;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const float p = __bfloat162float(pred[i * 16 + c]);
+                const float q = expf(-p);
+                const float yv = fmaxf(target[3 * t + c], 0.0f);
+                const float e = (1.0f - q) - yv / (1.0f + yv);
+                acc += e * e;
+                float g = 2.0f * e * q;
+                if (display) {
+                    const float ed = fminf(fmaxf(expm1f(p), 0.0f), 1.0f) - fminf(yv, 1.0f);
+                    acc += ed * ed;
+                    g += 2.0f * ed * expf(fminf(p, 0.69314718f));
+                }
+                d[c] = __float2bfloat16(g * inv_count);
+            }
+        }
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if ((int)threadIdx.x < k) s[threadIdx.x] += s[threadIdx.x + k];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(loss, s[0] * inv_count);
+}
+
+// The plain trace as the denoiser's fallback and judge, one block per
+// tile x tile piece of the picture (the last row and column of pieces
+// ragged): the two independent halves a and b of the trace's rays give the
+// noise of their mean m = (a + b) / 2 over the piece, and where the mean of
+// the denoised piece leaves m's by more than k times that noise (+0.001),
+// both in the tone x / (1 + x) of max(x, 0), the piece keeps m; out may be
+// den itself.
+__device__ __forceinline__ double tone01(float x) {
+    const double v = fmax((double)x, 0.0);
+    return v / (1.0 + v);
+}
+
+__global__ void k_dn_fallback(const float *a, const float *b, const float *den, int h, int w, int tile, float k,
+                              float *out, unsigned int *bad) {
+    __shared__ double s_ab[256], s_dm[256];
+    const int tx = (w + tile - 1) / tile;
+    const int x0 = (blockIdx.x % tx) * tile, y0 = (blockIdx.x / tx) * tile;
+    const int tw = min(tile, w - x0), th = min(tile, h - y0);
+    const int cnt = tw * th * 3;
+    double ab = 0.0, dm = 0.0;
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+        const int px = j / 3, c = j % 3;
+        const size_t i = ((size_t)(y0 + px / tw) * w + x0 + px % tw) * 3 + c;
+        const double ta = tone01(a[i]), tb = tone01(b[i]);
+        const double tm = tone01(0.5f * (a[i] + b[i]));
+        ab += (ta - tb) * (ta - tb);
+        dm += tone01(den[i]) - tm;
+    }
+    s_ab[threadIdx.x] = ab;
+    s_dm[threadIdx.x] = dm;
+    __syncthreads();
+    for (int r = blockDim.x / 2; r > 0; r >>= 1) {
+        if ((int)threadIdx.x < r) {
+            s_ab[threadIdx.x] += s_ab[threadIdx.x + r];
+            s_dm[threadIdx.x] += s_dm[threadIdx.x + r];
+        }
+        __syncthreads();
+    }
+    const double sigma = sqrt(s_ab[0] / cnt / 4.0 / cnt) + 1e-3;
+    const bool keep_plain = fabs(s_dm[0] / cnt) > (double)k * sigma;
+    if (keep_plain && threadIdx.x == 0) atomicAdd(bad, 1u);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+        const int px = j / 3, c = j % 3;
+        const size_t i = ((size_t)(y0 + px / tw) * w + x0 + px % tw) * 3 + c;
+        out[i] = keep_plain ? 0.5f * (a[i] + b[i]) : den[i];
+    }
+}
+
 // Adam on the FP32 master parameters
 __global__ void k_adam(float *param, const float *grad, float *m1, float *m2, size_t n, float lr, float b1, float b2,
                        float eps, float c1, float c2) {
@@ -256,6 +350,17 @@ void dn_l1_loss(const __nv_bfloat16 *pred, const float *target, int n, int h, in
                 __nv_bfloat16 *dpred, float *loss, cudaStream_t s) {
     float inv = 1.0f / (float)((size_t)n * h_src * w_src * 3);
     k_l1_loss<<<grid_for((size_t)n * h * w), 256, 0, s>>>(pred, target, n, h, w, h_src, w_src, inv, dpred, loss);
+}
+void dn_tone_loss(const __nv_bfloat16 *pred, const float *target, int n, int h, int w, int h_src, int w_src,
+                  int display, __nv_bfloat16 *dpred, float *loss, cudaStream_t s) {
+    float inv = 1.0f / (float)((size_t)n * h_src * w_src * 3);
+    k_tone_loss<<<grid_for((size_t)n * h * w), 256, 0, s>>>(pred, target, n, h, w, h_src, w_src, inv, display, dpred,
+                                                             loss);
+}
+void dn_fallback(const float *a, const float *b, const float *den, int h, int w, int tile, float k, float *out,
+                 unsigned int *bad, cudaStream_t s) {
+    const int tiles = ((w + tile - 1) / tile) * ((h + tile - 1) / tile);
+    k_dn_fallback<<<tiles, 256, 0, s>>>(a, b, den, h, w, tile, k, out, bad);
 }
 void dn_adam(float *param, const float *grad, float *m1, float *m2, size_t n, float lr, int t, cudaStream_t s) {
     const float b1 = 0.9f, b2 = 0.999f;

@@ -104,8 +104,9 @@ __global__ void k_dof_src(const DofPass d, const mb3d_cu_silight *g, const uint8
         src[i] = o;
     }
     if (d.forward) {
-        mr = __reduce_max_sync(0xffffffffu, __float_as_uint(mr));  // (non-negative: the bits order as the values)
-        if ((threadIdx.x & 31) == 0) atomicMax(max_r_bits, __float_as_uint(mr));
+        // (non-negative: the bits order as the values)
+        const unsigned int mb = __reduce_max_sync(0xffffffffu, __float_as_uint(mr));
+        if ((threadIdx.x & 31) == 0) atomicMax(max_r_bits, mb);
     }
 }
 

@@ -247,6 +247,9 @@ def lib():
         L.mb3d_cu_dn_free.restype = None
         L.mb3d_cu_dn_get_params.argtypes = [vp, vp]
         L.mb3d_cu_dn_set_params.argtypes = [vp, vp]
+        L.mb3d_cu_dn_set_loss.argtypes = [vp, ctypes.c_int]
+        L.mb3d_cu_dn_fallback.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int, ctypes.c_float, vp,
+                                          vp]
         L.mb3d_cu_dn_denoise.argtypes = [vp] + [ctypes.c_int] * 3 + [vp] * 4 + [ctypes.c_float, vp]
         L.mb3d_cu_dn_train_step.argtypes = [vp] + [ctypes.c_int] * 3 + [vp] * 4 + [ctypes.c_float, vp, ctypes.c_float, fp]
         L.mb3d_cu_dn_gradient.argtypes = [vp] + [ctypes.c_int] * 3 + [vp] * 4 + [ctypes.c_float, vp, fp, vp]
@@ -278,7 +281,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render", "mb3d_cu_mc_pass",
             "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24", "mb3d_cu_dof_default", "mb3d_cu_dof",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
-            "mb3d_cu_dn_set_params", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
+            "mb3d_cu_dn_set_params", "mb3d_cu_dn_set_loss", "mb3d_cu_dn_fallback", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
             "mb3d_cu_dn_conv_check", "mb3d_cu_dn_wait_check"]
 
 NOALLOC_MAX_PIXELS = 65536
@@ -593,6 +596,13 @@ class Denoiser:
         self.card._check(lib().mb3d_cu_dn_get_params(self._d, p.ctypes.data))
         return p
 
+    LOSS_L1_LOG, LOSS_TONE_MSE, LOSS_TONE_DISPLAY = 0, 1, 2
+
+    def set_loss(self, kind):
+        """The training loss: LOSS_L1_LOG (default), LOSS_TONE_MSE or
+        LOSS_TONE_DISPLAY."""
+        self.card._check(lib().mb3d_cu_dn_set_loss(self._d, kind))
+
     def set_params(self, p):
         p = np.ascontiguousarray(p, np.float32)
         assert p.size == self.n_params
@@ -613,6 +623,23 @@ class Denoiser:
         self.card._check(lib().mb3d_cu_dn_denoise(self._d, n, h, w, _fptr(radiance), _fptr(albedo), _fptr(normal),
                                                   _fptr(depth), depth_scale, _fptr(out)))
         return out
+
+    def fallback(self, half_a, half_b, den, tile=16, k=3.0, out=None):
+        """mb3d_cu_dn_fallback: the pieces of den whose mean leaves the plain
+        trace's ((half_a + half_b) / 2, two traces from disjoint halves of
+        the rays) by more than k times its noise keep the plain trace.
+        Pictures (h, w, 3) float32, numpy or torch CUDA tensors.  Returns
+        (picture, share of the pieces that keep the plain trace)."""
+        h, w = int(den.shape[0]), int(den.shape[1])
+        if isinstance(den, np.ndarray):
+            half_a, half_b, den = (np.ascontiguousarray(a, np.float32) for a in (half_a, half_b, den))
+        if out is None:
+            out = np.zeros((h, w, 3), np.float32) if isinstance(den, np.ndarray) else den.new_zeros((h, w, 3))
+        share = ctypes.c_float()
+        self.card._order(half_a, half_b, den, out)
+        self.card._check(lib().mb3d_cu_dn_fallback(self._d, h, w, _fptr(half_a), _fptr(half_b), _fptr(den), tile, k,
+                                                   _fptr(out), ctypes.byref(share)))
+        return out, share.value
 
     def train_step(self, radiance, target, albedo=None, normal=None, depth=None, depth_scale=None, lr=1e-3):
         n, h, w = self._shape(radiance)

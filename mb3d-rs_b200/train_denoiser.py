@@ -9,10 +9,14 @@ rendered at 256x256: the 4- and 16-ray pictures (rays 0..15) with their
 first surfaces' albedo, normal and depth, and an independent target of
 `--target-rays` rays (rays 16..); all kept in device memory.  Training:
 Adam on random 128x128 pieces (flipped and turned at random), the input
-taken at 4 or 16 rays, the L1 loss of the network in log space
-(mb3d_cu_dn_train_step: forward and backward on the card's own BF16
-convolution kernels), a cosine learning rate.  The weights go to
-weights/denoiser.f32 (FP32, little endian, the library's parameter order).
+taken at 4 or 16 rays, the loss `--loss` (mb3d_cu_dn_set_loss: the L1 loss
+in log space, the squared error of x / (1 + x), or that plus the squared
+error of the colour clamped to 0..1 that the default painter shows;
+mb3d_cu_dn_train_step: forward and backward on the card's own BF16
+convolution kernels), a cosine learning rate.  Of several learning rates and
+losses the network with the best held-out PSNR of the clamped colour is
+kept.  The weights go to weights/denoiser.f32 (FP32, little endian, the
+library's parameter order).
 """
 import argparse
 import json
@@ -84,9 +88,14 @@ def make_dataset(card, n_crops, target_rays, depth, size=256, seed=scenes.TRAIN_
     return data, time.time() - t0, skipped
 
 
-def train(card, data, steps, batch=8, piece=128, lr_max=2e-3, seed=1, log=print):
+LOSSES = {"l1": mb3dcu.Denoiser.LOSS_L1_LOG, "tone": mb3dcu.Denoiser.LOSS_TONE_MSE,
+          "display": mb3dcu.Denoiser.LOSS_TONE_DISPLAY}
+
+
+def train(card, data, steps, batch=8, piece=128, lr_max=2e-3, seed=1, loss="l1", log=print):
     torch = _torch()
     dn = mb3dcu.Denoiser(card, seed=seed)
+    dn.set_loss(LOSSES[loss])
     g = torch.Generator(device="cuda")
     g.manual_seed(seed)
     n, size = data["r4"].shape[0], data["r4"].shape[1]
@@ -121,18 +130,27 @@ def train(card, data, steps, batch=8, piece=128, lr_max=2e-3, seed=1, log=print)
     return dn, time.time() - t0, losses
 
 
-def val_loss(dn, data, lo, hi):
-    """The L1 loss in log space of the denoised held-out pictures (4 and 16
-    rays) against their targets."""
+def val_scores(dn, data, lo, hi):
+    """The denoised held-out pictures (4 and 16 rays) against their targets:
+    the L1 loss in log space, and the PSNRs of x / (1 + x) and of the colour
+    clamped to 0..1, per ray count."""
     torch = _torch()
-    tot = []
+    l1, se = [], {k: [[], []] for k in ("r4", "r16")}
     for i in range(lo, hi, 8):
         j = min(i + 8, hi)
+        tgt = data["tgt"][i:j].clamp(min=0)
         for k in ("r4", "r16"):
             den = dn.denoise(data[k][i:j].contiguous(), data["alb"][i:j].contiguous(), data["nrm"][i:j].contiguous(),
                              data["dep"][i:j, ..., 0].contiguous(), depth_scale=1.0)
-            tot.append(float((torch.log1p(den) - torch.log1p(data["tgt"][i:j].clamp(min=0))).abs().mean()))
-    return float(np.mean(tot))
+            l1.append(float((torch.log1p(den) - torch.log1p(tgt)).abs().mean()))
+            se[k][0].append(float(((den / (1 + den) - tgt / (1 + tgt)) ** 2).mean()))
+            se[k][1].append(float(((den.clamp(max=1) - tgt.clamp(max=1)) ** 2).mean()))
+    out = {"l1_log": float(np.mean(l1))}
+    for k in se:
+        out[f"psnr_tone_{k}"] = 10 * math.log10(1 / max(np.mean(se[k][0]), 1e-20))
+        out[f"psnr_clamp_{k}"] = 10 * math.log10(1 / max(np.mean(se[k][1]), 1e-20))
+    out["psnr_clamp"] = 0.5 * (out["psnr_clamp_r4"] + out["psnr_clamp_r16"])
+    return out
 
 
 def tonemap(x):
@@ -145,32 +163,15 @@ def psnr(a, ref):
     return 10.0 * math.log10(1.0 / max(mse, 1e-20))
 
 
-def fallback_tiles(noisy_a, noisy_b, den, tile=16, k=3.0):
-    """The tiles where the denoised picture leaves the noisy one by more than
-    k times the noise the two independent halves of the rays show: there the
-    plain trace is kept.  Returns the composite and the share of such tiles."""
-    h, w, _ = den.shape
-    noisy = 0.5 * (noisy_a + noisy_b)
-    out = den.copy()
-    n = bad = 0
-    for y in range(0, h - tile + 1, tile):
-        for x in range(0, w - tile + 1, tile):
-            sl = (slice(y, y + tile), slice(x, x + tile))
-            a, b, d, m = (tonemap(v[sl]) for v in (noisy_a, noisy_b, den, noisy))
-            sigma = np.sqrt(np.mean((a - b) ** 2) / 4.0 / (tile * tile * 3)) + 1e-3
-            n += 1
-            if abs(float(np.mean(d - m))) > k * sigma:
-                bad += 1
-                out[sl] = noisy[sl]
-    return out, bad / max(n, 1)
-
-
-def evaluate(card, dn, rect=(720, 405, 480, 270), ref_rays=1024, log=print):
-    """The 1920x1080 workload on a rectangle: the plain trace at ref_rays,
-    the 4..64-ray traces and their denoised pictures; times on the card.
-    PSNRs of the tone-mapped linear records (psnr_*) and of the 8-bit
-    pictures the reference's painter makes of them (psnr8_*, paint_recs with
-    the default display settings, on the card)."""
+def evaluate(card, dn, rect=None, ref_rays=1024, levels=(4, 8, 16, 32, 64), log=print):
+    """The 1920x1080 Monte Carlo workload (the whole frame, or a rectangle
+    (x, y, w, h)): the plain trace at ref_rays, and per ray count the method:
+    two traces of half the rays each (their mean is the plain trace of all
+    the rays), the denoised picture of their mean, the plain trace kept where
+    the denoised picture leaves it (mb3d_cu_dn_fallback, 16x16 pieces, 3
+    sigma); times on the card.  PSNRs of the tone-mapped linear records
+    (psnr_*) and of the 8-bit pictures the reference's painter makes of them
+    (psnr8_*, paint_recs with the default display settings, on the card)."""
     torch = _torch()
     sc = scenes.c5_mc()
     lv = mb3dcu.mc_light_default(sc)
@@ -181,7 +182,11 @@ def evaluate(card, dn, rect=(720, 405, 480, 270), ref_rays=1024, log=print):
         return r, card.stats()["ms_total"]
 
     ref, ms_ref = trace(ref_rays, ray0=4096)  # (rays of their own, each with its own Halton record (< 65536))
-    res = {"rect": list(rect), "ref_rays": ref_rays, "ms_ref": ms_ref, "levels": []}
+    st = card.stats()
+    area = list(rect) if rect else [0, 0, sc.width, sc.height]
+    res = {"rect": area, "ref_rays": ref_rays, "ms_ref": ms_ref,
+           "mpaths_per_s": area[2] * area[3] * ref_rays / ms_ref / 1e3, "de_evals_per_s": st["de_evals"] / ms_ref * 1e3,
+           "levels": []}
     paint_opts = mb3dcu.mc_paint_default()
     ref8 = card.mc_paint(ref["radiance"], paint_opts).astype(np.float64)
 
@@ -189,47 +194,54 @@ def evaluate(card, dn, rect=(720, 405, 480, 270), ref_rays=1024, log=print):
         mse = float(np.mean((card.mc_paint(x, paint_opts).astype(np.float64) - ref8) ** 2))
         return 10.0 * math.log10(255.0 ** 2 / max(mse, 1e-12))
 
-    for rays in (4, 8, 16, 32, 64):
-        r, ms = trace(rays)
-        dmax = float(r["depth"].max()) or 1.0
-        rad = torch.from_numpy(r["radiance"]).cuda()[None]
-        alb = torch.from_numpy(r["albedo"]).cuda()[None]
-        nrm = torch.from_numpy(r["normal"]).cuda()[None]
-        dp = torch.from_numpy(r["depth"]).cuda()[None]
-        dn.denoise(rad, alb, nrm, dp, depth_scale=1.0 / dmax)  # (warm)
-        ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        ev[0].record()
-        den = dn.denoise(rad, alb, nrm, dp, depth_scale=1.0 / dmax)
-        ev[1].record()
-        torch.cuda.synchronize()
-        ms_dn = ev[0].elapsed_time(ev[1])
-        den = den[0].cpu().numpy()
-        half = max(rays // 2, 1)
-        ha, _ = trace(half, 0)
-        hb, _ = trace(half, half)
-        comp, fb = fallback_tiles(ha["radiance"], hb["radiance"], den)
-        lvl = {"rays": rays, "ms_trace": ms, "ms_denoise": ms_dn, "psnr_noisy": psnr(r["radiance"], ref["radiance"]),
-               "psnr_denoised": psnr(den, ref["radiance"]), "psnr_with_fallback": psnr(comp, ref["radiance"]),
-               "fallback_rate": fb, "psnr8_noisy": psnr8(r["radiance"]), "psnr8_denoised": psnr8(den),
-               "psnr8_with_fallback": psnr8(comp)}
+    for rays in levels:
+        half = rays // 2
+        ha, ms_a = trace(half, 0)
+        hb, ms_b = trace(half, half)
+        dmax = float(ha["depth"].max()) or 1.0
+        a, b = (torch.from_numpy(v["radiance"]).cuda() for v in (ha, hb))
+        alb = torch.from_numpy(ha["albedo"]).cuda()[None]
+        nrm = torch.from_numpy(ha["normal"]).cuda()[None]
+        dp = torch.from_numpy(ha["depth"]).cuda()[None]
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        for it in range(2):  # (the first round warms)
+            ev[0].record()
+            noisy = 0.5 * (a + b)
+            den = dn.denoise(noisy[None], alb, nrm, dp, depth_scale=1.0 / dmax)[0]
+            ev[1].record()
+            comp, fb = dn.fallback(a, b, den, tile=16, k=3.0)
+            ev[2].record()
+            torch.cuda.synchronize()
+        ms_dn, ms_fb = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+        noisy, den, comp = (v.cpu().numpy() for v in (noisy, den, comp))
+        ms = ms_a + ms_b
+        lvl = {"rays": rays, "ms_trace": ms, "ms_denoise": ms_dn, "ms_fallback": ms_fb,
+               "psnr_noisy": psnr(noisy, ref["radiance"]), "psnr_denoised": psnr(den, ref["radiance"]),
+               "psnr_with_fallback": psnr(comp, ref["radiance"]), "fallback_rate": fb, "psnr8_noisy": psnr8(noisy),
+               "psnr8_denoised": psnr8(den), "psnr8_with_fallback": psnr8(comp)}
         res["levels"].append(lvl)
-        log(f"  {rays} rays: trace {ms:.1f} ms, denoise {ms_dn:.2f} ms, PSNR noisy {lvl['psnr_noisy']:.2f} "
-            f"denoised {lvl['psnr_denoised']:.2f} (fallback {fb:.3f}: {lvl['psnr_with_fallback']:.2f}); 8-bit "
-            f"noisy {lvl['psnr8_noisy']:.2f} denoised {lvl['psnr8_denoised']:.2f}", flush=True)
-    ok = [lv_ for lv_ in res["levels"] if lv_["psnr_denoised"] >= 35.0]
+        log(f"  {rays} rays: trace {ms:.1f} ms, denoise {ms_dn:.2f} ms, fallback {ms_fb:.2f} ms, PSNR noisy "
+            f"{lvl['psnr_noisy']:.2f} denoised {lvl['psnr_denoised']:.2f} (fallback {fb:.3f}: "
+            f"{lvl['psnr_with_fallback']:.2f}); 8-bit noisy {lvl['psnr8_noisy']:.2f} denoised "
+            f"{lvl['psnr8_denoised']:.2f} (with fallback {lvl['psnr8_with_fallback']:.2f})", flush=True)
+    for lv_ in res["levels"]:
+        lv_["ms_method"] = lv_["ms_trace"] + lv_["ms_denoise"] + lv_["ms_fallback"]
+        lv_["time_ratio_vs_ref"] = lv_["ms_method"] / ms_ref
+    ok = [lv_ for lv_ in res["levels"] if lv_["psnr_with_fallback"] >= 35.0]
     if ok:
-        best = min(ok, key=lambda l: l["ms_trace"] + l["ms_denoise"])
-        res["time_to_35db_ms"] = best["ms_trace"] + best["ms_denoise"]
+        best = min(ok, key=lambda l: l["ms_method"])
+        res["time_to_35db_ms"] = best["ms_method"]
         res["time_to_35db_rays"] = best["rays"]
-        res["time_ratio_vs_ref"] = res["time_to_35db_ms"] / ms_ref
+        res["time_ratio_vs_ref"] = best["ms_method"] / ms_ref
     plain = [lv_ for lv_ in res["levels"] if lv_["psnr_noisy"] >= 35.0]
     if plain:
         res["plain_to_35db_rays"] = min(l["rays"] for l in plain)
-    ok8 = [lv_ for lv_ in res["levels"] if lv_["psnr8_denoised"] >= 35.0]
+    ok8 = [lv_ for lv_ in res["levels"] if lv_["psnr8_with_fallback"] >= 35.0]
     if ok8:
-        best = min(ok8, key=lambda l: l["ms_trace"] + l["ms_denoise"])
-        res["time_to_35db_8bit_ms"] = best["ms_trace"] + best["ms_denoise"]
+        best = min(ok8, key=lambda l: l["ms_method"])
+        res["time_to_35db_8bit_ms"] = best["ms_method"]
         res["time_to_35db_8bit_rays"] = best["rays"]
+        res["time_ratio_8bit_vs_ref"] = best["ms_method"] / ms_ref
     plain8 = [lv_ for lv_ in res["levels"] if lv_["psnr8_noisy"] >= 35.0]
     if plain8:
         res["plain_to_35db_8bit_rays"] = min(l["rays"] for l in plain8)
@@ -247,6 +259,8 @@ def main():
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--report", default=None)
     ap.add_argument("--ref-rays", type=int, default=1024)
+    ap.add_argument("--loss", nargs="+", choices=sorted(LOSSES), default=["display"])
+    ap.add_argument("--rect", type=int, nargs=4, default=None, help="x y w h (default: the whole frame)")
     a = ap.parse_args()
     card = mb3dcu.Card(0)
     report = {}
@@ -258,19 +272,26 @@ def main():
         train_part = {k: v[:a.crops] for k, v in data.items()}
         best = None
         runs = []
-        for lr in a.lr:
-            dn, t_train, losses = train(card, train_part, a.steps, batch=a.batch, lr_max=lr)
-            vl = val_loss(dn, data, a.crops, a.crops + n_val)
-            print(f"lr {lr}: {a.steps} steps in {t_train:.0f} s, loss {np.mean(losses[:100]):.4f} -> "
-                  f"{np.mean(losses[-200:]):.4f}, held-out {vl:.4f}", flush=True)
-            runs.append(dict(lr=lr, s_train=t_train, loss_first=float(np.mean(losses[:100])),
-                             loss_last=float(np.mean(losses[-200:])), val_loss=vl))
-            if best is None or vl < best[0]:
-                if best is not None:
-                    best[1].close()
-                best = (vl, dn)
-            else:
-                dn.close()
+        if os.path.exists(a.out):
+            prev = mb3dcu.Denoiser(card)
+            prev.set_params(np.fromfile(a.out, "<f4"))
+            report["previous_weights_held_out"] = val_scores(prev, data, a.crops, a.crops + n_val)
+            print(f"previous weights: held-out {json.dumps(report['previous_weights_held_out'])}", flush=True)
+            prev.close()
+        for loss in a.loss:
+            for lr in a.lr:
+                dn, t_train, losses = train(card, train_part, a.steps, batch=a.batch, lr_max=lr, loss=loss)
+                vs = val_scores(dn, data, a.crops, a.crops + n_val)
+                print(f"{loss} lr {lr}: {a.steps} steps in {t_train:.0f} s, loss {np.mean(losses[:100]):.4f} -> "
+                      f"{np.mean(losses[-200:]):.4f}, held-out {json.dumps(vs)}", flush=True)
+                runs.append(dict(loss=loss, lr=lr, s_train=t_train, loss_first=float(np.mean(losses[:100])),
+                                 loss_last=float(np.mean(losses[-200:])), held_out=vs))
+                if best is None or vs["psnr_clamp"] > best[0]:
+                    if best is not None:
+                        best[1].close()
+                    best = (vs["psnr_clamp"], dn)
+                else:
+                    dn.close()
         dn = best[1]
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
         dn.get_params().astype("<f4").tofile(a.out)
@@ -280,7 +301,7 @@ def main():
     else:
         dn = mb3dcu.Denoiser(card)
         dn.set_params(np.fromfile(a.out, "<f4"))
-    report["eval"] = evaluate(card, dn, ref_rays=a.ref_rays)
+    report["eval"] = evaluate(card, dn, rect=tuple(a.rect) if a.rect else None, ref_rays=a.ref_rays)
     print(json.dumps(report))
     if a.report:
         with open(a.report, "w") as f:

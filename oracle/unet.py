@@ -157,6 +157,27 @@ def l1_loss(pred, target):
     return np.abs(e).sum() / cnt, d
 
 
+def tone_mse_loss(pred, target, display=False):
+    """The squared error of x / (1 + x) (prediction: log(1 + x), its tone
+    1 - exp(-pred)) and its gradient with respect to pred; with display, plus
+    the squared error of x clamped to 0..1, its gradient passed through the
+    clamp wherever the clamped colours differ (exp(pred) capped at 2)."""
+    p = pred[..., :3]
+    q = np.exp(-p)
+    y = np.maximum(target, 0.0)
+    e = (1.0 - q) - y / (1.0 + y)
+    cnt = e.size
+    loss = (e * e).sum()
+    g = 2.0 * e * q
+    if display:
+        ed = np.clip(np.expm1(p), 0.0, 1.0) - np.minimum(y, 1.0)
+        loss += (ed * ed).sum()
+        g += 2.0 * ed * np.exp(np.minimum(p, np.log(2.0)))
+    d = np.zeros_like(pred)
+    d[..., :3] = g / cnt
+    return loss / cnt, d
+
+
 def backward(params, c, dpred):
     """The gradient of the loss with respect to every parameter (flat)."""
     P = unpack(np.asarray(params, np.float64))

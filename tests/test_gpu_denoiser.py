@@ -70,10 +70,13 @@ def _batch(rng, n, h, w):
     return rad, alb, nrm, dep, tgt
 
 
-def test_network_gradient_matches_fp64_oracle(card):
+@pytest.mark.parametrize("kind", [mb3dcu.Denoiser.LOSS_L1_LOG, mb3dcu.Denoiser.LOSS_TONE_MSE,
+                                  mb3dcu.Denoiser.LOSS_TONE_DISPLAY])
+def test_network_gradient_matches_fp64_oracle(card, kind):
     rng = np.random.default_rng(5)
     dn = mb3dcu.Denoiser(card, seed=3)
     try:
+        dn.set_loss(kind)
         p = dn.get_params()
         # non-zero biases, so that every ReLU sees both signs
         p = p + np.where(np.arange(p.size) % 7 == 0, 0.01, 0.0).astype(np.float32)
@@ -82,7 +85,10 @@ def test_network_gradient_matches_fp64_oracle(card):
         loss, g = dn.gradient(rad, tgt, alb, nrm, dep, depth_scale=1.0)
         x = unet.pack_input(rad.astype(np.float64), alb, nrm, dep, 1.0)
         pred, cache = unet.forward(p, x)
-        le, dpred = unet.l1_loss(pred, tgt.astype(np.float64))
+        if kind == mb3dcu.Denoiser.LOSS_L1_LOG:
+            le, dpred = unet.l1_loss(pred, tgt.astype(np.float64))
+        else:
+            le, dpred = unet.tone_mse_loss(pred, tgt.astype(np.float64), kind == mb3dcu.Denoiser.LOSS_TONE_DISPLAY)
         ge = unet.backward(p, cache, dpred)
         assert abs(loss - le) <= 0.02 * le, (loss, le)
         o = 0
@@ -99,10 +105,83 @@ def test_network_gradient_matches_fp64_oracle(card):
         dn.close()
 
 
-def test_training_lowers_the_loss(card):
+def _fallback_np(a, b, den, tile, k):
+    """The fallback rule in FP64 numpy: per tile x tile piece (ragged at the
+    right and bottom), the keep-the-plain-trace decision and its margin."""
+    def tone(x):
+        x = np.maximum(x.astype(np.float64), 0.0)
+        return x / (1.0 + x)
+    h, w, _ = den.shape
+    m = 0.5 * (a + b)  # (float32, as the card forms it)
+    out = den.copy()
+    keep, margin = [], []
+    for y in range(0, h, tile):
+        for x in range(0, w, tile):
+            sl = (slice(y, y + tile), slice(x, x + tile))
+            cnt = den[sl].size
+            sigma = np.sqrt(np.sum((tone(a[sl]) - tone(b[sl])) ** 2) / cnt / 4.0 / cnt) + 1e-3
+            dev = abs(np.sum(tone(den[sl]) - tone(m[sl])) / cnt)
+            keep.append(dev > k * sigma)
+            margin.append(abs(dev - k * sigma) / (k * sigma))
+            if keep[-1]:
+                out[sl] = m[sl]
+    return out, np.array(keep), np.array(margin)
+
+
+def test_fallback_keeps_the_plain_trace_where_the_denoised_picture_is_off(card):
+    """The plain trace as the fallback and judge (mb3d_cu_dn_fallback): two
+    noisy halves of a smooth picture and a 'denoised' picture equal to the
+    smooth one except in two pieces made 60 % brighter (one of them the
+    ragged corner piece): exactly those keep the plain trace; the decisions
+    and the composite equal the FP64 rule's; device buffers and out == den
+    give the same."""
+    rng = np.random.default_rng(21)
+    h, w, tile = 50, 70, 16
+    yy, xx = np.mgrid[0:h, 0:w]
+    truth = (0.4 + 0.3 * np.sin(xx / 9.0)[..., None] * np.cos(yy / 7.0)[..., None] * np.array([1.0, 0.8, 0.6]))
+    truth = truth.astype(np.float32)
+    a = (truth * rng.gamma(8.0, 1 / 8.0, truth.shape)).astype(np.float32)
+    b = (truth * rng.gamma(8.0, 1 / 8.0, truth.shape)).astype(np.float32)
+    den = truth.copy()
+    den[16:32, 32:48] *= 1.6
+    den[48:50, 64:70] *= 1.6
+    want, keep, margin = _fallback_np(a, b, den, tile, 3.0)
+    assert margin.min() > 1e-4  # (no decision at the threshold's edge)
+    tiles_x = (w + tile - 1) // tile
+    assert keep[1 * tiles_x + 2] and keep[3 * tiles_x + 4]
+    dn = mb3dcu.Denoiser(card, seed=1)
+    try:
+        got, share = dn.fallback(a, b, den, tile=tile, k=3.0)
+        assert share == pytest.approx(keep.mean(), abs=1e-6)
+        assert np.array_equal(got, want)
+        import torch
+        t = [torch.from_numpy(v).cuda() for v in (a, b, den)]
+        got_d, share_d = dn.fallback(*t, tile=tile, k=3.0, out=t[2])
+        assert share_d == share and np.array_equal(got_d.cpu().numpy(), want)
+        # a denoised picture equal to the truth: few pieces, the rule's own
+        _, keep0, _ = _fallback_np(a, b, truth, tile, 3.0)
+        assert dn.fallback(a, b, truth, tile=tile)[1] == pytest.approx(keep0.mean(), abs=1e-6) and keep0.mean() < 0.2
+        with pytest.raises(mb3dcu.CardError):
+            dn.fallback(a, b, den, tile=0)
+    finally:
+        dn.close()
+
+
+def test_unknown_loss_is_refused(card):
+    dn = mb3dcu.Denoiser(card, seed=1)
+    try:
+        with pytest.raises(mb3dcu.CardError):
+            dn.set_loss(7)
+    finally:
+        dn.close()
+
+
+@pytest.mark.parametrize("kind", [mb3dcu.Denoiser.LOSS_L1_LOG, mb3dcu.Denoiser.LOSS_TONE_DISPLAY])
+def test_training_lowers_the_loss(card, kind):
     rng = np.random.default_rng(9)
     dn = mb3dcu.Denoiser(card, seed=4)
     try:
+        dn.set_loss(kind)
         rad, alb, nrm, dep, tgt = _batch(rng, 4, 64, 64)
         first = dn.train_step(rad, tgt, alb, nrm, dep, lr=2e-3)
         for _ in range(60):

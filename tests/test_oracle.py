@@ -324,6 +324,40 @@ def test_unet_oracle_backward_matches_finite_differences():
         assert abs(num - g[i]) <= 1e-4 * max(1.0, abs(num)), (i, num, g[i])
 
 
+def test_unet_oracle_tone_loss_gradient_matches_finite_differences():
+    """The tone-space squared error's gradient with respect to the
+    prediction (oracle/unet.py tone_mse_loss) against central differences."""
+    import unet
+    rng = np.random.default_rng(4)
+    pred = rng.normal(0.3, 0.6, (1, 4, 5, 16))
+    tgt = rng.gamma(1.0, 0.5, (1, 4, 5, 3))
+    tgt[0, 0, 0, 0] = -0.2  # a negative sample counts as 0
+    loss, d = unet.tone_mse_loss(pred, tgt)
+    assert np.all(d[..., 3:] == 0.0)
+    for idx in [(0, 0, 0, 0), (0, 1, 2, 1), (0, 3, 4, 2), (0, 2, 1, 0)]:
+        e = np.zeros_like(pred)
+        e[idx] = 1e-6
+        num = (unet.tone_mse_loss(pred + e, tgt)[0] - unet.tone_mse_loss(pred - e, tgt)[0]) / 2e-6
+        assert abs(num - d[idx]) <= 1e-6 * max(1.0, abs(num)), (idx, num, d[idx])
+    # the tone of the exact prediction log(1 + y) is y / (1 + y): no loss
+    exact = np.zeros_like(pred)
+    exact[..., :3] = np.log1p(np.maximum(tgt, 0.0))
+    assert unet.tone_mse_loss(exact, tgt)[0] < 1e-30
+    assert unet.tone_mse_loss(exact, tgt, display=True)[0] < 1e-30
+    # the display term: the true gradient where the clamp is open (0 < x < 1)
+    inner = rng.uniform(0.05, 0.65, pred.shape)
+    ld, dd = unet.tone_mse_loss(inner, tgt, display=True)
+    for idx in [(0, 0, 0, 0), (0, 1, 2, 1), (0, 3, 4, 2)]:
+        e = np.zeros_like(inner)
+        e[idx] = 1e-6
+        num = (unet.tone_mse_loss(inner + e, tgt, True)[0] - unet.tone_mse_loss(inner - e, tgt, True)[0]) / 2e-6
+        assert abs(num - dd[idx]) <= 1e-6 * max(1.0, abs(num)), (idx, num, dd[idx])
+    # a prediction above 1 for a target below 1 is pulled down, though clamped
+    hi = np.full((1, 1, 1, 16), 3.0)
+    assert unet.tone_mse_loss(hi, np.full((1, 1, 1, 3), 0.5), True)[1][0, 0, 0, 0] > \
+        unet.tone_mse_loss(hi, np.full((1, 1, 1, 3), 0.5))[1][0, 0, 0, 0]
+
+
 # ---- the screen space ambient occlusion (ssao::ssao24), the reference's own
 # tests restated (src/ssao.rs:338-417)
 
