@@ -472,8 +472,20 @@ void mb3d_cu_ssao_default(mb3d_cu_ssao_opts *out);
  * depth buffer alone: per pixel the largest elevation angle in 32 directions
  * on ever smoother levels of the depth buffer, their arctangents summed.
  * Regular or random sampling (EINVAL for an opts outside the documented
- * ranges); the older 15-bit variant is not on the card. */
+ * ranges); the older 15-bit variant is mb3d_cu_ssao15. */
 int mb3d_cu_ssao24(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_ssao_opts *opts,
+                   mb3d_cu_silight *gbuf);
+
+/* Replaces gpu::ssao15 (src/gpu.rs:3726; ssao15::ssao15,
+ * src/ssao15.rs:282-411, SsaoParams::bits15): the older "15 bit" ambient
+ * occlusion of the object pixels of the scene's whole G-buffer (host or
+ * device): the depth buffer scaled to 0..128 and smoothed into "a trous"
+ * levels, per pixel the steepest slope per 1/32 circle over rings of
+ * samples that widen with the level, the slopes' arctangents summed into
+ * amb_shadow.  Uses threshold, t0 and wrap_x of opts (border_mirror and
+ * random belong to the 24-bit pass); pictures below 4 x 4 are left as they
+ * are, as the reference does. */
+int mb3d_cu_ssao15(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_ssao_opts *opts,
                    mb3d_cu_silight *gbuf);
 
 /* ---- the learned denoiser of the Monte Carlo pictures ----

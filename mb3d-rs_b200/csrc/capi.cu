@@ -1051,6 +1051,42 @@ int mb3d_cu_ssao24(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_ssao_o
     return 0;
 }
 
+int mb3d_cu_ssao15(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_ssao_opts *o, mb3d_cu_silight *gbuf) {
+    if (!c || !sc || !o || !gbuf) return fail(MB3D_CU_EINVAL, "NULL argument");
+    if (!(o->threshold == o->threshold)) return fail(MB3D_CU_EINVAL, "threshold not a number");
+    DevParams p;
+    std::string err;
+    int r = setup_params(*sc, p, err);
+    if (r < 0) return fail(r, err);
+    const int w = p.width, h = p.height;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    cudaStream_t s = c->stream;
+    const size_t npix = (size_t)w * h, gb = npix * sizeof(mb3d_cu_silight);
+    const bool dev = is_device_ptr(gbuf);
+    const size_t scratch = (ssao15_scratch_bytes(w, h) + 255) & ~(size_t)255;
+    if (int e = grow((void **)&c->d_ssao, &c->ssao_cap, scratch + (dev ? 0 : gb))) return e;
+    mb3d_cu_silight *dg = dev ? gbuf : reinterpret_cast<mb3d_cu_silight *>(c->d_ssao + scratch);
+    if (!dev) CU_TRY(cudaMemcpyAsync(dg, gbuf, gb, cudaMemcpyHostToDevice, s));
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    uint32_t launches = 0;
+    const int rr = ssao15_run(dg, w, h, p.zc_mul, p.zcorr, *o, c->d_ssao, c->sms, s, &launches);
+    if (rr == -2) return fail(MB3D_CU_EIO, "ssao15: a ring's samples beyond the table");
+    if (int e = check_launch("k15_sample")) return e;
+    if (rr != 0) return fail(MB3D_CU_EIO, "ssao15: a CUDA call failed");
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    if (!dev) CU_TRY(cudaMemcpyAsync(gbuf, dg, gb, cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    c->stats.launches = launches;
+    return 0;
+}
+
 static int mc_halton(mb3d_cu_ctx *c) {
     if (c->d_halton) return 0;
     const std::vector<uint32_t> &t = mc_halton_table();

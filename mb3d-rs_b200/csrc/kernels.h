@@ -155,6 +155,12 @@ void mc_paint_launch(const float *col, const uint8_t *rays, uint32_t n, const mb
 // the 24-bit screen space ambient occlusion of a w x h G-buffer (ssao.cu);
 // scratch holds ssao_scratch_bytes(w, h, random)
 size_t ssao_scratch_bytes(int w, int h, int random);
+// the 15-bit screen space ambient occlusion of a w x h G-buffer in device
+// memory (ssao15.cu), scratch of ssao15_scratch_bytes(w, h); synchronises the
+// stream; 0, -1 (a CUDA call failed) or -2 (a ring beyond its table)
+size_t ssao15_scratch_bytes(int w, int h);
+int ssao15_run(mb3d_cu_silight *g, int w, int h, double zc_mul, double zcorr, const mb3d_cu_ssao_opts &o,
+               unsigned char *scratch, int sms, cudaStream_t s, uint32_t *launches);
 void ssao24_launch(mb3d_cu_silight *gbuf, int w, int h, double zc_mul, double zcorr, const mb3d_cu_ssao_opts &o,
                    void *scratch, int sms, cudaStream_t s);
 

@@ -271,6 +271,7 @@ def lib():
         L.mb3d_cu_ssao_default.argtypes = [ctypes.POINTER(SsaoOpts)]
         L.mb3d_cu_ssao_default.restype = None
         L.mb3d_cu_ssao24.argtypes = [vp, sp, ctypes.POINTER(SsaoOpts), vp]
+        L.mb3d_cu_ssao15.argtypes = [vp, sp, ctypes.POINTER(SsaoOpts), vp]
         _lib = L
     return _lib
 
@@ -279,7 +280,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_march_ex", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render", "mb3d_cu_mc_pass",
-            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24", "mb3d_cu_dof_default", "mb3d_cu_dof",
+            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24", "mb3d_cu_ssao15", "mb3d_cu_dof_default", "mb3d_cu_dof",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_set_loss", "mb3d_cu_dn_fallback", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
             "mb3d_cu_dn_conv_check", "mb3d_cu_dn_wait_check"]
@@ -498,6 +499,17 @@ class Card:
             gbuf = np.ascontiguousarray(gbuf).copy()
         self._order(gbuf)
         self._check(lib().mb3d_cu_ssao24(self._ctx, ctypes.byref(scene), ctypes.byref(opts), _ptr(gbuf)[0]))
+        return gbuf
+
+    def ssao15(self, scene, gbuf, opts=None):
+        """gpu::ssao15 on the card: the older 15-bit ambient occlusion
+        (threshold, t0 and wrap_x of opts); a numpy G-buffer is returned as a
+        new array, a torch CUDA byte tensor is changed in place."""
+        opts = ssao_default() if opts is None else opts
+        if isinstance(gbuf, np.ndarray):
+            gbuf = np.ascontiguousarray(gbuf).copy()
+        self._order(gbuf)
+        self._check(lib().mb3d_cu_ssao15(self._ctx, ctypes.byref(scene), ctypes.byref(opts), _ptr(gbuf)[0]))
         return gbuf
 
     def mc_render(self, scene, opts, light=None, precision=FP32_FP64, out=None, cancel=None):

@@ -273,11 +273,12 @@ def main():
         best = None
         runs = []
         if os.path.exists(a.out):
+            # the weights there now stay unless a new network beats them on the held-out pictures
             prev = mb3dcu.Denoiser(card)
             prev.set_params(np.fromfile(a.out, "<f4"))
-            report["previous_weights_held_out"] = val_scores(prev, data, a.crops, a.crops + n_val)
-            print(f"previous weights: held-out {json.dumps(report['previous_weights_held_out'])}", flush=True)
-            prev.close()
+            report["previous_weights_held_out"] = vs = val_scores(prev, data, a.crops, a.crops + n_val)
+            print(f"previous weights: held-out {json.dumps(vs)}", flush=True)
+            best = (vs["psnr_clamp"], prev)
         for loss in a.loss:
             for lr in a.lr:
                 dn, t_train, losses = train(card, train_part, a.steps, batch=a.batch, lr_max=lr, loss=loss)
@@ -293,6 +294,8 @@ def main():
                 else:
                     dn.close()
         dn = best[1]
+        report["kept"] = "previous" if "previous_weights_held_out" in report and \
+            best[0] == report["previous_weights_held_out"]["psnr_clamp"] else "new"
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
         dn.get_params().astype("<f4").tofile(a.out)
         report.update(crops=a.crops, held_out=n_val, target_rays=a.target_rays, steps=a.steps, batch=a.batch,

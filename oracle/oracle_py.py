@@ -50,6 +50,10 @@ def lib():
         L.oracle_paint.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp]
         L.oracle_ssao24.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_ssao15.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_float,
+                                    ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_ssao15_arctan.argtypes = [ctypes.c_int, ctypes.c_int]
+        L.oracle_ssao15_axis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]
         L.oracle_ssao_levels.argtypes = [ctypes.c_int, ctypes.c_int]
         L.oracle_ssao_rne.argtypes = [ctypes.c_float]
         L.oracle_ssao_rne.restype = ctypes.c_float
@@ -223,6 +227,26 @@ def ssao24(gbuf, w, h, zc_mul, zcorr, threshold=2.0, border_mirror=0.0, t0=False
     _chk(lib().oracle_ssao24(g.ctypes.data, w, h, zc_mul, zcorr, threshold, border_mirror, int(t0), int(wrap_x),
                              int(random)))
     return g
+
+
+def ssao15(gbuf, w, h, zc_mul, zcorr, threshold=2.0, t0=False, wrap_x=False, threads=0):
+    """ssao15::ssao15 (src/ssao15.rs:282-411): a copy of the G-buffer with
+    the 15-bit SSAO's amb_shadow on its object pixels."""
+    g = np.ascontiguousarray(gbuf).copy()
+    _chk(lib().oracle_ssao15(g.ctypes.data, w, h, zc_mul, zcorr, threshold, int(t0), int(wrap_x), threads))
+    return g
+
+
+def ssao15_arctan(y, x):
+    """fastIntArcTan2 (src/ssao15.rs:22-50)."""
+    return lib().oracle_ssao15_arctan(y, x)
+
+
+def ssao15_axis(pos, size, max_rad, step):
+    """axis_samples (src/ssao15.rs:193-231)."""
+    out = np.zeros(4096, np.int32)
+    n = lib().oracle_ssao15_axis(pos, size, max_rad, step, out.ctypes.data, out.size)
+    return [int(v) for v in out[:n]]
 
 
 def ssao_levels(w, h):

@@ -212,6 +212,43 @@ def test_ssao_matches_the_oracle(card):
     assert dev.cpu().numpy().tobytes() == host.tobytes()
 
 
+def test_ssao15_matches_the_oracle(card):
+    """gpu::ssao15 (the older 15-bit SSAO) against the oracle's
+    ssao15::ssao15 on the same G-buffers (the hybrid frame at 480x270, and
+    a small 37x23 picture where every pixel is near a border): the levels
+    and the slopes are the reference's bit for bit, the arctangents' sum
+    uses the card's atanf (one step apart where the sum sits at a rounding
+    boundary); the t0 variant, the threshold and the panorama's wrap."""
+    import torch
+    c2 = scenes.scaled(scenes.c2_hybrid(), 480, 270)
+    small = scenes.scaled(scenes.c2_hybrid(), 37, 23)
+    for sc in (c2, small):
+        g = O.march(sc, mb3dcu.SILIGHT)
+        zm, zr = zc(sc)
+        obj = ~mb3dcu.is_background(g)
+        assert obj.mean() > 0.2
+        for kw in [dict(), dict(threshold=1.5, t0=True), dict(wrap_x=True, threshold=3.0)]:
+            o = mb3dcu.ssao_default()
+            for k, v in kw.items():
+                setattr(o, k, v)
+            want = O.ssao15(g, sc.width, sc.height, zm, zr, **kw)
+            got = card.ssao15(sc, g, o)
+            d = np.abs(got["amb_shadow"].astype(np.int64) - want["amb_shadow"].astype(np.int64))[obj]
+            assert (d == 0).mean() >= 0.99 and d.max() <= 1, (sc.width, kw, (d == 0).mean(), d.max())
+            assert np.array_equal(got["amb_shadow"][~obj], g["amb_shadow"][~obj])
+            assert np.array_equal(got["zpos_fine"], g["zpos_fine"])
+    # a device G-buffer, changed in place, equals the host one
+    g = O.march(c2, mb3dcu.SILIGHT)
+    dev = torch.from_numpy(g.view(np.uint8).copy()).cuda()
+    card.ssao15(c2, dev)
+    torch.cuda.synchronize()
+    assert dev.cpu().numpy().tobytes() == card.ssao15(c2, g).tobytes()
+    # pictures below 4 x 4 stay as they are
+    tiny = scenes.scaled(scenes.c2_hybrid(), 3, 3)
+    gt = O.march(tiny, mb3dcu.SILIGHT)
+    assert card.ssao15(tiny, gt).tobytes() == gt.tobytes()
+
+
 def test_render_device_buffer_equals_host_buffer(card):
     import torch
     sc = scenes.scaled(scenes.c2_hybrid(), 240, 136)

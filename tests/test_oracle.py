@@ -511,3 +511,63 @@ def test_ssao_random_sampling_sees_the_pit_too():
     a = O.ssao24(gb, w, h, 300.0, 0.001, random=2)
     b = O.ssao24(gb, w, h, 300.0, 0.001, random=2)
     assert a.tobytes() == b.tobytes()
+
+
+# ---- the older 15-bit SSAO (ssao15::ssao15), the reference's own tests
+# restated (src/ssao15.rs:413-445)
+
+def test_ssao15_arctan_buckets():
+    assert O.ssao15_arctan(0, 1) == 16
+    assert O.ssao15_arctan(1, 0) == 24
+    assert O.ssao15_arctan(0, -1) == 0
+    assert O.ssao15_arctan(-1, 0) == 8
+    for y, x in [(3, 7), (-5, 2), (-1, -9), (6, -6)]:
+        assert 0 <= O.ssao15_arctan(y, x) < 32
+    # the buckets go round the circle once, in order, as the angle grows
+    prev, turns = None, 0
+    for k in range(360):
+        a = np.deg2rad(k + 0.5)
+        b = O.ssao15_arctan(int(round(1000 * np.sin(a))), int(round(1000 * np.cos(a))))
+        if prev is not None and b < prev:
+            turns += 1
+        prev = b
+    assert turns == 1
+
+
+def test_ssao15_axis_grid():
+    v = O.ssao15_axis(50, 100, 12, 2)
+    assert v[0] == -12 and v[-1] == 12 and len(v) == 13
+    assert O.ssao15_axis(3, 100, 12, 4)[:3] == [-3, 0, 4]
+    assert O.ssao15_axis(97, 100, 12, 4)[-1] == 2
+
+
+def test_ssao15_hole_is_darker_than_plane():
+    w = h = 64
+    yy, xx = np.mgrid[0:h, 0:w]
+    d = np.sqrt((xx - 32.0) ** 2 + (yy - 32.0) ** 2)
+    pit = np.where(d < 10.0, 3000.0 * (1.0 - d / 10.0), 0.0)
+    g = O.ssao15(_depth_gbuf(w, h, (4_000_000.0 - pit).astype(np.int64)), w, h, 300.0, 0.001)
+    center, far = int(g["amb_shadow"][32 * w + 32]), int(g["amb_shadow"][5 * w + 5])
+    assert center > far, (center, far)
+
+
+def test_ssao15_variants_and_background():
+    """The t0 variant and the wrap change the occlusion but keep it in
+    0..16383; the background keeps its record; the result does not depend
+    on the number of threads."""
+    w, h = 90, 70
+    yy, xx = np.mgrid[0:h, 0:w]
+    depth = 4_000_000 - ((xx * 7919 + yy * 104729) % 5000)
+    depth[:, :7] = -1  # background columns
+    g0 = _depth_gbuf(w, h, depth)
+    a = O.ssao15(g0, w, h, 300.0, 0.001, threads=1)
+    b = O.ssao15(g0, w, h, 300.0, 0.001, threads=5)
+    assert a.tobytes() == b.tobytes()
+    bg = (g0["zpos_fine"] >> 16) >= 32768
+    assert bg.sum() == 7 * h and np.array_equal(a[bg], g0[bg])
+    for kw in ({"t0": True}, {"wrap_x": True}, {"threshold": 0.5}):
+        c = O.ssao15(g0, w, h, 300.0, 0.001, **kw)
+        assert c["amb_shadow"].max() <= 16383 and not np.array_equal(c["amb_shadow"], a["amb_shadow"]), kw
+    # pictures below 4 x 4 stay as they are
+    small = _depth_gbuf(3, 3, np.full((3, 3), 4_000_000))
+    assert O.ssao15(small, 3, 3, 300.0, 0.001).tobytes() == small.tobytes()
