@@ -488,6 +488,47 @@ int mb3d_cu_ssao24(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_s
 int mb3d_cu_ssao15(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_ssao_opts *opts,
                    mb3d_cu_silight *gbuf);
 
+/* ---- the reflection pass's rays ----
+ * A ray of the reflection and transparency pass (RayReq, src/reflect.rs:
+ * 313-327): from a surface point along the reflected (or refracted) view
+ * vector, for the pixel whose view it continues. */
+typedef struct {
+    double origin[3]; /* where the ray starts */
+    double dir[3];    /* its direction, one step long (the pixel's view vector turned) */
+    double zz;        /* the view depth at the origin, in steps */
+    double max_len;   /* the longest march in steps; <= 0: the march's far end */
+    uint32_t pixel;   /* the pixel the ray belongs to: y * width + x of the scene's picture */
+    uint32_t rit;     /* the bounce, 1 for the first reflection: the hit's DE ambient
+                         occlusion has quality 2, 1, then 0 and the weight 8 / (8 + rit) */
+} mb3d_cu_reflect_ray;
+
+/* The march of a ray (RayHit, src/reflect.rs:329-337). */
+typedef struct {
+    mb3d_cu_silight si;  /* the hit's record: normal, depth, colour, shadow bits, ambient
+                            occlusion; the step count in shadow's low 10 bits; open air:
+                            zpos_fine 32768 << 16 */
+    uint8_t hit;         /* a surface was met */
+    uint8_t de_limited;  /* the march stopped on the DE (not on the iteration limit) */
+    uint8_t pad[2];
+    double pos[3];       /* where the march ended */
+    double zz;           /* the view depth there, in steps */
+    double zz2_paint;    /* the length marched before the surface search, in steps */
+    double zz2;          /* and after it */
+} mb3d_cu_reflect_hit;
+
+/* Replaces gpu::reflect_batch (src/gpu.rs:2521; on the CPU
+ * SrTracer::march_ray, src/reflect.rs:1464-1675): the n rays marched in
+ * double precision to their hits, which get their normal, colour, depth
+ * (through the fog formula with far_fog: LightVals far_fog or squared
+ * depth), the scene's hard or soft shadows (calc_hs, src/reflect.rs:805-952)
+ * and, with the scene's DE ambient occlusion on, its occlusion at the hit
+ * (deao_1pos, src/reflect.rs:954-1090).  Every ray is independent.  Rays and
+ * hits in host or device memory.  ENOTSUP for what the card's pass leaves
+ * to the CPU: a random first AO step (deao_first_step_random), dithering.
+ * EINVAL for a pixel outside the picture. */
+int mb3d_cu_reflect_batch(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_reflect_ray *rays, uint32_t n,
+                          int far_fog, mb3d_cu_reflect_hit *hits);
+
 /* ---- the learned denoiser of the Monte Carlo pictures ----
  * A 5-level U-Net of 3x3 convolutions (32/48/64/80/96 channels) that
  * takes the noisy colour and the albedo, normal and depth guides of a

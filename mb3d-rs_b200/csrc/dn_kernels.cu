@@ -190,8 +190,9 @@ __global__ void k_l1_loss(const __nv_bfloat16 *pred, const float *target, int n,
 
 // the squared error of the tone-mapped colour x / (1 + x) (the space the
 // pictures' PSNR is measured in) on channels 0..2 of the valid pixels: the
-// prediction p is log(1 + x), so its tone is 1 - exp(-p) (taken for every p,
-// a smooth continuation where the output clamps x at 0); with display set,
+// prediction p is log(1 + x), so its tone is 1 - exp(-p) (taken for every p
+// above -30, a smooth continuation where the output clamps x at 0; below, as
+// at -30); with display set,
 // plus the squared error of the colour clamped to 0..1 (what the painter
 // makes of a record with its default settings), whose gradient passes the
 // clamp wherever the two clamped colours differ (so that a prediction above
@@ -211,7 +212,7 @@ __global__ void k_tone_loss(const __nv_bfloat16 *pred, const float *target, int 
 #pragma unroll
             for (int c = 0; c < 3; c++) {
                 const float p = __bfloat162float(pred[i * 16 + c]);
-                const float q = expf(-p);
+                const float q = expf(-fmaxf(p, -30.0f));  // (bounded: an untrained network's outputs run wild)
                 const float yv = fmaxf(target[3 * t + c], 0.0f);
                 const float e = (1.0f - q) - yv / (1.0f + yv);
                 acc += e * e;

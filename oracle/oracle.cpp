@@ -1510,4 +1510,87 @@ void deao_row(Marcher &m, int y, SiLight *row, int n, int quality, float max_len
     }
 }
 
+// CalcAmbShadowDEfor1pos (deao_1pos, src/reflect.rs:954-1090): the DE
+// ambient occlusion at the marcher's position (the reflection pass's hits),
+// outside rendering, no cutting planes, no random first step; the depth
+// for the DE stop is m.mzz
+void deao_1pos(Marcher &m, SiLight &si, int quality, float max_len) {
+    si.amb_shadow = 0;
+    if (si.zpos() >= 32768 || si.si_gradient >= 32768) return;
+    const Params *p = m.p;
+    const double sw = p->step_width;
+    m.it.calc_sit = false;
+    Mat3 rot_v;
+    normalise_matrix_to(sw, p->vgrads, rot_v);
+    const double s_max_d = (double)max_len * 0.5 * std::sqrt((double)p->height * (double)p->height + (double)p->width * (double)p->width);
+    double ms_de_stop = (double)rminf((float)((double)p->de_stop * (1.0 + std::fabs(m.mzz) * (double)p->de_stop_factor)), 1e6f);
+    const double ic[3] = {m.it.c[0], m.it.c[1], m.it.c[2]};
+    const double step_ao = ms_de_stop / (double)p->de_stop;
+    const double max_dist = s_max_d * std::sqrt(step_ao);
+    const Rays base = build_rays(quality);
+    // (here in double precision: 1.8, or 1 + sin(abr))
+    const int q = std::min(std::max(quality, 0), 3);
+    const double d_step_mul = q == 0 ? 1.8 : 1.0 + std::sin((PI / 2.0) / ((double)q + 0.9));
+    if (p->de_stop_factor != 0.0f) ms_de_stop /= d_step_mul * d_step_mul;
+    else ms_de_stop = (double)p->de_stop / (d_step_mul * d_step_mul);
+    const auto &dirs = base.dirs;
+    const int ray_count = (int)dirs.size();
+    const double de_mul = std::sqrt((double)ray_count * 0.5);
+    const double abr = 1.2 / std::asin(rclamp(1.0 / de_mul, -1.0, 1.0));
+    const double md_d10 = 0.1 / (max_dist * de_mul);
+    float nrm[3];
+    {
+        float v[3] = {(float)si.normal[0], (float)si.normal[1], (float)si.normal[2]};
+        float l = rmaxf(std::sqrt(sdot(v, v)), 1e-30f);
+        nrm[0] = v[0] / l; nrm[1] = v[1] / l; nrm[2] = v[2] / l;
+    }
+    float rot_w[3][3];
+    normal_matrix(nrm, rot_w);
+    std::vector<float> min_ra(ray_count, 0.f);
+    for (int k = 0; k < ray_count; k++) {
+        const float *d = dirs[k].data();
+        float v[3] = {sdot(rot_w[0], d), sdot(rot_w[1], d), sdot(rot_w[2], d)};
+        double vd[3] = {(double)v[0], (double)v[1], (double)v[2]};
+        double sv[3];
+        rotate_vector_reverse(vd, rot_v, sv);
+        double dt1 = step_ao * d_step_mul;
+        double s = 1.0;
+        bool end = false;
+        for (int guard = 1;; guard++) {
+            if (dt1 > max_dist) {
+                dt1 = max_dist;
+                end = true;
+            }
+            std::memcpy(m.it.c, ic, sizeof(ic));
+            add_weight(m.it.c, sv, dt1);
+            const double d2 = m.calc_de();
+            s = rmin(s, (d2 - ms_de_stop + dt1 * md_d10) / dt1);
+            if (s < 0.02) break;
+            dt1 += rmax(d2, dt1 * d_step_mul);
+            if (end || guard > 100000) break;
+        }
+        min_ra[k] = (float)(rmax(s, 0.0) * de_mul);
+    }
+    double amount = 0.0;
+    for (int k = 0; k < ray_count; k++) {
+        float s_add = 0.f;
+        if (min_ra[k] < 1.0f) {
+            const float max_add = 1.0f - min_ra[k];
+            for (int k2 = 0; k2 < ray_count; k2++) {
+                if (k2 == k) continue;
+                const float dt = sdot(dirs[k].data(), dirs[k2].data());
+                if (dt > base.d_min_a_dif) {
+                    const float overlap = min_ra[k2] - (float)((double)std::acos(rclampf(dt, -1.0f, 1.0f)) * abr) + 1.0f;
+                    if (overlap > 0.0f) s_add += rminf(max_add, overlap) * base.correction_weight;
+                }
+            }
+        }
+        amount += (double)rminf(s_add + min_ra[k], 1.0f);
+    }
+    si.amb_shadow = sat_u16(rmax(rte(16383.0 * (1.0 - amount / (double)ray_count)), 0.0));
+    std::memcpy(m.it.c, ic, sizeof(ic));
+}
+
+uint16_t clip15(float s) { return min_max_clip_15bit(s); }
+
 }  // namespace oracle

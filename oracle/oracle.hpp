@@ -254,5 +254,7 @@ int32_t pixel_seed(int64_t y, int64_t x);
 void shadow_lights(const mb3d_cu_scene &sc, const Params &p, std::vector<HsLight> &out);
 int ao_ray_table(int quality, float *dirs, int cap);
 void deao_row(Marcher &m, int y, SiLight *row, int n, int quality, float max_len, bool first_step_random, int32_t &rnd);
+void deao_1pos(Marcher &m, SiLight &si, int quality, float max_len);
+uint16_t clip15(float s);  // MinMaxClip15bit
 
 }  // namespace oracle

@@ -159,11 +159,12 @@ def l1_loss(pred, target):
 
 def tone_mse_loss(pred, target, display=False):
     """The squared error of x / (1 + x) (prediction: log(1 + x), its tone
-    1 - exp(-pred)) and its gradient with respect to pred; with display, plus
+    1 - exp(-pred), pred taken as -30 below -30) and its gradient with
+    respect to pred; with display, plus
     the squared error of x clamped to 0..1, its gradient passed through the
     clamp wherever the clamped colours differ (exp(pred) capped at 2)."""
     p = pred[..., :3]
-    q = np.exp(-p)
+    q = np.exp(-np.maximum(p, -30.0))
     y = np.maximum(target, 0.0)
     e = (1.0 - q) - y / (1.0 + y)
     cnt = e.size

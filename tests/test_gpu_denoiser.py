@@ -80,6 +80,11 @@ def test_network_gradient_matches_fp64_oracle(card, kind):
         p = dn.get_params()
         # non-zero biases, so that every ReLU sees both signs
         p = p + np.where(np.arange(p.size) % 7 == 0, 0.01, 0.0).astype(np.float32)
+        if kind != mb3dcu.Denoiser.LOSS_L1_LOG:
+            # the output layer scaled down: the untrained network's outputs
+            # (about +-50) would put the tone's exp(-pred) far out of range
+            k_out = unet.layers()[-1][1] * 9 * unet.layers()[-1][0] + unet.layers()[-1][1]
+            p[-k_out:] *= 0.02
         dn.set_params(p)
         rad, alb, nrm, dep, tgt = _batch(rng, 2, 32, 48)
         loss, g = dn.gradient(rad, tgt, alb, nrm, dep, depth_scale=1.0)
@@ -222,8 +227,8 @@ def test_trained_network_beats_the_plain_trace(card):
     picture it was not trained on (the hybrid scene at 240x135), the 4-ray
     trace denoised with the committed weights is closer to an independent
     256-ray trace than the 4-ray trace itself (PSNR of x/(1+x), +2 dB at
-    least); the 16-ray trace denoised stays within 0.5 dB of the plain one
-    or above it (the network is trained for 4 and 16 rays)."""
+    least), and the 16-ray trace denoised gains too (0.3 dB at least; on
+    the whole C5 frame the committed network gains 2.0 dB there)."""
     import os
     import train_denoiser as T
     import scenes
@@ -243,4 +248,4 @@ def test_trained_network_beats_the_plain_trace(card):
     finally:
         dn.close()
     p4, pd4, p16, pd16 = (T.psnr(a, ref) for a in (r4["radiance"], den4, r16, den16))
-    assert pd4 >= p4 + 2.0 and pd16 >= p16 - 0.5, (p4, pd4, p16, pd16)
+    assert pd4 >= p4 + 2.0 and pd16 >= p16 + 0.3, (p4, pd4, p16, pd16)
