@@ -4,6 +4,7 @@
 // negative status and the caller decides what to do.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <cstdio>
 #include <cstdlib>
@@ -79,6 +80,8 @@ struct mb3d_cu_ctx {
     size_t mcitems_cap = 0;
     unsigned char *d_dof = nullptr;    // the depth of field's pictures, sources and keys
     size_t dof_cap = 0;
+    unsigned char *d_refl = nullptr;   // the reflection pass's rays, hits and AO table
+    size_t refl_cap = 0;
     unsigned char *d_paint = nullptr;  // the painter's staging of host buffers
     size_t paint_cap = 0;
     unsigned char *d_ssao = nullptr;   // the SSAO's levels and angles (and a host G-buffer's staging)
@@ -203,6 +206,7 @@ void mb3d_cu_free(mb3d_cu_ctx *c) {
     cudaFree(c->d_mcs);
     cudaFree(c->d_mcitems);
     cudaFree(c->d_dof);
+    cudaFree(c->d_refl);
     cudaFree(c->d_paint);
     cudaFree(c->d_ssao);
     for (auto &ev : c->ev)
@@ -1340,6 +1344,58 @@ int mb3d_cu_dof(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_dof_opts 
     cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
     c->stats.ms_total = ms;
     c->stats.launches = launches;
+    return 0;
+}
+
+
+int mb3d_cu_reflect_batch(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_reflect_ray *rays, uint32_t n,
+                          int far_fog, mb3d_cu_reflect_hit *hits) {
+    if (!c || !sc || (n && (!rays || !hits))) return fail(MB3D_CU_EINVAL, "NULL argument");
+    std::string why;
+    int u = unsupported_reason(*sc, why);
+    if (u < 0) return fail(u, why);
+    if (u == 1) return fail(MB3D_CU_ENOTSUP, why);
+    DevParams p;
+    std::string err;
+    int r = setup_params(*sc, p, err);
+    if (r < 0) return fail(r, err);
+    if (n == 0) return 0;
+    if (n > (1u << 26)) return fail(MB3D_CU_EINVAL, "more than 2^26 rays in one batch");
+    const bool dr = is_device_ptr(rays), dh = is_device_ptr(hits);
+    if (!dr) {
+        const uint32_t np = (uint32_t)p.width * (uint32_t)p.height;
+        for (uint32_t i = 0; i < n; i++)
+            if (rays[i].pixel >= np) return fail(MB3D_CU_EINVAL, "a ray's pixel is outside the picture");
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    const size_t br = (size_t)n * sizeof(mb3d_cu_reflect_ray), bh = (size_t)n * sizeof(mb3d_cu_reflect_hit);
+    const size_t o_tab = 0, o_r = align256(sizeof(ReflAO)), o_h = o_r + (dr ? 0 : align256(br));
+    const size_t need = o_h + (dh ? 0 : align256(bh));
+    if (int e = grow((void **)&c->d_refl, &c->refl_cap, need)) return e;
+    static ReflAO tab;  // (the same for every call; made once)
+    static std::once_flag tab_once;
+    std::call_once(tab_once, [] { reflect_ao_table(tab); });
+    cudaStream_t s = c->stream;
+    ReflAO *dtab = reinterpret_cast<ReflAO *>(c->d_refl + o_tab);
+    const mb3d_cu_reflect_ray *drays = dr ? rays : reinterpret_cast<const mb3d_cu_reflect_ray *>(c->d_refl + o_r);
+    mb3d_cu_reflect_hit *dhits = dh ? hits : reinterpret_cast<mb3d_cu_reflect_hit *>(c->d_refl + o_h);
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    CU_TRY(cudaMemcpyAsync(dtab, &tab, sizeof(ReflAO), cudaMemcpyHostToDevice, s));
+    if (!dr) CU_TRY(cudaMemcpyAsync((void *)drays, rays, br, cudaMemcpyHostToDevice, s));
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    const int blocks = (int)std::min<size_t>(((size_t)n + 127) / 128, (size_t)c->sms * 16);
+    launch_reflect(p, drays, n, far_fog ? 1 : 0, dtab, dhits, blocks, s);
+    if (int e = check_launch("k_reflect")) return e;
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    if (!dh) CU_TRY(cudaMemcpyAsync(hits, dhits, bh, cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    c->stats.launches = 1;
     return 0;
 }
 

@@ -65,6 +65,10 @@ void launch_mc(const DevParams &p, const McDev &m, bool mixed, bool batch, const
     }
     t->run(p, m, mixed, batch, acc, reqs, res, queue, n_items, list, sms, s);
 }
+void launch_reflect(const DevParams &p, const mb3d_cu_reflect_ray *rays, uint32_t n, int far_fog, const ReflAO *tab,
+                    mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s) {
+    table(p.fmask).reflect(p, rays, n, far_fog, tab, hits, blocks, s);
+}
 void launch_de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s) {
     table(p.fmask).de_probe(p, pos, n, de, its, mixed, s);
 }

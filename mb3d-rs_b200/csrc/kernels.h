@@ -52,6 +52,22 @@ struct PostStart {
 int kernel_set(int fmask);
 
 // the launches of one formula set's kernels (kern_*.cu)
+// the DE ambient occlusion of the reflection pass's hits (deao_1pos,
+// src/reflect.rs:954-1090) per quality 0..3: its directions, its step
+// multiplier and weight, and per pair of directions acos(dot) * abr as
+// single precision, or REFL_AO_NO where the pair does not count (the host
+// makes it with the C library's functions, as the reference's CPU does)
+constexpr int REFL_AO_MAX = 13;  // directions of quality 3
+constexpr float REFL_AO_NO = 1e30f;
+struct ReflAO {
+    int count[4], first[4];
+    double d_step_mul[4];
+    float corr_w[4];
+    float dirs[3 + 3 + 7 + 13][3];
+    float ang[4][REFL_AO_MAX][REFL_AO_MAX];
+};
+void reflect_ao_table(ReflAO &t);
+
 struct LaunchTable {
     void (*march)(const DevParams &, bool mixed, int row0, int rows, mb3d_cu_silight *out, Hand *list,
                   unsigned int *counters, unsigned long long *gcount, int blocks, cudaStream_t s);
@@ -71,12 +87,17 @@ struct LaunchTable {
                         mb3d_cu_silight *out, int blocks, cudaStream_t s);
     void (*finish_slow)(const DevParams &, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,
                         mb3d_cu_silight *out, int blocks, cudaStream_t s);
+    // the reflection pass's rays (reflect.cuh)
+    void (*reflect)(const DevParams &, const mb3d_cu_reflect_ray *rays, uint32_t n, int far_fog, const ReflAO *tab,
+                    mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s);
 };
 LaunchTable table_ip8();
 LaunchTable table_ip8box();
 LaunchTable table_mengerbox();
 LaunchTable table_all();
 
+void launch_reflect(const DevParams &p, const mb3d_cu_reflect_ray *rays, uint32_t n, int far_fog, const ReflAO *tab,
+                    mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s);
 void launch_march(const DevParams &p, bool mixed, int row0, int rows, mb3d_cu_silight *out, Hand *list,
                   unsigned int *counters, unsigned long long *gcount, int blocks, cudaStream_t s);
 void launch_finish(const DevParams &p, bool mixed, int row0, const Hand *list, unsigned int *counters, Hand *slow,

@@ -1360,6 +1360,10 @@ __global__ void k_de_probe(const __grid_constant__ DevParams p, const double *po
     its[i] = r.it;
 }
 
+}  // namespace mb3dcu
+#include "reflect.cuh"
+namespace mb3dcu {
+
 // ---------------------------------------------------------------------------
 // the launches of one formula set (instantiated per set in kern_*.cu)
 template <int FM>
@@ -1402,6 +1406,10 @@ struct Launch {
                         const unsigned int *count, float *min_ra, unsigned int *queue, int blocks, cudaStream_t s) {
         if (mixed) k_ao_rays<float, FM><<<blocks, 256, 0, s>>>(p, ps, gbuf, count, min_ra, queue);
         else k_ao_rays<double, FM><<<blocks, 256, 0, s>>>(p, ps, gbuf, count, min_ra, queue);
+    }
+    static void reflect(const DevParams &p, const mb3d_cu_reflect_ray *rays, uint32_t n, int far_fog, const ReflAO *tab,
+                        mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s) {
+        k_reflect<FM><<<blocks, 128, 0, s>>>(p, rays, n, far_fog, tab, hits);
     }
     static void de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s) {
         k_de_probe<FM><<<(n + 127) / 128, 128, 0, s>>>(p, pos, n, de, its, mixed ? 1 : 0);

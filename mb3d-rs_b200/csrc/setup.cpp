@@ -5,6 +5,7 @@
 // (render::shadow_job, src/render.rs:2383-2415) and the DE AO ray table
 // (deao::build_rays, src/deao.rs:75-104).
 #include "setup.h"
+#include "kernels.h"
 #include <cmath>
 #include <cstring>
 #include <algorithm>
@@ -406,6 +407,53 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
         p.ao_rays = nr;
     }
     return 0;
+}
+
+// deao_1pos's directions (ray_dir, src/reflect.rs:968-972) and constants
+// (:975-998) per quality, with the pairs' angle terms of its correction
+// (:1058-1084), in the reference's precisions
+void reflect_ao_table(ReflAO &t) {
+    std::memset(&t, 0, sizeof(t));
+    const double PI_ = 3.14159265358979323846, TAU_ = 2.0 * PI_;
+    auto ray_dir = [](double ya, double za, float *o) {
+        const double sy = std::sin(ya), cy = std::cos(ya), sz = std::sin(za), cz = std::cos(za);
+        o[0] = (float)(sy * cz);
+        o[1] = (float)(-sy * sz);
+        o[2] = (float)(-cy);
+    };
+    int at = 0;
+    for (int q = 0; q < 4; q++) {
+        t.first[q] = at;
+        float d_min_a_dif;
+        if (q == 0) {
+            const double abr = 60.0 * (PI_ / 180.0);
+            for (int i = 0; i < 3; i++) ray_dir(0.5 * abr, (double)i * TAU_ / 3.0, t.dirs[at++]);
+            t.d_step_mul[q] = 1.8;
+            d_min_a_dif = -1.0f;
+            t.corr_w[q] = 0.3f;
+        } else {
+            const double abr = (PI_ / 2.0) / ((double)q + 0.9);
+            ray_dir(0.0, 0.0, t.dirs[at++]);
+            for (int iy = 1; iy <= q; iy++) {
+                const int n = (int)std::nearbyint(std::sin(0.25) * TAU_ / abr);
+                for (int ix = 0; ix < n; ix++) ray_dir(abr * (double)iy, (double)ix * TAU_ / (double)n, t.dirs[at++]);
+            }
+            t.d_step_mul[q] = 1.0 + std::sin(abr);
+            d_min_a_dif = (float)std::cos(abr * 1.2);
+            t.corr_w[q] = q == 1 ? 0.2f : 0.1666f;
+        }
+        t.count[q] = at - t.first[q];
+        const double de_mul = std::sqrt((double)t.count[q] * 0.5);
+        const double abr_c = 1.2 / std::asin(std::fmin(std::fmax(1.0 / de_mul, -1.0), 1.0));
+        for (int k = 0; k < t.count[q]; k++)
+            for (int k2 = 0; k2 < t.count[q]; k2++) {
+                const float *a = t.dirs[t.first[q] + k], *b = t.dirs[t.first[q] + k2];
+                const float dt = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+                t.ang[q][k][k2] = k != k2 && dt > d_min_a_dif
+                                      ? (float)((double)std::acos(std::fmin(std::fmax(dt, -1.0f), 1.0f)) * abr_c)
+                                      : REFL_AO_NO;
+            }
+    }
 }
 
 }  // namespace mb3dcu

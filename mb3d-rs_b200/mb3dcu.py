@@ -203,6 +203,16 @@ MC_RECORD = np.dtype([("col", "<f4", (3,)), ("ysum", "<f4"), ("ysqr", "<f4"), ("
 assert MC_RECORD.itemsize == 24
 
 
+# a ray of the reflection pass (mb3d_cu_reflect_ray, RayReq: 72 bytes) and
+# its march (mb3d_cu_reflect_hit, RayHit: 72 bytes)
+REFLECT_RAY = np.dtype([("origin", "<f8", (3,)), ("dir", "<f8", (3,)), ("zz", "<f8"), ("max_len", "<f8"),
+                        ("pixel", "<u4"), ("rit", "<u4")])
+assert REFLECT_RAY.itemsize == 72
+REFLECT_HIT = np.dtype([("si", SILIGHT), ("hit", "u1"), ("de_limited", "u1"), ("pad", "u1", (2,)),
+                        ("pos", "<f8", (3,)), ("zz", "<f8"), ("zz2_paint", "<f8"), ("zz2", "<f8")])
+assert REFLECT_HIT.itemsize == 72
+
+
 class CardError(RuntimeError):
     def __init__(self, status, text):
         super().__init__(f"{text} (status {status})")
@@ -272,6 +282,7 @@ def lib():
         L.mb3d_cu_ssao_default.restype = None
         L.mb3d_cu_ssao24.argtypes = [vp, sp, ctypes.POINTER(SsaoOpts), vp]
         L.mb3d_cu_ssao15.argtypes = [vp, sp, ctypes.POINTER(SsaoOpts), vp]
+        L.mb3d_cu_reflect_batch.argtypes = [vp, sp, vp, ctypes.c_uint32, ctypes.c_int, vp]
         _lib = L
     return _lib
 
@@ -280,7 +291,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_march_ex", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render", "mb3d_cu_mc_pass",
-            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24", "mb3d_cu_ssao15", "mb3d_cu_dof_default", "mb3d_cu_dof",
+            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24", "mb3d_cu_ssao15", "mb3d_cu_reflect_batch", "mb3d_cu_dof_default", "mb3d_cu_dof",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_set_loss", "mb3d_cu_dn_fallback", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
             "mb3d_cu_dn_conv_check", "mb3d_cu_dn_wait_check"]
@@ -500,6 +511,21 @@ class Card:
         self._order(gbuf)
         self._check(lib().mb3d_cu_ssao24(self._ctx, ctypes.byref(scene), ctypes.byref(opts), _ptr(gbuf)[0]))
         return gbuf
+
+    def reflect_batch(self, scene, rays, far_fog=False, out=None):
+        """gpu::reflect_batch on the card: every ray of `rays` (REFLECT_RAY,
+        numpy or a torch CUDA byte tensor) marched to its hit with the hit's
+        normal, colour, depth, shadows and DE ambient occlusion; returns the
+        hits (REFLECT_HIT; `out` may give a device buffer)."""
+        n = len(rays) if isinstance(rays, np.ndarray) else rays.numel() // REFLECT_RAY.itemsize
+        if isinstance(rays, np.ndarray):
+            rays = np.ascontiguousarray(rays, REFLECT_RAY)
+        if out is None:
+            out = np.zeros(n, REFLECT_HIT)
+        self._order(rays, out)
+        self._check(lib().mb3d_cu_reflect_batch(self._ctx, ctypes.byref(scene), _ptr(rays)[0], n, int(far_fog),
+                                                _ptr(out)[0]))
+        return out
 
     def ssao15(self, scene, gbuf, opts=None):
         """gpu::ssao15 on the card: the older 15-bit ambient occlusion

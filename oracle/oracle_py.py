@@ -50,6 +50,8 @@ def lib():
         L.oracle_paint.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, vp]
         L.oracle_ssao24.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_float,
                                     ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.oracle_reflect_batch.argtypes = [vp, vp, ctypes.c_uint32, ctypes.c_int, vp, ctypes.c_int]
+        L.oracle_reflect_first_rays.argtypes = [vp, vp, vp, ctypes.c_uint32]
         L.oracle_ssao15.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_float,
                                     ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_ssao15_arctan.argtypes = [ctypes.c_int, ctypes.c_int]
@@ -235,6 +237,28 @@ def ssao15(gbuf, w, h, zc_mul, zcorr, threshold=2.0, t0=False, wrap_x=False, thr
     g = np.ascontiguousarray(gbuf).copy()
     _chk(lib().oracle_ssao15(g.ctypes.data, w, h, zc_mul, zcorr, threshold, int(t0), int(wrap_x), threads))
     return g
+
+
+def reflect_batch(scene, rays, far_fog=False, threads=0):
+    """SrTracer::march_ray (src/reflect.rs:1464-1675) with calc_hs and
+    deao_1pos for every ray (an mb3dcu.REFLECT_RAY array): the hits
+    (mb3dcu.REFLECT_HIT)."""
+    import mb3dcu
+    r = np.ascontiguousarray(rays, mb3dcu.REFLECT_RAY)
+    out = np.zeros(len(r), mb3dcu.REFLECT_HIT)
+    _chk(lib().oracle_reflect_batch(ctypes.addressof(scene), r.ctypes.data, len(r), int(far_fog), out.ctypes.data,
+                                    threads))
+    return out
+
+
+def reflect_first_rays(scene, gbuf):
+    """The first bounce of every object pixel (start_pixel and step's mirror
+    ray, src/reflect.rs:1686-1838, 1286-1311): an mb3dcu.REFLECT_RAY array."""
+    import mb3dcu
+    g = np.ascontiguousarray(gbuf)
+    out = np.zeros(len(g), mb3dcu.REFLECT_RAY)
+    n = _chk(lib().oracle_reflect_first_rays(ctypes.addressof(scene), g.ctypes.data, out.ctypes.data, len(out)))
+    return out[:n].copy()
 
 
 def ssao15_arctan(y, x):

@@ -301,3 +301,58 @@ extern "C" int oracle_reflect_batch(const mb3d_cu_scene *sc, const mb3d_cu_refle
     for (auto &th : pool) th.join();
     return 0;
 }
+
+/* The first bounce of every object pixel of a G-buffer (start_pixel,
+ * src/reflect.rs:1686-1838, outside rendering, no water, no cutting plane:
+ * the surface found again from the stored depth, then step's mirror ray,
+ * :1286-1311): the rays in pixel order into out (cap at most); returns the
+ * count. */
+extern "C" int oracle_reflect_first_rays(const mb3d_cu_scene *sc, const mb3d_cu_silight *gbuf, mb3d_cu_reflect_ray *out,
+                                         uint32_t cap) {
+    using namespace oracle;
+    if (!sc || !gbuf || !out) return -1;
+    Params p;
+    std::string err;
+    if (!make_params(*sc, p, err)) return -2;
+    const int w = sc->width, h = sc->height;
+    uint32_t n = 0;
+    auto zpos_of = [&](double iz) {
+        const double q = (8388351.5 - iz) / p.zc_mul + 1.0;
+        return (q * q - 1.0) / p.zcorr;
+    };
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {
+            const mb3d_cu_silight &g = gbuf[(size_t)y * w + x];
+            if ((g.zpos_fine >> 16) >= 32768u || g.si_gradient >= 32768) continue;
+            Marcher m(&p, 0);
+            m.cafy = ((double)y / (double)p.height - 0.5) * p.fov_y;
+            m.calc_vgrads_fov(x + 1);
+            m.calc_start_pos(x, y);
+            m.it.calc_sit = false;
+            const double zf = (double)(g.zpos_fine >> 8);
+            m.mzz = zpos_of(zf);
+            add_weight(m.it.c, m.vfov, m.mzz);
+            m.update_de_stop();
+            double d = m.calc_de();
+            if (d < (double)m.ms_de_stop * 0.5) continue;
+            const bool de_limited = m.it.it_result < m.max_its_result || d <= (double)m.ms_de_stop;
+            if (de_limited) m.bin_search(d, m.mzz - zpos_of(zf - 1.0));
+            else m.bin_search_it();
+            const double nrm0[3] = {(double)g.normal[0] / 32767.0, (double)g.normal[1] / 32767.0, (double)g.normal[2] / 32767.0};
+            double nrm[3];
+            rotate_vector_reverse(nrm0, p.vgrads, nrm);
+            const double k = 2.0 * dot3(nrm, m.vfov) / dot3(nrm, nrm);
+            if (n >= cap) return -3;
+            mb3d_cu_reflect_ray &r = out[n++];
+            std::memset(&r, 0, sizeof(r));
+            for (int i = 0; i < 3; i++) {
+                r.origin[i] = m.it.c[i];
+                r.dir[i] = m.vfov[i] - nrm[i] * k;
+            }
+            r.zz = m.mzz;
+            r.max_len = 0.0;
+            r.pixel = (uint32_t)(y * w + x);
+            r.rit = 1;
+        }
+    return (int)n;
+}

@@ -69,7 +69,8 @@ MIRRORS = [("mb3d_cu_slot", "Slot"), ("mb3d_cu_light", "Light"), ("mb3d_cu_scene
 
 
 # the numpy record types of the header's records (C name, dtype name)
-DTYPES = [("mb3d_cu_silight", "SILIGHT"), ("mb3d_cu_mc_record", "MC_RECORD")]
+DTYPES = [("mb3d_cu_silight", "SILIGHT"), ("mb3d_cu_mc_record", "MC_RECORD"), ("mb3d_cu_reflect_ray", "REFLECT_RAY"),
+          ("mb3d_cu_reflect_hit", "REFLECT_HIT")]
 
 
 def test_every_struct_mirror_matches_the_header(tmp_path):

@@ -1,0 +1,123 @@
+"""The reflection pass's rays on the card (mb3d_cu_reflect_batch, the
+counterpart of gpu::reflect_batch, src/gpu.rs:2521) against the oracle's
+SrTracer::march_ray (src/reflect.rs:1464-1675) with calc_hs and deao_1pos.
+
+The first bounce of every object pixel of the hybrid frame (the oracle's
+restatement of start_pixel and step's mirror ray) and the second bounce
+from those hits, marched on the card in double precision: hits, depths,
+normals, colours, shadow bits and ambient occlusion against the oracle's,
+per ray.  The card's FP64 arithmetic may fuse a multiply and an add where
+the oracle does not, so a ray that grazes a surface may land elsewhere; the
+bounds below allow for that on a small share of rays."""
+import numpy as np
+import pytest
+
+import mb3dcu
+import oracle_py as O
+import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def _agree(got, want):
+    h_g, h_w = got["hit"] == 1, want["hit"] == 1
+    both = h_g & h_w
+    r = {"hit_agree": float((h_g == h_w).mean()), "both": int(both.sum()),
+         "exact_si": float((got["si"][both] == want["si"][both]).mean())}
+    zg, zw = got["zz2"][both], want["zz2"][both]
+    rel = np.abs(zg - zw) / np.maximum(np.abs(zw), 1e-30)
+    r["zz2_rel_median"] = float(np.median(rel))
+    r["zz2_rel_p99"] = float(np.quantile(rel, 0.99))
+    r["shadow_agree"] = float(((got["si"]["shadow"][both] >> 10) == (want["si"]["shadow"][both] >> 10)).mean())
+    da = np.abs(got["si"]["amb_shadow"][both].astype(np.int64) - want["si"]["amb_shadow"][both].astype(np.int64))
+    r["amb_within_8"] = float((da <= 8).mean())
+    miss = ~h_g & ~h_w
+    r["miss_steps_agree"] = float(((got["si"]["shadow"][miss] & 0x3FF) == (want["si"]["shadow"][miss] & 0x3FF)).mean())
+    return r
+
+
+def _check(r):
+    assert r["hit_agree"] >= 0.98, r
+    assert r["exact_si"] >= 0.9, r
+    assert r["zz2_rel_median"] < 1e-9 and r["zz2_rel_p99"] < 1e-4, r
+    assert r["shadow_agree"] >= 0.97, r
+    assert r["amb_within_8"] >= 0.95, r
+    assert r["miss_steps_agree"] >= 0.97, r
+
+
+@pytest.fixture(scope="module")
+def c2_first():
+    sc = scenes.scaled(scenes.c2_hybrid(), 240, 135)
+    g = O.march(sc, mb3dcu.SILIGHT)
+    rays = O.reflect_first_rays(sc, g)
+    assert len(rays) > 0.2 * sc.width * sc.height
+    return sc, rays
+
+
+def test_first_bounce_matches_oracle(card, c2_first):
+    sc, rays = c2_first
+    want = O.reflect_batch(sc, rays)
+    got = card.reflect_batch(sc, rays)
+    assert 0.2 < want["hit"].mean() < 0.95  # (both hits and open air)
+    _check(_agree(got, want))
+
+
+def test_second_bounce_and_far_fog(card, c2_first):
+    sc, rays = c2_first
+    first = O.reflect_batch(sc, rays)
+    idx = np.nonzero(first["hit"] == 1)[0]
+    vg = np.ctypeslib.as_array(sc.vgrads).astype(np.float64).reshape(3, 3)
+    nrm = first["si"]["normal"][idx].astype(np.float64) / 32767.0 @ vg
+    d = rays["dir"][idx]
+    k = 2.0 * (nrm * d).sum(1) / np.maximum((nrm * nrm).sum(1), 1e-300)
+    r2 = np.zeros(len(idx), mb3dcu.REFLECT_RAY)
+    r2["origin"] = first["pos"][idx]
+    r2["dir"] = d - nrm * k[:, None]
+    r2["zz"] = first["zz"][idx]
+    r2["pixel"] = rays["pixel"][idx]
+    r2["rit"] = 2
+    for far_fog in (False, True):
+        want = O.reflect_batch(sc, r2, far_fog=far_fog)
+        got = card.reflect_batch(sc, r2, far_fog=far_fog)
+        _check(_agree(got, want))
+    # a limited march length ends rays in the open air
+    r3 = r2.copy()
+    r3["max_len"] = 2.0
+    want, got = O.reflect_batch(sc, r3), card.reflect_batch(sc, r3)
+    assert want["hit"].mean() < O.reflect_batch(sc, r2)["hit"].mean()
+    _check(_agree(got, want))
+
+
+def test_soft_shadow_and_no_occlusion(card, c2_first):
+    sc, rays = c2_first
+    soft = scenes.scene_copy(sc)
+    soft.shadow_soft, soft.soft_radius = 1, 2.0
+    soft.deao_quality = -1
+    want, got = O.reflect_batch(soft, rays), card.reflect_batch(soft, rays)
+    _check(_agree(got, want))
+    hit = want["hit"] == 1
+    assert np.all(want["si"]["amb_shadow"][hit] == 5000) and np.all(got["si"]["amb_shadow"][got["hit"] == 1] == 5000)
+    # the soft shadow's 6 bits take more than two values
+    assert len(np.unique(want["si"]["shadow"][hit] >> 10)) > 4
+
+
+def test_device_buffers_and_refusals(card, c2_first):
+    import torch
+    sc, rays = c2_first
+    host = card.reflect_batch(sc, rays[:500])
+    dr = torch.from_numpy(rays[:500].view(np.uint8).copy()).cuda()
+    dh = torch.zeros(500 * mb3dcu.REFLECT_HIT.itemsize, dtype=torch.uint8, device="cuda")
+    card.reflect_batch(sc, dr, out=dh)
+    torch.cuda.synchronize()
+    assert dh.cpu().numpy().tobytes() == host.tobytes()
+    bad = rays[:4].copy()
+    bad["pixel"][2] = sc.width * sc.height
+    with pytest.raises(mb3dcu.CardError) as e:
+        card.reflect_batch(sc, bad)
+    assert e.value.status == mb3dcu.EINVAL
+    rnd = scenes.scene_copy(sc)
+    rnd.deao_first_step_random = 1
+    with pytest.raises(mb3dcu.CardError) as e:
+        card.reflect_batch(rnd, rays[:4])
+    assert e.value.status == mb3dcu.ENOTSUP
+    assert len(card.reflect_batch(sc, rays[:0])) == 0
