@@ -529,6 +529,16 @@ typedef struct {
 int mb3d_cu_reflect_batch(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_reflect_ray *rays, uint32_t n,
                           int far_fog, mb3d_cu_reflect_hit *hits);
 
+/* The first bounce of every object pixel of a G-buffer (the scene's whole
+ * picture, width * height records, host or device): start_pixel
+ * (src/reflect.rs:1686-1838: the surface found again from the stored depth,
+ * outside rendering, no water or cutting plane) and the mirror ray of step
+ * (:1286-1311), rit 1, in pixel order into rays (room for width * height,
+ * host or device); *n_rays receives their count.  Pixels whose surface the
+ * search cannot find again send none, as in the reference. */
+int mb3d_cu_reflect_first_rays(mb3d_cu_ctx *ctx, const mb3d_cu_scene *scene, const mb3d_cu_silight *gbuf,
+                               mb3d_cu_reflect_ray *rays, uint32_t *n_rays);
+
 /* ---- the learned denoiser of the Monte Carlo pictures ----
  * A 5-level U-Net of 3x3 convolutions (32/48/64/80/96 channels) that
  * takes the noisy colour and the albedo, normal and depth guides of a

@@ -1399,6 +1399,67 @@ int mb3d_cu_reflect_batch(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu
     return 0;
 }
 
+int mb3d_cu_reflect_first_rays(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_silight *gbuf,
+                               mb3d_cu_reflect_ray *rays, uint32_t *n_rays) {
+    if (!c || !sc || !gbuf || !rays || !n_rays) return fail(MB3D_CU_EINVAL, "NULL argument");
+    *n_rays = 0;
+    std::string why;
+    int u = unsupported_reason(*sc, why);
+    if (u < 0) return fail(u, why);
+    if (u == 1) return fail(MB3D_CU_ENOTSUP, why);
+    DevParams p;
+    std::string err;
+    int r = setup_params(*sc, p, err);
+    if (r < 0) return fail(r, err);
+    const size_t npix = (size_t)p.width * p.height;
+    const size_t nblk = (npix + 1023) / 1024;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->resume.active = false;  // (this call reuses the scratch a stopped budgeted march keeps)
+    if (cudaSetDevice(c->device) != cudaSuccess) return fail(MB3D_CU_EIO, "cudaSetDevice failed");
+    const bool dg = is_device_ptr(gbuf), dr = is_device_ptr(rays);
+    const size_t bg = npix * sizeof(mb3d_cu_silight), br = npix * sizeof(mb3d_cu_reflect_ray);
+    const size_t o_tmp = 0, o_valid = o_tmp + align256(br), o_sum = o_valid + align256(npix),
+                 o_g = o_sum + align256(nblk * 4), o_out = o_g + (dg ? 0 : align256(bg));
+    const size_t need = o_out + (dr ? 0 : align256(br));
+    if (int e = grow((void **)&c->d_refl, &c->refl_cap, need)) return e;
+    unsigned char *B = c->d_refl;
+    mb3d_cu_reflect_ray *tmp = reinterpret_cast<mb3d_cu_reflect_ray *>(B + o_tmp);
+    unsigned char *valid = B + o_valid;
+    unsigned int *sums = reinterpret_cast<unsigned int *>(B + o_sum);
+    const mb3d_cu_silight *g = dg ? gbuf : reinterpret_cast<const mb3d_cu_silight *>(B + o_g);
+    mb3d_cu_reflect_ray *out = dr ? rays : reinterpret_cast<mb3d_cu_reflect_ray *>(B + o_out);
+    cudaStream_t s = c->stream;
+    std::memset(&c->stats, 0, sizeof(c->stats));
+    if (!dg) CU_TRY(cudaMemcpyAsync((void *)g, gbuf, bg, cudaMemcpyHostToDevice, s));
+    CU_TRY(cudaEventRecord(c->ev[0], s));
+    const int blocks = (int)std::min<size_t>((npix + 127) / 128, (size_t)c->sms * 16);
+    launch_reflect_first(p, g, tmp, valid, blocks, s);
+    if (int e = check_launch("k_reflect_first")) return e;
+    flag_count(valid, npix, sums, s);
+    std::vector<unsigned int> h(nblk);
+    CU_TRY(cudaMemcpyAsync(h.data(), sums, nblk * 4, cudaMemcpyDeviceToHost, s));
+    CU_TRY(cudaStreamSynchronize(s));
+    unsigned int total = 0;
+    for (size_t b = 0; b < nblk; b++) {
+        const unsigned int v = h[b];
+        h[b] = total;
+        total += v;
+    }
+    CU_TRY(cudaMemcpyAsync(sums, h.data(), nblk * 4, cudaMemcpyHostToDevice, s));
+    flag_scatter(valid, tmp, npix, sums, out, s);
+    if (int e = check_launch("k_flag_scatter")) return e;
+    CU_TRY(cudaEventRecord(c->ev[1], s));
+    if (!dr && total) CU_TRY(cudaMemcpyAsync(rays, out, (size_t)total * sizeof(mb3d_cu_reflect_ray), cudaMemcpyDeviceToHost, s));
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return fail(MB3D_CU_EIO, std::string("device: ") + cudaGetErrorString(e));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    c->stats.ms_total = ms;
+    c->stats.launches = 3;
+    *n_rays = total;
+    return 0;
+}
+
 int mb3d_cu_mc_pass(mb3d_cu_ctx *c, const mb3d_cu_scene *sc, const mb3d_cu_mc_light *lv, const mb3d_cu_mc_opts *o,
                     int precision, uint32_t pass_nr, mb3d_cu_mc_record *recs, const volatile int *cancel) {
     if (!c || !sc || !lv || !o || !recs) return fail(MB3D_CU_EINVAL, "NULL argument");

@@ -6,7 +6,7 @@ namespace mb3dcu {
 LaunchTable table_all() {
     typedef Launch<KSET_ALL> L;
     return LaunchTable{&L::march, &L::finish, &L::post_start, &L::shadow_rays, &L::ao_rays, &L::de_probe,
-                       &L::finish_fast, &L::finish_slow, &L::reflect};
+                       &L::finish_fast, &L::finish_slow, &L::reflect, &L::reflect_first};
 }
 
 // the kernels every formula set shares

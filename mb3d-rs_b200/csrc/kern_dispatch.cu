@@ -69,6 +69,54 @@ void launch_reflect(const DevParams &p, const mb3d_cu_reflect_ray *rays, uint32_
                     mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s) {
     table(p.fmask).reflect(p, rays, n, far_fog, tab, hits, blocks, s);
 }
+void launch_reflect_first(const DevParams &p, const mb3d_cu_silight *gbuf, mb3d_cu_reflect_ray *tmp,
+                          unsigned char *valid, int blocks, cudaStream_t s) {
+    table(p.fmask).reflect_first(p, gbuf, tmp, valid, blocks, s);
+}
+
+__global__ void __launch_bounds__(1024) k_flag_count(const unsigned char *valid, size_t n, unsigned int *block_sum) {
+    const size_t i = (size_t)blockIdx.x * 1024 + threadIdx.x;
+    const unsigned int v = __popc(__ballot_sync(0xffffffffu, i < n && valid[i]));
+    __shared__ unsigned int part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const unsigned int u = __reduce_add_sync(0xffffffffu, part[threadIdx.x]);
+        if (threadIdx.x == 0) block_sum[blockIdx.x] = u;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_flag_scatter(const unsigned char *valid, const mb3d_cu_reflect_ray *tmp,
+                                                      size_t n, const unsigned int *offset, mb3d_cu_reflect_ray *out) {
+    const size_t i = (size_t)blockIdx.x * 1024 + threadIdx.x;
+    const int lane = (int)(threadIdx.x & 31), warp = (int)(threadIdx.x >> 5);
+    const bool v = i < n && valid[i];
+    const unsigned int b = __ballot_sync(0xffffffffu, v);
+    __shared__ unsigned int wsum[32];
+    if (lane == 0) wsum[warp] = __popc(b);
+    __syncthreads();
+    if (warp == 0) {
+        // exclusive scan of the 32 warps' counts
+        const unsigned int c = wsum[lane];
+        unsigned int x = c;
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned int y = __shfl_up_sync(0xffffffffu, x, d);
+            if (lane >= d) x += y;
+        }
+        wsum[lane] = x - c;
+    }
+    __syncthreads();
+    if (v) out[offset[blockIdx.x] + wsum[warp] + __popc(b & ((1u << lane) - 1u))] = tmp[i];
+}
+
+void flag_count(const unsigned char *valid, size_t n, unsigned int *block_sum, cudaStream_t s) {
+    k_flag_count<<<(unsigned)((n + 1023) / 1024), 1024, 0, s>>>(valid, n, block_sum);
+}
+void flag_scatter(const unsigned char *valid, const mb3d_cu_reflect_ray *tmp, size_t n, const unsigned int *offset,
+                  mb3d_cu_reflect_ray *out, cudaStream_t s) {
+    k_flag_scatter<<<(unsigned)((n + 1023) / 1024), 1024, 0, s>>>(valid, tmp, n, offset, out);
+}
+
 void launch_de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s) {
     table(p.fmask).de_probe(p, pos, n, de, its, mixed, s);
 }

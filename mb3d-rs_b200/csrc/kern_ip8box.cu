@@ -5,6 +5,6 @@ namespace mb3dcu {
 LaunchTable table_ip8box() {
     typedef Launch<KSET_IP8BOX> L;
     return LaunchTable{&L::march, &L::finish, &L::post_start, &L::shadow_rays, &L::ao_rays, &L::de_probe,
-                       &L::finish_fast, &L::finish_slow, &L::reflect};
+                       &L::finish_fast, &L::finish_slow, &L::reflect, &L::reflect_first};
 }
 }  // namespace mb3dcu

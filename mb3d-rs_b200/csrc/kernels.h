@@ -90,12 +90,21 @@ struct LaunchTable {
     // the reflection pass's rays (reflect.cuh)
     void (*reflect)(const DevParams &, const mb3d_cu_reflect_ray *rays, uint32_t n, int far_fog, const ReflAO *tab,
                     mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s);
+    void (*reflect_first)(const DevParams &, const mb3d_cu_silight *gbuf, mb3d_cu_reflect_ray *tmp,
+                          unsigned char *valid, int blocks, cudaStream_t s);
 };
 LaunchTable table_ip8();
 LaunchTable table_ip8box();
 LaunchTable table_mengerbox();
 LaunchTable table_all();
 
+void launch_reflect_first(const DevParams &p, const mb3d_cu_silight *gbuf, mb3d_cu_reflect_ray *tmp,
+                          unsigned char *valid, int blocks, cudaStream_t s);
+// the flagged records of tmp in order into out: the count per block of 1024
+// (flag_count), then the scatter from the blocks' offsets (flag_scatter)
+void flag_count(const unsigned char *valid, size_t n, unsigned int *block_sum, cudaStream_t s);
+void flag_scatter(const unsigned char *valid, const mb3d_cu_reflect_ray *tmp, size_t n, const unsigned int *offset,
+                  mb3d_cu_reflect_ray *out, cudaStream_t s);
 void launch_reflect(const DevParams &p, const mb3d_cu_reflect_ray *rays, uint32_t n, int far_fog, const ReflAO *tab,
                     mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s);
 void launch_march(const DevParams &p, bool mixed, int row0, int rows, mb3d_cu_silight *out, Hand *list,

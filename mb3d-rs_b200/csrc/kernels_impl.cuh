@@ -1411,6 +1411,10 @@ struct Launch {
                         mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s) {
         k_reflect<FM><<<blocks, 128, 0, s>>>(p, rays, n, far_fog, tab, hits);
     }
+    static void reflect_first(const DevParams &p, const mb3d_cu_silight *gbuf, mb3d_cu_reflect_ray *tmp,
+                              unsigned char *valid, int blocks, cudaStream_t s) {
+        k_reflect_first<FM><<<blocks, 128, 0, s>>>(p, gbuf, tmp, valid);
+    }
     static void de_probe(const DevParams &p, const double *pos, int n, double *de, int *its, bool mixed, cudaStream_t s) {
         k_de_probe<FM><<<(n + 127) / 128, 128, 0, s>>>(p, pos, n, de, its, mixed ? 1 : 0);
     }

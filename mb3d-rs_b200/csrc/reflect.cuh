@@ -345,4 +345,52 @@ __global__ void __launch_bounds__(128) k_reflect(const __grid_constant__ DevPara
     }
 }
 
+// the first bounce of a pixel (start_pixel, src/reflect.rs:1686-1838, outside
+// rendering, no water, no cutting plane: the surface found again from the
+// stored depth, then step's mirror ray, :1286-1311) into tmp[i], valid[i]
+// 1 where the pixel sends one
+template <int FM>
+__global__ void __launch_bounds__(128) k_reflect_first(const __grid_constant__ DevParams p, const mb3d_cu_silight *g,
+                                                       mb3d_cu_reflect_ray *tmp, unsigned char *valid) {
+    const size_t npix = (size_t)p.width * p.height;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (size_t)gridDim.x * blockDim.x) {
+        valid[i] = 0;
+        G si;
+        si.load(g[i]);
+        if (si.zpos() >= 32768u || si.si_gradient >= 32768) continue;
+        const int x = (int)(i % (size_t)p.width), y = (int)(i / (size_t)p.width);
+        M64<FM> m(p);
+        pixel_ray(p, x, y, m.it.c, m.vfov);
+        m.it.calc_sit = false;
+        const double zf = (double)(si.zpos_fine >> 8);
+        auto zpos_of = [&](double iz) {
+            const double q = (8388351.5 - iz) / p.zc_mul + 1.0;
+            return (q * q - 1.0) / p.zcorr;
+        };
+        m.mzz = zpos_of(zf);
+        add_w(m.it.c, m.vfov, m.mzz);
+        m.update_de_stop();
+        double d = m.calc_de();
+        if (d < (double)m.ms_de_stop * 0.5) continue;
+        const bool de_limited = m.it.it_result < m.max_its_result || d <= (double)m.ms_de_stop;
+        if (de_limited) m.bin_search(d, m.mzz - zpos_of(zf - 1.0));
+        else m.bin_search_it();
+        const double n0[3] = {(double)si.n0 / 32767.0, (double)si.n1 / 32767.0, (double)si.n2 / 32767.0};
+        double nrm[3];
+        rot_rev(n0, p.vgrads, nrm);
+        const double k = 2.0 * dot3d(nrm, m.vfov) / dot3d(nrm, nrm);
+        mb3d_cu_reflect_ray r;
+        for (int c = 0; c < 3; c++) {
+            r.origin[c] = m.it.c[c];
+            r.dir[c] = m.vfov[c] - nrm[c] * k;
+        }
+        r.zz = m.mzz;
+        r.max_len = 0.0;
+        r.pixel = (uint32_t)i;
+        r.rit = 1;
+        tmp[i] = r;
+        valid[i] = 1;
+    }
+}
+
 }  // namespace mb3dcu

@@ -283,6 +283,7 @@ def lib():
         L.mb3d_cu_ssao24.argtypes = [vp, sp, ctypes.POINTER(SsaoOpts), vp]
         L.mb3d_cu_ssao15.argtypes = [vp, sp, ctypes.POINTER(SsaoOpts), vp]
         L.mb3d_cu_reflect_batch.argtypes = [vp, sp, vp, ctypes.c_uint32, ctypes.c_int, vp]
+        L.mb3d_cu_reflect_first_rays.argtypes = [vp, sp, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -291,7 +292,7 @@ EXPORTED = ["mb3d_cu_version", "mb3d_cu_last_error", "mb3d_cu_init", "mb3d_cu_fr
             "mb3d_cu_unsupported", "mb3d_cu_march", "mb3d_cu_march_ex", "mb3d_cu_post", "mb3d_cu_render", "mb3d_cu_de_probe",
             "mb3d_cu_stats_get", "mb3d_cu_set_counting", "mb3d_cu_fma_peak", "mb3d_cu_march_noalloc", "mb3d_cu_render_frames",
             "mb3d_cu_autotune", "mb3d_cu_mc_light_default", "mb3d_cu_mc_batch", "mb3d_cu_mc_render", "mb3d_cu_mc_pass",
-            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24", "mb3d_cu_ssao15", "mb3d_cu_reflect_batch", "mb3d_cu_dof_default", "mb3d_cu_dof",
+            "mb3d_cu_mc_paint_default", "mb3d_cu_mc_paint", "mb3d_cu_paint", "mb3d_cu_ssao_default", "mb3d_cu_ssao24", "mb3d_cu_ssao15", "mb3d_cu_reflect_batch", "mb3d_cu_reflect_first_rays", "mb3d_cu_dof_default", "mb3d_cu_dof",
             "mb3d_cu_dn_param_count", "mb3d_cu_dn_create", "mb3d_cu_dn_free", "mb3d_cu_dn_get_params",
             "mb3d_cu_dn_set_params", "mb3d_cu_dn_set_loss", "mb3d_cu_dn_fallback", "mb3d_cu_dn_denoise", "mb3d_cu_dn_train_step", "mb3d_cu_dn_gradient",
             "mb3d_cu_dn_conv_check", "mb3d_cu_dn_wait_check"]
@@ -526,6 +527,25 @@ class Card:
         self._check(lib().mb3d_cu_reflect_batch(self._ctx, ctypes.byref(scene), _ptr(rays)[0], n, int(far_fog),
                                                 _ptr(out)[0]))
         return out
+
+    def reflect_first_rays(self, scene, gbuf, out=None):
+        """mb3d_cu_reflect_first_rays: the first bounce of every object pixel
+        (REFLECT_RAY, pixel order).  A numpy G-buffer gives a numpy array of
+        the rays; with device buffers (`out`: a torch CUDA byte tensor with
+        room for width * height rays) returns (out, count)."""
+        n = ctypes.c_uint32()
+        if out is None:
+            buf = np.zeros(scene.width * scene.height, REFLECT_RAY)
+            if not isinstance(gbuf, np.ndarray):
+                raise ValueError("device G-buffer: give `out`")
+            g = np.ascontiguousarray(gbuf)
+            self._check(lib().mb3d_cu_reflect_first_rays(self._ctx, ctypes.byref(scene), _ptr(g)[0], _ptr(buf)[0],
+                                                         ctypes.byref(n)))
+            return buf[:n.value].copy()
+        self._order(gbuf, out)
+        self._check(lib().mb3d_cu_reflect_first_rays(self._ctx, ctypes.byref(scene), _ptr(gbuf)[0], _ptr(out)[0],
+                                                     ctypes.byref(n)))
+        return out, n.value
 
     def ssao15(self, scene, gbuf, opts=None):
         """gpu::ssao15 on the card: the older 15-bit ambient occlusion

@@ -121,3 +121,29 @@ def test_device_buffers_and_refusals(card, c2_first):
         card.reflect_batch(rnd, rays[:4])
     assert e.value.status == mb3dcu.ENOTSUP
     assert len(card.reflect_batch(sc, rays[:0])) == 0
+
+
+def test_first_rays_on_the_card(card, c2_first):
+    """mb3d_cu_reflect_first_rays against the oracle's start_pixel + mirror
+    ray: the same pixels send rays (in pixel order), their origins and
+    directions agree to the FP64 surface search's last bits, and the card's
+    batch over the card's rays agrees with the oracle's over the oracle's."""
+    import torch
+    sc, want = c2_first
+    g = O.march(sc, mb3dcu.SILIGHT)
+    got = card.reflect_first_rays(sc, g)
+    common = np.intersect1d(got["pixel"], want["pixel"])
+    assert len(common) >= 0.999 * max(len(got), len(want)), (len(got), len(want), len(common))
+    assert np.all(np.diff(got["pixel"].astype(np.int64)) > 0)
+    a = got[np.isin(got["pixel"], common)]
+    b = want[np.isin(want["pixel"], common)]
+    rel = np.abs(a["zz"] - b["zz"]) / np.maximum(np.abs(b["zz"]), 1e-30)
+    assert np.median(rel) < 1e-12 and np.quantile(rel, 0.99) < 1e-6, (np.median(rel), np.quantile(rel, 0.99))
+    assert np.abs(a["dir"] - b["dir"]).max() < 1e-6 * np.abs(b["dir"]).max()
+    _check(_agree(card.reflect_batch(sc, a), O.reflect_batch(sc, b)))
+    # device buffers
+    gd = torch.from_numpy(g.view(np.uint8).copy()).cuda()
+    out = torch.zeros(sc.width * sc.height * mb3dcu.REFLECT_RAY.itemsize, dtype=torch.uint8, device="cuda")
+    out, n = card.reflect_first_rays(sc, gd, out=out)
+    torch.cuda.synchronize()
+    assert n == len(got) and out[:n * mb3dcu.REFLECT_RAY.itemsize].cpu().numpy().tobytes() == got.tobytes()
