@@ -298,6 +298,38 @@ def paint_figures(card, sc, gbuf, g_a, g_b, flush, stream, reps=5):
             "note": "k_paint: render::paint with the default lighting, 20 bytes in and 3 out per pixel"}
 
 
+def reflect_figures(card, sc, gbuf, flush, stream, reps=3):
+    """The reflection pass's first bounce of the frame on the card
+    (mb3d_cu_reflect_first_rays, then mb3d_cu_reflect_batch: the FP64 march
+    of every object pixel's mirror ray with its hit's normal, colour, depth,
+    shadow and DE AO), device-resident; times from CUDA events."""
+    import torch
+    npix = sc.width * sc.height
+    rays = torch.empty(npix * mb3dcu.REFLECT_RAY.itemsize, dtype=torch.uint8, device="cuda")
+    hits = torch.empty(npix * mb3dcu.REFLECT_HIT.itemsize, dtype=torch.uint8, device="cuda")
+    _, n = card.reflect_first_rays(sc, gbuf, out=rays)
+    rb, hb = n * mb3dcu.REFLECT_RAY.itemsize, n * mb3dcu.REFLECT_HIT.itemsize
+    card.reflect_batch(sc, rays[:rb], out=hits[:hb])
+    t_first, t_batch = [], []
+    for _ in range(reps):
+        flush.zero_()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        card.reflect_first_rays(sc, gbuf, out=rays)
+        ev[1].record(stream)
+        card.reflect_batch(sc, rays[:rb], out=hits[:hb])
+        ev[2].record(stream)
+        ev[2].synchronize()
+        t_first.append(ev[0].elapsed_time(ev[1]))
+        t_batch.append(ev[1].elapsed_time(ev[2]))
+    h = np.frombuffer(hits[:hb].cpu().numpy().tobytes(), dtype=mb3dcu.REFLECT_HIT)
+    mb = statistics.mean(t_batch)
+    return {"rays": int(n), "ms_first_rays": statistics.mean(t_first), "ms_batch": mb,
+            "mrays_s": n / (mb / 1000.0) / 1e6, "hit_share": float((h["hit"] == 1).mean()) if n else 0.0,
+            "note": "the first bounce of every object pixel of the frame: k_reflect_first + compaction, then "
+                    "k_reflect (FP64, one thread per ray, with the hit's shadow and DE AO)"}
+
+
 def config_figures(card, flush, stream, reps=3):
     """The other workloads, one GPU, device-resident outputs: the plain
     Mandelbulb (640x480) and the deep zoom (1920x1080) in both precisions
@@ -600,6 +632,11 @@ def main():
                                  "mixed_over_fp64": om / ms}
             out["parity_vs_fp64"] = parity_vs_fp64(sc, mixed_g, other_g)
         out["paint"] = paint_figures(card, sc, gbuf, mixed_g, other_g, flush, stream)
+        if args.scale == 1.0:
+            try:
+                out["reflect"] = reflect_figures(card, sc, gbuf, flush, stream)
+            except Exception as e:  # (a figure beside the headline: its failure is reported, not fatal)
+                out["reflect"] = {"error": str(e)[:300]}
         card.set_stream(None)
         if not args.no_configs and args.scale == 1.0:
             out["configs"] = config_figures(card, flush, stream)
