@@ -330,7 +330,7 @@ def reflect_figures(card, sc, gbuf, flush, stream, reps=3):
                     "k_reflect (FP64, one thread per ray, with the hit's shadow and DE AO)"}
 
 
-def config_figures(card, flush, stream, reps=3):
+def config_figures(card, flush, stream, peak32=None, reps=3):
     """The other workloads, one GPU, device-resident outputs: the plain
     Mandelbulb (640x480) and the deep zoom (1920x1080) in both precisions
     with the mixed march's agreement with the FP64 one; the 240-frame
@@ -375,6 +375,26 @@ def config_figures(card, flush, stream, reps=3):
         "tune": {"blocks_per_sm": tune.blocks_per_sm, "refill_min": tune.refill_min, "streams": tune.streams},
         "autotune_s": tune_s, "launches_per_call": st["launches"]}
     del gbuf
+    # the flight's FP32 march kernel against the FP32 peak: the counted
+    # formula iterations and DEs of one frame over its mean launch time
+    f = frames[37]
+    g1 = torch.empty(npix * 20, dtype=torch.uint8, device="cuda")
+    card.set_counting(True)
+    card.render(f, mb3dcu.FP32_FP64, out=g1)
+    cst = card.stats()
+    card.set_counting(False)
+    kms = []
+    for _ in range(reps):
+        card.render(f, mb3dcu.FP32_FP64, out=g1)
+        s1 = card.stats()
+        kms.append(s1["ms_march"] - s1["ms_finish"])
+    k = statistics.mean(kms)
+    fl = march_flops(f, cst)
+    out["c4_flight_240x1280x720"]["roofline_frame37"] = {
+        "kernel": "k_march (FP32 bulk march)", "bound": "fp32-alu", "flops_per_launch": fl, "ms_per_launch": k,
+        "achieved": fl / (k / 1000.0) / 1e12, "peak": peak32, "unit": "TFLOP/s",
+        "frac": fl / (k / 1000.0) / 1e12 / peak32 if peak32 else None}
+    del g1
     card.set_stream(None)
     return out
 
@@ -639,7 +659,7 @@ def main():
                 out["reflect"] = {"error": str(e)[:300]}
         card.set_stream(None)
         if not args.no_configs and args.scale == 1.0:
-            out["configs"] = config_figures(card, flush, stream)
+            out["configs"] = config_figures(card, flush, stream, peak32)
         if not args.no_mc and args.scale == 1.0:
             out["mc"] = mc_figures(card, args.mc_ref_rays)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
