@@ -6,7 +6,8 @@ The first bounce of every object pixel of the hybrid frame (the oracle's
 restatement of start_pixel and step's mirror ray) and the second bounce
 from those hits, marched on the card in double precision: hits, depths,
 normals, colours, shadow bits and ambient occlusion against the oracle's,
-per ray.  The card's FP64 arithmetic may fuse a multiply and an add where
+per ray (the records bit for bit but for the occlusion, which takes the
+card's acos and sincos in its turn to the normal).  The card's FP64 arithmetic may fuse a multiply and an add where
 the oracle does not, so a ray that grazes a surface may land elsewhere; the
 bounds below allow for that on a small share of rays."""
 import numpy as np
@@ -22,8 +23,12 @@ pytestmark = pytest.mark.gpu
 def _agree(got, want):
     h_g, h_w = got["hit"] == 1, want["hit"] == 1
     both = h_g & h_w
-    r = {"hit_agree": float((h_g == h_w).mean()), "both": int(both.sum()),
-         "exact_si": float((got["si"][both] == want["si"][both]).mean())}
+    sg, sw = got["si"][both], want["si"][both]
+    same = np.ones(len(sg), bool)
+    for f in ("normal", "zpos_fine", "shadow", "si_gradient", "otrap"):
+        same &= (sg[f] == sw[f]).reshape(len(sg), -1).all(axis=1)
+    # (the ambient occlusion apart: its turn to the normal takes the card's acos and sincos)
+    r = {"hit_agree": float((h_g == h_w).mean()), "both": int(both.sum()), "exact_si": float(same.mean())}
     zg, zw = got["zz2"][both], want["zz2"][both]
     rel = np.abs(zg - zw) / np.maximum(np.abs(zw), 1e-30)
     r["zz2_rel_median"] = float(np.median(rel))
@@ -37,12 +42,13 @@ def _agree(got, want):
 
 
 def _check(r):
-    assert r["hit_agree"] >= 0.98, r
-    assert r["exact_si"] >= 0.9, r
-    assert r["zz2_rel_median"] < 1e-9 and r["zz2_rel_p99"] < 1e-4, r
-    assert r["shadow_agree"] >= 0.97, r
-    assert r["amb_within_8"] >= 0.95, r
-    assert r["miss_steps_agree"] >= 0.97, r
+    t = str(r)
+    assert r["hit_agree"] >= 0.98, t
+    assert r["exact_si"] >= 0.9, t
+    assert r["zz2_rel_median"] < 1e-9 and r["zz2_rel_p99"] < 1e-4, t
+    assert r["shadow_agree"] >= 0.97, t
+    assert r["amb_within_8"] >= 0.95, t
+    assert r["miss_steps_agree"] >= 0.97, t
 
 
 @pytest.fixture(scope="module")
