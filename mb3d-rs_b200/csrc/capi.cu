@@ -304,8 +304,9 @@ static int post_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int pa
     if (int r = grow((void **)&c->d_slist, &c->slist_cap, npix * sizeof(uint32_t))) return r;
     if (int r = grow((void **)&c->d_ps, &c->ps_cap, npix * sizeof(PostStart))) return r;
     if (passes & MB3D_CU_POST_DEAO)
-        if (int r = grow((void **)&c->d_minra, &c->minra_cap, npix * (size_t)p.ao_rays * sizeof(float))) return r;
-    unsigned int *cnt = c->d_counters + 8;  // [0] surfaces, [1] shadow queue, [2] AO queue, [3] start queue
+        if (int r = grow((void **)&c->d_minra, &c->minra_cap, (npix * (size_t)p.ao_rays + 4) * AO_MINRA_BYTES)) return r;
+    // [0] surfaces, [1] shadow queue, [2] AO queue, [3] start queue, [4] AO rays handed to FP64, [5] their queue
+    unsigned int *cnt = c->d_counters + 8;
     CU_TRY(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned int), s));
     CU_TRY(cudaEventRecord(c->ev[3], s));
     launch_surface(p, (int)npix, passes, dg, c->d_slist, cnt, c->sms * 4, s);
@@ -766,7 +767,7 @@ static int ensure_frame_resources(mb3d_cu_ctx *c, int streams, size_t npix, size
             CU_TRY(cudaMalloc(&sc.slow, npix * sizeof(Hand)));
             CU_TRY(cudaMalloc(&sc.slist, npix * sizeof(uint32_t)));
             CU_TRY(cudaMalloc(&sc.ps, npix * sizeof(PostStart)));
-            CU_TRY(cudaMalloc(&sc.minra, (nray > 0 ? nray : 1) * sizeof(float)));
+            CU_TRY(cudaMalloc(&sc.minra, (nray + 4) * AO_MINRA_BYTES));
             CU_TRY(cudaMalloc(&sc.counters, 64 * sizeof(unsigned int)));
             sc.npix = npix;
             sc.nray = nray;

@@ -27,6 +27,23 @@ struct Hand {
 #define HAND_REMARCH 8u  // march on in double precision from this state
 
 // Where a post pass starts on a surface pixel.
+// a DE AO ray the single precision kernel hands over to double precision:
+// its item, its length and openness so far, its step count (bit 31: the
+// ray's last step); the list follows the rays' openness array min_ra
+// (ao_slow_list), so that array holds AO_MINRA_BYTES per ray
+struct AoSlow {
+    uint32_t item;
+    float dt1, s;
+    uint32_t guard;
+};
+constexpr size_t AO_MINRA_BYTES = sizeof(float) + sizeof(AoSlow);
+__host__ __device__ inline AoSlow *ao_slow_list(float *min_ra, uint32_t n_items) {
+    return reinterpret_cast<AoSlow *>(min_ra + (((size_t)n_items + 3) & ~(size_t)3));
+}
+__host__ __device__ inline const AoSlow *ao_slow_list(const float *min_ra, uint32_t n_items) {
+    return reinterpret_cast<const AoSlow *>(min_ra + (((size_t)n_items + 3) & ~(size_t)3));
+}
+
 struct PostStart {
     double sh_c[3];  // the shadow rays' start (0.1 step in front of the surface)
     double sh_mzz;

@@ -35,6 +35,9 @@
 #endif
 // (the single precision march: 4 blocks of 64 registers, its spills cost
 // less than the warps it gains)
+#ifndef MB3D_MIN_BLOCKS_AO32
+#define MB3D_MIN_BLOCKS_AO32 4
+#endif
 #ifndef MB3D_MIN_BLOCKS_MARCH32
 #define MB3D_MIN_BLOCKS_MARCH32 4
 #endif
@@ -1222,7 +1225,7 @@ __device__ __forceinline__ AOc ao_consts(const DevParams &p, float ms_surface) {
 // deao_row (src/deao.rs:317-359) outside rendering, one DE per trip;
 // min_ra[k * npx + i] receives the ray's openness.
 template <typename R, int FM>
-__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_constant__ DevParams p, const PostStart *ps,
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_AO32 : MB3D_MIN_BLOCKS) k_ao_rays(const __grid_constant__ DevParams p, const PostStart *ps,
                                                  const mb3d_cu_silight *gbuf, const unsigned int *count,
                                                  float *min_ra, unsigned int *queue) {
     // the ray's type: single precision in the mixed mode (the DE AO's
@@ -1273,7 +1276,22 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_c
                 b_end = true;
             }
             T c[3] = {ic[0] + sv[0] * dt1, ic[1] + sv[1] * dt1, ic[2] + sv[2] * dt1};
-            DEr r = ray_de<R, FM>(p, c, ms_s);
+            DEr r;
+            if constexpr (sizeof(R) == 4) {
+                // a DE single precision cannot decide: the ray goes on in
+                // double precision in k_ao_slow (kept out of this kernel:
+                // the double DE's registers would cost this loop occupancy)
+                r = de_lock<float, FM, false, false, float>(p, c, ms_s);
+                if (r.need64) {
+                    AoSlow *list = ao_slow_list(min_ra, n_items);
+                    const unsigned int at = atomicAdd(queue + 2, 1u);
+                    list[at] = AoSlow{slot, (float)dt1, (float)s_tmp, (unsigned int)guard | (b_end ? 0x80000000u : 0u)};
+                    active = false;
+                    continue;
+                }
+            } else {
+                r = ray_de<R, FM>(p, c, ms_s);
+            }
             const T dt2 = (T)r.de;
             if constexpr (sizeof(R) == 4) s_tmp = fminf(s_tmp, __fdividef(dt2 - msd + dt1 * md_d10, dt1));
             else s_tmp = fmin(s_tmp, (dt2 - msd + dt1 * md_d10) / dt1);
@@ -1284,6 +1302,50 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_ao_rays(const __grid_c
                 active = false;
             }
         }
+    }
+}
+
+// the DE AO rays the single precision kernel handed over (AoSlow records),
+// one thread per ray, in double precision from where they stopped: the DE
+// there, then the rest of the ray as k_ao_rays<double> marches it
+template <int FM>
+__global__ void __launch_bounds__(128) k_ao_slow(const __grid_constant__ DevParams p, const PostStart *ps,
+                                                 const unsigned int *count, float *min_ra, unsigned int *queue) {
+    const uint32_t npx = count[0];
+    const uint32_t n_items = npx * (uint32_t)p.ao_rays;
+    const AoSlow *list = ao_slow_list(min_ra, n_items);
+    const unsigned int n = queue[2];
+    const double dsm = (double)p.ao_d_step_mul;
+    const double de_mul = sqrt((double)p.ao_rays * 0.5);
+    for (;;) {
+        const unsigned int at = atomicAdd(queue + 3, 1u);
+        if (at >= n) break;
+        const AoSlow rec = list[at];
+        const uint32_t i = rec.item % npx;
+        const int k = (int)(rec.item / npx);
+        const PostStart &s = ps[i];
+        const double ic[3] = {s.ao_c[0], s.ao_c[1], s.ao_c[2]};
+        const float *dk = p.ao_dirs[k];
+        const float vv[3] = {sdot3(s.ao_rot[0], dk), sdot3(s.ao_rot[1], dk), sdot3(s.ao_rot[2], dk)};
+        const double vd[3] = {(double)vv[0], (double)vv[1], (double)vv[2]};
+        double sv[3];
+        rot_rev(vd, p.ao_rot, sv);
+        const double msd = s.ao_msd, max_dist = s.ao_max_dist, md_d10 = s.ao_md_d10;
+        double dt1 = (double)rec.dt1, s_tmp = (double)rec.s;
+        int guard = (int)(rec.guard & 0x7FFFFFFFu);
+        bool b_end = (rec.guard & 0x80000000u) != 0;
+        for (;;) {
+            if (dt1 > max_dist) {
+                dt1 = max_dist;
+                b_end = true;
+            }
+            const double c[3] = {ic[0] + sv[0] * dt1, ic[1] + sv[1] * dt1, ic[2] + sv[2] * dt1};
+            const DEr r = de_lock<double, FM>(p, c, s.ao_ms);
+            s_tmp = fmin(s_tmp, (r.de - msd + dt1 * md_d10) / dt1);
+            if (s_tmp < 0.02 || b_end || ++guard > 100000) break;
+            dt1 += fmax(r.de, dt1 * dsm);
+        }
+        min_ra[rec.item] = (float)(fmax(s_tmp, 0.0) * de_mul);
     }
 }
 
@@ -1404,8 +1466,12 @@ struct Launch {
     }
     static void ao_rays(const DevParams &p, bool mixed, const PostStart *ps, const mb3d_cu_silight *gbuf,
                         const unsigned int *count, float *min_ra, unsigned int *queue, int blocks, cudaStream_t s) {
-        if (mixed) k_ao_rays<float, FM><<<blocks, 256, 0, s>>>(p, ps, gbuf, count, min_ra, queue);
-        else k_ao_rays<double, FM><<<blocks, 256, 0, s>>>(p, ps, gbuf, count, min_ra, queue);
+        if (mixed) {
+            k_ao_rays<float, FM><<<blocks, 256, 0, s>>>(p, ps, gbuf, count, min_ra, queue);
+            k_ao_slow<FM><<<blocks, 128, 0, s>>>(p, ps, count, min_ra, queue);
+        } else {
+            k_ao_rays<double, FM><<<blocks, 256, 0, s>>>(p, ps, gbuf, count, min_ra, queue);
+        }
     }
     static void reflect(const DevParams &p, const mb3d_cu_reflect_ray *rays, uint32_t n, int far_fog, const ReflAO *tab,
                         mb3d_cu_reflect_hit *hits, int blocks, cudaStream_t s) {

@@ -1527,10 +1527,39 @@ void deao_1pos(Marcher &m, SiLight &si, int quality, float max_len) {
     const double ic[3] = {m.it.c[0], m.it.c[1], m.it.c[2]};
     const double step_ao = ms_de_stop / (double)p->de_stop;
     const double max_dist = s_max_d * std::sqrt(step_ao);
-    const Rays base = build_rays(quality);
-    // (here in double precision: 1.8, or 1 + sin(abr))
-    const int q = std::min(std::max(quality, 0), 3);
-    const double d_step_mul = q == 0 ? 1.8 : 1.0 + std::sin((PI / 2.0) / ((double)q + 0.9));
+    // the directions (src/reflect.rs:973-998): not deao.rs's table -- every
+    // ring has the same number of rays, round(sin(0.25) * tau / abr); the
+    // step multiplier in double precision
+    Rays base;
+    double d_step_mul;
+    {
+        const int q = std::min(std::max(quality, 0), 3);
+        SVec d;
+        if (q == 0) {
+            const double abr = to_radians(60.0);
+            for (int i = 0; i < 3; i++) {
+                ray_dir(0.5 * abr, (double)i * TAU / 3.0, d);
+                base.dirs.push_back({d[0], d[1], d[2]});
+            }
+            d_step_mul = 1.8;
+            base.d_min_a_dif = -1.0f;
+            base.correction_weight = 0.3f;
+        } else {
+            const double abr = (PI / 2.0) / ((double)q + 0.9);
+            ray_dir(0.0, 0.0, d);
+            base.dirs.push_back({d[0], d[1], d[2]});
+            for (int iy = 1; iy <= q; iy++) {
+                const int n = (int)rte(std::sin(0.25) * TAU / abr);
+                for (int ix = 0; ix < n; ix++) {
+                    ray_dir(abr * (double)iy, (double)ix * TAU / (double)n, d);
+                    base.dirs.push_back({d[0], d[1], d[2]});
+                }
+            }
+            d_step_mul = 1.0 + std::sin(abr);
+            base.d_min_a_dif = (float)std::cos(abr * 1.2);
+            base.correction_weight = q == 1 ? 0.2f : 0.1666f;
+        }
+    }
     if (p->de_stop_factor != 0.0f) ms_de_stop /= d_step_mul * d_step_mul;
     else ms_de_stop = (double)p->de_stop / (d_step_mul * d_step_mul);
     const auto &dirs = base.dirs;
