@@ -46,6 +46,7 @@ struct mb3d_cu_ctx {
     unsigned int *d_counters = nullptr;
     unsigned int *h_counters = nullptr;  // (pinned) the march's list lengths, read back with each call
     bool read_slow = false;
+    bool read_status = false;  // h_counters holds the march's status word
     double *d_probe = nullptr;
     size_t probe_cap = 0;
     cudaEvent_t ev[9] = {};
@@ -287,8 +288,9 @@ static int march_device(mb3d_cu_ctx *c, const DevParams &p, int precision, int r
     // the slow list's length: the mixed mode's pixels finished by the
     // per-thread double precision marcher
     c->read_slow = mixed;
-    if (mixed) CU_TRY(cudaMemcpyAsync(c->h_counters, c->d_counters, (CNT_OVERFLOW + 1) * sizeof(unsigned int),
-                                      cudaMemcpyDeviceToHost, s));
+    c->read_status = true;
+    CU_TRY(cudaMemcpyAsync(c->h_counters, c->d_counters, (CNT_OVERFLOW + 1) * sizeof(unsigned int),
+                           cudaMemcpyDeviceToHost, s));
     return 0;
 }
 
@@ -357,6 +359,11 @@ static int finish_call(mb3d_cu_ctx *c, bool marched, bool posted) {
         c->stats.fp32_overflow_pixels = c->h_counters[CNT_OVERFLOW];
     }
     c->read_slow = false;
+    if (marched && c->read_status && (c->h_counters[CNT_STATUS] & ST_TRIP_CAP)) {
+        c->read_status = false;
+        return fail(MB3D_CU_EIO, "a march kernel ran out of its loop trips: rays left unmarched");
+    }
+    c->read_status = false;
     if (marched && c->counting && c->d_count) {
         unsigned long long h[16];
         CU_TRY(cudaMemcpy(h, c->d_count, sizeof(h), cudaMemcpyDeviceToHost));

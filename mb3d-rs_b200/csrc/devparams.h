@@ -77,5 +77,9 @@ struct DevParams {
 #define CNT_FINISH_Q 3    // the finish's queue
 #define CNT_SLOW_Q 4      // the slow finish's queue
 #define CNT_T0 32         // (two slots) %globaltimer of the call's first take
-#define CNT_STATUS 34     // bits: 1 the march, 2 the finish, 4 the slow finish stopped on the budget
+#define CNT_STATUS 34     // bits: 1 the march, 2 the finish, 4 the slow finish stopped on the budget;
+                          // ST_TRIP_CAP a march or finish warp ran out of loop trips
+#define ST_TRIP_CAP 8u
+// the wavefront kernels' loop limit (a warp's trips; one DE per trip)
+#define MB3D_TRIP_CAP 400000000u
 #define CNT_OVERFLOW 35   // pixels whose single precision DE overflowed

@@ -192,7 +192,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
     const int tid = (int)threadIdx.x;
     int hs = 0;
     int nb = 0;
-    for (unsigned int trip = 0; trip < 400000000u; trip++) {
+    unsigned int trip = 0;
+    for (; trip < MB3D_TRIP_CAP; trip++) {
         uint32_t item = warp_take_b(p, phase == PH_IDLE, counters, CNT_MARCH_Q, n_items, p.refill_min, open, 1u);
         if (item != UINT32_MAX) {
             item_pixel(item, tiles_x, x, ly);
@@ -374,6 +375,8 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             if (ov && (threadIdx.x & 31) == __ffs(ov) - 1) atomicAdd(&counters[CNT_OVERFLOW], (unsigned int)__popc(ov));
         }
     }
+    // (a warp that ran out of trips left rays unmarched: the host fails the call)
+    if (trip >= MB3D_TRIP_CAP && (threadIdx.x & 31) == 0) atomicOr(counters + CNT_STATUS, ST_TRIP_CAP);
     if (COUNT) cnt.flush(gcount);
 }
 
@@ -468,7 +471,8 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
     int itmp = 0, k_ax = 0;
     bool it_limited = false, b_first = false;
     unsigned int guard = 0;
-    for (unsigned int trip = 0; trip < 400000000u; trip++) {
+    unsigned int trip = 0;
+    for (; trip < MB3D_TRIP_CAP; trip++) {
         uint32_t item = warp_take_b(p, phase == F_IDLE, counters, CNT_FINISH_Q, n_items, p.refill_min, open, 2u);
         bool to_slow = false;
         Hand hs;
@@ -737,6 +741,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_co
         unsigned int busy = __ballot_sync(0xffffffffu, phase != F_IDLE);
         if (busy == 0 && !open) break;
     }
+    if (trip >= MB3D_TRIP_CAP && (threadIdx.x & 31) == 0) atomicOr(counters + CNT_STATUS, ST_TRIP_CAP);
 }
 
 // ---------------------------------------------------------------------------
@@ -813,7 +818,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __gri
     // the shadow search leaves the DE AO start at its sixth round and the
     // DE AO task is not run again)
     bool snap = !MIXED, ao_done = false;
-    for (unsigned int trip = 0; trip < 400000000u; trip++) {
+    for (unsigned int trip = 0; trip < MB3D_TRIP_CAP; trip++) {
         uint32_t item = warp_take(phase == Q_IDLE, queue, n_items, p.refill_min, open);
         bool begin = false;
         if (item != UINT32_MAX) {
@@ -1063,7 +1068,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_shadow_rays(const __gr
     float cs[3] = {0.f, 0.f, 0.f}, lv[3] = {0.f, 0.f, 0.f};
     float ms = 0.f, rsf = 2.f, zr = 1.f, zrs_mul = 0.f;
     bool stepped = false;
-    for (unsigned int trip = 0; trip < 400000000u; trip++) {
+    for (unsigned int trip = 0; trip < MB3D_TRIP_CAP; trip++) {
         uint32_t item = warp_take(!active, queue, n_items, p.refill_shadow, open);
         if (item != UINT32_MAX) {
             uint32_t i = item % npx;
@@ -1240,7 +1245,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_AO32 : M
     int guard = 0;
     const T dsm = (T)p.ao_d_step_mul;
     const double de_mul = sqrt((double)p.ao_rays * 0.5);
-    for (unsigned int trip = 0; trip < 400000000u; trip++) {
+    for (unsigned int trip = 0; trip < MB3D_TRIP_CAP; trip++) {
         uint32_t item = warp_take(!active, queue, n_items, p.refill_ao, open);
         if (item != UINT32_MAX) {
             uint32_t i = item % npx;
