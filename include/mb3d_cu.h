@@ -117,6 +117,14 @@ typedef struct mb3d_cu_scene {
     int32_t deao_dither;    /* 0 (only 0 on the card path) */
     float deao_max_len;     /* default 1 */
     int32_t deao_first_step_random;
+    /* the interpolation hybrid (Scene::interpolation, src/scene.rs:510;
+     * doInterpolHybridPas, src/iteration.rs:347-475): with interpolation
+     * non-zero the first two slots' formulas are applied to the same vector
+     * in every iteration and their results blended with ipol_weights
+     * (normalised to a sum of 1; the slots' iteration counts are not used) */
+    int32_t interpolation;
+    float ipol_weights[2];
+    int32_t pad1;
 } mb3d_cu_scene;
 
 /* The G-buffer record SiLight (src/gbuffer.rs:5-20), 20 bytes; mb3d-rs's

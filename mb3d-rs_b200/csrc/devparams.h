@@ -63,6 +63,10 @@ struct DevParams {
     // take no new rays once this many nanoseconds have passed since the
     // first warp of the call asked (their queue counters stay resumable)
     unsigned long long budget_ns;
+    // an interpolation hybrid (HybridMode::Ipol3D): the two first slots'
+    // formulas blended in every iteration with the normalised weights
+    int32_t ipol, pad_ipol;
+    float ipol_w[2];
 };
 
 // slot orders the single precision DE loop knows at compile time

@@ -352,4 +352,55 @@ __device__ __forceinline__ void f_amazing_box_x2(float scale, float min_r, float
     v[0] = pfma(x, mul, j[0]);
 }
 
+// The interpolation hybrid's loop (run_ipol, src/iteration.rs:347-401, 3D):
+// both of the first two slots' formulas on the same vector, the results and
+// their lengths blended with the normalised weights, the blend scaled to the
+// blended length; `de` blends the running derivative (w) of the analytic-DE
+// variant.  Every iteration counts; returns the count.
+template <typename R, int FM>
+__device__ __forceinline__ int ipol_run(const DevParams &p, R v[4], R j[3], R &rout, R &rold, R &otrap, int max_it,
+                                        R rstop, bool de) {
+    const R s1 = (R)p.ipol_w[0], s2 = (R)p.ipol_w[1];
+    const DevSlot &a = p.slots[0], &b = p.slots[1];
+    int it = 0;
+    for (int guard = 0; guard < (1 << 20); guard++) {
+        rold = rout;
+        const R y1[4] = {v[0], v[1], v[2], v[3]};
+        formula_iterate<R, FM>(a, v, j, rout);
+        if (a.julia_add) {
+            v[0] += j[0];
+            v[1] += j[1];
+            v[2] += j[2];
+        }
+        const R x1[4] = {v[0], v[1], v[2], v[3]};
+        v[0] = y1[0];
+        v[1] = y1[1];
+        v[2] = y1[2];
+        v[3] = y1[3];
+        formula_iterate<R, FM>(b, v, j, rout);
+        if (b.julia_add) {
+            v[0] += j[0];
+            v[1] += j[1];
+            v[2] += j[2];
+        }
+        const R x = v[0], y = v[1], z = v[2], w = v[3];
+        R xx = sqrt(x1[0] * x1[0] + x1[1] * x1[1] + x1[2] * x1[2]);
+        const R yy0 = sqrt(x * x + y * y + z * z);
+        xx = xx * s1 + yy0 * s2;
+        R nv[4] = {x1[0] * s1 + x * s2, x1[1] * s1 + y * s2, x1[2] * s1 + z * s2, x1[3] * s1 + w * s2};
+        if (de) nv[3] = fabs(x1[3]) * s1 + fabs(w) * s2;
+        const R l2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
+        const R q = xx / sqrt(l2 + (R)1e-40);
+        v[0] = nv[0] * q;
+        v[1] = nv[1] * q;
+        v[2] = nv[2] * q;
+        v[3] = nv[3];
+        it += 1;
+        rout = xx * xx;
+        if (rout < otrap) otrap = rout;
+        if (it >= max_it || rout > rstop) break;
+    }
+    return it;
+}
+
 }  // namespace mb3dcu

@@ -168,14 +168,27 @@ struct It64 {
         rout = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
         otrap = rout;
     }
-    __device__ void hybrid_3d(const DevParams &p) {  // doHybridPas
+    __device__ void hybrid_3d(const DevParams &p) {  // doHybridPas; doInterpolHybridPas
         start(p);
         v[3] = 0.0;
+        if (p.ipol) {
+            it_result = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, rstop, false);
+            if (calc_sit) smooth_iterations(p, 0);
+            return;
+        }
         int n = run(p);
         if (calc_sit) smooth_iterations(p, n);
     }
     __device__ double hybrid_3d_de(const DevParams &p) {  // doHybridPasDE
         start(p);
+        if (p.ipol) {  // doInterpolHybridPasDE (src/iteration.rs:441-455)
+            v[3] = ((p.de_option & 0x18) == 16) ? rout : 1.0;
+            it_result = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, rstop, true);
+            const double w = v[3];
+            const double r = ((p.de_option & 7) == 4) ? fabs(v[2]) * log(fabs(v[2])) / w : sqrt(rout) / fabs(w);
+            if (calc_sit) smooth_iterations(p, 0);
+            return r;
+        }
         v[3] = ((p.de_option & 0x38) == 16) ? rout : 1.0;
         int n = run(p);
         double w = v[3];

@@ -66,6 +66,27 @@ static int de_option_of(const int *des, const int *its, int n) {
     return opt;
 }
 
+// ipol_de_option (src/calc.rs:255-308): CheckDEoption of the two weighted
+// formulas (a weight counts when its bits as a signed integer are > 0)
+static int ipol_de_option(const int *des, const float *raw) {
+    int opt = -1;
+    for (int x = 0; x < 2; x++) {
+        int32_t bits;
+        std::memcpy(&bits, &raw[x], 4);
+        if (bits <= 0) continue;
+        const int de = des[x];
+        if (de < 0 || de > 20 || de == opt) continue;
+        if ((opt >= 0 && opt < 20 && de > 19) || (opt > 19 && de >= 0 && de < 20)) return -1;
+        if (opt == -1) opt = de;
+        else if (opt == 2) opt = (de == 2 || de == 5 || de == 6 || de == 11) ? 2 : 0;
+        else if (opt == 4) opt = (de == 5 || de == 6) ? 4 : 0;
+        else if (opt == 5) opt = de == 4 ? 4 : (de == 2 || de == 11) ? 2 : (de != 6 ? 0 : 5);
+        else if (opt == 6) opt = (de == 2 || de == 4 || de == 5 || de == 11) ? de : 0;
+        else if (opt == 11) opt = (de == 2 || de == 5) ? 2 : (de != 6 ? 0 : 11);
+    }
+    return opt > 19 ? 20 : opt;
+}
+
 int unsupported_reason(const mb3d_cu_scene &sc, std::string &why) {
     if (sc.width <= 0 || sc.height <= 0 || sc.width > 65536 || sc.height > 65536) {
         why = "the picture size must be 1..65536 pixels each way";
@@ -79,9 +100,14 @@ int unsupported_reason(const mb3d_cu_scene &sc, std::string &why) {
         why = "zoom and fov must be positive and iterations at least 1";
         return MB3D_CU_EINVAL;
     }
+    const bool ipol = sc.interpolation != 0;
+    if (ipol && sc.n_slots < 2) {
+        why = "an interpolation hybrid needs two formulas";
+        return MB3D_CU_EINVAL;
+    }
     bool any = false;
-    for (int i = 0; i < sc.n_slots; i++) {
-        if (sc.slots[i].iterations == 0) continue;
+    for (int i = 0; i < (ipol ? 2 : sc.n_slots); i++) {
+        if (sc.slots[i].iterations == 0 && !ipol) continue;
         any = true;
         if (!f_known(sc.slots[i].formula)) {
             why = "formula #" + std::to_string(sc.slots[i].formula) + " is not built into this backend";
@@ -104,13 +130,31 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     if (u < 0) return u;
     if (u > 0) return MB3D_CU_ENOTSUP;
     std::memset(&p, 0, sizeof(p));
-    int n = sc.n_slots;
+    // an interpolation hybrid (src/calc.rs:378-409): the two first formulas,
+    // one iteration each, counted, with their weights normalised to a sum
+    // of 1 in single precision
+    const bool ipol = sc.interpolation != 0;
+    float ipw[2] = {1.0f, 0.0f};
+    if (ipol) {
+        float x1 = sc.ipol_weights[0], x2 = sc.ipol_weights[1];
+        float y1 = x1 + x2;
+        if (y1 < 1e-10f) {
+            y1 = 1.0f;
+            x1 = 1.0f;
+            x2 = 0.0f;
+        } else {
+            y1 = 1.0f / y1;
+        }
+        ipw[0] = x1 * y1;
+        ipw[1] = x2 * y1;
+    }
+    int n = ipol ? 2 : sc.n_slots;
     int its[6] = {0}, des[6] = {0}, fs[6] = {0};
     bool unc[6] = {false};
     for (int i = 0; i < n; i++) {
-        its[i] = std::abs(sc.slots[i].iterations);
-        unc[i] = sc.slots[i].iterations < 0;
-        fs[i] = sc.slots[i].iterations != 0 ? sc.slots[i].formula : MB3D_CU_F_INTPOW;
+        its[i] = ipol ? 1 : std::abs(sc.slots[i].iterations);
+        unc[i] = !ipol && sc.slots[i].iterations < 0;
+        fs[i] = (sc.slots[i].iterations != 0 || ipol) ? sc.slots[i].formula : MB3D_CU_F_INTPOW;
         des[i] = f_de_option(fs[i]);
     }
     // CheckHybridOptions: the last slot with iterations ends the hybrid
@@ -124,6 +168,13 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     if (sc.disable_analytic_de) {
         if (de_option == 2 || de_option == 11) de_option = 0;
         else if (de_option == 5 || de_option == 6) de_option = 4;
+    }
+    if (ipol) {
+        de_option = ipol_de_option(des, sc.ipol_weights);
+        if (de_option >= 20) {
+            err = "dIFS formulas do not work in an interpolation hybrid";
+            return MB3D_CU_EINVAL;
+        }
     }
     if (de_option < 0) {
         err = "formula option is not valid";
@@ -143,28 +194,30 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     for (int x = 0; x < nsl; x++) {
         if (its[x] == 0) continue;
         const mb3d_cu_slot &s = sc.slots[x];
-        if (!unc[x]) {
+        if (ipol || !unc[x]) {
             double sip = f_si_pow(s);
             double z1 = sip > 1.0 ? sip : f_first_option(s);
             fhln[x] = (float)(1.0 / std::log(std::fmax(2.0, std::fabs(z1))));
         }
-        double w = (double)its[x];
+        // (an interpolation hybrid: weighted by the weights, counted once)
+        double w = ipol ? (double)ipw[x] : (double)its[x];
+        const double cnt = ipol ? 1.0 : w;
         int j = des[x];
-        if (custom && !unc[x] && (j == 5 || j == 11)) {
-            cnt_n += w;
-            cnt_i += w;
+        if (custom && (ipol || !unc[x]) && (j == 5 || j == 11)) {
+            cnt_n += cnt;
+            cnt_i += cnt;
             double x2 = f_first_option(s);
             if (x2 == 0.0) x2 = 1e-40;
             sum_x += x2 < 0.0 ? 0.65 * w : (x2 * 1.2 + 1.0) / x2 * w;
             sum_y += std::fabs(x2) * w;
-        } else if (j >= 0) {
-            cnt_n += w;
+        } else if (j >= 0 || ipol) {
+            cnt_n += cnt;
             sum_x += (custom ? 1.0 : f_de_scale(fs[x])) * w;
         }
     }
     double dde = 1.0;
     float col_plus = 0.f;
-    if (cnt_n > 0.0 && de_option != 20) dde = sum_x / cnt_n;
+    if (cnt_n > 0.0 && de_option != 20) dde = ipol ? sum_x : sum_x / cnt_n;
     if (cnt_n > 0.0 && cnt_i > 0.0) col_plus = (float)(std::pow(std::fabs(sum_y / cnt_i), 0.25) * 40.0 - 49.0);
     // mctColVarDEstopMul (src/calc.rs:591-652), one hybrid part
     float col_var = 0.6f;
@@ -172,11 +225,11 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
         double a = 0, b = 0;
         int ia = 0, itmp = 0;
         for (int x = 0; x < nsl; x++) {
-            if (!(its[x] > 0 && !unc[x])) {
+            if (!(ipol || (its[x] > 0 && !unc[x]))) {
                 if (its[x] > 0) (x > end_to ? ia : itmp)++;
                 continue;
             }
-            double w = (double)its[x];
+            double w = ipol ? (double)ipw[x] : (double)its[x];
             int de = des[x];
             if (de == 0 || de == 4) {
                 a += w * 0.6;
@@ -321,6 +374,15 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     double eps32 = 1.1920928955078125e-07;
     double prec = custom ? sw / (coord * eps32) : (double)p.de_offset / (coord * eps32);
     p.all_fp64 = custom ? (prec < 64.0) : (prec < 3.0);
+    // an interpolation hybrid: the double precision DE only (the single
+    // precision march and rays do not carry its blend)
+    p.ipol = ipol ? 1 : 0;
+    p.ipol_w[0] = ipw[0];
+    p.ipol_w[1] = ipw[1];
+    if (ipol) {
+        p.all_fp64 = 1;
+        p.sched = SCHED_GENERIC;
+    }
     p.coord_eps = coord * eps32;
     p.hand_margin = 4.0f;
     p.hand_back = 2;

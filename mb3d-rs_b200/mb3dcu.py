@@ -60,6 +60,7 @@ class Scene(ctypes.Structure):
         ("soft_radius", ctypes.c_float), ("hs_max_len_mul", ctypes.c_float),
         ("deao_quality", ctypes.c_int32), ("deao_dither", ctypes.c_int32),
         ("deao_max_len", ctypes.c_float), ("deao_first_step_random", ctypes.c_int32),
+        ("interpolation", ctypes.c_int32), ("ipol_weights", ctypes.c_float * 2), ("pad1", ctypes.c_int32),
     ]
 
 

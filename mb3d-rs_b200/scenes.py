@@ -120,6 +120,19 @@ def preset(name, width=None, height=None):
 PRESETS = ["Integer Power", "Real Power", "Tricorn", "Amazing Box", "Bulbox", "Folding Int Pow"]
 
 
+def interpolated(first, second, weights, width=None, height=None):
+    """An interpolation hybrid (Scene::interpolation): preset `first`'s
+    camera and formula, blended in every iteration with preset `second`'s
+    formula by `weights` (normalised by the library)."""
+    sc = preset(first, width, height)
+    a, b = sc.slots[0], preset(second).slots[0]
+    a, b = (slot(s.formula, 1, *list(s.options)) for s in (a, b))
+    set_slots(sc, [a, b])
+    sc.interpolation = 1
+    sc.ipol_weights[0], sc.ipol_weights[1] = weights
+    return sc
+
+
 def splitmix64(state):
     state = (state + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
     z = state

@@ -334,6 +334,40 @@ static int combine_de_options(const std::vector<Slot> &slots, int end_to) {
     return de_option;
 }
 
+// ipol_de_option (src/calc.rs:255-308): CheckDEoption of the two weighted
+// formulas (a weight counts when its bits as a signed integer are > 0)
+static int ipol_de_option(const std::vector<Slot> &slots, const float raw[2]) {
+    int de_option = -1;
+    for (int x = 0; x < 2 && x < (int)slots.size(); x++) {
+        int32_t bits;
+        std::memcpy(&bits, &raw[x], 4);
+        if (bits <= 0) continue;
+        const int de = slots[x].f.de_option();
+        if (de < 0 || de > 20 || de == de_option) continue;
+        if ((de_option >= 0 && de_option < 20 && de > 19) || (de_option > 19 && de >= 0 && de < 20)) return -1;
+        switch (de_option) {
+            case -1: de_option = de; break;
+            case 2: if (!(de == 2 || de == 5 || de == 6 || de == 11)) de_option = 0; break;
+            case 4: if (!(de == 5 || de == 6)) de_option = 0; break;
+            case 5:
+                if (de == 4) de_option = 4;
+                else if (de == 2 || de == 11) de_option = 2;
+                else if (de != 6) de_option = 0;
+                else de_option = 5;
+                break;
+            case 6: de_option = (de == 2 || de == 4 || de == 5 || de == 11) ? de : 0; break;
+            case 11:
+                if (de == 2 || de == 5) de_option = 2;
+                else if (de != 6) de_option = 0;
+                else de_option = 11;
+                break;
+            default: break;
+        }
+    }
+    if (de_option > 19) de_option = 20;
+    return de_option;
+}
+
 // CalcParams::new (src/calc.rs:375-891), the alternating 3D hybrid without
 // DE combination, interpolation, dIFS, cutting planes, inside rendering,
 // stereo or the ground.
@@ -342,20 +376,39 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     if (sc.width <= 0 || sc.height <= 0) { err = "bad picture size"; return false; }
     int n = sc.n_slots;
     if (n < 1 || n > 6) { err = "n_slots must be 1..6"; return false; }
-    bool any = false;
+    // an interpolation hybrid: the two first formulas with their weights,
+    // normalised to a sum of 1 (src/calc.rs:378-397)
+    const bool ipol = sc.interpolation != 0;
+    float ipw[2] = {1.f, 0.f};
+    if (ipol) {
+        if (n < 2) { err = "an interpolation hybrid needs two formulas"; return false; }
+        float x1 = sc.ipol_weights[0], x2 = sc.ipol_weights[1];
+        float y1 = x1 + x2;
+        if (y1 < 1e-10f) {
+            y1 = 1.0f;
+            x1 = 1.0f;
+            x2 = 0.0f;
+        } else {
+            y1 = 1.0f / y1;
+        }
+        ipw[0] = x1 * y1;
+        ipw[1] = x2 * y1;
+        n = 2;
+    }
+    bool any = ipol;
     for (int i = 0; i < n; i++) any = any || sc.slots[i].iterations != 0;
     if (!any) { err = "no formula with iterations > 0"; return false; }
     std::vector<Slot> slots;
     for (int i = 0; i < n; i++) {
         Slot s;
-        if (sc.slots[i].iterations != 0) {
+        if (sc.slots[i].iterations != 0 || ipol) {
             if (!formula_from_slot(sc.slots[i], s.f, err)) return false;
         } else {
             s.f.kind = F_INTPOW;  // an empty slot (src/m3p.rs:790-792)
             s.f.o[0] = 8; s.f.o[1] = -1;
         }
-        s.iterations = std::abs(sc.slots[i].iterations);
-        s.uncounted = sc.slots[i].iterations < 0;
+        s.iterations = ipol ? 1 : std::abs(sc.slots[i].iterations);
+        s.uncounted = !ipol && sc.slots[i].iterations < 0;
         s.ade = false;
         s.julia_add = sc.julia && s.f.julia_adds();
         slots.push_back(s);
@@ -371,7 +424,12 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
         if (de_option == 2 || de_option == 11) de_option = 0;
         else if (de_option == 5 || de_option == 6) de_option = 4;
     }
-    if (de_option < 0) { err = "formula option is not valid"; return false; }
+    if (de_option < 0 && !ipol) { err = "formula option is not valid"; return false; }
+    if (ipol) {
+        de_option = ipol_de_option(slots, sc.ipol_weights);
+        if (de_option >= 20) { err = "dIFS formulas do not work in an interpolation hybrid"; return false; }
+        if (de_option < 0) { err = "formula option is not valid"; return false; }
+    }
     if (de_option >= 4 && de_option <= 6) { err = "4D hybrids are not supported"; return false; }
     bool is_custom_de = de_option == 2 || de_option == 5 || de_option == 6 || de_option == 11 || de_option == 20;
     for (auto &s : slots) {
@@ -386,14 +444,15 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     for (size_t x = 0; x < slots.size(); x++) {
         const Slot &s = slots[x];
         if (s.iterations == 0) continue;
-        if (!s.uncounted) {
+        if (ipol || !s.uncounted) {
             double sip = s.f.si_pow();
             double z1 = sip > 1.0 ? sip : s.f.first_option();
             fhln[x] = (float)(1.0 / std::log(rmax(2.0, std::fabs(z1))));
         }
-        double z1 = (double)s.iterations, cnt = (double)s.iterations;
+        // (an interpolation hybrid: weighted by the weights, counted once)
+        double z1 = ipol ? (double)ipw[x] : (double)s.iterations, cnt = ipol ? 1.0 : (double)s.iterations;
         int j = s.f.de_option();
-        if (is_custom_de && !s.uncounted && (j == 5 || j == 11)) {
+        if (is_custom_de && (ipol || !s.uncounted) && (j == 5 || j == 11)) {
             nn += cnt;
             ii += cnt;
             double x2 = s.f.first_option();
@@ -401,14 +460,14 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
             if (x2 < 0.0) x1 += 0.65 * z1;
             else x1 += (x2 * 1.2 + 1.0) / x2 * z1;
             y1 += std::fabs(x2) * z1;
-        } else if (j >= 0) {
+        } else if (j >= 0 || ipol) {
             nn += cnt;
             x1 += (is_custom_de ? s.f.ade_scale() : s.f.de_scale()) * z1;
         }
     }
     float d_col_plus = 0.f;
     double d_de_scale = 1.0;
-    if (nn > 0.0 && de_option != 20) d_de_scale = x1 / nn;
+    if (nn > 0.0 && de_option != 20) d_de_scale = ipol ? x1 : x1 / nn;
     if (nn > 0.0 && ii > 0.0) d_col_plus = (float)(std::pow(std::fabs(y1 / ii), 0.25) * 40.0 - 49.0);
     // mctColVarDEstopMul (src/calc.rs:591-652)
     float col_var = 0.6f;
@@ -417,7 +476,7 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
         int ia = 0, itmp = 0;
         for (size_t x = 0; x < slots.size(); x++) {
             const Slot &s = slots[x];
-            bool counted = s.iterations > 0 && !s.uncounted;
+            bool counted = ipol || (s.iterations > 0 && !s.uncounted);
             if (!counted) {
                 if (s.iterations > 0) {
                     if ((int)x > end_to) ia++;
@@ -425,7 +484,7 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
                 }
                 continue;
             }
-            double x2 = (double)s.iterations;
+            double x2 = ipol ? (double)ipw[x] : (double)s.iterations;
             int de = s.f.de_option();
             if (de == 0 || de == 4) {
                 yy1 += x2 * 0.6;
@@ -543,6 +602,9 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     for (int k = 0; k < 6; k++) p.fhln[k] = fhln[k];
     p.end_to = end_to;
     p.repeat_from = repeat_from;
+    p.ipol = ipol;
+    p.ipol_w[0] = ipw[0];
+    p.ipol_w[1] = ipw[1];
     return true;
 }
 
@@ -598,19 +660,75 @@ int Iteration::run(const std::vector<Slot> &slots) {
     }
 }
 
-// doHybridPas (src/iteration.rs:521-535)
+// run_ipol (src/iteration.rs:347-401), 3D: both formulas on the same
+// vector, the results and their lengths blended with the weights; `de`
+// blends the running derivative (w) of the analytic-DE variant
+void Iteration::run_ipol(const std::vector<Slot> &slots, bool de) {
+    const double s1 = (double)ipol_w[0], s2 = (double)ipol_w[1];
+    it_result = 0;
+    for (;;) {
+        rold = rout;
+        const double y1[4] = {v[0], v[1], v[2], v[3]};
+        slots[0].f.iterate(v, j, rout, slots[0].ade);
+        if (slots[0].julia_add)
+            for (int k = 0; k < 3; k++) v[k] += j[k];
+        const double x1[4] = {v[0], v[1], v[2], v[3]};
+        for (int k = 0; k < 4; k++) v[k] = y1[k];
+        slots[1].f.iterate(v, j, rout, slots[1].ade);
+        if (slots[1].julia_add)
+            for (int k = 0; k < 3; k++) v[k] += j[k];
+        const double x = v[0], y = v[1], z = v[2], w = v[3];
+        double xx = std::sqrt(x1[0] * x1[0] + x1[1] * x1[1] + x1[2] * x1[2]);
+        const double yy0 = std::sqrt(x * x + y * y + z * z);
+        xx = xx * s1 + yy0 * s2;
+        double nv[4] = {x1[0] * s1 + x * s2, x1[1] * s1 + y * s2, x1[2] * s1 + z * s2, x1[3] * s1 + w * s2};
+        if (de) nv[3] = std::fabs(x1[3]) * s1 + std::fabs(w) * s2;
+        const double l2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
+        const double yy = xx / std::sqrt(l2 + 1e-40);
+        nv[0] *= yy;
+        nv[1] *= yy;
+        nv[2] *= yy;
+        for (int k = 0; k < 4; k++) v[k] = nv[k];
+        it_result += 1;
+        rout = xx * xx;
+        if (rout < otrap) otrap = rout;
+        if (it_result >= max_it || rout > rstop) break;
+    }
+}
+
+// doHybridPas (src/iteration.rs:521-535); an interpolation hybrid:
+// doInterpolHybridPas (src/iteration.rs:403-439)
 void Iteration::hybrid_3d(const std::vector<Slot> &slots) {
     if (do_julia) { j[0] = ju[0]; j[1] = ju[1]; j[2] = ju[2]; }
     else { j[0] = c[0]; j[1] = c[1]; j[2] = c[2]; }
     v[0] = c[0]; v[1] = c[1]; v[2] = c[2]; v[3] = 0.0;
     rout = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
     otrap = rout;
+    if (ipol) {
+        run_ipol(slots, false);
+        if (calc_sit) smooth_iterations(0);
+        return;
+    }
     int n = run(slots);
     if (calc_sit) smooth_iterations(n);
 }
 
-// doHybridPasDE (src/iteration.rs:539-574)
+// doHybridPasDE (src/iteration.rs:539-574); an interpolation hybrid:
+// doInterpolHybridPasDE (src/iteration.rs:441-455)
 double Iteration::hybrid_3d_de(const std::vector<Slot> &slots) {
+    if (ipol) {
+        if (do_julia) { j[0] = ju[0]; j[1] = ju[1]; j[2] = ju[2]; }
+        else { j[0] = c[0]; j[1] = c[1]; j[2] = c[2]; }
+        v[0] = c[0]; v[1] = c[1]; v[2] = c[2];
+        rout = c[0] * c[0] + c[1] * c[1] + c[2] * c[2];
+        otrap = rout;
+        v[3] = (de_option & 0x18) == 16 ? rout : 1.0;
+        run_ipol(slots, true);
+        const double w = v[3];
+        const double r = (de_option & 7) == 4 ? std::fabs(v[2]) * std::log(std::fabs(v[2])) / w : std::sqrt(rout) / std::fabs(w);
+        if (calc_sit) smooth_iterations(0);
+        return r;
+    }
     if (do_julia) { j[0] = ju[0]; j[1] = ju[1]; j[2] = ju[2]; }
     else { j[0] = c[0]; j[1] = c[1]; j[2] = c[2]; }
     v[0] = c[0]; v[1] = c[1]; v[2] = c[2];
@@ -658,6 +776,9 @@ Marcher::Marcher(const Params *pp, int32_t s) : p(pp), seed(s) {
     it.end_to = p->end_to;
     it.repeat_from = p->repeat_from;
     for (int k = 0; k < 6; k++) it.fhln[k] = p->fhln[k];
+    it.ipol = p->ipol;
+    it.ipol_w[0] = p->ipol_w[0];
+    it.ipol_w[1] = p->ipol_w[1];
     ms_de_stop = p->de_stop;
     max_its_result = p->max_it;
 }

@@ -177,6 +177,8 @@ struct Params {
     float ms_de_sub = 0;
     float fhln[6];
     int end_to = 0, repeat_from = 0;
+    bool ipol = false;              // an interpolation hybrid (HybridMode::Ipol3D)
+    float ipol_w[2] = {1.f, 0.f};   // its normalised weights
 };
 
 bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err);
@@ -194,8 +196,11 @@ struct Iteration {
     int de_option = 0;
     int end_to = 0, repeat_from = 0;
     float fhln[6];
+    bool ipol = false;
+    float ipol_w[2] = {1.f, 0.f};
     void smooth_iterations(int n);
     int run(const std::vector<Slot> &slots);
+    void run_ipol(const std::vector<Slot> &slots, bool de);
     void hybrid_3d(const std::vector<Slot> &slots);
     double hybrid_3d_de(const std::vector<Slot> &slots);
 };

@@ -55,6 +55,52 @@ def test_fp64_march_matches_oracle(card, name):
     assert r.get("depth_rel_p99", 0.0) < 1e-6, r
 
 
+def _ipol_scenes():
+    a = scenes.interpolated("Integer Power", "Tricorn", (0.7, 0.3), 160, 120)
+    b = scenes.interpolated("Amazing Box", "Amazing Box", (0.5, 0.5), 160, 120)
+    b.slots[1].options[0] = 2.5  # (two boxes: the analytic DE's blend)
+    c = scenes.interpolated("Integer Power", "Folding Int Pow", (0.5, 0.5), 160, 120)
+    return [("ip8+tricorn", a), ("box+box", b), ("ip8+fip", c)]
+
+
+def test_interpolation_hybrid_matches_oracle(card):
+    """Interpolation hybrids (doInterpolHybridPas[DE], src/iteration.rs:347-
+    455): the numerical DE's blend (Integer Power with Tricorn, with Folding
+    Int Pow) and the analytic one's (two Amazing Boxes), the FP64 march
+    against the oracle with the same bounds as the single formulas; the
+    mixed mode marches them in FP64 (the precision rule sends every pixel
+    there) and gives the same records; the DE probe at points."""
+    for name, sc in _ipol_scenes():
+        ref = O.march(sc, mb3dcu.SILIGHT)
+        g = card.march(sc, mb3dcu.FP64)
+        r = compare(g, ref, *zc(sc))
+        assert r["hit_agree"] >= 0.999 and r["exact"] >= 0.95, (name, r)
+        assert r.get("depth_rel_p99", 0.0) < 1e-6, (name, r)
+        gm = card.march(sc, mb3dcu.FP32_FP64)
+        assert card.stats()["fp64_pixels"] == sc.width * sc.height
+        assert gm.tobytes() == g.tobytes(), name
+        pts = np.array([[0.3, 0.2, -2.0], [0.7, -0.4, 0.5], [0.1, 0.9, -0.3], [1.2, -0.2, 0.4]])
+        d0, i0 = O.de_at(sc, pts)
+        d1, i1 = card.de_probe(sc, pts, mb3dcu.FP64)
+        assert np.array_equal(i0, i1), (name, i0, i1)
+        assert np.all(np.abs(d1 - d0) <= 1e-6 * np.maximum(np.abs(d0), 1e-3)), (name, d0, d1)
+
+
+def test_interpolation_hybrid_shadows_and_ao(card):
+    """The post passes on an interpolation hybrid (their DEs blend too): hard
+    shadows and DE AO of the card's FP64 render against the oracle's passes
+    on the oracle's G-buffer."""
+    name, sc = _ipol_scenes()[0]
+    sc.shadow_lights, sc.deao_quality = 1, 1
+    ref = O.deao(sc, O.shadows(sc, O.march(sc, mb3dcu.SILIGHT), per_pixel=True))
+    g = card.render(sc, mb3dcu.FP64)
+    obj = ~mb3dcu.is_background(ref) & ~mb3dcu.is_background(g)
+    assert obj.mean() > 0.1
+    sh = (g["shadow"][obj] >> 10) == (ref["shadow"][obj] >> 10)
+    da = np.abs(g["amb_shadow"][obj].astype(np.int64) - ref["amb_shadow"][obj].astype(np.int64))
+    assert sh.mean() >= 0.98 and (da <= 16).mean() >= 0.97, (sh.mean(), (da <= 16).mean())
+
+
 def test_menger_hybrid_fp64_and_mixed(card):
     sc = scenes.scaled(scenes.c4_frames(8)[0], 160, 90)
     ref = O.march(sc, mb3dcu.SILIGHT)

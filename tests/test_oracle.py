@@ -571,3 +571,32 @@ def test_ssao15_variants_and_background():
     # pictures below 4 x 4 stay as they are
     small = _depth_gbuf(3, 3, np.full((3, 3), 4_000_000))
     assert O.ssao15(small, 3, 3, 300.0, 0.001).tobytes() == small.tobytes()
+
+
+# ---- the interpolation hybrid, the reference's own test restated
+# (tests/render.rs:179-214, interpolation_hybrid_blends_two_formulas)
+
+def test_interpolation_hybrid_blends_two_formulas():
+    """Weights 1 : 0 give the first formula alone, for the gradient DE
+    (Integer Power) and the analytic one (Amazing Box): the same iteration
+    counts and DEs within 1e-9; a real blend is finite and renders."""
+    for a, b in (("Integer Power", "Real Power"), ("Amazing Box", "Integer Power")):
+        single = scenes.preset(a, 96, 72)
+        ip = scenes.interpolated(a, b, (2.0, 0.0), 96, 72)
+        pos = np.array([[0.3, 0.2, -2.0], [0.7, -0.4, 0.5], [0.0, 1.5, -6.0]])
+        d1, i1 = O.de_at(single, pos)
+        d2, i2 = O.de_at(ip, pos)
+        assert np.array_equal(i1, i2), (a, i1, i2)
+        assert np.all(np.abs(d1 - d2) <= 1e-9 * np.maximum(np.abs(d1), 1e-3)), (a, d1, d2)
+        blend = scenes.interpolated(a, b, (0.5, 0.5), 96, 72)
+        d3, _ = O.de_at(blend, pos[1:2])
+        assert np.isfinite(d3).all()
+        g = O.march(blend, mb3dcu.SILIGHT)
+        assert (~mb3dcu.is_background(g)).mean() > 0.01, a
+
+
+def test_interpolation_needs_two_formulas_and_valid_options():
+    ip = scenes.interpolated("Integer Power", "Amazing Box", (0.6, 0.4), 32, 24)
+    ip.n_slots = 1
+    with pytest.raises(RuntimeError):
+        O.march(ip, mb3dcu.SILIGHT)
