@@ -50,6 +50,7 @@ extern "C" {
  * as a custom .m3f formula and this library has built in. ---- */
 #define MB3D_CU_F_INTPOW 0        /* Integer Power: options power(2..8), z_mul */
 #define MB3D_CU_F_REALPOWER 1     /* Real Power: power, z_mul */
+#define MB3D_CU_F_QUATERNION 2    /* Quaternion (4D): yw_mul, w_add */
 #define MB3D_CU_F_TRICORN 3       /* Tricorn: z_mul, cz_mul */
 #define MB3D_CU_F_AMAZINGBOX 4    /* Amazing Box: scale, min_r, fold */
 #define MB3D_CU_F_BULBOX 5        /* Bulbox: scale, min_r, fold, bulb_scale, r_thr, r_thr2 */
@@ -125,6 +126,9 @@ typedef struct mb3d_cu_scene {
     int32_t interpolation;
     float ipol_weights[2];
     int32_t pad1;
+    /* the 4D rotation of a 4D hybrid (Scene::rot_4d, src/scene.rs:459): the
+     * XW, YW and ZW plane angles in radians (BuildSMatrix4) */
+    double rot_4d[3];
 } mb3d_cu_scene;
 
 /* The G-buffer record SiLight (src/gbuffer.rs:5-20), 20 bytes; mb3d-rs's

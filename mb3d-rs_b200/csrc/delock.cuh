@@ -22,6 +22,7 @@
 #pragma once
 #include "devparams.h"
 #include "formulas.cuh"
+#include "marcher64.cuh"
 
 namespace mb3dcu {
 
@@ -145,82 +146,67 @@ __device__ __forceinline__ float smooth_of(const DevParams &p, R rout, R rold, c
     }
 }
 
-// The interpolation hybrid's DE (calc_de of HybridMode::Ipol3D,
-// src/calc.rs:1495-1557 with doInterpolHybridPas[DE]): in double precision
-// only, one orbit at a time -- the centre, then for the numerical DE the
-// three offset points with the centre's count as their limit and RStop3D as
-// the bailout, as the reference runs them; the single precision form hands
-// the point to double precision (need64).  Kept out of line: it is no part
-// of the ordinary hybrids' loop.
-template <typename R, int FM, bool COUNT, bool FULL, typename P>
-__device__ __noinline__ DEr de_ipol(const DevParams &p, const P c[3], float ms_de_stop, DECount *cnt, DEstate *st,
-                                    bool calc_sit, int max_add) {
+// The DE of the hybrids the lock-step loop does not carry -- interpolation
+// hybrids, 4D hybrids, any hybrid with a Quaternion (its j has four
+// components) -- in double precision, one orbit at a time on the
+// sequential FP64 iteration record: calc_de_part (src/calc.rs:1495-1557)
+// with mand_function / mand_function_de of the scene's mode, the numerical
+// DE's three offset points limited by the centre's count and bailing out at
+// RStop3D, as the reference runs them.  Kept out of line: it is no part of
+// the ordinary hybrids' loop.
+template <int FM, bool FULL, typename P>
+__device__ __noinline__ DEr de_seq(const DevParams &p, const P c[3], float ms_de_stop, DEstate *st, bool calc_sit,
+                                   int max_add) {
     DEr out;
     out.need64 = false;
     out.overflow = false;
-    out.de = 0.0;
-    out.it = 0;
-    if constexpr (sizeof(R) == 4) {
-        out.need64 = true;
+    It64<FM> it;
+    for (int k = 0; k < 3; k++) it.c[k] = (double)c[k];
+    for (int k = 0; k < 4; k++) it.v[k] = 0.0;
+    it.rout = it.rold = it.otrap = 0.0;
+    it.it_result = 0;
+    it.max_it = p.max_it + max_add;
+    it.rstop = p.d_rstop;
+    it.calc_sit = FULL && calc_sit;
+    it.smooth_it = 0.f;
+    if (p.is_custom_de) {
+        out.de = it.hybrid_3d_de(p) * (double)p.d_de_scale;
+        out.it = it.it_result;
+        if (FULL) {
+            st->rout = it.rout;
+            st->rold = it.rold;
+            st->otrap = it.otrap;
+            st->v[0] = it.v[0]; st->v[1] = it.v[1]; st->v[2] = it.v[2];
+            st->smooth_it = it.smooth_it;
+        }
     } else {
-        const int max_it = p.max_it + max_add;
-        auto start = [&](const double cc[3], double v[4], double j[3], double &rout) {
-            for (int k = 0; k < 3; k++) {
-                v[k] = cc[k];
-                j[k] = p.do_julia ? p.ju[k] : cc[k];
-            }
-            rout = cc[0] * cc[0] + cc[1] * cc[1] + cc[2] * cc[2];
-        };
-        const double cd[3] = {(double)c[0], (double)c[1], (double)c[2]};
-        double v[4], j[3], rout, rold = 0.0, otrap;
-        start(cd, v, j, rout);
-        otrap = rout;
-        if (p.is_custom_de) {
-            v[3] = ((p.de_option & 0x18) == 16) ? rout : 1.0;
-            const int it = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, p.d_rstop, true);
-            if (FULL) {
-                st->rout = rout;
-                st->rold = rold;
-                st->otrap = otrap;
-                st->v[0] = v[0]; st->v[1] = v[1]; st->v[2] = v[2];
-                st->smooth_it = calc_sit ? smooth_of<double>(p, rout, rold, v, it, 0) : 0.f;
-            }
-            const double w = v[3];
-            const double r = ((p.de_option & 7) == 4) ? fabs(v[2]) * log(fabs(v[2])) / w : sqrt(rout) / fabs(w);
-            out.de = r * (double)p.d_de_scale;
-            out.it = it;
-            if (COUNT) cnt->its[0] += it, cnt->its[1] += it;
+        it.hybrid_3d(p);
+        const double R0 = it.rout;
+        const int it0 = it.it_result;
+        const float sit = it.smooth_it;
+        if (R0 < 1e-200) {
+            out.de = 0.0;
         } else {
-            v[3] = 0.0;
-            const int it = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, p.d_rstop, false);
-            const double R0 = rout;
-            float sit = 0.f;
-            if (FULL && calc_sit) sit = smooth_of<double>(p, rout, rold, v, it, 0);
-            if (COUNT) cnt->its[0] += it, cnt->its[1] += it;
-            if (R0 < 1e-200) {
-                out.de = 0.0;
-            } else {
-                double g = 0.0;
-                for (int k = 0; k < 3; k++) {
-                    double cc[3] = {cd[0], cd[1], cd[2]};
-                    cc[k] += (double)p.de_offset;
-                    start(cc, v, j, rout);
-                    otrap = rout;
-                    v[3] = 0.0;
-                    const int ik = ipol_run<double, FM>(p, v, j, rout, rold, otrap, it, p.rstop3d, false);
-                    if (COUNT) cnt->its[0] += ik, cnt->its[1] += ik;
-                    g += (R0 - rout) * (R0 - rout);
-                }
-                out.de = R0 * log(R0) * (double)p.d_de_scale / (sqrt(g) + (double)p.de_offset006);
+            it.calc_sit = false;
+            it.max_it = it0;
+            it.rstop = p.rstop3d;
+            double g = 0.0;
+            for (int k = 0; k < 3; k++) {
+                const double b = it.c[k];
+                it.c[k] = b + (double)p.de_offset;
+                it.hybrid_3d(p);
+                g += (R0 - it.rout) * (R0 - it.rout);
+                it.c[k] = b;
             }
-            if (FULL) {
-                st->rout = R0;
-                st->rold = rold;
-                st->otrap = otrap;
-                st->v[0] = v[0]; st->v[1] = v[1]; st->v[2] = v[2];
-                st->smooth_it = sit;
-            }
-            out.it = it;
+            out.de = R0 * log(R0) * (double)p.d_de_scale / (sqrt(g) + (double)p.de_offset006);
+        }
+        out.it = it0;
+        if (FULL) {
+            st->rout = R0;
+            st->rold = it.rold;
+            st->otrap = it.otrap;
+            st->v[0] = it.v[0]; st->v[1] = it.v[1]; st->v[2] = it.v[2];
+            st->smooth_it = sit;
         }
     }
     const double mn = (double)ms_de_stop * 0.25;
@@ -236,10 +222,10 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const P c[3], float m
                                        DEstate *st = nullptr, bool calc_sit = false, int max_add = 0) {
     static_assert(sizeof(P) == 8 || sizeof(R) == 4, "a single precision position needs the single precision DE");
     if (COUNT) cnt->evals++;
-    // (an interpolation hybrid runs in double precision only: its scenes are
-    // all-FP64, so the single precision kernels never see one)
+    // (those hybrids run in double precision only: their scenes are all-FP64,
+    // so the single precision kernels never see one)
     if constexpr (sizeof(R) == 8) {
-        if (p.ipol) return de_ipol<R, FM, COUNT, FULL, P>(p, c, ms_de_stop, cnt, st, calc_sit, max_add);
+        if (p.seq_de) return de_seq<FM, FULL, P>(p, c, ms_de_stop, st, calc_sit, max_add);
     }
     DEr out;
     out.need64 = false;

@@ -67,6 +67,13 @@ struct DevParams {
     // formulas blended in every iteration with the normalised weights
     int32_t ipol, pad_ipol;
     float ipol_w[2];
+    // a 4D hybrid (HybridMode::Alt4D, the 4D numerical DE) and its rotation
+    // (BuildSMatrix4, single precision values)
+    int32_t four_d;
+    // the DE runs on the sequential FP64 record (de_seq): interpolation and
+    // 4D hybrids and hybrids with a Quaternion
+    int32_t seq_de;
+    double smatrix4[4][4];
 };
 
 // slot orders the single precision DE loop knows at compile time

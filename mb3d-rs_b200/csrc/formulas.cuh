@@ -209,9 +209,13 @@ __device__ __forceinline__ void f_menger(R s, R cx, R cy, R cz, R v[4], bool ade
 #define FKIND_BULBOX 64
 #define FKIND_FIP 128
 #define FKIND_ALL 255
+#define FKIND_QUAT 256  // (only in the all-formula kernels' switch: a 4-component j)
 
-template <typename R, int FM = FKIND_ALL>
-__device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], const R j[3], R rout) {
+// J4: j has four components (the sequential FP64 iteration's record); only
+// then is the Quaternion (4D, it reads j's fourth) on the switch -- the
+// lock-step DE's j has three, and scenes with a Quaternion never reach it
+template <typename R, int FM = FKIND_ALL, bool J4 = false>
+__device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], const R *j, R rout) {
     const bool ade = s.ade != 0;
     if (FM == FKIND_IP8) {
         f_int_pow<R>(8, Num<R>::opt(s, 1), v, j);
@@ -239,6 +243,15 @@ __device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], const 
             f_menger<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), Num<R>::opt(s, 2), Num<R>::opt(s, 3), v, ade);
             break;
         case MB3D_CU_F_REALPOWER: f_real_power<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), v, j, rout); break;
+        case MB3D_CU_F_QUATERNION:  // src/formulas.rs:580-586
+            if constexpr (J4) {
+                const R x = v[0], y = v[1], z = v[2], w = v[3];
+                v[0] = x * x - y * y - z * z - w * w + j[0];
+                v[1] = R(2) * (y * x + z * w) + j[1];
+                v[2] = R(2) * (z * x + Num<R>::opt(s, 0) * y * w) + j[2];
+                v[3] = R(2) * (w * x + y * z) + Num<R>::opt(s, 1) + j[3];
+            }
+            break;
         case MB3D_CU_F_TRICORN: {
             R x = v[0], y = v[1], z = v[2];
             v[2] = z * x * Num<R>::opt(s, 0) + j[2] * Num<R>::opt(s, 1);
@@ -358,7 +371,7 @@ __device__ __forceinline__ void f_amazing_box_x2(float scale, float min_r, float
 // blended length; `de` blends the running derivative (w) of the analytic-DE
 // variant.  Every iteration counts; returns the count.
 template <typename R, int FM>
-__device__ __forceinline__ int ipol_run(const DevParams &p, R v[4], R j[3], R &rout, R &rold, R &otrap, int max_it,
+__device__ __forceinline__ int ipol_run(const DevParams &p, R v[4], R j[4], R &rout, R &rold, R &otrap, int max_it,
                                         R rstop, bool de) {
     const R s1 = (R)p.ipol_w[0], s2 = (R)p.ipol_w[1];
     const DevSlot &a = p.slots[0], &b = p.slots[1];
@@ -366,7 +379,7 @@ __device__ __forceinline__ int ipol_run(const DevParams &p, R v[4], R j[3], R &r
     for (int guard = 0; guard < (1 << 20); guard++) {
         rold = rout;
         const R y1[4] = {v[0], v[1], v[2], v[3]};
-        formula_iterate<R, FM>(a, v, j, rout);
+        formula_iterate<R, FM, true>(a, v, j, rout);
         if (a.julia_add) {
             v[0] += j[0];
             v[1] += j[1];
@@ -377,7 +390,7 @@ __device__ __forceinline__ int ipol_run(const DevParams &p, R v[4], R j[3], R &r
         v[1] = y1[1];
         v[2] = y1[2];
         v[3] = y1[3];
-        formula_iterate<R, FM>(b, v, j, rout);
+        formula_iterate<R, FM, true>(b, v, j, rout);
         if (b.julia_add) {
             v[0] += j[0];
             v[1] += j[1];

@@ -18,7 +18,9 @@ static inline double deg2rad(double d) { return d * (kPi / 180.0); }
 
 // Formula meta data (src/formulas.rs:492-569); the Menger IFS has its .m3f
 // header's values (.DEoption 2, .DEscale 0.2, .RStop 1024).
-static int f_de_option(int f) { return f == MB3D_CU_F_AMAZINGBOX ? 11 : f == MB3D_CU_F_MENGERIFS ? 2 : 0; }
+static int f_de_option(int f) {
+    return f == MB3D_CU_F_AMAZINGBOX ? 11 : f == MB3D_CU_F_MENGERIFS ? 2 : f == MB3D_CU_F_QUATERNION ? 4 : 0;
+}
 static double f_de_scale(int f) {
     if (f == MB3D_CU_F_AMAZINGBOX || f == MB3D_CU_F_BULBOX || f == MB3D_CU_F_MENGERIFS) return 0.2;
     if (f == MB3D_CU_F_FOLDINGINTPOW) return 0.5;
@@ -46,7 +48,8 @@ static bool f_first_is_zmul(int f) { return f == MB3D_CU_F_INTPOW || f == MB3D_C
 static double f_first_option(const mb3d_cu_slot &s) { return f_first_is_zmul(s.formula) ? s.options[1] : s.options[0]; }
 static bool f_known(int f) {
     return f == MB3D_CU_F_INTPOW || f == MB3D_CU_F_REALPOWER || f == MB3D_CU_F_TRICORN || f == MB3D_CU_F_AMAZINGBOX ||
-           f == MB3D_CU_F_BULBOX || f == MB3D_CU_F_FOLDINGINTPOW || f == MB3D_CU_F_MENGERIFS;
+           f == MB3D_CU_F_BULBOX || f == MB3D_CU_F_FOLDINGINTPOW || f == MB3D_CU_F_MENGERIFS ||
+           f == MB3D_CU_F_QUATERNION;
 }
 
 // CheckFormulaOptions (src/calc.rs:315-372)
@@ -64,6 +67,34 @@ static int de_option_of(const int *des, const int *its, int n) {
         else if (opt == 11) opt = (de == 2 || de == 5) ? 2 : (de != 6 ? 0 : 11);
     }
     return opt;
+}
+
+// BuildSMatrix4 (src/math.rs:176-206): the 4D rotation from the XW, YW and
+// ZW plane angles, each element rounded to single precision
+static void build_smatrix4(double xw, double yw, double zw, double out[4][4]) {
+    auto ini = [](double m[4][4]) {
+        for (int i = 0; i < 4; i++)
+            for (int k = 0; k < 4; k++) m[i][k] = i == k ? 1.0 : 0.0;
+    };
+    auto mul = [](const double a[4][4], const double b[4][4], double r[4][4]) {
+        for (int i = 0; i < 4; i++)
+            for (int k = 0; k < 4; k++) {
+                double acc = 0.0;
+                for (int q = 0; q < 4; q++) acc += a[i][q] * b[q][k];
+                r[i][k] = acc;
+            }
+    };
+    double m1[4][4], m2[4][4], m3[4][4], t[4][4];
+    ini(m1);
+    m1[0][0] = std::cos(xw); m1[3][3] = std::cos(xw); m1[0][3] = -std::sin(xw); m1[3][0] = std::sin(xw);
+    ini(m2);
+    m2[1][1] = std::cos(yw); m2[3][3] = std::cos(yw); m2[1][3] = -std::sin(yw); m2[3][1] = std::sin(yw);
+    mul(m2, m1, t);
+    ini(m3);
+    m3[2][2] = std::cos(zw); m3[3][3] = std::cos(zw); m3[2][3] = -std::sin(zw); m3[3][2] = std::sin(zw);
+    mul(m3, t, out);
+    for (int i = 0; i < 4; i++)
+        for (int k = 0; k < 4; k++) out[i][k] = (double)(float)out[i][k];
 }
 
 // ipol_de_option (src/calc.rs:255-308): CheckDEoption of the two weighted
@@ -180,8 +211,11 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
         err = "formula option is not valid";
         return MB3D_CU_EINVAL;
     }
-    if (de_option >= 4 && de_option <= 6) {
-        err = "4D hybrids are not built into this backend";
+    // a 4D hybrid (HybridMode::Alt4D) with the 4D numerical DE (option 4);
+    // the analytic 4D DE (options 5, 6) and 4D interpolation are not built
+    const bool four_d = de_option >= 4 && de_option <= 6;
+    if (four_d && (de_option != 4 || ipol)) {
+        err = "4D hybrids with the analytic DE or interpolated are not built into this backend";
         return MB3D_CU_ENOTSUP;
     }
     bool custom = de_option == 2 || de_option == 5 || de_option == 6 || de_option == 11 || de_option == 20;
@@ -350,6 +384,7 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
             case MB3D_CU_F_REALPOWER: d.kind = 16; break;
             case MB3D_CU_F_TRICORN: d.kind = 32; break;
             case MB3D_CU_F_BULBOX: d.kind = 64; break;
+            case MB3D_CU_F_QUATERNION: d.kind = 256; break;
             default: d.kind = 128; break;
         }
         if (its[i] > 0) p.fmask |= d.kind;
@@ -379,7 +414,12 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     p.ipol = ipol ? 1 : 0;
     p.ipol_w[0] = ipw[0];
     p.ipol_w[1] = ipw[1];
-    if (ipol) {
+    p.four_d = four_d ? 1 : 0;
+    build_smatrix4(sc.rot_4d[0], sc.rot_4d[1], sc.rot_4d[2], p.smatrix4);
+    bool quat = false;
+    for (int i = 0; i < nsl; i++) quat = quat || (fs[i] == MB3D_CU_F_QUATERNION && its[i] > 0);
+    p.seq_de = (ipol || four_d || quat) ? 1 : 0;
+    if (p.seq_de) {
         p.all_fp64 = 1;
         p.sched = SCHED_GENERIC;
     }

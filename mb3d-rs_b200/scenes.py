@@ -10,7 +10,7 @@ import math
 import numpy as np
 
 from mb3dcu import Scene, Slot, Light, F_INTPOW, F_AMAZINGBOX, F_MENGERIFS, F_REALPOWER, F_TRICORN, F_BULBOX, \
-    F_FOLDINGINTPOW
+    F_FOLDINGINTPOW, F_QUATERNION
 
 PI = math.pi
 
@@ -107,6 +107,11 @@ def preset(name, width=None, height=None):
         f, zs, zoom, its, rot = slot(F_TRICORN, 1, -2.0, 1.0), -3.0, 0.6, 12, (0.6, 0.2)
     elif n == "real power":
         f, zs, zoom, its, rot = slot(F_REALPOWER, 1, 8.0, -1.0), -2.5, 0.8, 12, (-0.55, 0.45)
+    elif n == "quaternion":
+        f, zs, zoom, its, rot = slot(F_QUATERNION, 1, -1.0, 0.0), -3.0, 0.8, 12, (0.4, 0.3)
+        sc.julia = 1
+        for k, v in enumerate((-0.2, 0.6, 0.2, 0.0)):
+            sc.julia_c[k] = v
     else:  # Integer Power
         f, zs, zoom, its, rot = intpow(), -2.5, 0.8, 12, (-0.55, 0.45)
     sc.z_start, sc.zoom, sc.iterations = zs, zoom, its
@@ -117,7 +122,7 @@ def preset(name, width=None, height=None):
     return sc
 
 
-PRESETS = ["Integer Power", "Real Power", "Tricorn", "Amazing Box", "Bulbox", "Folding Int Pow"]
+PRESETS = ["Integer Power", "Real Power", "Quaternion", "Tricorn", "Amazing Box", "Bulbox", "Folding Int Pow"]
 
 
 def interpolated(first, second, weights, width=None, height=None):

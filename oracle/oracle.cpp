@@ -55,6 +55,7 @@ int Formula::power() const {
 int Formula::de_option() const {
     switch (kind) {
         case F_AMAZINGBOX: return 11;
+        case F_QUATERNION: return 4;  // the 4D numerical DE
         case F_MENGER: return 2;  // the .m3f header's .DEoption = 2
         default: return 0;
     }
@@ -246,6 +247,14 @@ void Formula::iterate(double v[4], double j[4], double rout, bool ade) const {
     switch (kind) {
         case F_INTPOW: int_pow(power(), o[1], v, j); break;
         case F_REALPOWER: real_power(o[0], o[1], v, j, rout); break;
+        case F_QUATERNION: {
+            const double x = v[0], y = v[1], z = v[2], w = v[3];
+            v[0] = x * x - y * y - z * z - w * w + j[0];
+            v[1] = 2.0 * (y * x + z * w) + j[1];
+            v[2] = 2.0 * (z * x + o[0] * y * w) + j[2];
+            v[3] = 2.0 * (w * x + y * z) + o[1] + j[3];
+            break;
+        }
         case F_TRICORN: {
             double x = v[0], y = v[1], z = v[2];
             v[2] = z * x * o[0] + j[2] * o[1];
@@ -292,8 +301,8 @@ void Formula::iterate(double v[4], double j[4], double rout, bool ade) const {
 
 bool formula_from_slot(const mb3d_cu_slot &s, Formula &f, std::string &err) {
     switch (s.formula) {
-        case F_INTPOW: case F_REALPOWER: case F_TRICORN: case F_AMAZINGBOX: case F_BULBOX: case F_FOLDINGINTPOW:
-        case F_MENGER:
+        case F_INTPOW: case F_REALPOWER: case F_QUATERNION: case F_TRICORN: case F_AMAZINGBOX: case F_BULBOX:
+        case F_FOLDINGINTPOW: case F_MENGER:
             f.kind = s.formula;
             for (int k = 0; k < 16; k++) f.o[k] = s.options[k];
             return true;
@@ -332,6 +341,34 @@ static int combine_de_options(const std::vector<Slot> &slots, int end_to) {
         }
     }
     return de_option;
+}
+
+// BuildSMatrix4 (src/math.rs:176-206): the 4D rotation from the XW, YW and
+// ZW plane angles, each element rounded to single precision
+static void build_smatrix4(double xw, double yw, double zw, double out[4][4]) {
+    auto ini = [](double m[4][4]) {
+        for (int i = 0; i < 4; i++)
+            for (int k = 0; k < 4; k++) m[i][k] = i == k ? 1.0 : 0.0;
+    };
+    auto mul = [](const double a[4][4], const double b[4][4], double r[4][4]) {
+        for (int i = 0; i < 4; i++)
+            for (int k = 0; k < 4; k++) {
+                double s = 0.0;
+                for (int q = 0; q < 4; q++) s += a[i][q] * b[q][k];
+                r[i][k] = s;
+            }
+    };
+    double m[4][4], m2[4][4], m3[4][4], t[4][4];
+    ini(m);
+    m[0][0] = std::cos(xw); m[3][3] = std::cos(xw); m[0][3] = -std::sin(xw); m[3][0] = std::sin(xw);
+    ini(m2);
+    m2[1][1] = std::cos(yw); m2[3][3] = std::cos(yw); m2[1][3] = -std::sin(yw); m2[3][1] = std::sin(yw);
+    mul(m2, m, t);
+    ini(m3);
+    m3[2][2] = std::cos(zw); m3[3][3] = std::cos(zw); m3[2][3] = -std::sin(zw); m3[3][2] = std::sin(zw);
+    mul(m3, t, out);
+    for (int i = 0; i < 4; i++)
+        for (int k = 0; k < 4; k++) out[i][k] = (double)(float)out[i][k];
 }
 
 // ipol_de_option (src/calc.rs:255-308): CheckDEoption of the two weighted
@@ -430,7 +467,11 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
         if (de_option >= 20) { err = "dIFS formulas do not work in an interpolation hybrid"; return false; }
         if (de_option < 0) { err = "formula option is not valid"; return false; }
     }
-    if (de_option >= 4 && de_option <= 6) { err = "4D hybrids are not supported"; return false; }
+    // a 4D hybrid (HybridMode::Alt4D): with the 4D numerical DE (option 4);
+    // the analytic 4D DE (options 5, 6) is not restated
+    const bool four_d = de_option >= 4 && de_option <= 6;
+    if (four_d && de_option != 4) { err = "4D hybrids with the analytic DE are not supported"; return false; }
+    if (four_d && ipol) { err = "4D interpolation hybrids are not supported"; return false; }
     bool is_custom_de = de_option == 2 || de_option == 5 || de_option == 6 || de_option == 11 || de_option == 20;
     for (auto &s : slots) {
         s.ade = is_custom_de;
@@ -605,6 +646,8 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     p.ipol = ipol;
     p.ipol_w[0] = ipw[0];
     p.ipol_w[1] = ipw[1];
+    p.four_d = four_d;
+    build_smatrix4(sc.rot_4d[0], sc.rot_4d[1], sc.rot_4d[2], p.smatrix4);
     return true;
 }
 
@@ -653,8 +696,8 @@ int Iteration::run(const std::vector<Slot> &slots) {
             continue;
         }
         it_result += 1;
-        double x = v[0], y = v[1], z = v[2];
-        rout = x * x + y * y + z * z;
+        double x = v[0], y = v[1], z = v[2], w = v[3];
+        rout = four_d ? x * x + y * y + z * z + w * w : x * x + y * y + z * z;
         if (rout < otrap) otrap = rout;
         if (it_result >= max_it || rout > rstop) return n;
     }
@@ -696,9 +739,28 @@ void Iteration::run_ipol(const std::vector<Slot> &slots, bool de) {
     }
 }
 
+// doHybrid4DPas (src/iteration.rs:757-772): the 3D point turned into 4D
+// (Rotate4Dex, src/math.rs:209-215), the hybrid on four components
+void Iteration::hybrid_4d(const std::vector<Slot> &slots) {
+    double v4[4];
+    for (int i = 0; i < 4; i++) v4[i] = c[0] * smatrix4[i][0] + c[1] * smatrix4[i][1] + c[2] * smatrix4[i][2];
+    for (int k = 0; k < 4; k++) {
+        v[k] = v4[k];
+        j[k] = do_julia ? ju[k] : v4[k];
+    }
+    rout = v4[0] * v4[0] + v4[1] * v4[1] + v4[2] * v4[2] + v4[3] * v4[3];
+    otrap = rout;
+    int n = run(slots);
+    if (calc_sit) smooth_iterations(n);
+}
+
 // doHybridPas (src/iteration.rs:521-535); an interpolation hybrid:
-// doInterpolHybridPas (src/iteration.rs:403-439)
+// doInterpolHybridPas (src/iteration.rs:403-439); a 4D hybrid: hybrid_4d
 void Iteration::hybrid_3d(const std::vector<Slot> &slots) {
+    if (four_d) {
+        hybrid_4d(slots);
+        return;
+    }
     if (do_julia) { j[0] = ju[0]; j[1] = ju[1]; j[2] = ju[2]; }
     else { j[0] = c[0]; j[1] = c[1]; j[2] = c[2]; }
     v[0] = c[0]; v[1] = c[1]; v[2] = c[2]; v[3] = 0.0;
@@ -779,6 +841,8 @@ Marcher::Marcher(const Params *pp, int32_t s) : p(pp), seed(s) {
     it.ipol = p->ipol;
     it.ipol_w[0] = p->ipol_w[0];
     it.ipol_w[1] = p->ipol_w[1];
+    it.four_d = p->four_d;
+    std::memcpy(it.smatrix4, p->smatrix4, sizeof(it.smatrix4));
     ms_de_stop = p->de_stop;
     max_its_result = p->max_it;
 }

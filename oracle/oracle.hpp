@@ -112,7 +112,7 @@ inline void build_view_vector_dfov(double xa, double ya, double out[3]) {
     out[2] = v[2] * n;
 }
 // ---- formulas (src/formulas.rs) ----
-enum FormulaKind { F_INTPOW = 0, F_REALPOWER = 1, F_TRICORN = 3, F_AMAZINGBOX = 4, F_BULBOX = 5, F_FOLDINGINTPOW = 6, F_MENGER = 100 };
+enum FormulaKind { F_INTPOW = 0, F_REALPOWER = 1, F_QUATERNION = 2, F_TRICORN = 3, F_AMAZINGBOX = 4, F_BULBOX = 5, F_FOLDINGINTPOW = 6, F_MENGER = 100 };
 
 struct Formula {
     int kind = F_INTPOW;
@@ -179,6 +179,8 @@ struct Params {
     int end_to = 0, repeat_from = 0;
     bool ipol = false;              // an interpolation hybrid (HybridMode::Ipol3D)
     float ipol_w[2] = {1.f, 0.f};   // its normalised weights
+    bool four_d = false;            // a 4D alternating hybrid (HybridMode::Alt4D)
+    double smatrix4[4][4] = {{0}};  // its 4D rotation (BuildSMatrix4)
 };
 
 bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err);
@@ -198,7 +200,10 @@ struct Iteration {
     float fhln[6];
     bool ipol = false;
     float ipol_w[2] = {1.f, 0.f};
+    bool four_d = false;
+    double smatrix4[4][4] = {{0}};
     void smooth_iterations(int n);
+    void hybrid_4d(const std::vector<Slot> &slots);
     int run(const std::vector<Slot> &slots);
     void run_ipol(const std::vector<Slot> &slots, bool de);
     void hybrid_3d(const std::vector<Slot> &slots);

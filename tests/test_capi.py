@@ -38,7 +38,9 @@ def test_unsupported_answers_on_the_host():
     assert mb3dcu.unsupported(scenes.c2_hybrid()) is None
     assert mb3dcu.unsupported(scenes.c1_plain_bulb()) is None
     s = scenes.default_scene()
-    s.slots[0].formula = 2  # Quaternion: a 4D formula, not on this card
+    s.slots[0].formula = 2  # Quaternion: a 4D formula, on this card (the sequential FP64 DE)
+    assert mb3dcu.unsupported(s) is None
+    s.slots[0].formula = 9  # Aexion C: not on this card
     r = mb3dcu.unsupported(s)
     assert r and "formula" in r
     s.n_slots = 0
@@ -124,6 +126,11 @@ def test_null_arguments_fail_on_the_host():
         lambda: L.mb3d_cu_mc_paint(None, col.ctypes.data, None, 64 * 48, ctypes.byref(mb3dcu.mc_paint_default()),
                                    rgb.ctypes.data),
         lambda: L.mb3d_cu_ssao24(None, ctypes.byref(sc), ctypes.byref(mb3dcu.ssao_default()), buf.ctypes.data),
+        lambda: L.mb3d_cu_ssao15(None, ctypes.byref(sc), ctypes.byref(mb3dcu.ssao_default()), buf.ctypes.data),
+        lambda: L.mb3d_cu_reflect_batch(None, ctypes.byref(sc), None, 1, 0, None),
+        lambda: L.mb3d_cu_reflect_first_rays(None, ctypes.byref(sc), buf.ctypes.data, None, None),
+        lambda: L.mb3d_cu_dn_fallback(None, 48, 64, col.ctypes.data, col.ctypes.data, col.ctypes.data, 16, 3.0,
+                                      col.ctypes.data, None),
     ]
     for call in calls:
         assert call() == mb3dcu.EINVAL

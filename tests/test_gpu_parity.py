@@ -31,7 +31,7 @@ def zc(sc):
 
 def test_de_probe_matches_oracle(card):
     rng = np.random.default_rng(1)
-    for name in ("Integer Power", "Amazing Box", "Bulbox", "Tricorn", "Real Power", "Folding Int Pow"):
+    for name in ("Integer Power", "Amazing Box", "Bulbox", "Tricorn", "Real Power", "Folding Int Pow", "Quaternion"):
         sc = scenes.preset(name, 96, 72)
         pts = rng.uniform(-1.6, 1.6, size=(2000, 3))
         d0, i0 = O.de_at(sc, pts)
@@ -84,6 +84,24 @@ def test_interpolation_hybrid_matches_oracle(card):
         d1, i1 = card.de_probe(sc, pts, mb3dcu.FP64)
         assert np.array_equal(i0, i1), (name, i0, i1)
         assert np.all(np.abs(d1 - d0) <= 1e-6 * np.maximum(np.abs(d0), 1e-3)), (name, d0, d1)
+
+
+def test_quaternion_4d_rotation_and_hybrid(card):
+    """The 4D hybrid (doHybrid4DPas, src/iteration.rs:757-772): the Quaternion
+    preset turned in 4D (BuildSMatrix4 of three plane angles), and the
+    Quaternion in a 3D alternating hybrid with Integer Power (the DE options
+    combine to the 3D numerical DE), the FP64 march against the oracle."""
+    a = scenes.preset("Quaternion", 160, 120)
+    a.rot_4d[0], a.rot_4d[1], a.rot_4d[2] = 0.3, -0.15, 0.2
+    b = scenes.preset("Quaternion", 160, 120)
+    scenes.set_slots(b, [scenes.slot(mb3dcu.F_QUATERNION, 1, -1.0, 0.0), scenes.intpow(8, -1.0, 1)])
+    for name, sc in (("4d-rotated", a), ("quaternion+ip8", b)):
+        ref = O.march(sc, mb3dcu.SILIGHT)
+        assert (~mb3dcu.is_background(ref)).mean() > 0.02, name
+        g = card.march(sc, mb3dcu.FP64)
+        r = compare(g, ref, *zc(sc))
+        assert r["hit_agree"] >= 0.999 and r["exact"] >= 0.95, (name, r)
+        assert card.march(sc, mb3dcu.FP32_FP64).tobytes() == g.tobytes(), name
 
 
 def test_interpolation_hybrid_shadows_and_ao(card):

