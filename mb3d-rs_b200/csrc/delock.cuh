@@ -222,9 +222,9 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const P c[3], float m
                                        DEstate *st = nullptr, bool calc_sit = false, int max_add = 0) {
     static_assert(sizeof(P) == 8 || sizeof(R) == 4, "a single precision position needs the single precision DE");
     if (COUNT) cnt->evals++;
-    // (those hybrids run in double precision only: their scenes are all-FP64,
-    // so the single precision kernels never see one)
-    if constexpr (sizeof(R) == 8) {
+    // (those hybrids run in double precision only and in the all-formula
+    // kernels: their scenes are all-FP64 and carry every formula bit)
+    if constexpr (sizeof(R) == 8 && FM == FKIND_ALL) {
         if (p.seq_de) return de_seq<FM, FULL, P>(p, c, ms_de_stop, st, calc_sit, max_add);
     }
     DEr out;

@@ -101,7 +101,8 @@ __device__ __forceinline__ void pixel_ray(const DevParams &p, int x, int y, doub
 // the formula set the kernel is built for
 template <int FM>
 struct It64 {
-    double v[4], c[3], j[4];
+    // (j's fourth component: the Quaternion's, only in the all-formula kernels)
+    double v[4], c[3], j[FM == FKIND_ALL ? 4 : 3];
     double rout, rold, otrap, rstop;
     int it_result, max_it;
     bool calc_sit;
@@ -135,7 +136,7 @@ struct It64 {
                 if (++guard > 64) return n;
             }
             const DevSlot &s = p.slots[n];
-            formula_iterate<double, FM, true>(s, v, j, rout);
+            formula_iterate<double, FM, FM == FKIND_ALL>(s, v, j, rout);
             if (s.julia_add) {
                 v[0] += j[0];
                 v[1] += j[1];
@@ -147,7 +148,9 @@ struct It64 {
                 continue;
             }
             it_result += 1;
-            rout = p.four_d ? v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3] : v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+            // (4D hybrids hold a Quaternion: only the all-formula kernels meet them)
+            if (FM == FKIND_ALL && p.four_d) rout = v[0] * v[0] + v[1] * v[1] + v[2] * v[2] + v[3] * v[3];
+            else rout = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
             if (rout < otrap) otrap = rout;
             if (it_result >= max_it || rout > rstop) return n;
         }
@@ -162,7 +165,7 @@ struct It64 {
             j[1] = c[1];
             j[2] = c[2];
         }
-        j[3] = p.ju[3];
+        if constexpr (FM == FKIND_ALL) j[3] = p.ju[3];
         v[0] = c[0];
         v[1] = c[1];
         v[2] = c[2];
@@ -172,11 +175,12 @@ struct It64 {
     // doHybrid4DPas (src/iteration.rs:757-772): the point turned into 4D
     // (Rotate4Dex, src/math.rs:209-215), the hybrid on four components
     __device__ void hybrid_4d(const DevParams &p) {
+        if constexpr (FM != FKIND_ALL) return;
         double v4[4];
         for (int i = 0; i < 4; i++) v4[i] = c[0] * p.smatrix4[i][0] + c[1] * p.smatrix4[i][1] + c[2] * p.smatrix4[i][2];
         for (int k = 0; k < 4; k++) {
             v[k] = v4[k];
-            j[k] = p.do_julia ? p.ju[k] : v4[k];
+            if constexpr (FM == FKIND_ALL) j[k] = p.do_julia ? p.ju[k] : v4[k];
         }
         rout = v4[0] * v4[0] + v4[1] * v4[1] + v4[2] * v4[2] + v4[3] * v4[3];
         otrap = rout;
@@ -184,29 +188,33 @@ struct It64 {
         if (calc_sit) smooth_iterations(p, n);
     }
     __device__ void hybrid_3d(const DevParams &p) {  // doHybridPas; doInterpolHybridPas; a 4D hybrid
-        if (p.four_d) {
+        if (FM == FKIND_ALL && p.four_d) {
             hybrid_4d(p);
             return;
         }
         start(p);
         v[3] = 0.0;
-        if (p.ipol) {
-            it_result = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, rstop, false);
-            if (calc_sit) smooth_iterations(p, 0);
-            return;
+        if constexpr (FM == FKIND_ALL) {
+            if (p.ipol) {
+                it_result = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, rstop, false);
+                if (calc_sit) smooth_iterations(p, 0);
+                return;
+            }
         }
         int n = run(p);
         if (calc_sit) smooth_iterations(p, n);
     }
     __device__ double hybrid_3d_de(const DevParams &p) {  // doHybridPasDE
         start(p);
-        if (p.ipol) {  // doInterpolHybridPasDE (src/iteration.rs:441-455)
-            v[3] = ((p.de_option & 0x18) == 16) ? rout : 1.0;
-            it_result = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, rstop, true);
-            const double w = v[3];
-            const double r = ((p.de_option & 7) == 4) ? fabs(v[2]) * log(fabs(v[2])) / w : sqrt(rout) / fabs(w);
-            if (calc_sit) smooth_iterations(p, 0);
-            return r;
+        if constexpr (FM == FKIND_ALL) {
+            if (p.ipol) {  // doInterpolHybridPasDE (src/iteration.rs:441-455)
+                v[3] = ((p.de_option & 0x18) == 16) ? rout : 1.0;
+                it_result = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, rstop, true);
+                const double w = v[3];
+                const double r = ((p.de_option & 7) == 4) ? fabs(v[2]) * log(fabs(v[2])) / w : sqrt(rout) / fabs(w);
+                if (calc_sit) smooth_iterations(p, 0);
+                return r;
+            }
         }
         v[3] = ((p.de_option & 0x38) == 16) ? rout : 1.0;
         int n = run(p);

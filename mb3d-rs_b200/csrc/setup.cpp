@@ -422,6 +422,7 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     if (p.seq_de) {
         p.all_fp64 = 1;
         p.sched = SCHED_GENERIC;
+        p.fmask |= KSET_ALL;  // (only the all-formula kernels carry the sequential DE)
     }
     p.coord_eps = coord * eps32;
     p.hand_margin = 4.0f;
