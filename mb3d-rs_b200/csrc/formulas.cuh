@@ -397,17 +397,20 @@ __device__ __forceinline__ int ipol_run(const DevParams &p, R v[4], R j[4], R &r
             v[2] += j[2];
         }
         const R x = v[0], y = v[1], z = v[2], w = v[3];
-        R xx = sqrt(x1[0] * x1[0] + x1[1] * x1[1] + x1[2] * x1[2]);
-        const R yy0 = sqrt(x * x + y * y + z * z);
+        const bool fd = p.four_d != 0;  // (doInterpolHybridPas4D: four components)
+        R xx = fd ? sqrt(x1[0] * x1[0] + x1[1] * x1[1] + x1[2] * x1[2] + x1[3] * x1[3])
+                  : sqrt(x1[0] * x1[0] + x1[1] * x1[1] + x1[2] * x1[2]);
+        const R yy0 = fd ? sqrt(x * x + y * y + z * z + w * w) : sqrt(x * x + y * y + z * z);
         xx = xx * s1 + yy0 * s2;
         R nv[4] = {x1[0] * s1 + x * s2, x1[1] * s1 + y * s2, x1[2] * s1 + z * s2, x1[3] * s1 + w * s2};
-        if (de) nv[3] = fabs(x1[3]) * s1 + fabs(w) * s2;
-        const R l2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
+        if (de && !fd) nv[3] = fabs(x1[3]) * s1 + fabs(w) * s2;
+        const R l2 = fd ? nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2] + nv[3] * nv[3]
+                        : nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
         const R q = xx / sqrt(l2 + (R)1e-40);
         v[0] = nv[0] * q;
         v[1] = nv[1] * q;
         v[2] = nv[2] * q;
-        v[3] = nv[3];
+        v[3] = fd ? nv[3] * q : nv[3];
         it += 1;
         rout = xx * xx;
         if (rout < otrap) otrap = rout;

@@ -184,6 +184,11 @@ struct It64 {
         }
         rout = v4[0] * v4[0] + v4[1] * v4[1] + v4[2] * v4[2] + v4[3] * v4[3];
         otrap = rout;
+        if (p.ipol) {  // doInterpolHybridPas4D (src/iteration.rs:457-464)
+            it_result = ipol_run<double, FM>(p, v, j, rout, rold, otrap, max_it, rstop, false);
+            if (calc_sit) smooth_iterations(p, 0);
+            return;
+        }
         int n = run(p);
         if (calc_sit) smooth_iterations(p, n);
     }

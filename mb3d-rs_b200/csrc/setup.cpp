@@ -214,8 +214,8 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     // a 4D hybrid (HybridMode::Alt4D) with the 4D numerical DE (option 4);
     // the analytic 4D DE (options 5, 6) and 4D interpolation are not built
     const bool four_d = de_option >= 4 && de_option <= 6;
-    if (four_d && (de_option != 4 || ipol)) {
-        err = "4D hybrids with the analytic DE or interpolated are not built into this backend";
+    if (four_d && de_option != 4) {
+        err = "4D hybrids with the analytic DE are not built into this backend";
         return MB3D_CU_ENOTSUP;
     }
     bool custom = de_option == 2 || de_option == 5 || de_option == 6 || de_option == 11 || de_option == 20;

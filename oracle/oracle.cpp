@@ -471,7 +471,7 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     // the analytic 4D DE (options 5, 6) is not restated
     const bool four_d = de_option >= 4 && de_option <= 6;
     if (four_d && de_option != 4) { err = "4D hybrids with the analytic DE are not supported"; return false; }
-    if (four_d && ipol) { err = "4D interpolation hybrids are not supported"; return false; }
+
     bool is_custom_de = de_option == 2 || de_option == 5 || de_option == 6 || de_option == 11 || de_option == 20;
     for (auto &s : slots) {
         s.ade = is_custom_de;
@@ -707,6 +707,7 @@ int Iteration::run(const std::vector<Slot> &slots) {
 // vector, the results and their lengths blended with the weights; `de`
 // blends the running derivative (w) of the analytic-DE variant
 void Iteration::run_ipol(const std::vector<Slot> &slots, bool de) {
+    const bool fd = four_d;  // (doInterpolHybridPas4D: lengths and the blend's scale on four components)
     const double s1 = (double)ipol_w[0], s2 = (double)ipol_w[1];
     it_result = 0;
     for (;;) {
@@ -721,16 +722,24 @@ void Iteration::run_ipol(const std::vector<Slot> &slots, bool de) {
         if (slots[1].julia_add)
             for (int k = 0; k < 3; k++) v[k] += j[k];
         const double x = v[0], y = v[1], z = v[2], w = v[3];
-        double xx = std::sqrt(x1[0] * x1[0] + x1[1] * x1[1] + x1[2] * x1[2]);
-        const double yy0 = std::sqrt(x * x + y * y + z * z);
+        double xx, yy0;
+        if (fd) {
+            xx = std::sqrt(x1[0] * x1[0] + x1[1] * x1[1] + x1[2] * x1[2] + x1[3] * x1[3]);
+            yy0 = std::sqrt(x * x + y * y + z * z + w * w);
+        } else {
+            xx = std::sqrt(x1[0] * x1[0] + x1[1] * x1[1] + x1[2] * x1[2]);
+            yy0 = std::sqrt(x * x + y * y + z * z);
+        }
         xx = xx * s1 + yy0 * s2;
         double nv[4] = {x1[0] * s1 + x * s2, x1[1] * s1 + y * s2, x1[2] * s1 + z * s2, x1[3] * s1 + w * s2};
-        if (de) nv[3] = std::fabs(x1[3]) * s1 + std::fabs(w) * s2;
-        const double l2 = nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
+        if (de && !fd) nv[3] = std::fabs(x1[3]) * s1 + std::fabs(w) * s2;
+        const double l2 = fd ? nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2] + nv[3] * nv[3]
+                             : nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2];
         const double yy = xx / std::sqrt(l2 + 1e-40);
         nv[0] *= yy;
         nv[1] *= yy;
         nv[2] *= yy;
+        if (fd) nv[3] *= yy;
         for (int k = 0; k < 4; k++) v[k] = nv[k];
         it_result += 1;
         rout = xx * xx;
@@ -750,6 +759,11 @@ void Iteration::hybrid_4d(const std::vector<Slot> &slots) {
     }
     rout = v4[0] * v4[0] + v4[1] * v4[1] + v4[2] * v4[2] + v4[3] * v4[3];
     otrap = rout;
+    if (ipol) {  // doInterpolHybridPas4D (src/iteration.rs:457-464)
+        run_ipol(slots, false);
+        if (calc_sit) smooth_iterations(0);
+        return;
+    }
     int n = run(slots);
     if (calc_sit) smooth_iterations(n);
 }

@@ -60,7 +60,9 @@ def _ipol_scenes():
     b = scenes.interpolated("Amazing Box", "Amazing Box", (0.5, 0.5), 160, 120)
     b.slots[1].options[0] = 2.5  # (two boxes: the analytic DE's blend)
     c = scenes.interpolated("Integer Power", "Folding Int Pow", (0.5, 0.5), 160, 120)
-    return [("ip8+tricorn", a), ("box+box", b), ("ip8+fip", c)]
+    d = scenes.interpolated("Quaternion", "Quaternion", (0.5, 0.5), 160, 120)
+    d.slots[1].options[1] = 0.1  # (two Quaternions: the 4D interpolation, doInterpolHybridPas4D)
+    return [("ip8+tricorn", a), ("box+box", b), ("ip8+fip", c), ("quat+quat 4d", d)]
 
 
 def test_interpolation_hybrid_matches_oracle(card):

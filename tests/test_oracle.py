@@ -616,3 +616,16 @@ def test_quaternion_4d_rotation_turns_the_set():
     c.rot_4d[0] = 2 * math.pi
     assert O.march(c, mb3dcu.SILIGHT)["zpos_fine"].tobytes() == g0["zpos_fine"].tobytes() or \
         (O.march(c, mb3dcu.SILIGHT)["zpos_fine"] == g0["zpos_fine"]).mean() > 0.99
+
+
+def test_interpolation_4d_with_weights_one_and_zero_is_the_first_formula():
+    """doInterpolHybridPas4D (src/iteration.rs:457-464) as the reference's
+    interpolation test asks of the 3D one: weights 1 : 0 of two Quaternions
+    give the first alone (the 4D preset)."""
+    one = scenes.interpolated("Quaternion", "Quaternion", (2.0, 0.0), 96, 72)
+    one.slots[1].options[1] = 0.3
+    pos = np.array([[0.3, 0.2, -0.5], [0.1, -0.4, 0.2], [0.5, 0.5, 0.5]])
+    d1, i1 = O.de_at(scenes.preset("Quaternion", 96, 72), pos)
+    d2, i2 = O.de_at(one, pos)
+    assert np.array_equal(i1, i2)
+    assert np.all(np.abs(d1 - d2) <= 1e-9 * np.maximum(np.abs(d1), 1e-3)), (d1, d2)
