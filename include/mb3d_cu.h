@@ -55,6 +55,7 @@ extern "C" {
 #define MB3D_CU_F_AMAZINGBOX 4    /* Amazing Box: scale, min_r, fold */
 #define MB3D_CU_F_BULBOX 5        /* Bulbox: scale, min_r, fold, bulb_scale, r_thr, r_thr2 */
 #define MB3D_CU_F_FOLDINGINTPOW 6 /* Folding Int Pow: power, z_mul, fold */
+#define MB3D_CU_F_AEXIONC 9       /* Aexion C: power, z_mul, rot_c, cond_phi, power_c, cz_mul, powc_dist, mode */
 #define MB3D_CU_F_MENGERIFS 100   /* Menger IFS: scale, cscale_x, cscale_y, cscale_z */
 
 #define MB3D_CU_SLOTS 6

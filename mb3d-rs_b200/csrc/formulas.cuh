@@ -210,12 +210,79 @@ __device__ __forceinline__ void f_menger(R s, R cx, R cy, R cz, R v[4], bool ade
 #define FKIND_FIP 128
 #define FKIND_ALL 255
 #define FKIND_QUAT 256  // (only in the all-formula kernels' switch: a 4-component j)
+#define FKIND_AEXION 512  // (likewise: it writes j)
 
 // J4: j has four components (the sequential FP64 iteration's record); only
 // then is the Quaternion (4D, it reads j's fourth) on the switch -- the
 // lock-step DE's j has three, and scenes with a Quaternion never reach it
+// aexion_c (src/formulas.rs:640-705), double precision: a real power bulb
+// step with the angles as atan2 (theta from the y axis), then with "rotate
+// C" the constant replaced by a power of its own angles (it writes j).
+// Options: power, z_mul, rot_c, cond_phi, power_c, cz_mul, powc_dist, mode.
+__device__ __forceinline__ void f_aexion_c(const DevSlot &s, double v[4], double *j) {
+    const double power = s.o[0], z_mul = s.o[1], power_c = s.o[4], cz_mul = s.o[5];
+    const bool rot_c = s.o[2] != 0.0, cond_phi = s.o[3] != 0.0, powc_dist = s.o[6] != 0.0;
+    const int mode = (int)s.o[7];
+    const double x = v[0], y = v[1], z = v[2];
+    double r1 = x * x + y * y + z * z;
+    const double th = atan2(sqrt(x * x + z * z), y) * power;
+    const double ph = atan2(z, x) * power;
+    r1 = exp(log(r1) * power * 0.5);
+    double st, ct, sp, cp;
+    sincos(th, &st, &ct);
+    sincos(ph, &sp, &cp);
+    v[0] = cp * ct * r1 + j[0];
+    v[2] = st * r1 * z_mul + j[2];
+    v[1] = ct * sp * r1 + j[1];
+    if (!rot_c) return;
+    double pd = power_c;
+    if (powc_dist) {
+        const double d0 = v[0] - j[0], d1 = v[1] - j[1], d2 = v[2] - j[2];
+        pd *= sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+    }
+    const double r = sqrt(j[0] * j[0] + j[1] * j[1] + j[2] * j[2]);
+    double a = j[1], b = j[2], c = j[0];
+    if (mode & 16) {
+        a = v[1] - j[1];
+        b = v[2] - j[2];
+        c = v[0] - j[0];
+    }
+    int ofs = 0, ecx = 8;
+    if (mode & 8) {
+        const double t = a;
+        a = b;
+        b = t;
+        ecx = 16;
+    }
+    const double sb2 = sqrt(b * b + c * c);
+    double tha = (mode & 1) ? atan2(a, sb2) : atan2(sb2, a);
+    double pha;
+    if (mode & 2) {
+        ofs = 24 - ecx;
+        pha = atan2(c, b);
+    } else {
+        pha = atan2(b, c);
+    }
+    if (mode & 4) {
+        const double t = tha;
+        tha = pha;
+        pha = t;
+        ofs = ecx;
+    }
+    if (cond_phi) {
+        const double t = ofs == 0 ? v[0] : ofs == 8 ? v[1] : v[2];
+        if (!signbit(t)) pha = -pha;
+    }
+    double sa, ca, sb, cb;
+    sincos(pha * pd, &sa, &ca);
+    sincos(tha * pd, &sb, &cb);
+    j[0] = ca * cb * r;
+    j[2] = sb * r * cz_mul;
+    j[1] = cb * sa * r;
+}
+
 template <typename R, int FM = FKIND_ALL, bool J4 = false>
-__device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], const R *j, R rout) {
+__device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], R *j, R rout) {
     const bool ade = s.ade != 0;
     if (FM == FKIND_IP8) {
         f_int_pow<R>(8, Num<R>::opt(s, 1), v, j);
@@ -243,6 +310,9 @@ __device__ __forceinline__ void formula_iterate(const DevSlot &s, R v[4], const 
             f_menger<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), Num<R>::opt(s, 2), Num<R>::opt(s, 3), v, ade);
             break;
         case MB3D_CU_F_REALPOWER: f_real_power<R>(Num<R>::opt(s, 0), Num<R>::opt(s, 1), v, j, rout); break;
+        case MB3D_CU_F_AEXIONC:
+            if constexpr (J4 && sizeof(R) == 8) f_aexion_c(s, v, j);
+            break;
         case MB3D_CU_F_QUATERNION:  // src/formulas.rs:580-586
             if constexpr (J4) {
                 const R x = v[0], y = v[1], z = v[2], w = v[3];

@@ -39,7 +39,7 @@ static int f_ipow(const mb3d_cu_slot &s) {
 static double f_si_pow(const mb3d_cu_slot &s) {
     switch (s.formula) {
         case MB3D_CU_F_INTPOW: return (double)f_ipow(s);
-        case MB3D_CU_F_REALPOWER: return s.options[0] == 0.0 ? 1e-40 : s.options[0];
+        case MB3D_CU_F_REALPOWER: case MB3D_CU_F_AEXIONC: return s.options[0] == 0.0 ? 1e-40 : s.options[0];
         case MB3D_CU_F_MENGERIFS: return 0.0;
         default: return 2.0;
     }
@@ -49,7 +49,7 @@ static double f_first_option(const mb3d_cu_slot &s) { return f_first_is_zmul(s.f
 static bool f_known(int f) {
     return f == MB3D_CU_F_INTPOW || f == MB3D_CU_F_REALPOWER || f == MB3D_CU_F_TRICORN || f == MB3D_CU_F_AMAZINGBOX ||
            f == MB3D_CU_F_BULBOX || f == MB3D_CU_F_FOLDINGINTPOW || f == MB3D_CU_F_MENGERIFS ||
-           f == MB3D_CU_F_QUATERNION;
+           f == MB3D_CU_F_QUATERNION || f == MB3D_CU_F_AEXIONC;
 }
 
 // CheckFormulaOptions (src/calc.rs:315-372)
@@ -385,6 +385,7 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
             case MB3D_CU_F_TRICORN: d.kind = 32; break;
             case MB3D_CU_F_BULBOX: d.kind = 64; break;
             case MB3D_CU_F_QUATERNION: d.kind = 256; break;
+            case MB3D_CU_F_AEXIONC: d.kind = 512; break;
             default: d.kind = 128; break;
         }
         if (its[i] > 0) p.fmask |= d.kind;
@@ -417,7 +418,10 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     p.four_d = four_d ? 1 : 0;
     build_smatrix4(sc.rot_4d[0], sc.rot_4d[1], sc.rot_4d[2], p.smatrix4);
     bool quat = false;
-    for (int i = 0; i < nsl; i++) quat = quat || (fs[i] == MB3D_CU_F_QUATERNION && its[i] > 0);
+    // (the Quaternion reads a fourth component of j, Aexion C writes j: both
+    // only on the sequential record)
+    for (int i = 0; i < nsl; i++)
+        quat = quat || ((fs[i] == MB3D_CU_F_QUATERNION || fs[i] == MB3D_CU_F_AEXIONC) && its[i] > 0);
     p.seq_de = (ipol || four_d || quat) ? 1 : 0;
     if (p.seq_de) {
         p.all_fp64 = 1;

@@ -22,7 +22,7 @@ LIB_PATH = os.environ.get("MB3D_CU_LIB") or os.path.join(HERE, "libmb3dcu.so")
 OK, EINVAL, ENOMEM, ENODEV, EIO, ECANCELED, ETIMEDOUT, EOVERFLOW, ENOTSUP = 0, -22, -12, -19, -5, -125, -110, -75, -95
 
 F_INTPOW, F_REALPOWER, F_TRICORN, F_AMAZINGBOX, F_BULBOX, F_FOLDINGINTPOW, F_MENGERIFS = 0, 1, 3, 4, 5, 6, 100
-F_QUATERNION = 2
+F_QUATERNION, F_AEXIONC = 2, 9
 FP64, FP32_FP64 = 0, 1
 POST_SHADOW, POST_DEAO = 1, 2
 

@@ -10,7 +10,7 @@ import math
 import numpy as np
 
 from mb3dcu import Scene, Slot, Light, F_INTPOW, F_AMAZINGBOX, F_MENGERIFS, F_REALPOWER, F_TRICORN, F_BULBOX, \
-    F_FOLDINGINTPOW, F_QUATERNION
+    F_FOLDINGINTPOW, F_QUATERNION, F_AEXIONC
 
 PI = math.pi
 
@@ -107,6 +107,8 @@ def preset(name, width=None, height=None):
         f, zs, zoom, its, rot = slot(F_TRICORN, 1, -2.0, 1.0), -3.0, 0.6, 12, (0.6, 0.2)
     elif n == "real power":
         f, zs, zoom, its, rot = slot(F_REALPOWER, 1, 8.0, -1.0), -2.5, 0.8, 12, (-0.55, 0.45)
+    elif n == "aexion c":
+        f, zs, zoom, its, rot = slot(F_AEXIONC, 1, 8.0, 1.0, 1.0, 1.0, 8.0, 1.0, 0.0, 0.0), -3.0, 0.65, 10, (0.45, 0.3)
     elif n == "quaternion":
         f, zs, zoom, its, rot = slot(F_QUATERNION, 1, -1.0, 0.0), -3.0, 0.8, 12, (0.4, 0.3)
         sc.julia = 1
@@ -122,7 +124,8 @@ def preset(name, width=None, height=None):
     return sc
 
 
-PRESETS = ["Integer Power", "Real Power", "Quaternion", "Tricorn", "Amazing Box", "Bulbox", "Folding Int Pow"]
+PRESETS = ["Integer Power", "Real Power", "Quaternion", "Tricorn", "Amazing Box", "Bulbox", "Folding Int Pow",
+           "Aexion C"]
 
 
 def interpolated(first, second, weights, width=None, height=None):

@@ -79,7 +79,7 @@ double Formula::default_rstop() const {
 double Formula::si_pow() const {
     switch (kind) {
         case F_INTPOW: return (double)power();
-        case F_REALPOWER: return o[0] == 0.0 ? 1e-40 : o[0];
+        case F_REALPOWER: case F_AEXIONC: return o[0] == 0.0 ? 1e-40 : o[0];
         case F_MENGER: return 0.0;
         default: return 2.0;
     }
@@ -242,6 +242,64 @@ static void menger_ifs(const double *o, double v[4], bool ade) {
     v[2] = z;
 }
 
+// aexion_c (src/formulas.rs:640-705): a real power bulb step with the angles
+// as atan2 (theta from the y axis), then with "rotate C" the constant
+// replaced by a power of its own angles.  Options: power, z_mul, rot_c,
+// cond_phi, power_c, cz_mul, powc_dist, mode.
+static void aexion_c(const double *o, double v[4], double j[4]) {
+    const double power = o[0], z_mul = o[1], power_c = o[4], cz_mul = o[5];
+    const bool rot_c = o[2] != 0.0, cond_phi = o[3] != 0.0, powc_dist = o[6] != 0.0;
+    const int mode = (int)o[7];
+    const double x = v[0], y = v[1], z = v[2];
+    double r1 = x * x + y * y + z * z;
+    const double th = std::atan2(std::sqrt(x * x + z * z), y) * power;
+    const double ph = std::atan2(z, x) * power;
+    r1 = std::exp(std::log(r1) * power * 0.5);
+    const double st = std::sin(th), ct = std::cos(th), sp = std::sin(ph), cp = std::cos(ph);
+    v[0] = cp * ct * r1 + j[0];
+    v[2] = st * r1 * z_mul + j[2];
+    v[1] = ct * sp * r1 + j[1];
+    if (!rot_c) return;
+    double pd = power_c;
+    if (powc_dist) {
+        const double d[3] = {v[0] - j[0], v[1] - j[1], v[2] - j[2]};
+        pd *= std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    }
+    const double r = std::sqrt(j[0] * j[0] + j[1] * j[1] + j[2] * j[2]);
+    double a, b, c;
+    if (mode & 16) {
+        a = v[1] - j[1]; b = v[2] - j[2]; c = v[0] - j[0];
+    } else {
+        a = j[1]; b = j[2]; c = j[0];
+    }
+    int ofs = 0, ecx = 8;
+    if (mode & 8) {
+        std::swap(a, b);
+        ecx = 16;
+    }
+    const double s = std::sqrt(b * b + c * c);
+    double tha = (mode & 1) ? std::atan2(a, s) : std::atan2(s, a);
+    double pha;
+    if (mode & 2) {
+        ofs = 24 - ecx;
+        pha = std::atan2(c, b);
+    } else {
+        pha = std::atan2(b, c);
+    }
+    if (mode & 4) {
+        std::swap(tha, pha);
+        ofs = ecx;
+    }
+    if (cond_phi) {
+        const double t = ofs == 0 ? v[0] : ofs == 8 ? v[1] : v[2];
+        if (!std::signbit(t)) pha = -pha;
+    }
+    const double sa = std::sin(pha * pd), ca = std::cos(pha * pd), sb = std::sin(tha * pd), cb = std::cos(tha * pd);
+    j[0] = ca * cb * r;
+    j[2] = sb * r * cz_mul;
+    j[1] = cb * sa * r;
+}
+
 // Formula::iterate (src/formulas.rs:576-637)
 void Formula::iterate(double v[4], double j[4], double rout, bool ade) const {
     switch (kind) {
@@ -295,6 +353,7 @@ void Formula::iterate(double v[4], double j[4], double rout, bool ade) const {
             int_pow(power(), o[1], v, j);
             break;
         case F_MENGER: menger_ifs(o, v, ade); break;
+        case F_AEXIONC: aexion_c(o, v, j); break;
         default: break;
     }
 }
@@ -302,7 +361,7 @@ void Formula::iterate(double v[4], double j[4], double rout, bool ade) const {
 bool formula_from_slot(const mb3d_cu_slot &s, Formula &f, std::string &err) {
     switch (s.formula) {
         case F_INTPOW: case F_REALPOWER: case F_QUATERNION: case F_TRICORN: case F_AMAZINGBOX: case F_BULBOX:
-        case F_FOLDINGINTPOW: case F_MENGER:
+        case F_FOLDINGINTPOW: case F_AEXIONC: case F_MENGER:
             f.kind = s.formula;
             for (int k = 0; k < 16; k++) f.o[k] = s.options[k];
             return true;

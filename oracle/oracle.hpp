@@ -112,7 +112,7 @@ inline void build_view_vector_dfov(double xa, double ya, double out[3]) {
     out[2] = v[2] * n;
 }
 // ---- formulas (src/formulas.rs) ----
-enum FormulaKind { F_INTPOW = 0, F_REALPOWER = 1, F_QUATERNION = 2, F_TRICORN = 3, F_AMAZINGBOX = 4, F_BULBOX = 5, F_FOLDINGINTPOW = 6, F_MENGER = 100 };
+enum FormulaKind { F_INTPOW = 0, F_REALPOWER = 1, F_QUATERNION = 2, F_TRICORN = 3, F_AMAZINGBOX = 4, F_BULBOX = 5, F_FOLDINGINTPOW = 6, F_AEXIONC = 9, F_MENGER = 100 };
 
 struct Formula {
     int kind = F_INTPOW;

@@ -40,7 +40,7 @@ def test_unsupported_answers_on_the_host():
     s = scenes.default_scene()
     s.slots[0].formula = 2  # Quaternion: a 4D formula, on this card (the sequential FP64 DE)
     assert mb3dcu.unsupported(s) is None
-    s.slots[0].formula = 9  # Aexion C: not on this card
+    s.slots[0].formula = 7  # (no formula 7: not on this card)
     r = mb3dcu.unsupported(s)
     assert r and "formula" in r
     s.n_slots = 0

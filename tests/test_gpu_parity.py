@@ -31,7 +31,8 @@ def zc(sc):
 
 def test_de_probe_matches_oracle(card):
     rng = np.random.default_rng(1)
-    for name in ("Integer Power", "Amazing Box", "Bulbox", "Tricorn", "Real Power", "Folding Int Pow", "Quaternion"):
+    for name in ("Integer Power", "Amazing Box", "Bulbox", "Tricorn", "Real Power", "Folding Int Pow", "Quaternion",
+                 "Aexion C"):
         sc = scenes.preset(name, 96, 72)
         pts = rng.uniform(-1.6, 1.6, size=(2000, 3))
         d0, i0 = O.de_at(sc, pts)

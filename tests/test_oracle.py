@@ -629,3 +629,26 @@ def test_interpolation_4d_with_weights_one_and_zero_is_the_first_formula():
     d2, i2 = O.de_at(one, pos)
     assert np.array_equal(i1, i2)
     assert np.all(np.abs(d1 - d2) <= 1e-9 * np.maximum(np.abs(d1), 1e-3)), (d1, d2)
+
+
+def test_aexion_c_matches_pascal_reference():
+    """src/formulas.rs:878-911: Aexion C with its defaults (power 8, z_mul 1,
+    rotate C, conditional phi, power C 8, Cz 1, mode 0) against the
+    spherical reference formula, for Z and for the turned C."""
+    opts = [8.0, 1.0, 1.0, 1.0, 8.0, 1.0, 0.0, 0.0]
+    for x, y, z, cx, cy, cz in ((0.3, -0.4, 0.5, 0.2, 0.1, -0.3), (-0.7, 0.2, 0.1, -0.5, 0.4, 0.6),
+                                (0.05, 0.9, -0.2, 0.3, -0.8, 0.1)):
+        v, j = O.formula_iterate(mb3dcu.F_AEXIONC, opts, [x, y, z, 0.0], [cx, cy, cz, 0.0])
+        p = 8.0
+        r1 = (x * x + y * y + z * z) ** (p * 0.5)
+        th = math.atan2(math.sqrt(x * x + z * z), y) * p
+        ph = math.atan2(z, x) * p
+        xn, yn, zn = math.cos(th) * math.cos(ph) * r1 + cx, math.cos(th) * math.sin(ph) * r1 + cy, r1 * math.sin(th) + cz
+        r = math.sqrt(cx * cx + cy * cy + cz * cz)
+        th2 = math.atan2(math.sqrt(cx * cx + cz * cz), cy) * 8.0
+        ph2 = math.atan2(cz, cx) * 8.0
+        if xn > 0.0:
+            ph2 = -ph2
+        jr = [math.cos(th2) * math.cos(ph2) * r, math.cos(th2) * math.sin(ph2) * r, r * math.sin(th2)]
+        assert np.allclose(v[:3], [xn, yn, zn], atol=1e-9), (v, [xn, yn, zn])
+        assert np.allclose(j[:3], jr, atol=1e-9), (j, jr)
