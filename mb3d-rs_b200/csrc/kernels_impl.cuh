@@ -35,6 +35,12 @@
 #endif
 // (the single precision march: 4 blocks of 64 registers, its spills cost
 // less than the warps it gains)
+#ifndef MB3D_MIN_BLOCKS_FINISH
+#define MB3D_MIN_BLOCKS_FINISH MB3D_MIN_BLOCKS
+#endif
+#ifndef MB3D_MIN_BLOCKS_POST
+#define MB3D_MIN_BLOCKS_POST MB3D_MIN_BLOCKS
+#endif
 #ifndef MB3D_MIN_BLOCKS_AO32
 #define MB3D_MIN_BLOCKS_AO32 4
 #endif
@@ -457,7 +463,7 @@ __global__ void __launch_bounds__(128) k_finish_slow(const __grid_constant__ Dev
 #define F_BSI2 9  // ... and 0.001 behind it
 
 template <int FM>
-__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_finish(const __grid_constant__ DevParams p, int row0, const Hand *list,
+__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_FINISH) k_finish(const __grid_constant__ DevParams p, int row0, const Hand *list,
                                                 unsigned int *counters, Hand *slow, mb3d_cu_silight *out) {
     const uint32_t n_items = counters[0];
     // RMdoBinSearchIt's target count and its limit (the search iterates once more)
@@ -797,7 +803,7 @@ __global__ void k_surface(const __grid_constant__ DevParams p, int npix, int pas
 #define Q_BSI2 5  // ... and 0.001 behind it
 
 template <int FM, bool MIXED>
-__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_post_start(const __grid_constant__ DevParams p, int row0, int passes,
+__global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_POST) k_post_start(const __grid_constant__ DevParams p, int row0, int passes,
                                                     const mb3d_cu_silight *gbuf, const uint32_t *list,
                                                     const unsigned int *count, unsigned int *queue, PostStart *ps) {
     const uint32_t n_items = count[0];

@@ -334,7 +334,7 @@ __device__ void refl_march(const DevParams &p, const mb3d_cu_reflect_ray &r, int
 
 // one thread per ray
 template <int FM>
-__global__ void __launch_bounds__(128) k_reflect(const __grid_constant__ DevParams p, const mb3d_cu_reflect_ray *rays,
+__global__ void __maxnreg__(168) k_reflect(const __grid_constant__ DevParams p, const mb3d_cu_reflect_ray *rays,
                                                  uint32_t n, int far_fog, const ReflAO *tab,
                                                  mb3d_cu_reflect_hit *hits) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(128) k_reflect(const __grid_constant__ DevPara
 // stored depth, then step's mirror ray, :1286-1311) into tmp[i], valid[i]
 // 1 where the pixel sends one
 template <int FM>
-__global__ void __launch_bounds__(128) k_reflect_first(const __grid_constant__ DevParams p, const mb3d_cu_silight *g,
+__global__ void __maxnreg__(168) k_reflect_first(const __grid_constant__ DevParams p, const mb3d_cu_silight *g,
                                                        mb3d_cu_reflect_ray *tmp, unsigned char *valid) {
     const size_t npix = (size_t)p.width * p.height;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += (size_t)gridDim.x * blockDim.x) {
