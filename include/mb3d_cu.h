@@ -130,6 +130,22 @@ typedef struct mb3d_cu_scene {
     /* the 4D rotation of a 4D hybrid (Scene::rot_4d, src/scene.rs:459): the
      * XW, YW and ZW plane angles in radians (BuildSMatrix4) */
     double rot_4d[3];
+    /* a DE combination of two hybrid parts (Scene::decomb, src/scene.rs:2178-2200;
+     * CalcDEfull with FormulaType > 0, src/calc.rs:1365-1455): decomb 0 is
+     * none, 1 min, 2 max, 3 max with the second part inverted, 4 smooth min
+     * (linear), 5 smooth min, 6 mix (its second part must be dIFS, which is
+     * not on the card: EINVAL as in the reference).  Slots are 0-based: part 1
+     * is slots 0..decomb_end1, part 2 decomb_start2..decomb_end2 repeating
+     * from decomb_repeat2, with decomb_iterations2 maximum iterations (0: the
+     * scene's). decomb_smooth is the smooth combinations' distance (sDEcombS). Part 2
+     * sits at part2_offset, turned by part2_rotation (degrees about x, y, z)
+     * and scaled by part2_scale (Scene::part2_place; 0 reads as 1). Ignored in
+     * an interpolation hybrid, as in the reference. */
+    int32_t decomb;
+    int32_t decomb_end1, decomb_start2, decomb_end2, decomb_repeat2, decomb_iterations2;
+    float decomb_smooth, decomb_mix_pow;
+    int32_t decomb_mix_color, pad2;
+    double part2_offset[3], part2_rotation[3], part2_scale;
 } mb3d_cu_scene;
 
 /* The G-buffer record SiLight (src/gbuffer.rs:5-20), 20 bytes; mb3d-rs's

@@ -29,6 +29,7 @@ namespace mb3dcu {
 struct DEr {
     double de;
     int it;
+    int max_its;    // the iteration limit of the part that ruled (max_its_result; a DE combination's)
     bool need64;    // single precision cannot resolve the offset here
     bool overflow;  // ... because its DE overflowed (not finite)
 };
@@ -41,6 +42,15 @@ struct DEstate {
     double rout, rold, otrap, v[3];
     float smooth_it;
 };
+
+// The iteration count at which a DE's point counts as in the set: the
+// scene's maximum, or in a DE combination the ruling part's (only the
+// all-formula kernels meet one)
+template <int FM>
+__device__ __forceinline__ int its_cap(const DevParams &p, const DEr &r) {
+    if constexpr (FM == FKIND_ALL) return r.max_its;
+    return p.max_it;
+}
 
 __device__ __forceinline__ float fsqrt_fast(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
 
@@ -168,7 +178,21 @@ __device__ __noinline__ DEr de_seq(const DevParams &p, const P c[3], float ms_de
     it.max_it = p.max_it + max_add;
     it.rstop = p.d_rstop;
     it.calc_sit = FULL && calc_sit;
+    it.part2 = false;
     it.smooth_it = 0.f;
+    out.max_its = it.max_it;
+    if (p.dc_kind) {
+        out.de = de_comb<FM>(p, it, ms_de_stop, out.max_its);
+        out.it = it.it_result;
+        if (FULL) {
+            st->rout = it.rout;
+            st->rold = it.rold;
+            st->otrap = it.otrap;
+            st->v[0] = it.v[0]; st->v[1] = it.v[1]; st->v[2] = it.v[2];
+            st->smooth_it = it.smooth_it;
+        }
+        return out;
+    }
     if (p.is_custom_de) {
         out.de = it.hybrid_3d_de(p) * (double)p.d_de_scale;
         out.it = it.it_result;
@@ -231,6 +255,7 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const P c[3], float m
     out.need64 = false;
     out.overflow = false;
     const int max_it = p.max_it + max_add;  // (max_add: doBinSearchIt's one more iteration)
+    out.max_its = max_it;
     const R rstop = param_f<R>(p, p.d_rstop, p.d_rstop_f);
     if (p.is_custom_de) {
         R v[1][4], j[1][3], rout[1];

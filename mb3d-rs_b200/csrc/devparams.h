@@ -74,6 +74,16 @@ struct DevParams {
     // 4D hybrids and hybrids with a Quaternion
     int32_t seq_de;
     double smatrix4[4][4];
+    // a DE combination (DeComb, src/calc.rs:224-236): its kind (0: none,
+    // 1..5) and its second hybrid part (HybridPart, :210-220), which runs on
+    // the sequential FP64 record too
+    int32_t dc_kind, dc_start2, dc_end2, dc_rep2;
+    int32_t dc_max_it2, dc_de_option2, dc_custom2, dc_place;
+    float dc_d_de_scale2, pad_dc;
+    double dc_smooth;           // the smoothing distance in steps
+    double dc_offset[3];        // Place: m * (p - offset), distances times scale
+    double dc_m[3][3];
+    double dc_scale;
 };
 
 // slot orders the single precision DE loop knows at compile time

@@ -239,6 +239,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
             cur_it = r.it;
             T dtmp = (T)r.de;
             int it = r.it;
+            const int itc = its_cap<FM>(p, r);
             bool skip_half = false, decide = true;
             if (MIXED && r.need64) {
                 overflowed = r.overflow;
@@ -247,7 +248,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                 resume = !full;
                 decide = false;
             } else if (phase == PH_START) {
-                if (it >= p.max_it || dtmp < (T)ms) {
+                if (it >= itc || dtmp < (T)ms) {
                     hand = true;  // inside the set at the start plane
                     full = true;
                     decide = false;
@@ -275,7 +276,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                 skip_half = true;
             }
             if (decide) {
-                if (!skip_half && it >= p.max_it) {
+                if (!skip_half && it >= itc) {
                     // src/calc.rs:2544-2551: half a step back
                     const T dt1 = (T)-0.5 * last_step;
                     mzz += (double)dt1;
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? MB3D_MIN_BLOCKS_MARCH32 
                     ms = MIXED ? de_stop_at_f(p, mzz) : de_stop_at(p, mzz);
                     last_step = -dt1;
                     phase = PH_HALF;
-                } else if (it < p.min_it || (it < p.max_it && dtmp >= (T)ms)) {
+                } else if (it < p.min_it || (it < itc && dtmp >= (T)ms)) {
                     if (MIXED) {
                         if (dtmp >= (T)p.hand_margin * (T)ms && !first) nb = 0;
                         else if (nb >= 0 && nb < p.hand_back) nb++;
@@ -525,6 +526,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_FINISH) k_finish(const __
         DEr r;
         r.de = 0.0;
         r.it = 0;
+        r.max_its = p.max_it;
         r.need64 = false;
         DEstate st;
         st.rout = st.rold = st.otrap = 0.0;
@@ -568,7 +570,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_FINISH) k_finish(const __
                 go = 1;
             } else if (phase == F_BISECT) {
                 dtmp = r.de;
-                if (r.it >= p.max_it) dt1 = -fabs(dt1);
+                if (r.it >= its_cap<FM>(p, r)) dt1 = -fabs(dt1);
                 else dt1 = (dtmp - (double)ms) < 0.0 ? fabs(dt1) * -0.55 : fabs(dt1) * 0.55;
                 go = 3;
             } else if (phase == F_BSI1) {
@@ -623,14 +625,14 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_FINISH) k_finish(const __
                 }
             }
             if (go == 1) {
-                if (!skip_half && r.it >= p.max_it) {
+                if (!skip_half && r.it >= its_cap<FM>(p, r)) {
                     double h1 = -0.5 * last_step;
                     mzz += h1;
                     add_w(c, vf, h1);
                     ms = de_stop_at(p, mzz);
                     last_step = -h1;
                     phase = F_HALF;
-                } else if (r.it < p.min_it || (r.it < p.max_it && dtmp >= (double)ms)) {
+                } else if (r.it < p.min_it || (r.it < its_cap<FM>(p, r) && dtmp >= (double)ms)) {
                     last_de = dtmp;
                     double d = fmax(0.11, (dtmp - (double)p.ms_de_sub * (double)ms) * (double)p.z_step_div * (double)rsf);
                     double s1 = (double)(fmaxf(ms, 0.4f) * p.mh04zsd);
@@ -657,7 +659,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_FINISH) k_finish(const __
             if (go == 2) {
                 // surface_found: the binary search on the DE or on the
                 // iteration count, then the normals
-                it_limited = !(r.it < p.max_it || dtmp < (double)ms);
+                it_limited = !(r.it < its_cap<FM>(p, r) || dtmp < (double)ms);
                 if (p.de_add_steps == 0) {
                     go = 4;
                 } else if (it_limited) {
@@ -873,6 +875,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_POST) k_post_start(const 
         DEr r;
         r.de = 0.0;
         r.it = 0;
+        r.max_its = p.max_it;
         r.need64 = false;
         DEstate st;
         st.smooth_it = 0.f;
@@ -892,7 +895,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_POST) k_post_start(const 
             const int bsi_steps = ao ? BSI_AO : BSI_SH;
             if (phase == Q_D0) {
                 if (!ao) {
-                    const bool limited = r.it < p.max_it || r.de < (double)ms;
+                    const bool limited = r.it < its_cap<FM>(p, r) || r.de < (double)ms;
                     if (!p64 && (r.need64 || !limited)) {
                         p64 = true;
                         snap = true;
@@ -907,7 +910,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_POST) k_post_start(const 
                     }
                 } else {
                     dcur = fmin(r.de, (double)ms * 2.0);
-                    const bool limited = r.it < p.max_it || dcur < (double)ms;
+                    const bool limited = r.it < its_cap<FM>(p, r) || dcur < (double)ms;
                     if (!p64 && (r.need64 || !limited)) {
                         p64 = true;
                         POST_BEGIN();
@@ -935,7 +938,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS_POST) k_post_start(const 
                 } else {
                     dcur = r.de;
                     if (phase == Q_BIS) {
-                        if (r.it >= p.max_it) dt1 = -fabs(dt1);
+                        if (r.it >= its_cap<FM>(p, r)) dt1 = -fabs(dt1);
                         else dt1 = (dcur - (double)ms) < 0.0 ? fabs(dt1) * -0.55 : fabs(dt1) * 0.55;
                         go = 1;
                     } else {
@@ -1140,7 +1143,7 @@ __global__ void __launch_bounds__(256, MB3D_MIN_BLOCKS) k_shadow_rays(const __gr
                     double r8 = (rr * rr) * (rr * rr);
                     zr = fminf(zr, (float)((dn - (double)ms) * (double)zrs_mul / (dmax - dt1 + 0.11) + r8 * r8));
                 }
-                if (r.it >= p.max_it || dn <= (double)ms) {
+                if (r.it >= its_cap<FM>(p, r) || dn <= (double)ms) {
                     end = true;  // a surface in the way
                     shadowed = dt1 > 0.0;
                 } else {

@@ -106,6 +106,9 @@ struct It64 {
     double rout, rold, otrap, rstop;
     int it_result, max_it;
     bool calc_sit;
+    // the second part of a DE combination is set (set_part, src/calc.rs:1476-1489):
+    // its slot range and DE option (only the all-formula kernels meet one)
+    bool part2;
     float smooth_it;
 
     __device__ void smooth_iterations(const DevParams &p, int n) {  // CalcSmoothIterations
@@ -122,8 +125,15 @@ struct It64 {
     }
     // run_with (src/iteration.rs:268-313)
     __device__ int run(const DevParams &p) {
-        int n = 0;
-        int btmp = p.slots[0].iterations;
+        int n = 0, end = p.end_to, rep = p.repeat_from;
+        if constexpr (FM == FKIND_ALL) {
+            if (part2) {
+                n = p.dc_start2;
+                end = p.dc_end2;
+                rep = p.dc_rep2;
+            }
+        }
+        int btmp = p.slots[n].iterations;
         it_result = 0;
         unsigned int unc_guard = 0;
         for (;;) {
@@ -131,7 +141,7 @@ struct It64 {
             int guard = 0;
             while (btmp <= 0) {
                 n += 1;
-                if (n > p.end_to) n = p.repeat_from;
+                if (n > end) n = rep;
                 btmp = p.slots[n].iterations;
                 if (++guard > 64) return n;
             }
@@ -221,14 +231,127 @@ struct It64 {
                 return r;
             }
         }
-        v[3] = ((p.de_option & 0x38) == 16) ? rout : 1.0;
+        int deo = p.de_option;
+        if constexpr (FM == FKIND_ALL) deo = part2 ? p.dc_de_option2 : deo;
+        v[3] = ((deo & 0x38) == 16) ? rout : 1.0;
         int n = run(p);
         double w = v[3];
-        double r = ((p.de_option & 7) == 4) ? fabs(v[1]) * log(fabs(v[1])) / w : sqrt(rout) / fabs(w);
+        double r = ((deo & 7) == 4) ? fabs(v[1]) * log(fabs(v[1])) / w : sqrt(rout) / fabs(w);
         if (calc_sit) smooth_iterations(p, n);
         return r;
     }
 };
+
+// calc_de_part (src/calc.rs:1495-1557) of the part the record is set to,
+// outside rendering: the analytic DE or the numerical one (the offsets'
+// runs to the centre's iteration count), at least a quarter of the DE stop;
+// `max_its` takes the iteration limit of the part (max_its_result)
+template <int FM>
+__device__ __forceinline__ double de_part(const DevParams &p, It64<FM> &it, float ms_de_stop, bool custom,
+                                          float d_de_scale, int &max_its) {
+    double result;
+    if (custom) {
+        result = it.hybrid_3d_de(p) * (double)d_de_scale;
+    } else {
+        it.hybrid_3d(p);
+        if (it.rout < 1e-200) {
+            result = 0.0;
+        } else {
+            const bool bsit = it.calc_sit;
+            const int bmax = it.max_it;
+            const double brout = it.rout;
+            it.calc_sit = false;
+            it.max_it = it.it_result;
+            it.rstop = p.rstop3d;
+            double g = 0.0;
+            for (int k = 0; k < 3; k++) {
+                const double b = it.c[k];
+                it.c[k] = b + (double)p.de_offset;
+                it.hybrid_3d(p);
+                g += (brout - it.rout) * (brout - it.rout);
+                it.c[k] = b;
+            }
+            result = brout * log(brout) * (double)d_de_scale / (sqrt(g) + (double)p.de_offset006);
+            it.rout = brout;
+            it.it_result = it.max_it;
+            it.max_it = bmax;
+            it.calc_sit = bsit;
+            it.rstop = p.d_rstop;
+        }
+    }
+    max_its = it.max_it;
+    const double mn = (double)ms_de_stop * 0.25;
+    if (result < mn || isnan(result)) result = mn;
+    return result;
+}
+
+// A DE combination (CalcDEfull with FormulaType > 0, src/calc.rs:1369-1455):
+// part 1's distance, then part 2's in its own place (PrepareF1DEcomb and
+// set_part), combined by min, max, max of the inverted part 2 or one of
+// the smooth minima; the colour values and the iteration limit are the
+// ruling part's (the smooth minima blend the colour values by distance).
+// Part 1's iteration limit holds afterwards (RestoreF1DEcomb: it.max_it is
+// the scene's again, which the iteration count search reads back).
+template <int FM>
+__device__ __noinline__ double de_comb(const DevParams &p, It64<FM> &it, float ms_de_stop, int &max_its) {
+    it.part2 = false;
+    double result = de_part<FM>(p, it, ms_de_stop, p.is_custom_de != 0, p.d_de_scale, max_its);
+    const int b_it = it.it_result, b_max = max_its;
+    const double b_otrap = it.otrap;
+    const float b_sit = it.smooth_it;
+    it.part2 = true;
+    it.max_it = p.dc_max_it2;
+    const double c0[3] = {it.c[0], it.c[1], it.c[2]};
+    if (p.dc_place) {
+        const double d[3] = {c0[0] - p.dc_offset[0], c0[1] - p.dc_offset[1], c0[2] - p.dc_offset[2]};
+        for (int i = 0; i < 3; i++) it.c[i] = p.dc_m[i][0] * d[0] + p.dc_m[i][1] * d[1] + p.dc_m[i][2] * d[2];
+    }
+    const int kind = p.dc_kind;
+    const double ms = (double)ms_de_stop;
+    double rst = de_part<FM>(p, it, ms_de_stop, p.dc_custom2 != 0, p.dc_d_de_scale2, max_its);
+    if (kind == 3) {  // the part "inside" (bCalcInside)
+        rst = ms * 4.0 - rst * 3.0;
+        if (rst >= ms) it.it_result -= 1;
+    }
+    if (p.dc_place) {
+        rst *= p.dc_scale;
+        for (int i = 0; i < 3; i++) it.c[i] = c0[i];
+    }
+    bool restore = false;
+    if (kind == 1) {
+        if (rst >= result) restore = true;
+        else result = rst;
+    } else if (kind == 2 || kind == 3) {
+        if (rst > result) result = rst;
+        else restore = true;
+    } else {  // 4, 5: smooth minima
+        if (!(rst < result)) {
+            it.it_result = b_it;
+            max_its = b_max;
+        }
+        const double sm = p.dc_smooth;
+        if (kind == 4) {
+            result = fmin(rst - fmax(sm - result, 0.0), result - fmax(sm - rst, 0.0));
+        } else {
+            const double rd1 = fmax(sm - result - ms, 0.0);
+            const double d2 = fmax(sm - rst - ms, 0.0);
+            result = fmin(rst - rd1 * (sm - d2) / sm, result - d2 * (sm - rd1) / sm);
+        }
+        const double r2 = fabs(rst), w = fabs(result);
+        const double f = 1.0 / (w + r2 + 1e-10);
+        it.smooth_it = (float)(((double)it.smooth_it * w + (double)b_sit * r2) * f);
+        it.otrap = (it.otrap * w + b_otrap * r2) * f;
+    }
+    if (restore) {
+        it.it_result = b_it;
+        it.smooth_it = b_sit;
+        it.otrap = b_otrap;
+        max_its = b_max;
+    }
+    it.part2 = false;
+    it.max_it = p.max_it;
+    return result;
+}
 
 template <int FM>
 struct M64 {
@@ -247,6 +370,7 @@ struct M64 {
         it.max_it = p.max_it;
         it.rstop = p.d_rstop;
         it.calc_sit = false;
+        it.part2 = false;
         it.rout = it.rold = it.otrap = 0.0;
         it.smooth_it = 0.f;
         it.it_result = 0;
@@ -260,6 +384,9 @@ struct M64 {
 
     // calc_de -> calc_de_part (src/calc.rs:1333-1557), one hybrid part
     __device__ double calc_de() {
+        if constexpr (FM == FKIND_ALL) {
+            if (p.dc_kind) return de_comb<FM>(p, it, ms_de_stop, max_its_result);
+        }
         double result;
         if (p.is_custom_de) {
             result = it.hybrid_3d_de(p) * (double)p.d_de_scale;

@@ -413,7 +413,7 @@ struct McRun {
             }
             case W_M0:
                 L.dtmp = r.de;
-                if (L.probe && (r.it >= p.max_it || r.de < (double)L.ms)) {
+                if (L.probe && (r.it >= r.max_its || r.de < (double)L.ms)) {
                     // the start is inside the set
                     if (BATCH) {
                         uint16_t sg = 0, ot = 0;
@@ -469,7 +469,7 @@ struct McRun {
             case W_MSTEP:
                 L.dtmp = r.de;
                 L.it_last = r.it;
-                if (r.it >= p.max_it) {
+                if (r.it >= r.max_its) {
                     // doBinSearchIt on the iteration-limited surface
                     L.de_limited = false;
                     L.bzz0 = L.zz;
@@ -812,7 +812,7 @@ struct McRun {
             }
             case W_SSTEP:
                 L.dtmp = r.de;
-                if (r.it >= p.max_it || !(L.dtmp >= (double)L.ms) || !(L.dtmp < 1e30)) {
+                if (r.it >= r.max_its || !(L.dtmp >= (double)L.ms) || !(L.dtmp < 1e30)) {
                     L.phase = L_SDONE;
                     break;
                 }
@@ -954,6 +954,7 @@ __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_con
     DEr r;
     r.de = 0.0;
     r.it = 0;
+    r.max_its = p.max_it;
     r.need64 = false;
     DEstate st;
     st.rout = 0.0; st.rold = 0.0; st.otrap = 0.0;
@@ -1050,6 +1051,7 @@ __global__ void __launch_bounds__(128) k_mc_logic(const __grid_constant__ DevPar
     DEr r;
     r.de = 0.0;
     r.it = 0;
+    r.max_its = p.max_it;
     r.need64 = false;
     DEstate st;
     st.rout = 0.0; st.rold = 0.0; st.otrap = 0.0;

@@ -52,10 +52,11 @@ static bool f_known(int f) {
            f == MB3D_CU_F_QUATERNION || f == MB3D_CU_F_AEXIONC;
 }
 
-// CheckFormulaOptions (src/calc.rs:315-372)
-static int de_option_of(const int *des, const int *its, int n) {
+// CheckFormulaOptions (combine_de_options_range, src/calc.rs:315-372): the
+// DE option of slots start..end
+static int de_option_of(const int *des, const int *its, int start, int end) {
     int opt = -1;
-    for (int x = 0; x < n; x++) {
+    for (int x = start; x <= end; x++) {
         if (its[x] == 0) continue;
         int de = des[x];
         if (de < 0 || de == opt) continue;
@@ -193,9 +194,18 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     while (last > 0 && its[last] == 0) last--;
     int nsl = last + 1;
     int end_to = last;
+    // a DE combination (src/calc.rs:421-431): part 1 ends at decomb_end1
+    // when both parts have slots; none in an interpolation hybrid
+    if (sc.decomb < 0 || sc.decomb > 6) {
+        err = "decomb must be 0..6";
+        return MB3D_CU_EINVAL;
+    }
+    auto slot_of = [](int v) { return std::min(std::max(v, 0), 5); };
+    const bool dc = !ipol && sc.decomb != 0 && slot_of(sc.decomb_end1) < last && slot_of(sc.decomb_start2) <= last;
+    if (dc) end_to = slot_of(sc.decomb_end1);
     int rep = std::min(std::max(sc.repeat_from, 0), end_to);
     while (rep > 0 && its[rep] <= 0) rep--;
-    int de_option = de_option_of(des, its, nsl);
+    int de_option = de_option_of(des, its, 0, end_to);
     if (sc.disable_analytic_de) {
         if (de_option == 2 || de_option == 11) de_option = 0;
         else if (de_option == 5 || de_option == 6) de_option = 4;
@@ -219,14 +229,53 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
         return MB3D_CU_ENOTSUP;
     }
     bool custom = de_option == 2 || de_option == 5 || de_option == 6 || de_option == 11 || de_option == 20;
+    // the second part of a DE combination (src/calc.rs:491-520; the card
+    // has no dIFS formulas, options 20 and up)
+    int s2 = 0, e2 = 0, rep2 = 0, de2 = -1;
+    if (dc) {
+        s2 = std::min(slot_of(sc.decomb_start2), last);
+        e2 = std::min(std::max(slot_of(sc.decomb_end2), s2), last);
+        de2 = de_option_of(des, its, s2, e2);
+        if (sc.disable_analytic_de) {
+            if (de2 == 2 || de2 == 11) de2 = 0;
+            else if (de2 == 5 || de2 == 6) de2 = 4;
+        }
+        if (de2 < 0) {
+            err = "DE combination: the second formula part has no valid DE option";
+            return MB3D_CU_EINVAL;
+        }
+        if (sc.decomb == 6 && de2 != 20) {
+            err = "DE combination 'mix': the second hybrid part must be dIFS";
+            return MB3D_CU_EINVAL;
+        }
+        if (four_d || (de2 >= 4 && de2 <= 6)) {
+            err = "4D hybrids in a DE combination are not built into this backend";
+            return MB3D_CU_ENOTSUP;
+        }
+        rep2 = std::min(std::max(slot_of(sc.decomb_repeat2), s2), e2);
+        while (rep2 > s2 && its[rep2] <= 0) rep2--;
+    }
+    const bool custom2 = dc && (de2 == 2 || de2 == 5 || de2 == 6 || de2 == 11 || de2 == 20);
     for (int i = 0; i < nsl; i++) unc[i] = unc[i] || des[i] < 0 || des[i] > 20;
 
     // DE scale, colour helpers and the smooth iteration logs
+    const bool custom_p1 = custom;
     float fhln[6];
     for (int k = 0; k < 6; k++) fhln[k] = (float)(1.0 / std::log(2.0));
     double cnt_n = 0, sum_x = 0, sum_y = 0, cnt_i = 0;
+    // (a DE combination: part 1's scale is taken at part 2's first slot and
+    // the sums start again)
+    bool have_p1 = false;
+    double dde_p1 = 1.0;
     for (int x = 0; x < nsl; x++) {
         if (its[x] == 0) continue;
+        const bool second = dc && x > end_to;
+        if (second && !have_p1) {
+            dde_p1 = (cnt_n > 0.0 && de_option != 20) ? sum_x / cnt_n : 1.0;
+            have_p1 = true;
+            cnt_n = sum_x = sum_y = cnt_i = 0.0;
+        }
+        const bool custom = second ? custom2 : custom_p1;
         const mb3d_cu_slot &s = sc.slots[x];
         if (ipol || !unc[x]) {
             double sip = f_si_pow(s);
@@ -249,19 +298,33 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
             sum_x += (custom ? 1.0 : f_de_scale(fs[x])) * w;
         }
     }
-    double dde = 1.0;
+    double dde = 1.0, dde2 = 1.0;
     float col_plus = 0.f;
-    if (cnt_n > 0.0 && de_option != 20) dde = ipol ? sum_x : sum_x / cnt_n;
+    if (have_p1) {
+        dde = dde_p1;
+        if (cnt_n > 0.0 && de2 != 20) dde2 = sum_x / cnt_n;
+    } else if (cnt_n > 0.0 && de_option != 20) {
+        dde = ipol ? sum_x : sum_x / cnt_n;
+    }
     if (cnt_n > 0.0 && cnt_i > 0.0) col_plus = (float)(std::pow(std::fabs(sum_y / cnt_i), 0.25) * 40.0 - 49.0);
-    // mctColVarDEstopMul (src/calc.rs:591-652), one hybrid part
+    // mctColVarDEstopMul (src/calc.rs:591-652): of the first part, or of a
+    // DE combination's part with more iterations
     float col_var = 0.6f;
     {
-        double a = 0, b = 0;
+        double a = 0, b = 0, b1 = 0;
         int ia = 0, itmp = 0;
+        bool second = false;
         for (int x = 0; x < nsl; x++) {
             if (!(ipol || (its[x] > 0 && !unc[x]))) {
                 if (its[x] > 0) (x > end_to ? ia : itmp)++;
                 continue;
+            }
+            if (x > end_to && !second) {
+                second = true;
+                col_var = b > 0.0 ? (float)(a / b) : 0.6f;
+                b1 = b;
+                a = b = 0.0;
+                if (!dc || de2 == 20) break;
             }
             double w = ipol ? (double)ipw[x] : (double)its[x];
             int de = des[x];
@@ -281,8 +344,8 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
                 }
             }
         }
-        if ((b >= 0.0 && b > 1e-3) || (ia > itmp && std::fabs(b) < 1e-3 && b > 1e-3)) col_var = (float)(a / b);
-        else col_var = 0.6f;
+        if ((b >= b1 && b > 1e-3) || (ia > itmp && std::fabs(b - b1) < 1e-3 && b > 1e-3)) col_var = (float)(a / b);
+        else if (b1 < 1e-3) col_var = 0.6f;
     }
     double rstop = sc.rstop;
     if (!(rstop > 0.0)) {
@@ -326,6 +389,7 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
         p.ystart[k] = sc.mid[k] + z1 * p.vgrads[2][k] - (H * 0.5) * p.vgrads[1][k] - (W * 0.5) * p.vgrads[0][k];
     float de_off = std::fmin(de_stop * 0.1f, 0.004f);
     p.d_de_scale = custom ? (float)((double)(float)dde / sw) : (float)dde * de_off;
+    p.dc_d_de_scale2 = custom2 ? (float)((double)(float)dde2 / sw) : (float)dde2 * de_off;
     p.de_offset006 = de_off * 0.06f;
     p.de_offset = (float)((double)de_off * sw);
     p.z_step_div = zsd0;
@@ -340,8 +404,11 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     p.rstop3d = (double)(float)((p.d_rstop * p.d_rstop) * 64.0);
     p.d_rstop_f = (float)p.d_rstop;
     p.rstop3d_f = (float)p.rstop3d;
-    p.mcts_m = 32767.0f / (float)std::max(sc.iterations + 1, 1);
-    p.d_col_plus = col_plus + (float)sc.iterations * 0.1f;
+    // the iterations of both parts of a DE combination (iMaxitF2)
+    const int it2 = sc.decomb_iterations2 > 0 ? sc.decomb_iterations2 : sc.iterations;
+    const int its_all = !dc ? sc.iterations : sc.decomb > 5 ? sc.iterations + it2 : std::max(sc.iterations, it2);
+    p.mcts_m = 32767.0f / (float)std::max(its_all + 1, 1);
+    p.d_col_plus = col_plus + (float)its_all * 0.1f;
     p.col_var = col_var;
     p.mct_color_mul = (float)(sc.color_mul * 512.0);
     p.de_stop = de_stop;
@@ -359,7 +426,7 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     p.color_option = std::min(sc.color_option, 5);
     p.color_on_it = sc.color_on_it;
     p.dfog_on_it = sc.dfog_on_it;
-    p.normals_on_de = (sc.normals_on_de || custom) ? 1 : 0;
+    p.normals_on_de = (sc.normals_on_de || custom || dc) ? 1 : 0;
     p.first_step_random = sc.first_step_random ? 1 : 0;
     p.do_julia = sc.julia ? 1 : 0;
     p.width = sc.width;
@@ -374,7 +441,7 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
         d.formula = fs[i];
         d.iterations = its[i];
         d.uncounted = unc[i];
-        d.ade = custom;
+        d.ade = (dc && i > end_to) ? custom2 : custom;
         d.julia_add = sc.julia && fs[i] == MB3D_CU_F_MENGERIFS;
         d.ipow = f_ipow(sc.slots[i]);
         switch (fs[i]) {
@@ -422,7 +489,41 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     // only on the sequential record)
     for (int i = 0; i < nsl; i++)
         quat = quat || ((fs[i] == MB3D_CU_F_QUATERNION || fs[i] == MB3D_CU_F_AEXIONC) && its[i] > 0);
-    p.seq_de = (ipol || four_d || quat) ? 1 : 0;
+    // the DE combination's second part (DeComb, src/calc.rs:730-760): its
+    // place turns the point into the part's own space, m * (p - offset)
+    // with m the rotation divided by the size, and scales its distances
+    if (dc) {
+        p.dc_kind = sc.decomb;
+        p.dc_start2 = s2;
+        p.dc_end2 = e2;
+        p.dc_rep2 = rep2;
+        p.dc_max_it2 = std::max(it2, 1);
+        p.dc_de_option2 = de2;
+        p.dc_custom2 = custom2 ? 1 : 0;
+        p.dc_smooth = (double)std::max(sc.decomb_smooth, 1e-30f) / sw;
+        const double scale = sc.part2_scale > 0.0 ? sc.part2_scale : 1.0;
+        const double *o = sc.part2_offset, *r = sc.part2_rotation;
+        const bool placed = o[0] != 0.0 || o[1] != 0.0 || o[2] != 0.0 || r[0] != 0.0 || r[1] != 0.0 || r[2] != 0.0 ||
+                            scale != 1.0;
+        p.dc_place = (placed && sc.decomb != 6) ? 1 : 0;
+        if (p.dc_place) {
+            // build_rot_matrix (src/math.rs:466-475), rows to length 1 / scale
+            const double sx = std::sin(deg2rad(r[0])), cx = std::cos(deg2rad(r[0]));
+            const double sy = std::sin(deg2rad(r[1])), cy = std::cos(deg2rad(r[1]));
+            const double sz = std::sin(deg2rad(r[2])), cz = std::cos(deg2rad(r[2]));
+            const double m[3][3] = {{cy * cz, -cy * sz, sy},
+                                    {sx * sy * cz + cx * sz, cx * cz - sx * sy * sz, -sx * cy},
+                                    {sx * sz - cx * sy * cz, cx * sy * sz + sx * cz, cx * cy}};
+            const double len = 1.0 / std::fmax(scale, 1e-300);
+            for (int i = 0; i < 3; i++) {
+                const double d = len / std::sqrt(m[i][0] * m[i][0] + m[i][1] * m[i][1] + m[i][2] * m[i][2]);
+                for (int k = 0; k < 3; k++) p.dc_m[i][k] = m[i][k] * d;
+                p.dc_offset[i] = o[i];
+            }
+            p.dc_scale = scale;
+        }
+    }
+    p.seq_de = (ipol || four_d || quat || dc) ? 1 : 0;
     if (p.seq_de) {
         p.all_fp64 = 1;
         p.sched = SCHED_GENERIC;
@@ -431,7 +532,9 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
     p.coord_eps = coord * eps32;
     p.hand_margin = 4.0f;
     p.hand_back = 2;
-    p.finish_slow = (p.sm_normals > 0 || !p.normals_on_de || p.color_on_it != 0) ? 1 : 0;
+    // (a DE combination's surfaces too: the FP64 marcher keeps the ruling
+    // part's iteration limit between its DEs, as the reference's marcher)
+    p.finish_slow = (p.sm_normals > 0 || !p.normals_on_de || p.color_on_it != 0 || dc) ? 1 : 0;
     // (measured on the 1920x1080 hybrid frame: the march and its finish are
     // fastest when a warp takes new rays only once all of its lanes are idle
     // -- rays that start together iterate alike -- the shadow and DE AO rays

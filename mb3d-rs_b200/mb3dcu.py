@@ -63,6 +63,11 @@ class Scene(ctypes.Structure):
         ("deao_max_len", ctypes.c_float), ("deao_first_step_random", ctypes.c_int32),
         ("interpolation", ctypes.c_int32), ("ipol_weights", ctypes.c_float * 2), ("pad1", ctypes.c_int32),
         ("rot_4d", ctypes.c_double * 3),
+        ("decomb", ctypes.c_int32), ("decomb_end1", ctypes.c_int32), ("decomb_start2", ctypes.c_int32),
+        ("decomb_end2", ctypes.c_int32), ("decomb_repeat2", ctypes.c_int32), ("decomb_iterations2", ctypes.c_int32),
+        ("decomb_smooth", ctypes.c_float), ("decomb_mix_pow", ctypes.c_float), ("decomb_mix_color", ctypes.c_int32),
+        ("pad2", ctypes.c_int32), ("part2_offset", ctypes.c_double * 3), ("part2_rotation", ctypes.c_double * 3),
+        ("part2_scale", ctypes.c_double),
     ]
 
 

@@ -141,6 +141,43 @@ def interpolated(first, second, weights, width=None, height=None):
     return sc
 
 
+DECOMB_KINDS = {"min": 1, "max": 2, "max_inverted": 3, "smooth_linear": 4, "smooth": 5}
+
+
+def two_objects(kind="min", width=160, height=120, place=True, smooth=0.5):
+    """A DE combination (Scene::decomb): a Mandelbulb (Integer Power 8) as
+    part 1 and an Amazing Box as part 2, the box moved to x = 3.2, turned by
+    20 and 30 degrees and scaled to 0.4, with the camera on both -- the
+    reference's own scene of two objects (tests/data/two_objects.m3s:
+    de_combination, decomb_*, part2_*, mid, zoom, z_start, rotation, de_stop,
+    raystep, smooth_normals, bin_search).  `place` False leaves the box at
+    the origin over the bulb, scaled to 0.12 (about the bulb's size), with
+    the camera closer: the scene for the combinations that need both objects
+    in one place."""
+    sc = default_scene()
+    sc.width, sc.height = width, height
+    sc.iterations = 30
+    sc.zoom, sc.z_start, sc.z_end = (0.55 if place else 1.2), -10.0, 30.0
+    sc.mid[0], sc.mid[1], sc.mid[2] = (1.6 if place else 0.0), 0.0, 0.0
+    set_vgrads(sc, vgrads_from_angles(math.radians(-30.0), math.radians(20.0), 0.0))
+    sc.de_stop, sc.z_step_div = 0.8, 0.4
+    sc.smooth_normals, sc.bin_search_steps = 3, 8
+    set_slots(sc, [intpow(8, -1.0), amazing_box(2.0, 0.5, 1.0)])
+    sc.decomb = DECOMB_KINDS[kind]
+    sc.decomb_end1, sc.decomb_start2, sc.decomb_end2, sc.decomb_repeat2 = 0, 1, 1, 1
+    sc.decomb_iterations2 = 30
+    sc.decomb_smooth, sc.decomb_mix_pow = smooth, 2.0
+    if place:
+        for k, v in enumerate((3.2, 0.0, 0.0)):
+            sc.part2_offset[k] = v
+        for k, v in enumerate((20.0, 30.0, 0.0)):
+            sc.part2_rotation[k] = v
+        sc.part2_scale = 0.4
+    else:
+        sc.part2_scale = 0.12
+    return sc
+
+
 def splitmix64(state):
     state = (state + 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF
     z = state

@@ -372,10 +372,11 @@ bool formula_from_slot(const mb3d_cu_slot &s, Formula &f, std::string &err) {
 }
 
 // ---------------------------------------------------------------------------
-// CheckFormulaOptions (src/calc.rs:311-372)
-static int combine_de_options(const std::vector<Slot> &slots, int end_to) {
+// CheckFormulaOptions (combine_de_options_range, src/calc.rs:311-372): the
+// DE option of slots start..end_to
+static int combine_de_options(const std::vector<Slot> &slots, int end_to, int start = 0) {
     int de_option = -1;
-    for (int x = 0; x <= end_to && x < (int)slots.size(); x++) {
+    for (int x = start; x <= end_to && x < (int)slots.size(); x++) {
         const Slot &s = slots[x];
         if (s.iterations == 0) continue;
         int de = s.f.de_option();
@@ -512,7 +513,12 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     int last = (int)slots.size() - 1;
     while (last > 0 && slots[last].iterations == 0) last--;
     slots.resize(last + 1);
-    int end_to = last;
+    // a DE combination (src/calc.rs:421-431): slots 0-based, clamped to 0..5
+    // as the scene text's are; none in an interpolation hybrid
+    if (sc.decomb < 0 || sc.decomb > 6) { err = "decomb must be 0..6"; return false; }
+    auto slot_of = [](int v) { return std::min(std::max(v, 0), 5); };
+    const bool dc = !ipol && sc.decomb != 0 && slot_of(sc.decomb_end1) < last && slot_of(sc.decomb_start2) <= last;
+    int end_to = dc ? std::min(slot_of(sc.decomb_end1), last) : last;
     int repeat_from = std::min(std::max(sc.repeat_from, 0), end_to);
     while (repeat_from > 0 && slots[repeat_from].iterations <= 0) repeat_from--;
     int de_option = combine_de_options(slots, end_to);
@@ -532,8 +538,27 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     if (four_d && de_option != 4) { err = "4D hybrids with the analytic DE are not supported"; return false; }
 
     bool is_custom_de = de_option == 2 || de_option == 5 || de_option == 6 || de_option == 11 || de_option == 20;
-    for (auto &s : slots) {
-        s.ade = is_custom_de;
+    // the second part of a DE combination (src/calc.rs:491-520); no formula
+    // of this restatement is a dIFS one
+    int start2 = 0, end2 = 0, rep2 = 0, de2 = -1;
+    if (dc) {
+        start2 = std::min(slot_of(sc.decomb_start2), last);
+        end2 = std::min(std::max(slot_of(sc.decomb_end2), start2), last);
+        de2 = combine_de_options(slots, end2, start2);
+        if (sc.disable_analytic_de) {
+            if (de2 == 2 || de2 == 11) de2 = 0;
+            else if (de2 == 5 || de2 == 6) de2 = 4;
+        }
+        if (de2 < 0) { err = "DE combination: the second formula part has no valid DE option"; return false; }
+        if (sc.decomb == 6 && de2 != 20) { err = "DE combination 'mix': the second hybrid part must be dIFS"; return false; }
+        if (four_d || (de2 >= 4 && de2 <= 6)) { err = "4D hybrids in a DE combination are not restated"; return false; }
+        rep2 = std::min(std::max(slot_of(sc.decomb_repeat2), start2), end2);
+        while (rep2 > start2 && slots[rep2].iterations <= 0) rep2--;
+    }
+    const bool is_custom_de2 = dc && (de2 == 2 || de2 == 5 || de2 == 6 || de2 == 11 || de2 == 20);
+    for (size_t x = 0; x < slots.size(); x++) {
+        Slot &s = slots[x];
+        s.ade = (dc && (int)x > end_to) ? is_custom_de2 : is_custom_de;
         int de = s.f.de_option();
         s.uncounted = s.uncounted || de < 0 || de > 20;
     }
@@ -541,9 +566,18 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     float fhln[6];
     for (int k = 0; k < 6; k++) fhln[k] = (float)(1.0 / std::log(2.0));
     double nn = 0, x1 = 0, y1 = 0, ii = 0;
+    bool have_p1 = false;
+    double p1_scale = 1.0;  // part 1's d_de_scale in a DE combination
     for (size_t x = 0; x < slots.size(); x++) {
         const Slot &s = slots[x];
         if (s.iterations == 0) continue;
+        const bool second = dc && (int)x > end_to;
+        if (second && !have_p1) {
+            p1_scale = (nn > 0.0 && de_option != 20) ? x1 / nn : 1.0;
+            have_p1 = true;
+            nn = x1 = y1 = ii = 0.0;
+        }
+        const bool is_custom_de_x = second ? is_custom_de2 : is_custom_de;
         if (ipol || !s.uncounted) {
             double sip = s.f.si_pow();
             double z1 = sip > 1.0 ? sip : s.f.first_option();
@@ -552,7 +586,7 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
         // (an interpolation hybrid: weighted by the weights, counted once)
         double z1 = ipol ? (double)ipw[x] : (double)s.iterations, cnt = ipol ? 1.0 : (double)s.iterations;
         int j = s.f.de_option();
-        if (is_custom_de && (ipol || !s.uncounted) && (j == 5 || j == 11)) {
+        if (is_custom_de_x && (ipol || !s.uncounted) && (j == 5 || j == 11)) {
             nn += cnt;
             ii += cnt;
             double x2 = s.f.first_option();
@@ -562,27 +596,41 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
             y1 += std::fabs(x2) * z1;
         } else if (j >= 0 || ipol) {
             nn += cnt;
-            x1 += (is_custom_de ? s.f.ade_scale() : s.f.de_scale()) * z1;
+            x1 += (is_custom_de_x ? s.f.ade_scale() : s.f.de_scale()) * z1;
         }
     }
     float d_col_plus = 0.f;
-    double d_de_scale = 1.0;
-    if (nn > 0.0 && de_option != 20) d_de_scale = ipol ? x1 : x1 / nn;
+    double d_de_scale = 1.0, d_de_scale2 = 1.0;
+    if (have_p1) {
+        d_de_scale = p1_scale;
+        if (nn > 0.0 && de2 != 20) d_de_scale2 = x1 / nn;
+    } else if (nn > 0.0 && de_option != 20) {
+        d_de_scale = ipol ? x1 : x1 / nn;
+    }
     if (nn > 0.0 && ii > 0.0) d_col_plus = (float)(std::pow(std::fabs(y1 / ii), 0.25) * 40.0 - 49.0);
     // mctColVarDEstopMul (src/calc.rs:591-652)
     float col_var = 0.6f;
     {
         double yy1 = 0, z1 = 0, z2 = 0;
         int ia = 0, itmp = 0;
+        bool second = false;
         for (size_t x = 0; x < slots.size(); x++) {
             const Slot &s = slots[x];
             bool counted = ipol || (s.iterations > 0 && !s.uncounted);
             if (!counted) {
-                if (s.iterations > 0) {
+                if (!ipol && s.iterations > 0) {
                     if ((int)x > end_to) ia++;
                     else itmp++;
                 }
                 continue;
+            }
+            if ((int)x > end_to && !second) {
+                second = true;
+                col_var = z1 > 0.0 ? (float)(yy1 / z1) : 0.6f;
+                z2 = z1;
+                z1 = 0.0;
+                yy1 = 0.0;
+                if (!dc || de2 == 20) break;
             }
             double x2 = ipol ? (double)ipw[x] : (double)s.iterations;
             int de = s.f.de_option();
@@ -643,6 +691,7 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     for (int k = 0; k < 3; k++) p.ystart[k] = sc.mid[k] + z1 * vg[2][k] - yh * vg[1][k] - xh * vg[0][k];
     float de_offset = rminf(de_stop * 0.1f, 0.004f);
     float dds = is_custom_de ? (float)((double)(float)d_de_scale / step_width) : (float)d_de_scale * de_offset;
+    float dds2 = is_custom_de2 ? (float)((double)(float)d_de_scale2 / step_width) : (float)d_de_scale2 * de_offset;
     float de_offset006 = de_offset * 0.06f;
     de_offset = (float)((double)de_offset * step_width);
     float z_step_div = z_step_div0, ms_de_sub = 0.f;
@@ -655,7 +704,9 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     float ln_rstop = (float)std::log(std::log(rstop));
     double d_rstop = (double)(float)(rstop * rstop);
     double rstop3d = (double)(float)((d_rstop * d_rstop) * 64.0);
-    int its = max_it;
+    // the iterations of both parts of a DE combination (iMaxitF2)
+    const int iterations2 = sc.decomb_iterations2 > 0 ? sc.decomb_iterations2 : sc.iterations;
+    int its = !dc ? max_it : sc.decomb > 5 ? max_it + iterations2 : std::max(max_it, iterations2);
     float mcts_m = 32767.0f / (float)std::max(its + 1, 1);
     d_col_plus = d_col_plus + (float)its * 0.1f;
 
@@ -694,7 +745,7 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     p.mh04zsd = mh04zsd;
     p.de_stop_factor = de_stop_factor;
     p.ln_rstop = ln_rstop;
-    p.normals_on_de = sc.normals_on_de || is_custom_de;
+    p.normals_on_de = sc.normals_on_de || is_custom_de || dc;
     p.de_offset = de_offset;
     p.de_offset006 = de_offset006;
     p.mcts_m = mcts_m;
@@ -707,6 +758,37 @@ bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err) {
     p.ipol_w[1] = ipw[1];
     p.four_d = four_d;
     build_smatrix4(sc.rot_4d[0], sc.rot_4d[1], sc.rot_4d[2], p.smatrix4);
+    // the DeComb (src/calc.rs:730-760) and its part 2's place: the rotation
+    // (build_rot_matrix, src/math.rs:466-475) with rows 1 / scale long; a
+    // placement of all defaults (part2_scale 0 reads as 1) is none
+    p.dc_kind = dc ? sc.decomb : 0;
+    if (dc) {
+        DeCombPart &q = p.dc_part2;
+        q.start = start2;
+        q.end = end2;
+        q.repeat = rep2;
+        q.de_option = de2;
+        q.is_custom_de = is_custom_de2;
+        q.d_de_scale = dds2;
+        q.max_it = std::max(iterations2, 1);
+        p.dc_smooth = (double)rmaxf(sc.decomb_smooth, 1e-30f) / step_width;
+        const double scale = sc.part2_scale > 0.0 ? sc.part2_scale : 1.0;
+        const double *o = sc.part2_offset, *r = sc.part2_rotation;
+        const bool placed = o[0] != 0.0 || o[1] != 0.0 || o[2] != 0.0 || r[0] != 0.0 || r[1] != 0.0 || r[2] != 0.0 ||
+                            scale != 1.0;
+        p.dc_place = placed && sc.decomb != 6;
+        if (p.dc_place) {
+            double sx = std::sin(to_radians(r[0])), cx = std::cos(to_radians(r[0]));
+            double sy = std::sin(to_radians(r[1])), cy = std::cos(to_radians(r[1]));
+            double sz = std::sin(to_radians(r[2])), cz = std::cos(to_radians(r[2]));
+            Mat3 m = {{cy * cz, -cy * sz, sy},
+                      {sx * sy * cz + cx * sz, cx * cz - sx * sy * sz, -sx * cy},
+                      {sx * sz - cx * sy * cz, cx * sy * sz + sx * cz, cx * cy}};
+            normalise_matrix_to(1.0 / rmax(scale, 1e-300), m, p.dc_m);
+            for (int k = 0; k < 3; k++) p.dc_offset[k] = o[k];
+            p.dc_scale = scale;
+        }
+    }
     return true;
 }
 
@@ -729,7 +811,7 @@ void Iteration::smooth_iterations(int n) {
 
 // run_with (src/iteration.rs:268-313)
 int Iteration::run(const std::vector<Slot> &slots) {
-    int n = 0;
+    int n = start_from;
     int btmp = std::max(slots[n].iterations, 0);
     it_result = 0;
     uint32_t uncounted_guard = 0;
@@ -920,13 +1002,88 @@ Marcher::Marcher(const Params *pp, int32_t s) : p(pp), seed(s) {
     max_its_result = p->max_it;
 }
 
-// calc_de -> calc_de_fractal -> calc_de_part (src/calc.rs:1333-1557), one
-// hybrid part, outside rendering
+// set_part (src/calc.rs:1476-1489): the slot range, iteration limit and DE
+// option the iteration runs with
+void Marcher::set_part(int start, int end, int repeat, int max_it, int de_option) {
+    it.start_from = start;
+    it.end_to = end;
+    it.repeat_from = repeat;
+    it.max_it = max_it;
+    it.de_option = de_option;
+}
+
+// calc_de -> calc_de_fractal (src/calc.rs:1333-1455), outside rendering: one
+// hybrid part, or a DE combination of two (CalcDEfull with FormulaType > 0)
 double Marcher::calc_de() {
     if (count_de) g_de_evals.fetch_add(1, std::memory_order_relaxed);
+    if (p->dc_kind == 0) return calc_de_part(p->is_custom_de, p->d_de_scale, false);
+    const DeCombPart &q = p->dc_part2;
+    double result = calc_de_part(p->is_custom_de, p->d_de_scale, false);
+    // PrepareF1DEcomb
+    const int b_it = it.it_result, b_max = max_its_result;
+    const double b_otrap = it.otrap;
+    const float b_sit = it.smooth_it;
+    set_part(q.start, q.end, q.repeat, q.max_it, q.de_option);
+    // the second part in its own place
+    const Vec3 c0 = {it.c[0], it.c[1], it.c[2]};
+    if (p->dc_place) {
+        const double d[3] = {c0[0] - p->dc_offset[0], c0[1] - p->dc_offset[1], c0[2] - p->dc_offset[2]};
+        for (int i = 0; i < 3; i++) it.c[i] = p->dc_m[i][0] * d[0] + p->dc_m[i][1] * d[1] + p->dc_m[i][2] * d[2];
+    }
+    double rst = calc_de_part(q.is_custom_de, q.d_de_scale, p->dc_kind == 3);
+    if (p->dc_place) {
+        rst *= p->dc_scale;
+        for (int i = 0; i < 3; i++) it.c[i] = c0[i];
+    }
+    const double ms = (double)ms_de_stop;
+    auto restore1 = [&]() {
+        it.it_result = b_it;
+        it.smooth_it = b_sit;
+        it.otrap = b_otrap;
+        max_its_result = b_max;
+    };
+    switch (p->dc_kind) {
+        case 1:
+            if (rst >= result) restore1();
+            else result = rst;
+            break;
+        case 2:
+        case 3:
+            if (rst > result) result = rst;
+            else restore1();
+            break;
+        default: {  // 4, 5: the smooth minima, colour values blended by distance
+            if (!(rst < result)) {
+                it.it_result = b_it;
+                max_its_result = b_max;
+            }
+            const double sm = p->dc_smooth;
+            if (p->dc_kind == 4) {
+                result = std::fmin(rst - std::fmax(sm - result, 0.0), result - std::fmax(sm - rst, 0.0));
+            } else {
+                const double rd1 = std::fmax(sm - result - ms, 0.0);
+                const double d2 = std::fmax(sm - rst - ms, 0.0);
+                result = std::fmin(rst - rd1 * (sm - d2) / sm, result - d2 * (sm - rd1) / sm);
+            }
+            const double r2 = std::fabs(rst), w = std::fabs(result);
+            const double f = 1.0 / (w + r2 + 1e-10);
+            it.smooth_it = (float)(((double)it.smooth_it * w + (double)b_sit * r2) * f);
+            it.otrap = (it.otrap * w + b_otrap * r2) * f;
+            break;
+        }
+    }
+    // RestoreF1DEcomb
+    set_part(0, p->end_to, p->repeat_from, p->max_it, p->de_option);
+    return result;
+}
+
+// calc_de_part (src/calc.rs:1495-1557) of the part the iteration is set to:
+// the analytic DE or the numerical one; `invert` calculates the part as
+// "inside" (the inverted max combination)
+double Marcher::calc_de_part(bool is_custom_de, float d_de_scale, bool invert) {
     double result;
-    if (p->is_custom_de) {
-        result = it.hybrid_3d_de(p->slots) * (double)p->d_de_scale;
+    if (is_custom_de) {
+        result = it.hybrid_3d_de(p->slots) * (double)d_de_scale;
     } else {
         it.hybrid_3d(p->slots);
         if (it.rout < 1e-200) {
@@ -947,7 +1104,7 @@ double Marcher::calc_de() {
                 g[k] = (buf_rout - it.rout) * (buf_rout - it.rout);
                 it.c[k] = bufd;
             }
-            result = buf_rout * std::log(buf_rout) * (double)p->d_de_scale /
+            result = buf_rout * std::log(buf_rout) * (double)d_de_scale /
                      (std::sqrt(g[0] + g[1] + g[2]) + (double)p->de_offset006);
             it.rout = buf_rout;
             it.it_result = it.max_it;
@@ -959,6 +1116,10 @@ double Marcher::calc_de() {
     max_its_result = it.max_it;
     double mn = (double)ms_de_stop * 0.25;
     if (result < mn || std::isnan(result)) result = mn;
+    if (invert) {
+        result = (double)ms_de_stop * 4.0 - result * 3.0;
+        if (result >= (double)ms_de_stop) it.it_result -= 1;
+    }
     return result;
 }
 

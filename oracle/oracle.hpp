@@ -139,6 +139,15 @@ struct Slot {
     bool julia_add = false;
 };
 
+// ---- one part of a DE combination (HybridPart, src/calc.rs:210-220) ----
+struct DeCombPart {
+    int start = 0, end = 0, repeat = 0;
+    int de_option = 0;
+    bool is_custom_de = false;
+    float d_de_scale = 1.f;
+    int max_it = 0;
+};
+
 // ---- per-render parameters: CalcParams (src/calc.rs:21-134), built by
 // CalcParams::new (src/calc.rs:375-891) for the alternating 3D hybrid ----
 struct Params {
@@ -181,6 +190,15 @@ struct Params {
     float ipol_w[2] = {1.f, 0.f};   // its normalised weights
     bool four_d = false;            // a 4D alternating hybrid (HybridMode::Alt4D)
     double smatrix4[4][4] = {{0}};  // its 4D rotation (BuildSMatrix4)
+    // a DE combination (DeComb, src/calc.rs:224-236): kind 0 none, 1..5;
+    // its second part, smoothing distance (steps) and part 2's place
+    int dc_kind = 0;
+    DeCombPart dc_part2;
+    double dc_smooth = 0;
+    bool dc_place = false;
+    Mat3 dc_m = {{0}};
+    Vec3 dc_offset = {0};
+    double dc_scale = 1;
 };
 
 bool make_params(const mb3d_cu_scene &sc, Params &p, std::string &err);
@@ -196,7 +214,7 @@ struct Iteration {
     float smooth_it = 0;
     float ln_rstop = 0;
     int de_option = 0;
-    int end_to = 0, repeat_from = 0;
+    int start_from = 0, end_to = 0, repeat_from = 0;
     float fhln[6];
     bool ipol = false;
     float ipol_w[2] = {1.f, 0.f};
@@ -239,6 +257,8 @@ struct Marcher {
 
     Marcher(const Params *pp, int32_t s);
     double calc_de();
+    void set_part(int start, int end, int repeat, int max_it, int de_option);
+    double calc_de_part(bool is_custom_de, float d_de_scale, bool invert);
     void calc_vgrads_fov(int ix);
     void calc_start_pos(int ix, int iy);
     void step(double d);

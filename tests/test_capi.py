@@ -51,6 +51,32 @@ def test_unsupported_answers_on_the_host():
         assert e.status == mb3dcu.EINVAL
 
 
+def test_de_combination_checks_on_the_host():
+    """A DE combination (src/calc.rs:421-431,491-520) of kinds 1..5 is on the
+    card; 'mix' without a dIFS part 2 and kinds beyond 6 are errors; a 4D
+    part is not on the card; a combination whose part 1 ends at the last
+    slot is none."""
+    for kind in scenes.DECOMB_KINDS:
+        assert mb3dcu.unsupported(scenes.two_objects(kind)) is None, kind
+    for kind in (6, 7, -1):
+        s = scenes.two_objects("min")
+        s.decomb = kind
+        try:
+            mb3dcu.unsupported(s)
+            assert False, kind
+        except mb3dcu.CardError as e:
+            assert e.status == mb3dcu.EINVAL
+            if kind == 6:
+                assert "dIFS" in str(e)
+    s = scenes.two_objects("min")
+    s.slots[1].formula = mb3dcu.F_QUATERNION
+    r = mb3dcu.unsupported(s)
+    assert r and "4D" in r
+    s = scenes.two_objects("min")
+    s.decomb_end1 = 1  # (part 1 takes every slot: no combination)
+    assert mb3dcu.unsupported(s) is None
+
+
 def test_init_without_device_fails_loudly():
     import torch
     if torch.cuda.is_available():

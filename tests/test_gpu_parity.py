@@ -107,6 +107,55 @@ def test_quaternion_4d_rotation_and_hybrid(card):
         assert card.march(sc, mb3dcu.FP32_FP64).tobytes() == g.tobytes(), name
 
 
+def _decomb_scenes():
+    out = [("two objects (min)", scenes.two_objects("min"))]
+    for kind in ("max", "max_inverted", "smooth_linear", "smooth"):
+        out.append((kind, scenes.two_objects(kind, place=False)))
+    return out
+
+
+def test_de_combinations_match_oracle(card):
+    """DE combinations (CalcDEfull with FormulaType > 0, src/calc.rs:1365-
+    1455): the reference's scene of two objects (a Mandelbulb and an Amazing
+    Box moved, turned and scaled as part 2, combined by min) and the bulb with
+    a box over it combined by max, max with the inverted box and the two
+    smooth minima: the FP64 march against the oracle with the single
+    formulas' bounds, the mixed mode giving the same records (every pixel in
+    FP64), and the DE probe with its iteration counts at points of both
+    parts (the reference's grid of both_parts_of_a_de_combination_use_their
+    _compiled_loops, tests/render.rs:345-382)."""
+    i = np.arange(8000)
+    grid = np.stack([(i % 20) * 0.25 - 1.3, ((i // 20) % 20) * 0.14 - 1.3, (i // 400) * 0.14 - 1.3], 1)
+    for name, sc in _decomb_scenes():
+        ref = O.march(sc, mb3dcu.SILIGHT)
+        assert (~mb3dcu.is_background(ref)).mean() > 0.03, name
+        g = card.march(sc, mb3dcu.FP64)
+        r = compare(g, ref, *zc(sc))
+        assert r["hit_agree"] >= 0.999 and r["exact"] >= 0.95, (name, r)
+        assert r.get("depth_rel_p99", 0.0) < 1e-6, (name, r)
+        assert card.march(sc, mb3dcu.FP32_FP64).tobytes() == g.tobytes(), name
+        d0, i0 = O.de_at(sc, grid)
+        d1, i1 = card.de_probe(sc, grid, mb3dcu.FP64)
+        assert (i0 == i1).mean() > 0.999, name
+        rel = np.abs(d0 - d1) / np.maximum(np.abs(d0), 1e-300)
+        assert np.median(rel) < 1e-12 and (rel < 1e-6).mean() > 0.999, (name, np.max(rel))
+
+
+def test_de_combination_shadows_and_ao(card):
+    """Hard shadows and DE AO on the scene of two objects (their DEs are the
+    combination's, their surface tests take the ruling part's iteration
+    limit): the card's FP64 render against the oracle's passes."""
+    sc = scenes.two_objects("min")
+    sc.shadow_lights, sc.deao_quality = 1, 1
+    ref = O.deao(sc, O.shadows(sc, O.march(sc, mb3dcu.SILIGHT), per_pixel=True))
+    g = card.render(sc, mb3dcu.FP64)
+    obj = ~mb3dcu.is_background(ref) & ~mb3dcu.is_background(g)
+    assert obj.mean() > 0.1
+    sh = (g["shadow"][obj] >> 10) == (ref["shadow"][obj] >> 10)
+    da = np.abs(g["amb_shadow"][obj].astype(np.int64) - ref["amb_shadow"][obj].astype(np.int64))
+    assert sh.mean() >= 0.98 and (da <= 16).mean() >= 0.97, (sh.mean(), (da <= 16).mean())
+
+
 def test_interpolation_hybrid_shadows_and_ao(card):
     """The post passes on an interpolation hybrid (their DEs blend too): hard
     shadows and DE AO of the card's FP64 render against the oracle's passes

@@ -652,3 +652,79 @@ def test_aexion_c_matches_pascal_reference():
         jr = [math.cos(th2) * math.cos(ph2) * r, math.cos(th2) * math.sin(ph2) * r, r * math.sin(th2)]
         assert np.allclose(v[:3], [xn, yn, zn], atol=1e-9), (v, [xn, yn, zn])
         assert np.allclose(j[:3], jr, atol=1e-9), (j, jr)
+
+
+# ---- DE combinations (CalcDEfull with FormulaType > 0, src/calc.rs:1365-1455)
+
+def _grid():
+    i = np.arange(8000)
+    return np.stack([(i % 20) * 0.25 - 1.3, ((i // 20) % 20) * 0.14 - 1.3, (i // 400) * 0.14 - 1.3], 1)
+
+
+def test_de_combination_grid_reaches_both_parts():
+    """tests/render.rs:345-382 (both_parts_of_a_de_combination_use_their_
+    compiled_loops): on the scene of two objects, a grid over both (the box
+    stands at x = 3.2, size 0.4) has more than 1000 points near part 2, and
+    more than 100 points on each side iterate 10 times or more."""
+    c = _grid()
+    _, its = O.de_at(scenes.two_objects("min"), c)
+    far = c[:, 0] > 2.5
+    assert far.sum() > 1000
+    assert ((its >= 10) & ~far).sum() > 100 and ((its >= 10) & far).sum() > 100
+
+
+def test_de_combination_min_and_max_are_the_two_parts():
+    """min and max of one pair of parts hold the two parts' distances (each
+    at least a quarter of the DE stop, calc_de_part): min + max = part 1 +
+    part 2, with part 1 the bulb alone; the smooth minima lie below the min
+    (src/calc.rs:1398-1430)."""
+    c = _grid()[::7]
+    d_min, _ = O.de_at(scenes.two_objects("min", place=False), c)
+    d_max, _ = O.de_at(scenes.two_objects("max", place=False), c)
+    alone = scenes.two_objects("min", place=False)
+    alone.decomb = 0
+    scenes.set_slots(alone, [scenes.intpow(8, -1.0)])
+    alone.rstop = 1024.0  # (the combination's bailout: the largest of its formulas')
+    d1, _ = O.de_at(alone, c)
+    assert np.all(d_min <= d_max)
+    assert np.all((np.abs(d_min - d1) <= 1e-12 * d1) | (np.abs(d_max - d1) <= 1e-12 * d1))
+    d2 = d_min + d_max - d1
+    assert np.all(d2 >= d_min - 1e-12) and (d2 > d1).any() and (d2 < d1).any()
+    for kind in ("smooth_linear", "smooth"):
+        d_s, _ = O.de_at(scenes.two_objects(kind, place=False), c)
+        assert np.all(d_s <= d_min + 1e-12), kind
+        assert (d_s < d_min - 1e-9).any(), kind
+
+
+def test_de_combination_inverted_max_cuts_the_box_out():
+    """max with the inverted part 2 (kind 3, calc_de_part's `invert`): the
+    box's inside counts as outside, so the bulb's points inside the box are
+    away from the surface and its points outside keep the bulb's distance."""
+    c = _grid()[::5]
+    d_inv, _ = O.de_at(scenes.two_objects("max_inverted", place=False), c)
+    alone = scenes.two_objects("min", place=False)
+    alone.decomb = 0
+    scenes.set_slots(alone, [scenes.intpow(8, -1.0)])
+    alone.rstop = 1024.0  # (the combination's bailout: the largest of its formulas')
+    d1, _ = O.de_at(alone, c)
+    assert np.all(d_inv >= d1 - 1e-12 * d1)
+    assert (d_inv > d1 * 1.5).any() and (np.abs(d_inv - d1) <= 1e-12 * d1).mean() > 0.3
+
+
+def test_de_combination_checks_and_interpolation_wins():
+    """The checks of the second part (src/calc.rs:491-520): 'mix' needs a
+    dIFS part 2, a kind beyond 6 is refused; in an interpolation hybrid the
+    combination is ignored (src/calc.rs:421)."""
+    bad = scenes.two_objects("min")
+    bad.decomb = 6
+    with pytest.raises(Exception):
+        O.de_at(bad, np.zeros((1, 3)))
+    bad.decomb = 7
+    with pytest.raises(Exception):
+        O.de_at(bad, np.zeros((1, 3)))
+    ip = scenes.interpolated("Integer Power", "Amazing Box", (0.6, 0.4), 32, 24)
+    c = _grid()[::40]
+    d0, i0 = O.de_at(ip, c)
+    ip.decomb, ip.decomb_end1, ip.decomb_start2, ip.decomb_end2 = 1, 0, 1, 1
+    d1, i1 = O.de_at(ip, c)
+    assert np.array_equal(d0, d1) and np.array_equal(i0, i1)
