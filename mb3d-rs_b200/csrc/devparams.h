@@ -20,8 +20,8 @@ struct DevSlot {
     int32_t ipow;       // the integer power (IntPow, FoldingIntPow)
     int32_t kind;       // FKIND_* bit of the formula (IntPow 8 apart from the other powers)
     int32_t pad;
-    double o[6];        // options
-    float of[6];        // options, single precision
+    double o[8];        // options (Aexion C reads eight)
+    float of[8];        // options, single precision
 };
 
 struct DevParams {

@@ -456,7 +456,7 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
             default: d.kind = 128; break;
         }
         if (its[i] > 0) p.fmask |= d.kind;
-        for (int k = 0; k < 6; k++) {
+        for (int k = 0; k < 8; k++) {
             d.o[k] = sc.slots[i].options[k];
             d.of[k] = (float)sc.slots[i].options[k];
         }
