@@ -16,12 +16,18 @@
 // block comes with its input box.  Nine tcgen05.mma (M=128, N=BN, K=16,
 // BF16 x BF16 -> FP32) per group add into the accumulator in tensor memory.
 // The blocks are persistent (one per SM) and take every grid-th tile.  Roles
-// in a block of 192 threads: lane 0 of warp 0 issues the TMA loads through a
+// in a block of 320 threads: lane 0 of warp 0 issues the TMA loads through a
 // ring of stages, lane 0 of warp 1 the MMAs (each group's commit frees its
-// stage; tile i accumulates in TMEM buffer i % 2, so that the epilogue of one
-// tile overlaps the MMAs of the next), and warps 2..5 read the accumulator
-// (warp w holds TMEM lanes 32 (w % 4) .. + 31, i.e. pixels), add the bias,
-// apply the ReLU, store bf16 NHWC and free the buffer.
+// stage; tile i accumulates in TMEM buffer i % NBUF -- four buffers where
+// they fit in the 512 columns, else two -- so that the epilogues of earlier
+// tiles overlap the MMAs of the next), and two groups of four epilogue warps
+// (warps 2..5 the even tiles, 6..9 the odd ones) read the accumulator (warp w
+// holds TMEM lanes 32 (w % 4) .. + 31, i.e. four rows of the tile's pixels),
+// add the bias (kept in shared memory), apply the ReLU and free the buffer.
+// The plain store (no mask, no accumulation, cout <= 128) goes through a
+// shared memory tile per warp, [4 rows][8 pixels][cout] bf16, that one lane
+// writes to the picture with a TMA tensor store (the box clips at the
+// picture's edge); the others store 16 bytes per lane.
 // Every wait is bounded (about a second of clock cycles); a wait that runs out
 // sets the error word and the block stops issuing, and frees its tensor memory.
 #include <cuda.h>
@@ -42,6 +48,9 @@ constexpr uint32_t BOX_BYTES = HALO_W * HALO_H * 16;
 constexpr uint32_t HALF_BYTES = (BOX_BYTES + 127) / 128 * 128;
 constexpr uint32_t A_BYTES = 2 * HALF_BYTES;
 constexpr int MAX_STAGES = 16;
+constexpr int EPI_WARPS = 8;                            // two groups of four
+constexpr int CONV_THREADS = 64 + 32 * EPI_WARPS;
+constexpr int TS_MAX_BN = 128;                          // the TMA store epilogue up to this many output channels
 constexpr uint32_t SMEM_BUDGET = 200 * 1024;           // the dynamic shared memory a block takes
 constexpr uint32_t RESIDENT_MAX = 112 * 1024;          // weights up to this stay in shared memory
 constexpr long long TC_WAIT_CYCLES = 2000000000LL;     // ~1 s at 1.9-2 GHz
@@ -62,6 +71,8 @@ struct ConvTc {
     int *err;
     long long wait_cycles;  // the limit of every wait
     int no_issue;           // (a test of the limit: the TMA and MMA lanes issue nothing)
+    int tstore;             // the TMA store epilogue (its staging after the stages)
+    uint32_t stage_out;     // bytes of one warp's staging tile (32 pixels x cout bf16)
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -104,6 +115,18 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_
                  : "memory");
 }
 
+// a tile of shared memory to the picture (the box of the output map at
+// {c0, c1, c2, c3}), in the warp's bulk group; and the waits on the group
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap *map, uint32_t src, int c0, int c1, int c2, int c3) {
+    asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(
+                     (uint64_t)map),
+                 "r"(src), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+                 : "memory");
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 // shared memory descriptor of a K-major operand without swizzle: core
 // matrices of 8 rows x 16 bytes (rows 16 bytes apart), `lbo` bytes between the
 // two 8-element halves of K, `sbo` bytes between 8-row groups
@@ -124,12 +147,11 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 // 16 accumulator columns of one pixel: bias, ReLU, (the old value), (the
 // mask), bf16
 __device__ __forceinline__ void store16(__nv_bfloat16 *o, const __nv_bfloat16 *mk, int nb, const uint32_t (&r)[16],
-                                        const ConvTc &a) {
+                                        const ConvTc &a, const float *sbias) {
     float v[16];
 #pragma unroll
     for (int k = 0; k < 16; k++) {
-        v[k] = __uint_as_float(r[k]);
-        if (a.bias && nb + k < a.cout) v[k] += a.bias[nb + k];
+        v[k] = __uint_as_float(r[k]) + sbias[nb + k];
         if (a.relu) v[k] = fmaxf(v[k], 0.0f);
     }
     if (nb + 16 <= a.cout) {
@@ -183,18 +205,22 @@ __device__ __forceinline__ void tile_of(const ConvTc &a, int g, int &img, int &x
 }
 
 template <int BN>
-__global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ CUtensorMap ta, const ConvTc a) {
+__global__ void __launch_bounds__(CONV_THREADS, 1) k_conv3x3_tc(const __grid_constant__ CUtensorMap ta,
+                                                                const __grid_constant__ CUtensorMap to, const ConvTc a) {
     constexpr uint32_t COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;  // one accumulator
+    constexpr int NBUF = 4 * COLS <= 512 ? 4 : 2;                                     // accumulators in TMEM
     constexpr uint32_t B_TAP = BN * 32;                                               // one tap's weights
     extern __shared__ __align__(1024) uint8_t dyn[];
-    __shared__ __align__(8) uint64_t full[MAX_STAGES], empty[MAX_STAGES], acc_full[2], acc_empty[2], wbar;
+    __shared__ __align__(8) uint64_t full[MAX_STAGES], empty[MAX_STAGES], acc_full[4], acc_empty[4], wbar;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
+    __shared__ float sbias[256];
     // (the dynamic area is aligned to 1024 bytes by hand): the resident
     // weights, then the stages (input box, and the group's weights when they
-    // are not resident)
+    // are not resident), then the epilogue warps' staging tiles
     uint8_t *base = dyn + ((1024u - (smem_addr(dyn) & 1023u)) & 1023u);
     const uint32_t w0 = smem_addr(base), st0 = w0 + (a.resident ? a.w_bytes : 0u);
+    const uint32_t out0 = (st0 + (uint32_t)a.stages * a.stage_bytes + 127u) & ~127u;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int groups = a.cin >> 4, ns = a.stages;
     const int total = a.n * a.tiles_y * a.tiles_x;
@@ -205,7 +231,7 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
             mbar_init(smem_addr(&full[s]), 1);
             mbar_init(smem_addr(&empty[s]), 1);
         }
-        for (int b = 0; b < 2; b++) {
+        for (int b = 0; b < NBUF; b++) {
             mbar_init(smem_addr(&acc_full[b]), 1);
             mbar_init(smem_addr(&acc_empty[b]), 4);
         }
@@ -213,10 +239,11 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    for (int k = tid; k < 256; k += blockDim.x) sbias[k] = (a.bias && k < a.cout) ? a.bias[k] : 0.0f;
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&tmem_slot)),
-                     "r"(2 * COLS)
+                     "r"(NBUF * COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -253,14 +280,14 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
         }
     } else if (warp == 1) {
         if (lane == 0 && !a.no_issue) {
-            // the MMA issuer: nine taps per group; tile i accumulates in buffer i % 2
+            // the MMA issuer: nine taps per group; tile i accumulates in buffer i % NBUF
             const uint32_t idesc = idesc_bf16<BN>();
             if (a.resident && !mbar_wait(smem_addr(&wbar), 0, &abort_flag, a.wait_cycles)) abort_flag = 1;
             uint32_t q = 0;
             int i = 0;
             for (int g = blockIdx.x; g < total && !abort_flag; g += gridDim.x, i++) {
-                const int buf = i & 1;
-                if (i >= 2 && !mbar_wait(smem_addr(&acc_empty[buf]), ((i >> 1) - 1) & 1, &abort_flag, a.wait_cycles)) {
+                const int buf = i % NBUF;
+                if (i >= NBUF && !mbar_wait(smem_addr(&acc_empty[buf]), ((i / NBUF) - 1) & 1, &abort_flag, a.wait_cycles)) {
                     abort_flag = 1;
                     break;
                 }
@@ -298,12 +325,16 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
             }
         }
     } else {
-        // the epilogue warps 2..5: warp w reads TMEM lanes 32 (w % 4) .. + 31
+        // the epilogue: group e = 0 (warps 2..5) takes the even tiles, e = 1
+        // (warps 6..9) the odd ones; warp w reads TMEM lanes 32 (w % 4) .. + 31
+        const int ew = warp - 2, e = ew >> 2;
         const int quarter = warp & 3, row = quarter * 32 + lane;
-        int i = 0;
-        for (int g = blockIdx.x; g < total; g += gridDim.x, i++) {
-            const int buf = i & 1;
-            bool ready = mbar_wait(smem_addr(&acc_full[buf]), (i >> 1) & 1, &abort_flag, a.wait_cycles);
+        const uint32_t stg = out0 + (uint32_t)ew * a.stage_out;  // (the TMA store's staging tile)
+        bool pending = false;                                    // (lane 0: a store of the warp in flight)
+        int i = e;
+        for (int g = blockIdx.x + e * gridDim.x; g < total; g += 2 * gridDim.x, i += 2) {
+            const int buf = i % NBUF;
+            bool ready = mbar_wait(smem_addr(&acc_full[buf]), (i / NBUF) & 1, &abort_flag, a.wait_cycles);
             ready = __all_sync(0xffffffffu, ready);
             if (!ready) {
                 abort_flag = 1;
@@ -314,6 +345,59 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
             tile_of(a, g, img, x0, y0);
             const int px = x0 + row % TILE_W, py = y0 + row / TILE_W;
             const bool valid = px < a.w && py < a.h;
+            if (a.tstore) {
+                // the staging tile is free once the warp's last store has read it
+                if (lane == 0 && pending) bulk_wait_read();
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < BN; c += 16) {
+                    uint32_t r[16];
+                    const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(buf * COLS + c);
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                        "[%16];"
+                        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                        : "r"(taddr)
+                        : "memory");
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    uint32_t pk[8];
+#pragma unroll
+                    for (int k = 0; k < 8; k++) {
+                        float v0 = __uint_as_float(r[2 * k]) + sbias[c + 2 * k];
+                        float v1 = __uint_as_float(r[2 * k + 1]) + sbias[c + 2 * k + 1];
+                        if (a.relu) {
+                            v0 = fmaxf(v0, 0.0f);
+                            v1 = fmaxf(v1, 0.0f);
+                        }
+                        const __nv_bfloat162 b2 = __floats2bfloat162_rn(v0, v1);
+                        pk[k] = *reinterpret_cast<const uint32_t *>(&b2);
+                    }
+                    // the lane's pixel is entry `lane` of the [4][8] tile
+                    const uint32_t sp = stg + (uint32_t)(lane * BN + c) * 2u;
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sp), "r"(pk[0]), "r"(pk[1]), "r"(pk[2]),
+                                 "r"(pk[3])
+                                 : "memory");
+                    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(sp + 16u), "r"(pk[4]), "r"(pk[5]),
+                                 "r"(pk[6]), "r"(pk[7])
+                                 : "memory");
+                }
+                // (the accumulator is read: free it before the store goes out)
+                tc_fence_before();
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) {
+                    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&acc_empty[buf])) : "memory");
+                    const int ry = y0 + quarter * 4;
+                    if (ry < a.h) {
+                        tma_store_4d(&to, stg, a.out_off, x0, ry, img);
+                        pending = true;
+                    } else {
+                        pending = false;
+                    }
+                }
+                continue;
+            }
             const size_t pix = (size_t)(img * a.h + (valid ? py : 0)) * a.w + (valid ? px : 0);
             __nv_bfloat16 *o = a.out + pix * a.out_c + a.out_off;
             const __nv_bfloat16 *mk = a.mask ? a.mask + pix * a.mask_c + a.mask_off : nullptr;
@@ -329,20 +413,23 @@ __global__ void __launch_bounds__(192, 1) k_conv3x3_tc(const __grid_constant__ C
                     : "r"(taddr)
                     : "memory");
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (valid && c < a.cout) store16(o, mk, c, r, a);
+                if (valid && c < a.cout) store16(o, mk, c, r, a, sbias);
             }
-            // the accumulator buffer is free for the MMAs of tile i + 2
+            // the accumulator buffer is free for the MMAs of tile i + NBUF
             tc_fence_before();
             __syncwarp();
             if (lane == 0)
                 asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&acc_empty[buf])) : "memory");
         }
+        // (the warp's last store has left shared memory and reached the picture)
+        if (lane == 0 && pending) bulk_wait_all();
+        __syncwarp();
     }
     tc_fence_before();
     __syncthreads();
     if (tid == 0 && abort_flag) atomicExch(a.err, 1);
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * COLS) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NBUF * COLS) : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -593,20 +680,25 @@ int sm_count() {
 }
 
 template <int BN>
-void launch_tc(const CUtensorMap &ta, ConvTc c, int total, cudaStream_t s) {
-    // the weights stay in shared memory where they leave room for 8 stages
+void launch_tc(const CUtensorMap &ta, const CUtensorMap &to, ConvTc c, int total, cudaStream_t s) {
+    // the weights stay in shared memory where they leave room for 8 stages;
+    // the TMA store epilogue's staging tiles (8 warps x 32 pixels x cout
+    // bf16) come off the stages' room
     const uint32_t grp_bytes = 9u * BN * 32u;
+    c.stage_out = 32u * BN * 2u;
+    const uint32_t out_bytes = c.tstore ? (uint32_t)EPI_WARPS * c.stage_out + 128u : 0u;
+    const uint32_t budget = SMEM_BUDGET - out_bytes;
     c.w_bytes = (uint32_t)(c.cin / 16) * grp_bytes;
-    c.resident = c.w_bytes <= RESIDENT_MAX && c.w_bytes + 8 * A_BYTES <= SMEM_BUDGET;
+    c.resident = c.w_bytes <= RESIDENT_MAX && c.w_bytes + 8 * A_BYTES <= budget;
     c.stage_bytes = c.resident ? A_BYTES : A_BYTES + grp_bytes;
-    const uint32_t room = SMEM_BUDGET - (c.resident ? c.w_bytes : 0u);
+    const uint32_t room = budget - (c.resident ? c.w_bytes : 0u);
     int st = (int)(room / c.stage_bytes);
     c.stages = st > MAX_STAGES ? MAX_STAGES : st < 2 ? 2 : st;
-    const size_t smem = 1024 + (c.resident ? c.w_bytes : 0u) + (size_t)c.stages * c.stage_bytes;
+    const size_t smem = 1024 + (c.resident ? c.w_bytes : 0u) + (size_t)c.stages * c.stage_bytes + out_bytes;
     cudaFuncSetAttribute(k_conv3x3_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int grid = sm_count();
     if (grid > total) grid = total;
-    k_conv3x3_tc<BN><<<grid, 192, smem, s>>>(ta, c);
+    k_conv3x3_tc<BN><<<grid, CONV_THREADS, smem, s>>>(ta, to, c);
 }
 
 }  // namespace
@@ -654,24 +746,39 @@ int dn_conv(const ConvArgs &a, cudaStream_t s) {
     if (enc(&ta, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.in, da, sa, ba, ea, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return -1;
+    // the output, for the TMA store epilogue (no mask, no accumulation, up to
+    // TS_MAX_BN channels): dims (channels, x, y, image), the box cout
+    // channels x 8 x 4 pixels, one epilogue warp's four rows of a tile
+    CUtensorMap to = ta;
+    c.tstore = 0;
+    if (!a.mask && !a.accumulate && a.cout <= TS_MAX_BN) {
+        cuuint64_t dout[4] = {(cuuint64_t)a.out_c, (cuuint64_t)a.w, (cuuint64_t)a.h, (cuuint64_t)a.n};
+        cuuint64_t sout[3] = {(cuuint64_t)a.out_c * 2, (cuuint64_t)a.out_c * 2 * a.w, (cuuint64_t)a.out_c * 2 * a.w * a.h};
+        cuuint32_t bout[4] = {(cuuint32_t)a.cout, (cuuint32_t)TILE_W, 4, 1};
+        if (enc(&to, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)a.out, dout, sout, bout, ea, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+            c.tstore = 1;
+        else
+            to = ta;
+    }
     const int tiles = a.n * c.tiles_y * c.tiles_x;
     switch (a.cout) {
-        case 16: launch_tc<16>(ta, c, tiles, s); break;
-        case 32: launch_tc<32>(ta, c, tiles, s); break;
-        case 48: launch_tc<48>(ta, c, tiles, s); break;
-        case 64: launch_tc<64>(ta, c, tiles, s); break;
-        case 80: launch_tc<80>(ta, c, tiles, s); break;
-        case 96: launch_tc<96>(ta, c, tiles, s); break;
-        case 112: launch_tc<112>(ta, c, tiles, s); break;
-        case 128: launch_tc<128>(ta, c, tiles, s); break;
-        case 144: launch_tc<144>(ta, c, tiles, s); break;
-        case 160: launch_tc<160>(ta, c, tiles, s); break;
-        case 176: launch_tc<176>(ta, c, tiles, s); break;
-        case 192: launch_tc<192>(ta, c, tiles, s); break;
-        case 208: launch_tc<208>(ta, c, tiles, s); break;
-        case 224: launch_tc<224>(ta, c, tiles, s); break;
-        case 240: launch_tc<240>(ta, c, tiles, s); break;
-        default: launch_tc<256>(ta, c, tiles, s); break;
+        case 16: launch_tc<16>(ta, to, c, tiles, s); break;
+        case 32: launch_tc<32>(ta, to, c, tiles, s); break;
+        case 48: launch_tc<48>(ta, to, c, tiles, s); break;
+        case 64: launch_tc<64>(ta, to, c, tiles, s); break;
+        case 80: launch_tc<80>(ta, to, c, tiles, s); break;
+        case 96: launch_tc<96>(ta, to, c, tiles, s); break;
+        case 112: launch_tc<112>(ta, to, c, tiles, s); break;
+        case 128: launch_tc<128>(ta, to, c, tiles, s); break;
+        case 144: launch_tc<144>(ta, to, c, tiles, s); break;
+        case 160: launch_tc<160>(ta, to, c, tiles, s); break;
+        case 176: launch_tc<176>(ta, to, c, tiles, s); break;
+        case 192: launch_tc<192>(ta, to, c, tiles, s); break;
+        case 208: launch_tc<208>(ta, to, c, tiles, s); break;
+        case 224: launch_tc<224>(ta, to, c, tiles, s); break;
+        case 240: launch_tc<240>(ta, to, c, tiles, s); break;
+        default: launch_tc<256>(ta, to, c, tiles, s); break;
     }
     return 0;
 }
