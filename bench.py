@@ -159,17 +159,31 @@ def cpu_rows(sc, seconds, timer_rows=16):
 
 
 def cpu_baseline(sc, seconds):
-    """The oracle (C++ restatement of the reference CPU renderer) on a row sample."""
+    """The oracle (C++ restatement of the reference CPU renderer) on a row
+    sample; returns the figure, the rows and the oracle's records of them
+    (the checker of the card's frame)."""
     O = _oracle()
     rows = cpu_rows(sc, seconds)
     t = time.perf_counter()
-    O.render_rows(sc, mb3dcu.SILIGHT, rows)
+    recs = O.render_rows(sc, mb3dcu.SILIGHT, rows)
     dt = time.perf_counter() - t
     rays = len(rows) * sc.width
-    return {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{len(rows)} evenly spaced rows of the {sc.width}x{sc.height} frame ({rays} primary rays, "
-                      f"march + hard shadows + DE AO), {dt:.1f} s, all host threads, C++ restatement of the "
-                      f"reference CPU renderer"}
+    fig = {"value": rays / dt / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(), "kind": "port",
+           "sample": f"{len(rows)} evenly spaced rows of the {sc.width}x{sc.height} frame ({rays} primary rays, "
+                     f"march + hard shadows + DE AO), {dt:.1f} s, all host threads, C++ restatement of the "
+                     f"reference CPU renderer"}
+    return fig, rows, recs
+
+
+def parity_vs_oracle(sc, card_g, rows, ref):
+    """The card's G-buffer against the oracle's records of the same rows:
+    hit agreement and the per-pixel relative depth error of the pixels both
+    call a surface (the painted-picture and record figures are the parity
+    tests' business)."""
+    g = card_g.reshape(sc.height, sc.width)[rows].reshape(-1)
+    r = parity_vs_fp64(sc, g, ref)
+    r["pixels"] = int(len(g))
+    return r
 
 
 def run_reference(args):
@@ -663,7 +677,12 @@ def main():
         if not args.no_mc and args.scale == 1.0:
             out["mc"] = mc_figures(card, args.mc_ref_rays)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(frame(0, args.scale), args.cpu_seconds)
+        fig, rows, ref = cpu_baseline(frame(0, args.scale), args.cpu_seconds)
+        out["cpu_baseline"] = fig
+        # both card modes against the oracle on the rows the baseline rendered
+        if prec == mb3dcu.FP32_FP64:
+            out["parity_vs_oracle"] = {"mixed": parity_vs_oracle(sc, mixed_g, rows, ref),
+                                       "fp64": parity_vs_oracle(sc, other_g, rows, ref)}
     if rank == 0:
         print(json.dumps(out), flush=True)
     card.close()
