@@ -394,9 +394,9 @@ __device__ __forceinline__ void f_int_pow8_x2(float zmul, float2 v[3], const flo
     const float2 r = padd(xx, yy);
     const float2 rr = pmul(r, r);
     const float2 zzzz = pmul(zz, zz);
-    float2 sr;  // sqrt(r): r * rsqrt(r), 0 where r is not positive
-    sr.x = r.x > 0.0f ? rsqrtf(r.x) : 0.0f;
-    sr.y = r.y > 0.0f ? rsqrtf(r.y) : 0.0f;
+    float2 sr;  // sqrt(r): r * rsqrt(r), 0 where r is 0 (r * rsqrt(1e-30))
+    sr.x = rsqrtf(fmaxf(r.x, 1e-30f));
+    sr.y = rsqrtf(fmaxf(r.y, 1e-30f));
     sr = pmul(r, sr);
     // t = (zzzz - 6 r zz + rr) (zz - r) sqrt(r)
     const float2 t = pmul(pmul(padd(pfma(pmul(p2(-6.0f), r), zz, zzzz), rr), psub(zz, r)), sr);
@@ -414,22 +414,28 @@ __device__ __forceinline__ void f_int_pow8_x2(float zmul, float2 v[3], const flo
     v[0] = pfma(a, pfma(p2(-28.0f), pmul(pmul(xx, yy), padd(yyyy, xxxx)), s0), j[0]);
 }
 
-// |x + f| - (|x - f| + x), box_fold on a pair
-__device__ __forceinline__ float2 box_fold_x2(float2 x, float2 f) {
-    return psub(pabs(padd(x, f)), padd(pabs(psub(x, f)), x));
+// box_fold on a pair, |x + f| - (|x - f| + x), in the equal form
+// t clamp(x, -a, a) - x with a = |f|, t = 2 sign(f) (for f >= 0: x inside the
+// fold, 2f - x above, -2f - x below; the sign of f flips |x + f| - |x - f|),
+// which has no rounding of its own inside the fold and needs no absolute
+// values (the packed instructions take no operand modifiers)
+__device__ __forceinline__ float2 box_fold_x2(float2 x, float a, float t) {
+    const float2 c = make_float2(fminf(fmaxf(x.x, -a), a), fminf(fmaxf(x.y, -a), a));
+    return pfma(c, p2(t), pmul(x, p2(-1.0f)));
 }
 
 // the Amazing Box (HybridCube) on a pair of orbits; the numeric DE does not
 // use the derivative w, which is left out
 __device__ __forceinline__ void f_amazing_box_x2(float scale, float min_r, float fold, float2 v[3], const float2 j[3]) {
-    const float2 F = p2(fold);
-    const float2 x = box_fold_x2(v[0], F), y = box_fold_x2(v[1], F), z = box_fold_x2(v[2], F);
+    const float fa = fabsf(fold), ft = copysignf(2.0f, fold);
+    const float2 x = box_fold_x2(v[0], fa, ft), y = box_fold_x2(v[1], fa, ft), z = box_fold_x2(v[2], fa, ft);
     const float2 r = pfma(x, x, pfma(y, y, pmul(z, z)));
     const float m = fmaxf(min_r, 1.2e-38f), sqr_min_r = m * m;
-    const bool bx = r.x < sqr_min_r, by = r.y < sqr_min_r;
+    // scale / minR^2 below minR^2, scale / r up to 1, scale above: scale /
+    // clamp(r, minR^2, 1) (when minR >= 1 the first branch rules, as there)
     float2 mul;
-    mul.x = (!bx && 1.0f < r.x) ? scale : __fdividef(scale, bx ? sqr_min_r : r.x);
-    mul.y = (!by && 1.0f < r.y) ? scale : __fdividef(scale, by ? sqr_min_r : r.y);
+    mul.x = __fdividef(scale, r.x < sqr_min_r ? sqr_min_r : fminf(r.x, 1.0f));
+    mul.y = __fdividef(scale, r.y < sqr_min_r ? sqr_min_r : fminf(r.y, 1.0f));
     v[2] = pfma(z, mul, j[2]);
     v[1] = pfma(y, mul, j[1]);
     v[0] = pfma(x, mul, j[0]);
