@@ -390,6 +390,12 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const P c[3], float m
                 const float2 r01 = psq3(V[0]), r23 = psq3(V[1]);
                 rout[0] = r01.x;
                 const float rn[4] = {0.0f, r01.y, r23.x, r23.y};
+                // (an offset orbit bails out at RStop3D = 64 RStop^4, far above
+                // the centre's bailout, so it rarely stops first: without the
+                // colour state, one test of the largest length skips the
+                // per-orbit bookkeeping -- fmaxf drops a NaN, which never stops)
+                if (!FULL && !(fmaxf(rn[1], fmaxf(rn[2], rn[3])) > (float)rstop3d))
+                    return it >= max_it || rout[0] > rstop;
 #pragma unroll
                 for (int q = 1; q < 4; q++) {
                     const bool stop = live[q] && rn[q] > (float)rstop3d;
