@@ -391,11 +391,17 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const P c[3], float m
                 rout[0] = r01.x;
                 const float rn[4] = {0.0f, r01.y, r23.x, r23.y};
                 // (an offset orbit bails out at RStop3D = 64 RStop^4, far above
-                // the centre's bailout, so it rarely stops first: without the
-                // colour state, one test of the largest length skips the
-                // per-orbit bookkeeping -- fmaxf drops a NaN, which never stops)
-                if (!FULL && !(fmaxf(rn[1], fmaxf(rn[2], rn[3])) > (float)rstop3d))
+                // the centre's bailout, so it rarely stops first: one test of
+                // the largest length skips the per-orbit bookkeeping, but for
+                // the z offset orbit's length that the colour state keeps --
+                // fmaxf drops a NaN, which never stops)
+                if (!(fmaxf(rn[1], fmaxf(rn[2], rn[3])) > (float)rstop3d)) {
+                    if (FULL) {  // (the colour state follows the z offset orbit)
+                        otrap3 = (live[3] && rn[3] < otrap3) ? rn[3] : otrap3;
+                        rout[3] = live[3] ? rn[3] : rout[3];
+                    }
                     return it >= max_it || rout[0] > rstop;
+                }
 #pragma unroll
                 for (int q = 1; q < 4; q++) {
                     const bool stop = live[q] && rn[q] > (float)rstop3d;
