@@ -940,7 +940,7 @@ __device__ __noinline__ DEr mc_de64(const DevParams &p, double c0, double c1, do
 }
 
 #ifndef MB3D_MC_MIN_BLOCKS
-#define MB3D_MC_MIN_BLOCKS 5  // (the whole C5 frame at 4 rays: 3 blocks 210.4 ms, 4 215.6, 5 206.8)
+#define MB3D_MC_MIN_BLOCKS 6  // (the whole C5 frame at 4 rays: 5 blocks 201.2 ms, 6 196.4, 7 205.4, 8 214.0)
 #endif
 template <typename R, int FM, bool BATCH>
 __global__ void __launch_bounds__(128, MB3D_MC_MIN_BLOCKS) k_mc(const __grid_constant__ DevParams p, const __grid_constant__ McDev m,
