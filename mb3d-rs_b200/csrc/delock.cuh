@@ -274,6 +274,41 @@ __device__ __forceinline__ DEr de_lock(const DevParams &p, const P c[3], float m
         R rold0 = 0, otrap0 = rout[0];
         int n = 0, btmp = p.slots[0].iterations, it = 0;
         unsigned int unc = 0;
+        if constexpr ((FM & FKIND_MENGER) && (FM & FKIND_BOX)) {
+            if (p.sched == SCHED_MENGER_BOX) {
+                // Menger IFS, Amazing Box, repeating, every iteration counted:
+                // the slots' order unrolled (the same formulas in the same
+                // order as the slot loop below, without its bookkeeping)
+                const DevSlot &s0 = p.slots[0], &s1 = p.slots[1];
+                const R m_s = Num<R>::opt(s0, 0), m_cx = Num<R>::opt(s0, 1), m_cy = Num<R>::opt(s0, 2),
+                        m_cz = Num<R>::opt(s0, 3);
+                const R b_s = Num<R>::opt(s1, 0), b_min = Num<R>::opt(s1, 1), b_fold = Num<R>::opt(s1, 2);
+                const bool m_ade = s0.ade != 0, b_ade = s1.ade != 0;
+                for (;;) {
+                    if (FULL) rold0 = rout[0];
+                    f_menger<R>(m_s, m_cx, m_cy, m_cz, v[0], m_ade);
+                    if (COUNT) cnt->its[0] += 1;
+                    it += 1;
+                    rout[0] = v[0][0] * v[0][0] + v[0][1] * v[0][1] + v[0][2] * v[0][2];
+                    if (FULL && rout[0] < otrap0) otrap0 = rout[0];
+                    if (it >= max_it || rout[0] > rstop) {
+                        n = 0;
+                        break;
+                    }
+                    if (FULL) rold0 = rout[0];
+                    f_amazing_box<R>(b_s, b_min, b_fold, v[0], j[0], b_ade);
+                    if (COUNT) cnt->its[1] += 1;
+                    it += 1;
+                    rout[0] = v[0][0] * v[0][0] + v[0][1] * v[0][1] + v[0][2] * v[0][2];
+                    if (FULL && rout[0] < otrap0) otrap0 = rout[0];
+                    if (it >= max_it || rout[0] > rstop) {
+                        n = 1;
+                        break;
+                    }
+                }
+                goto done_a;
+            }
+        }
         for (;;) {
             if (FULL) rold0 = rout[0];
             int guard = 0;

@@ -90,6 +90,7 @@ struct DevParams {
 #define SCHED_GENERIC 0
 #define SCHED_BOX2_IP8 1  // Amazing Box x2, Integer Power 8 x1, repeating from slot 0
 #define SCHED_IP8 2       // one Integer Power 8 slot
+#define SCHED_MENGER_BOX 3  // Menger IFS x1, Amazing Box x1, repeating from slot 0 (the analytic DE's loop)
 
 // the counters' slots (unsigned int) the march kernels share with the host
 #define CNT_HAND 0        // hand-over list length

@@ -468,6 +468,10 @@ int setup_params(const mb3d_cu_scene &sc, DevParams &p, std::string &err) {
         p.sched = SCHED_BOX2_IP8;
     else if (nsl == 1 && its[0] >= 1 && !unc[0] && p.slots[0].kind == 1 && !p.slots[0].julia_add)
         p.sched = SCHED_IP8;
+    else if (nsl == 2 && end_to == 1 && rep == 0 && its[0] == 1 && its[1] == 1 && !unc[0] && !unc[1] &&
+             fs[0] == MB3D_CU_F_MENGERIFS && fs[1] == MB3D_CU_F_AMAZINGBOX && !p.slots[0].julia_add &&
+             !p.slots[1].julia_add)
+        p.sched = SCHED_MENGER_BOX;
     // single precision coordinates are good enough when the numerical DE
     // offset spans >= 3 single steps at the size of the coordinates, or a
     // pixel step >= 64 of them with an analytic DE (gpu::precision,
